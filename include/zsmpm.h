@@ -1,0 +1,240 @@
+/* zsmpm: B200-native explicit MLS/APIC MPM substep on a sparse grid of 8^3 blocks.
+ *
+ * C ABI of libzsmpm.so.  It replaces the CUDA launches that zpc's execution policy makes
+ * for its legacy MPM operators (a zs::CudaExecutionPolicy applying functors over
+ * range(Np) or Collapse{nblocks, cells}) with hand-written sm_100a kernels.  Plain
+ * pointers and sizes only; no C++ types cross the boundary; no exceptions escape.
+ *
+ * Reference interfaces replaced (paths inside the zpc repository, include/zensim/...):
+ *   zsmpm_activate_blocks  CleanSparsity + ComputeSparsity + EnlargeSparsity launched over
+ *                          range(tableSize)/range(Np)/range(cnt)
+ *                          (simulation/sparsity/SparsityOp.hpp:41-112,
+ *                           simulation/sparsity/SparsityCompute.tpp:5-26)
+ *   zsmpm_bin_particles    SpatiallyCount + exclusive_scan + SpatiallyDistribute
+ *                          (SparsityOp.hpp:115-196, simulation/particle/Query.tpp:8-58)
+ *   zsmpm_p2g              CleanGridBlocks + P2GTransfer
+ *                          (simulation/grid/GridOp.hpp:54-69, simulation/transfer/P2G.hpp:45-127,
+ *                           CUDA twin cuda/simulation/transfer/P2G.hpp:35-117)
+ *   zsmpm_grid_update      ComputeGridBlockVelocity + ApplyBoundaryConditionOnGridBlocks
+ *                          (GridOp.hpp:72-164, geometry/Collider.h:80-110)
+ *   zsmpm_g2p              G2PTransfer (simulation/transfer/G2P.hpp:43-84) with the
+ *                          constitutive update (physics/ConstitutiveModel_Vol_dP.hpp:10-46,
+ *                          :241-325; physics/plasticity_models/SnowPlasticity.hpp:24-32)
+ *   zsmpm_get_table_view   HashTableView fields (container/HashTable.hpp:279-293, 509-513)
+ *   zsmpm_get_grid_view    GridsView / TileVector<f32,512> blocks (geometry/Structure.hpp:33-130)
+ *   zsmpm_scene_*          py_interop handle style: container__tv_* / del_container__tv_*
+ *                          (py_interop/TileVectorInstantiations.cpp:5-155)
+ *   particle views         TileVectorViewLite<f32,32> element (chn, i) at
+ *                          ((i/32)*nchn + chn)*32 + i%32 (py_interop/TileVectorView.hpp:10-60)
+ *
+ * Ownership: the library allocates and frees all device memory of a scene; views are
+ * non-owning.  Threading: a scene is bound to one device; calls on one scene must not
+ * overlap (as a zs policy bound to a stream is not re-entrant).  Errors: every entry point
+ * returns a zsmpm_status; zsmpm_last_error_string() describes the last failure of the
+ * calling thread.  Device-side failures (hash table full, particle outside the block-key
+ * range, bounded waits that gave up) are recorded in a per-scene status word that
+ * zsmpm_scene_status() reads; kernels never trap.
+ */
+#ifndef ZSMPM_H
+#define ZSMPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define ZSMPM_API __declspec(dllexport)
+#else
+#define ZSMPM_API __attribute__((visibility("default")))
+#endif
+
+typedef enum {
+  ZSMPM_OK = 0,
+  ZSMPM_ERR_TABLE_FULL = 1,    /* hash table load limit reached (HashTable.hpp:369 "proximity") */
+  ZSMPM_ERR_CAPACITY = 2,      /* particle / block / output capacity exceeded */
+  ZSMPM_ERR_INVALID_ARG = 3,
+  ZSMPM_ERR_CUDA = 4,          /* a CUDA runtime call failed (message has the CUDA error) */
+  ZSMPM_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up */
+  ZSMPM_ERR_OUT_OF_DOMAIN = 6, /* a particle position is NaN/Inf or beyond the key range */
+  ZSMPM_ERR_NO_DEVICE = 7,
+  ZSMPM_ERR_NOT_READY = 8      /* stage called before its inputs exist (e.g. p2g before bin) */
+} zsmpm_status;
+
+typedef enum {
+  ZSMPM_FIXED_COROTATED = 0, /* FixedCorotatedConfig (ConstitutiveModel.hpp:760) */
+  ZSMPM_DRUCKER_PRAGER = 1,  /* DruckerPragerConfig with compute_stress_sand */
+  ZSMPM_SNOW = 2             /* fixed corotated + Stomakhin snow projection */
+} zsmpm_model;
+
+typedef enum {
+  /* Standard ordering: the return map runs at the end of G2P and its projected F is
+   * stored; the stress used by the next P2G comes from that F. */
+  ZSMPM_PLASTICITY_COMMITTED = 0,
+  /* The reference's ordering: the return map acts on a copy of F inside the stress
+   * evaluation of P2G and only logJp is kept (P2G.hpp:87-100); stored F is the trial F. */
+  ZSMPM_PLASTICITY_REFERENCE = 1
+} zsmpm_plasticity_mode;
+
+typedef enum {
+  ZSMPM_WALL_STICKY = 0,   /* collider_e::Sticky */
+  ZSMPM_WALL_SLIP = 1,     /* collider_e::Slip */
+  ZSMPM_WALL_SEPARATE = 2, /* collider_e::Separate */
+  ZSMPM_WALL_NONE = 3
+} zsmpm_wall;
+
+typedef enum {
+  ZSMPM_BLOCK_ORDER_SORTED = 0,   /* active blocks ascending by (bx, by, bz), bz fastest */
+  ZSMPM_BLOCK_ORDER_INSERTION = 1 /* the order a sequential ComputeSparsity+EnlargeSparsity
+                                     inserts them (first particle, then enlargement) */
+} zsmpm_block_order;
+
+typedef enum {
+  ZSMPM_CLOSURE_PLAIN = 0,   /* analytic return map */
+  ZSMPM_CLOSURE_LEARNED = 1  /* MLP closure (zsmpm_closure_*), falls back per particle */
+} zsmpm_closure_kind;
+
+typedef struct {
+  int32_t model;            /* zsmpm_model */
+  int32_t plasticity_mode;  /* zsmpm_plasticity_mode */
+  float E, nu, rho;
+  float volume;             /* particle rest volume V0 (MaterialConfig::volume) */
+  float friction_deg;       /* Drucker-Prager friction angle (DruckerPragerConfig::fa) */
+  float cohesion;           /* Drucker-Prager log-strain shift (DruckerPragerConfig::cohesion) */
+  float beta;               /* Drucker-Prager volume-correction factor */
+  int32_t volume_correction;
+  float hardening;          /* snow xi */
+  float theta_c, theta_s;   /* snow critical compression / stretch */
+} zsmpm_material;
+
+typedef struct {
+  float dx;
+  float dt;
+  float gravity[3];
+  int32_t wall_type;        /* zsmpm_wall */
+  int32_t wall_cells;       /* walls are planes wall_cells*dx inside each face of [0,1]^3 */
+  zsmpm_material material;
+  int64_t max_particles;    /* capacity; 0 = the count of the first upload */
+  int32_t table_expected;   /* HashTable expected entries; 0 = max(Np/512, 64)
+                               (SparsityCompute.tpp:11-14); capacity next_2pow(n)*16 */
+  int32_t block_order;      /* zsmpm_block_order */
+  int32_t device;           /* CUDA device ordinal */
+  int32_t threads_per_cta;  /* 0 = autotuned/default; else 128, 256 or 512 */
+} zsmpm_scene_desc;
+
+/* Particle arrays in the reference's zs::Particles<f32,3> layout: one array per attribute,
+ * vectors and matrices stored per particle (x: 3n, F and C: 9n column-major).  Any of
+ * v, C, F, plastic may be NULL on upload (zero, zero, identity, zero/one).  `plastic` is
+ * logJp for Drucker-Prager and Jp for snow. */
+typedef struct {
+  float *m;
+  float *x;
+  float *v;
+  float *C;
+  float *F;
+  float *plastic;
+} zsmpm_particle_arrays;
+
+/* TileVector<f32,32>-style AoSoA view: element (chn, i) at ((i/32)*nchn + chn)*32 + i%32.
+ * Channel offsets of the attributes, -1 when absent. */
+typedef struct {
+  float *base;
+  int32_t num_channels;
+  int32_t lane_width;  /* must be 32 */
+  int32_t off_m, off_x, off_v, off_C, off_F, off_plastic;
+} zsmpm_tilevector_view;
+
+/* HashTableView<cuda, HashTable<i32,3,int>> fields, device pointers. */
+typedef struct {
+  int32_t *keys;        /* [table_size][3], INT32_MAX when empty */
+  int32_t *indices;     /* [table_size], -1 when empty */
+  int32_t *status;      /* [table_size], -1 (unlocked) */
+  int32_t *active_keys; /* [capacity][3], key of block index b */
+  int32_t *cnt;         /* device counter of active blocks */
+  int32_t table_size;
+} zsmpm_table_view;
+
+/* Grid blocks: TileVector<f32,512> with 4 channels (m, v.x, v.y, v.z); channel c of cell
+ * `cell` ((lx<<6)|(ly<<3)|lz) of block b at base[(b*4 + c)*512 + cell]. */
+typedef struct {
+  float *base;
+  int32_t num_channels;
+  int32_t num_blocks;   /* host copy, valid after the last activation was synchronised */
+  int32_t *keys;        /* device, [num_blocks][3] */
+} zsmpm_grid_view;
+
+typedef struct zsmpm_scene zsmpm_scene;
+
+ZSMPM_API const char *zsmpm_last_error_string(void);
+ZSMPM_API const char *zsmpm_version(void);
+/* number of visible CUDA devices (0 when none); never fails */
+ZSMPM_API int zsmpm_device_count(void);
+
+/* ---- scene lifetime -------------------------------------------------------------- */
+ZSMPM_API zsmpm_status zsmpm_scene_create(const zsmpm_scene_desc *desc, zsmpm_scene **out);
+ZSMPM_API zsmpm_status zsmpm_scene_destroy(zsmpm_scene *scene);
+/* Copies n particles into the scene (host or device pointers; `on_device` selects).  The
+ * particles are binned and sorted on the device; particle identity is kept so downloads
+ * return the upload order.  Also evaluates the stress of the uploaded state. */
+ZSMPM_API zsmpm_status zsmpm_scene_upload(zsmpm_scene *scene, const zsmpm_particle_arrays *p,
+                                          int64_t n, int32_t on_device, void *stream);
+ZSMPM_API zsmpm_status zsmpm_scene_upload_tilevector(zsmpm_scene *scene,
+                                                     const zsmpm_tilevector_view *tv,
+                                                     int64_t n, void *stream);
+/* Copies particles out in upload order (host or device pointers).  C is recovered from
+ * the stored affine momentum; in ZSMPM_PLASTICITY_REFERENCE mode logJp is the value the
+ * next P2G would use (one projection ahead of the reference's stored logJp). */
+ZSMPM_API zsmpm_status zsmpm_scene_download(zsmpm_scene *scene, zsmpm_particle_arrays *p,
+                                            int32_t on_device, void *stream);
+ZSMPM_API zsmpm_status zsmpm_scene_download_tilevector(zsmpm_scene *scene,
+                                                       const zsmpm_tilevector_view *tv,
+                                                       void *stream);
+ZSMPM_API int64_t zsmpm_scene_num_particles(const zsmpm_scene *scene);
+/* Synchronises the scene's last stream and returns its device status word. */
+ZSMPM_API zsmpm_status zsmpm_scene_status(zsmpm_scene *scene);
+
+/* ---- stages (each enqueues on `stream`, NULL = legacy default stream) --------------- */
+ZSMPM_API zsmpm_status zsmpm_activate_blocks(zsmpm_scene *scene, void *stream);
+ZSMPM_API zsmpm_status zsmpm_bin_particles(zsmpm_scene *scene, void *stream);
+ZSMPM_API zsmpm_status zsmpm_p2g(zsmpm_scene *scene, void *stream);
+ZSMPM_API zsmpm_status zsmpm_grid_update(zsmpm_scene *scene, void *stream);
+ZSMPM_API zsmpm_status zsmpm_g2p(zsmpm_scene *scene, void *stream);
+/* One full substep (activate, bin, P2G, grid update + walls, G2P). */
+ZSMPM_API zsmpm_status zsmpm_substep(zsmpm_scene *scene, void *stream);
+/* nsteps substeps replayed from a CUDA graph of one substep (captured on first use);
+ * checks the device status word once at the end. */
+ZSMPM_API zsmpm_status zsmpm_run(zsmpm_scene *scene, int32_t nsteps, void *stream);
+
+/* ---- views and diagnostics ------------------------------------------------------- */
+ZSMPM_API zsmpm_status zsmpm_get_table_view(zsmpm_scene *scene, zsmpm_table_view *out);
+ZSMPM_API zsmpm_status zsmpm_get_grid_view(zsmpm_scene *scene, zsmpm_grid_view *out);
+/* Number of active blocks of the last activation (synchronises). */
+ZSMPM_API zsmpm_status zsmpm_num_blocks(zsmpm_scene *scene, int32_t *out);
+/* Copies the active keys [nb][3] and the grid [nb][4][512] to host memory. */
+ZSMPM_API zsmpm_status zsmpm_download_grid(zsmpm_scene *scene, int32_t *keys, float *grid,
+                                           int32_t cap_blocks, int32_t *out_nblocks);
+/* Host copies of the per-slot particle order of the last binning: order[slot] = upload
+ * index of the particle in slot, block_start[nb+1]. */
+ZSMPM_API zsmpm_status zsmpm_download_binning(zsmpm_scene *scene, int32_t *order,
+                                              int32_t *block_start, int32_t cap_blocks);
+/* Per-stage device times (ms) of the last zsmpm_substep when timing is enabled. */
+ZSMPM_API zsmpm_status zsmpm_set_stage_timing(zsmpm_scene *scene, int32_t enabled);
+ZSMPM_API zsmpm_status zsmpm_stage_times(zsmpm_scene *scene, float *ms, int32_t count);
+/* Number of kernels one zsmpm_substep launches. */
+ZSMPM_API int32_t zsmpm_kernels_per_substep(const zsmpm_scene *scene);
+
+/* ---- stand-alone kernels (device pointers), for parity tests of single operators ---- */
+/* 3x3 SVD of `count` column-major matrices (math/matrix/SVD.hpp:15-1025). */
+ZSMPM_API zsmpm_status zsmpm_svd3(const float *A, float *U, float *S, float *V, int64_t count,
+                                  void *stream);
+/* Constitutive update of `count` particles: F (in/out, projected as the model does),
+ * plastic (in/out) and tau = V0 P F^T (out). */
+ZSMPM_API zsmpm_status zsmpm_constitutive(const zsmpm_material *mat, float *F, float *plastic,
+                                          float *tau, int64_t count, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZSMPM_H */

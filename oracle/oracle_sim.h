@@ -1,0 +1,402 @@
+/* Test infrastructure (oracle): the substep restatement, written once and instantiated
+ * for float (SFX=_f32) and double (SFX=_f64) by oracle.c.  Every expression keeps the
+ * reference's operand order (the FP32 instance is pinned bit-exactly against the compiled
+ * reference under a sequential schedule); see oracle.h for the file:line list.
+ *
+ * Required macros: R (float or double), SFX, R_LOG/R_EXP/R_SQRT/R_FLOOR (logf/expf/sqrtf/
+ * floorf or their double forms), OR_SVD (oracle_svd_f32 / oracle_svd_f64).
+ */
+#define OR_CAT2(a, b) a##b
+#define OR_CAT(a, b) OR_CAT2(a, b)
+#define OR_NAME(base) OR_CAT(base, SFX)
+
+/* ConstitutiveModel.hpp:34-38.  The reference evaluates mu with a double literal 0.5,
+ * so for T=float mu = float(0.5 * double(E) / double(1 + nu)); lambda stays in T. */
+static void OR_NAME(lame)(R E, R nu, R *mu, R *lam) {
+  *mu = (R)(0.5 * (double)E / (double)((R)1 + nu));
+  *lam = E * nu / (((R)1 + nu) * ((R)1 - (R)2 * nu));
+}
+
+/* out[3c+r] = sum_k U[3k+r] d[k] V[3k+c], products as ((U d) V)  (MatrixUtils.h:26-45) */
+static void OR_NAME(mat_diag_matT)(R *out, const R *U, const R *d, const R *V) {
+  for (int c = 0; c != 3; ++c)
+    for (int r = 0; r != 3; ++r)
+      out[3 * c + r] = U[r] * d[0] * V[c] + U[3 + r] * d[1] * V[3 + c] +
+                       U[6 + r] * d[2] * V[6 + c];
+}
+
+/* PF[3c+r] = (sum_k P[3k+r] F[3k+c]) * volume, i.e. volume * P F^T */
+static void OR_NAME(p_ft)(R *PF, const R *P, const R *F, R volume) {
+  for (int c = 0; c != 3; ++c)
+    for (int r = 0; r != 3; ++r)
+      PF[3 * c + r] = (P[r] * F[c] + P[3 + r] * F[3 + c] + P[6 + r] * F[6 + c]) * volume;
+}
+
+/* ConstitutiveModel_Vol_dP.hpp:10-46 */
+static void OR_NAME(stress_fc)(R volume, R mu, R lambda, const R *F, R *PF) {
+  R U[9], S[3], V[9], P[9];
+  OR_SVD(F, U, S, V);
+  R J = S[0] * S[1] * S[2];
+  R scaled_mu = (R)2 * mu;
+  R scaled_lambda = lambda * (J - (R)1);
+  R Ph[3];
+  Ph[0] = scaled_mu * (S[0] - (R)1) + scaled_lambda * (S[1] * S[2]);
+  Ph[1] = scaled_mu * (S[1] - (R)1) + scaled_lambda * (S[0] * S[2]);
+  Ph[2] = scaled_mu * (S[2] - (R)1) + scaled_lambda * (S[0] * S[1]);
+  for (int c = 0; c != 3; ++c)
+    for (int r = 0; r != 3; ++r)
+      P[3 * c + r] = Ph[0] * U[r] * V[c] + Ph[1] * U[3 + r] * V[3 + c] +
+                     Ph[2] * U[6 + r] * V[6 + c];
+  OR_NAME(p_ft)(PF, P, F, volume);
+}
+
+/* ConstitutiveModel_Vol_dP.hpp:241-325 (F projected in place, logJp updated) */
+static void OR_NAME(stress_sand)(R volume, R mu, R lambda, R cohesion, R beta,
+                                 R yieldSurface, int volCorrection, R *logJp, R *F, R *PF) {
+  R U[9], S[3], V[9];
+  OR_SVD(F, U, S, V);
+  R scaled_mu = (R)2 * mu;
+  R epsilon[3], New_S[3] = {0, 0, 0}, New_F[9];
+  for (int i = 0; i != 3; ++i) {
+    R abs_S = S[i] > 0 ? S[i] : -S[i];
+    /* `abs_S > 1e-4 ? abs_S : 1e-4` compares against the double literal */
+    abs_S = ((double)abs_S > 1e-4) ? abs_S : (R)1e-4;
+    epsilon[i] = R_LOG(abs_S) - cohesion;
+  }
+  R sum_epsilon = epsilon[0] + epsilon[1] + epsilon[2];
+  R trace_epsilon = sum_epsilon + *logJp;
+  R epsilon_hat[3];
+  for (int i = 0; i != 3; ++i) epsilon_hat[i] = epsilon[i] - (trace_epsilon / (R)3);
+  R epsilon_hat_norm = R_SQRT(epsilon_hat[0] * epsilon_hat[0] + epsilon_hat[1] * epsilon_hat[1] +
+                              epsilon_hat[2] * epsilon_hat[2]);
+  if (trace_epsilon >= (R)0) {
+    New_S[0] = New_S[1] = New_S[2] = R_EXP(cohesion);
+    OR_NAME(mat_diag_matT)(New_F, U, New_S, V);
+    for (int i = 0; i != 9; ++i) F[i] = New_F[i];
+    if (volCorrection) *logJp = beta * sum_epsilon + *logJp;
+  } else if (mu != 0) {
+    *logJp = 0;
+    R delta_gamma = epsilon_hat_norm +
+                    ((R)3 * lambda + scaled_mu) / scaled_mu * trace_epsilon * yieldSurface;
+    R H[3];
+    if (delta_gamma <= 0) {
+      for (int i = 0; i != 3; ++i) H[i] = epsilon[i] + cohesion;
+    } else {
+      for (int i = 0; i != 3; ++i)
+        H[i] = epsilon[i] - (delta_gamma / epsilon_hat_norm) * epsilon_hat[i] + cohesion;
+    }
+    for (int i = 0; i != 3; ++i) New_S[i] = R_EXP(H[i]);
+    OR_NAME(mat_diag_matT)(New_F, U, New_S, V);
+    for (int i = 0; i != 9; ++i) F[i] = New_F[i];
+  }
+  R New_S_log[3] = {R_LOG(New_S[0]), R_LOG(New_S[1]), R_LOG(New_S[2])};
+  R trace_log_S = New_S_log[0] + New_S_log[1] + New_S_log[2];
+  R P_hat[3], P[9];
+  for (int i = 0; i != 3; ++i)
+    P_hat[i] = (scaled_mu * New_S_log[i] + lambda * trace_log_S) / New_S[i];
+  OR_NAME(mat_diag_matT)(P, U, P_hat, V);
+  OR_NAME(p_ft)(PF, P, F, volume);
+}
+
+/* Snow: SnowPlasticity::do_project_sigma (SnowPlasticity.hpp:24-32) on the singular values
+ * of the trial F, committed to F = U diag(S_clamped) V^T; the plastic volume ratio is
+ * accumulated, Jp <- Jp * prod(S) / max(prod(S_clamped), 1e-6) (the reference recomputes
+ * it from the current step only, which equals this when Jp starts at 1 each step); then
+ * fixed-corotated stress with mu, lambda scaled by exp(hardening * (1 - Jp)). */
+static void OR_NAME(stress_snow)(R volume, R mu, R lambda, R hardening, R theta_c,
+                                 R theta_s, R *Jp, R *F, R *PF) {
+  R U[9], S[3], V[9], Sc[3], Fe[9];
+  OR_SVD(F, U, S, V);
+  R J = S[0] * S[1] * S[2];
+  for (int d = 0; d != 3; ++d) {
+    R s = S[d] < (R)1 + theta_s ? S[d] : (R)1 + theta_s;
+    Sc[d] = s > (R)1 - theta_c ? s : (R)1 - theta_c;
+  }
+  R Jc = Sc[0] * Sc[1] * Sc[2];
+  R jp = *Jp * (J / (Jc > (R)1e-6 ? Jc : (R)1e-6));
+  *Jp = jp;
+  R e = R_EXP(hardening * ((R)1 - jp));
+  OR_NAME(mat_diag_matT)(Fe, U, Sc, V);
+  for (int i = 0; i != 9; ++i) F[i] = Fe[i];
+  OR_NAME(stress_fc)(volume, mu * e, lambda * e, F, PF);
+}
+
+typedef struct {
+  int model, mode, wall_type, wall_cells, vc;
+  R dx, dt, g[3], E, nu, volume, fa, coh, beta, ys, hard, tc, ts, mu, lam;
+} OR_NAME(cfg);
+
+static void OR_NAME(make_cfg)(const oracle_params *p, OR_NAME(cfg) * c) {
+  c->model = p->model;
+  c->mode = p->mode;
+  c->wall_type = p->wall_type;
+  c->wall_cells = p->wall_cells;
+  c->vc = p->volume_correction;
+  c->dx = (R)p->dx;
+  c->dt = (R)p->dt;
+  c->g[0] = (R)p->gx;
+  c->g[1] = (R)p->gy;
+  c->g[2] = (R)p->gz;
+  c->E = (R)p->E;
+  c->nu = (R)p->nu;
+  c->volume = (R)p->volume;
+  c->fa = (R)p->friction_deg;
+  c->coh = (R)p->cohesion;
+  c->beta = (R)p->beta;
+  c->hard = (R)p->hardening;
+  c->tc = (R)p->theta_c;
+  c->ts = (R)p->theta_s;
+  {
+    /* DruckerPragerConfig::yieldSurface (ConstitutiveModel.hpp:752) */
+    R sin_phi = (R)sin((double)p->friction_deg / 180.0 * 3.14159265358979323846);
+    c->ys = (R)0.816496580927726 * (R)2 * sin_phi / ((R)3 - sin_phi);
+    if (sizeof(R) == sizeof(float))
+      c->ys = (R)(0.816496580927726f * 2.f * (float)sin_phi / (3.f - (float)sin_phi));
+  }
+  OR_NAME(lame)(c->E, c->nu, &c->mu, &c->lam);
+}
+
+/* Stress of one particle; projects F / updates the plastic variable as the model does. */
+static void OR_NAME(stress)(const OR_NAME(cfg) * c, R *F, R *plastic, R *PF) {
+  if (c->model == ORACLE_FC)
+    OR_NAME(stress_fc)(c->volume, c->mu, c->lam, F, PF);
+  else if (c->model == ORACLE_DP)
+    OR_NAME(stress_sand)(c->volume, c->mu, c->lam, c->coh, c->beta, c->ys, c->vc, plastic, F, PF);
+  else
+    OR_NAME(stress_snow)(c->volume, c->mu, c->lam, c->hard, c->tc, c->ts, plastic, F, PF);
+}
+
+void OR_NAME(oracle_stress)(const oracle_params *p, R *F, R *plastic, R *PF) {
+  OR_NAME(cfg) c;
+  OR_NAME(make_cfg)(p, &c);
+  OR_NAME(stress)(&c, F, plastic, PF);
+}
+
+/* quadratic B-spline stencil (Utils.hpp:30-70, InterpolationKernel.hpp:51-57, :93-130) */
+typedef struct {
+  int corner[3];
+  R w[3][3];
+  R localPos[3]; /* (X - corner) * dx */
+} OR_NAME(arena);
+
+static void OR_NAME(make_arena)(OR_NAME(arena) * a, R dx, const R *pos) {
+  for (int d = 0; d != 3; ++d) {
+    R X = pos[d] / dx;
+    a->corner[d] = (int)R_FLOOR(X - (R)0.5);
+    R lp = X - (R)a->corner[d];
+    R d0 = lp - (R)(int)R_FLOOR(lp - (R)0.5);
+    a->w[d][0] = (R)0.5 * ((R)1.5 - d0) * ((R)1.5 - d0);
+    R d1 = d0 - (R)1.0;
+    a->w[d][1] = (R)0.75 - d1 * d1;
+    R zz = (R)0.5 + d1;
+    a->w[d][2] = (R)0.5 * zz * zz;
+    a->localPos[d] = lp * dx;
+  }
+}
+
+static int OR_NAME(block_of)(const R *x, R dxinv, int32_t *out) {
+  for (int d = 0; d != 3; ++d) {
+    R v = x[d] * dxinv + (R)0.5;
+    if (!(v > -1e9 && v < 1e9)) return 1;
+    int32_t c = (int32_t)R_FLOOR(v) - 2;
+    out[d] = (c + (c < 0 ? -7 : 0)) / 8;
+  }
+  return 0;
+}
+
+int OR_NAME(oracle_run)(const oracle_params *p, int n, const R *m, R *x, R *v, R *C, R *F,
+                        R *plastic, int nsteps, int cap_blocks, int *out_nblocks,
+                        int *out_keys, R *out_grid) {
+  OR_NAME(cfg) cfg;
+  OR_NAME(make_cfg)(p, &cfg);
+  const R dx = cfg.dx, dt = cfg.dt;
+  const R dx_inv = (R)1 / dx;
+  const R D_inv = (R)4 * dx_inv * dx_inv;
+  oracle_table t;
+  if (oracle_table_init(&t, p->table_expected)) return 3;
+  R *grid = NULL;
+  size_t grid_blocks = 0;
+  R *tau = NULL;
+  int status = 0;
+  if (cfg.mode == ORACLE_MODE_COMMITTED) {
+    /* stress of the initial state, computed as the end of a G2P would */
+    tau = (R *)malloc(sizeof(R) * 9 * (size_t)(n > 0 ? n : 1));
+    for (int i = 0; i != n; ++i) OR_NAME(stress)(&cfg, &F[9 * i], &plastic[i], &tau[9 * i]);
+  }
+  for (int step = 0; step != nsteps && !status; ++step) {
+    /* 1. activation (SparsityOp.hpp:58-112) and canonical order */
+    oracle_table_clear(&t);
+    for (int i = 0; i != n && !status; ++i) {
+      int32_t b[3];
+      if (OR_NAME(block_of)(&x[3 * i], dx_inv, b)) status = 4;
+      else if (oracle_table_insert(&t, b, -1) < 0) status = 2;
+    }
+    const int npb = t.count;
+    for (int i = 0; i != npb && !status; ++i) {
+      int32_t k[3] = {t.active[3 * i], t.active[3 * i + 1], t.active[3 * i + 2]};
+      for (int a = 0; a != 2; ++a)
+        for (int b = 0; b != 2; ++b)
+          for (int c = 0; c != 2; ++c) {
+            int32_t nk[3] = {k[0] + a, k[1] + b, k[2] + c};
+            if (oracle_table_insert(&t, nk, -1) < 0) status = 2;
+          }
+    }
+    if (status) break;
+    if (t.count >= t.size - 20) {
+      status = 2;
+      break;
+    }
+    oracle_table_canonicalize(&t);
+    const int nb = t.count;
+    if ((size_t)nb > grid_blocks) {
+      free(grid);
+      grid_blocks = (size_t)nb;
+      grid = (R *)malloc(sizeof(R) * 7 * 512 * grid_blocks);
+    }
+    memset(grid, 0, sizeof(R) * 7 * 512 * (size_t)nb);
+
+    /* 2. P2G (P2G.hpp:45-127) */
+    for (int i = 0; i != n; ++i) {
+      const R *xp = &x[3 * i], *vp = &v[3 * i], *Cp = &C[9 * i];
+      const R mass = m[i];
+      R contrib[9];
+      if (cfg.mode == ORACLE_MODE_REFERENCE) {
+        R Fl[9];
+        for (int k = 0; k != 9; ++k) Fl[k] = F[9 * i + k];
+        OR_NAME(stress)(&cfg, Fl, &plastic[i], contrib);
+      } else {
+        for (int k = 0; k != 9; ++k) contrib[k] = tau[9 * i + k];
+      }
+      for (int k = 0; k != 9; ++k) contrib[k] = contrib[k] * -dt * D_inv;
+      OR_NAME(arena) a;
+      OR_NAME(make_arena)(&a, dx, xp);
+      for (int ii = 0; ii != 3; ++ii)
+        for (int jj = 0; jj != 3; ++jj)
+          for (int kk = 0; kk != 3; ++kk) {
+            int32_t coord[3] = {a.corner[0] + ii, a.corner[1] + jj, a.corner[2] + kk};
+            int32_t loc[3], bk[3];
+            for (int d = 0; d != 3; ++d) {
+              loc[d] = coord[d] & 7;
+              bk[d] = (coord[d] - loc[d]) / 8;
+            }
+            int32_t blk = oracle_table_query(&t, bk);
+            if (blk < 0) {
+              status = 5;
+              continue;
+            }
+            R xixp[3] = {(R)ii * dx - a.localPos[0], (R)jj * dx - a.localPos[1],
+                         (R)kk * dx - a.localPos[2]};
+            R W = a.w[0][ii] * a.w[1][jj] * a.w[2][kk];
+            int cell = (loc[0] << 6) | (loc[1] << 3) | loc[2];
+            R *g = &grid[(size_t)blk * 7 * 512];
+            g[0 * 512 + cell] += mass * W;
+            for (int d = 0; d != 3; ++d) {
+              g[(1 + d) * 512 + cell] +=
+                  W * mass * (vp[d] + (Cp[d] * xixp[0] + Cp[3 + d] * xixp[1] + Cp[6 + d] * xixp[2]));
+              g[(4 + d) * 512 + cell] +=
+                  (contrib[d] * xixp[0] + contrib[3 + d] * xixp[1] + contrib[6 + d] * xixp[2]) * W;
+            }
+          }
+    }
+    if (status) break;
+
+    /* 3. grid velocity, v = (mv + rhs) / m + g dt (restated), then walls */
+    const R lo = (R)cfg.wall_cells * dx, hi = (R)1 - (R)cfg.wall_cells * dx;
+    for (int b = 0; b != nb; ++b) {
+      R *g = &grid[(size_t)b * 7 * 512];
+      const int32_t *key = &t.active[3 * b];
+      for (int cell = 0; cell != 512; ++cell) {
+        R mass = g[cell];
+        if (mass != 0) {
+          mass = (R)1 / mass;
+          R vel[3];
+          for (int d = 0; d != 3; ++d)
+            vel[d] = (g[(1 + d) * 512 + cell] + g[(4 + d) * 512 + cell]) * mass + cfg.g[d] * dt;
+          for (int d = 0; d != 3; ++d) g[(1 + d) * 512 + cell] = vel[d];
+        }
+      }
+      if (cfg.wall_type == ORACLE_WALL_NONE) continue;
+      /* ApplyBoundaryConditionOnGridBlocks once per wall, walls x-,x+,y-,y+,z-,z+ */
+      for (int w = 0; w != 6; ++w) {
+        const int axis = w / 2;
+        const R sgn = (w & 1) ? (R)-1 : (R)1;
+        const R origin = (w & 1) ? hi : lo;
+        for (int cell = 0; cell != 512; ++cell) {
+          if (!(g[cell] > 0)) continue;
+          const int cc[3] = {cell >> 6, (cell >> 3) & 7, cell & 7};
+          R pos = ((R)key[axis] * (R)8 + (R)cc[axis]) * dx;
+          R sd = sgn * (pos - origin);
+          if (!(sd < 0)) continue;
+          if (cfg.wall_type == ORACLE_WALL_STICKY) {
+            for (int d = 0; d != 3; ++d) g[(1 + d) * 512 + cell] = 0;
+          } else {
+            R proj = sgn * g[(1 + axis) * 512 + cell];
+            if (cfg.wall_type == ORACLE_WALL_SLIP || proj < 0)
+              g[(1 + axis) * 512 + cell] = g[(1 + axis) * 512 + cell] - proj * sgn;
+          }
+        }
+      }
+    }
+
+    /* 4. G2P (G2P.hpp:43-84), then in committed mode the constitutive update */
+    for (int i = 0; i != n; ++i) {
+      R *xp = &x[3 * i], *vp = &v[3 * i], *Cp = &C[9 * i], *Fp = &F[9 * i];
+      R vel[3] = {0, 0, 0}, Cn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      OR_NAME(arena) a;
+      OR_NAME(make_arena)(&a, dx, xp);
+      for (int ii = 0; ii != 3; ++ii)
+        for (int jj = 0; jj != 3; ++jj)
+          for (int kk = 0; kk != 3; ++kk) {
+            int32_t coord[3] = {a.corner[0] + ii, a.corner[1] + jj, a.corner[2] + kk};
+            int32_t loc[3], bk[3];
+            for (int d = 0; d != 3; ++d) {
+              loc[d] = coord[d] & 7;
+              bk[d] = (coord[d] - loc[d]) / 8;
+            }
+            int32_t blk = oracle_table_query(&t, bk);
+            R xixp[3] = {(R)ii * dx - a.localPos[0], (R)jj * dx - a.localPos[1],
+                         (R)kk * dx - a.localPos[2]};
+            R W = a.w[0][ii] * a.w[1][jj] * a.w[2][kk];
+            int cell = (loc[0] << 6) | (loc[1] << 3) | loc[2];
+            const R *g = &grid[(size_t)blk * 7 * 512];
+            R vi[3] = {g[1 * 512 + cell], g[2 * 512 + cell], g[3 * 512 + cell]};
+            for (int d = 0; d != 3; ++d) vel[d] += vi[d] * W;
+            for (int d = 0; d != 9; ++d) Cn[d] += W * vi[d % 3] * xixp[d / 3] * D_inv;
+          }
+      for (int d = 0; d != 3; ++d) xp[d] += vel[d] * dt;
+      {
+        R tmp[9], Fn[9];
+        for (int d = 0; d != 9; ++d) tmp[d] = Cn[d] * dt + ((d & 0x3) ? (R)0 : (R)1);
+        for (int c = 0; c != 3; ++c)
+          for (int r = 0; r != 3; ++r)
+            Fn[3 * c + r] = tmp[r] * Fp[3 * c] + tmp[3 + r] * Fp[3 * c + 1] + tmp[6 + r] * Fp[3 * c + 2];
+        for (int d = 0; d != 9; ++d) Fp[d] = Fn[d];
+      }
+      for (int d = 0; d != 3; ++d) vp[d] = vel[d];
+      for (int d = 0; d != 9; ++d) Cp[d] = Cn[d];
+      if (cfg.mode == ORACLE_MODE_COMMITTED) OR_NAME(stress)(&cfg, Fp, &plastic[i], &tau[9 * i]);
+    }
+  }
+  if (!status) {
+    const int nb = t.count;
+    if (out_nblocks) *out_nblocks = nb;
+    if (out_keys) {
+      if (nb > cap_blocks) status = 1;
+      else
+        for (int b = 0; b != nb; ++b) {
+          for (int d = 0; d != 3; ++d) out_keys[3 * b + d] = t.active[3 * b + d];
+          for (int ch = 0; ch != 4; ++ch)
+            for (int cell = 0; cell != 512; ++cell)
+              out_grid[((size_t)b * 4 + ch) * 512 + cell] = grid[((size_t)b * 7 + ch) * 512 + cell];
+        }
+    }
+  }
+  free(grid);
+  free(tau);
+  oracle_table_free(&t);
+  return status;
+}
+
+#undef OR_NAME
+#undef OR_CAT
+#undef OR_CAT2

@@ -1,0 +1,151 @@
+// Test infrastructure: command-line front end of the reference driver (ref_driver.cpp).
+// The reference library is run in its own process and fed through raw little-endian
+// files: loaded into a Python process with ctypes, its host-side runtime intermittently
+// blocked on a futex before the first operator launch, while the same calls from a plain
+// C/C++ process never did.  Usage:  zsref_cli <request file> <reply file>
+//
+// Request: int32 command, then
+//   1 run:       zsref_params, int32 n, int32 nsteps, int32 cap_blocks,
+//                f32 m[n], x[3n], v[3n], C[9n], F[9n], logJp[n]
+//     reply:     int32 status, int32 nblocks, f64 seconds, x, v, C, F, logJp,
+//                int32 keys[3*nblocks], f32 grid[nblocks*4*512]   (keys/grid if status==0)
+//   2 activate:  int32 n, f32 dx, int32 table_expected, int32 cap, f32 x[3n]
+//     reply:     int32 status, nblocks, nparblocks, table_size, keys[3*nb], slots[nb]
+//   3 stress:    int32 count, int32 model, f32 volume, E, nu, friction_deg, cohesion, beta,
+//                int32 volume_correction, f32 F[9*count], logJp[count]
+//     reply:     f32 PF[9*count], F[9*count], logJp[count]
+//   4 svd:       int32 count, f32 A[9*count]
+//     reply:     f32 U[9*count], S[3*count], V[9*count]
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+extern "C" {
+struct zsref_params {
+  int model, policy, threads, order, wall_type, wall_cells, table_expected, volume_correction;
+  float dx, dt, gx, gy, gz;
+  float E, nu, volume;
+  float friction_deg, cohesion, beta;
+};
+int zsref_run(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
+              float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
+              float *out_grid, double *out_seconds);
+void zsref_stress(int model, float volume, float E, float nu, float friction_deg,
+                  float cohesion, float beta, int volume_correction, float *F, float *logJp,
+                  float *PF);
+void zsref_svd(const float *A, float *U, float *S, float *V);
+int zsref_activate(int n, const float *x, float dx, int table_expected, int cap,
+                   int *out_nblocks, int *out_nparblocks, int *out_keys, int *out_slots,
+                   int *out_table_size);
+}
+
+namespace {
+  FILE *in_f, *out_f;
+  template <typename T> T rd() {
+    T v{};
+    if (std::fread(&v, sizeof(T), 1, in_f) != 1) {
+      std::fprintf(stderr, "zsref_cli: short request\n");
+      std::exit(3);
+    }
+    return v;
+  }
+  template <typename T> void rdv(std::vector<T> &v, size_t n) {
+    v.resize(n);
+    if (n && std::fread(v.data(), sizeof(T), n, in_f) != n) {
+      std::fprintf(stderr, "zsref_cli: short request array\n");
+      std::exit(3);
+    }
+  }
+  template <typename T> void wr(const T &v) { std::fwrite(&v, sizeof(T), 1, out_f); }
+  template <typename T> void wrv(const T *p, size_t n) {
+    if (n) std::fwrite(p, sizeof(T), n, out_f);
+  }
+}  // namespace
+
+int main(int argc, char **argv) {
+  if (argc != 3) {
+    std::fprintf(stderr, "usage: zsref_cli <request> <reply>\n");
+    return 2;
+  }
+  in_f = std::fopen(argv[1], "rb");
+  out_f = std::fopen(argv[2], "wb");
+  if (!in_f || !out_f) return 2;
+  const int cmd = rd<int32_t>();
+  if (cmd == 1) {
+    auto p = rd<zsref_params>();
+    const int n = rd<int32_t>(), nsteps = rd<int32_t>(), cap = rd<int32_t>();
+    std::vector<float> m, x, v, C, F, lj;
+    rdv(m, n);
+    rdv(x, 3 * (size_t)n);
+    rdv(v, 3 * (size_t)n);
+    rdv(C, 9 * (size_t)n);
+    rdv(F, 9 * (size_t)n);
+    rdv(lj, n);
+    std::vector<int> keys(3 * (size_t)cap);
+    std::vector<float> grid((size_t)cap * 4 * 512);
+    int nb = 0;
+    double secs = 0;
+    int st = zsref_run(&p, n, m.data(), x.data(), v.data(), C.data(), F.data(), lj.data(),
+                       nsteps, cap, &nb, cap ? keys.data() : nullptr,
+                       cap ? grid.data() : nullptr, &secs);
+    wr<int32_t>(st);
+    wr<int32_t>(nb);
+    wr<double>(secs);
+    wrv(x.data(), x.size());
+    wrv(v.data(), v.size());
+    wrv(C.data(), C.size());
+    wrv(F.data(), F.size());
+    wrv(lj.data(), lj.size());
+    if (st == 0 && cap) {
+      wrv(keys.data(), 3 * (size_t)nb);
+      wrv(grid.data(), (size_t)nb * 4 * 512);
+    }
+  } else if (cmd == 2) {
+    const int n = rd<int32_t>();
+    const float dx = rd<float>();
+    const int expected = rd<int32_t>(), cap = rd<int32_t>();
+    std::vector<float> x;
+    rdv(x, 3 * (size_t)n);
+    std::vector<int> keys(3 * (size_t)cap), slots(cap);
+    int nb = 0, npb = 0, ts = 0;
+    int st = zsref_activate(n, x.data(), dx, expected, cap, &nb, &npb, keys.data(),
+                            slots.data(), &ts);
+    wr<int32_t>(st);
+    wr<int32_t>(nb);
+    wr<int32_t>(npb);
+    wr<int32_t>(ts);
+    if (st == 0) {
+      wrv(keys.data(), 3 * (size_t)nb);
+      wrv(slots.data(), (size_t)nb);
+    }
+  } else if (cmd == 3) {
+    const int count = rd<int32_t>(), model = rd<int32_t>();
+    const float vol = rd<float>(), E = rd<float>(), nu = rd<float>(), fa = rd<float>(),
+                coh = rd<float>(), beta = rd<float>();
+    const int vc = rd<int32_t>();
+    std::vector<float> F, lj, PF(9 * (size_t)count);
+    rdv(F, 9 * (size_t)count);
+    rdv(lj, count);
+    for (int i = 0; i != count; ++i)
+      zsref_stress(model, vol, E, nu, fa, coh, beta, vc, &F[9 * (size_t)i], &lj[i],
+                   &PF[9 * (size_t)i]);
+    wrv(PF.data(), PF.size());
+    wrv(F.data(), F.size());
+    wrv(lj.data(), lj.size());
+  } else if (cmd == 4) {
+    const int count = rd<int32_t>();
+    std::vector<float> A, U(9 * (size_t)count), S(3 * (size_t)count), V(9 * (size_t)count);
+    rdv(A, 9 * (size_t)count);
+    for (int i = 0; i != count; ++i)
+      zsref_svd(&A[9 * (size_t)i], &U[9 * (size_t)i], &S[3 * (size_t)i], &V[9 * (size_t)i]);
+    wrv(U.data(), U.size());
+    wrv(S.data(), S.size());
+    wrv(V.data(), V.size());
+  } else {
+    std::fprintf(stderr, "zsref_cli: unknown command %d\n", cmd);
+    return 2;
+  }
+  std::fclose(out_f);
+  return 0;
+}

@@ -1,0 +1,292 @@
+// Test infrastructure: drives the REFERENCE's own MPM operators (zpc, compiled from its
+// sources by oracle/build_ref.sh) through its own seq/omp execution policies.  The entry
+// points below are called by oracle/ref_cli.cpp, which the Python tests and the CPU
+// baseline arm of the benchmark run as a subprocess.  Nothing here is linked into the
+// product library.
+//
+// One substep is the canonical explicit MLS/APIC substep that the reference's operators
+// compose into (the reference ships the operators but no driver):
+//   1. CleanSparsity + ComputeSparsity + EnlargeSparsity{0..2}^3
+//        (simulation/sparsity/SparsityOp.hpp:41-112, driver SparsityCompute.tpp:5-26)
+//   2. optional canonical re-ordering of the active keys (ascending (bx,by,bz)) followed by
+//      ResetHashTable + ReinsertHashTable (container/HashTable.hpp:215-247), which assigns
+//      index == position in the sorted key list
+//   3. CleanGridBlocks + P2GTransfer (simulation/grid/GridOp.hpp:54-69,
+//      simulation/transfer/P2G.hpp:45-127)
+//   4. grid velocity v = (mv + rhs)/m + g dt.  The reference's ComputeGridBlockVelocity
+//      (GridOp.hpp:93-99) computes mv/m + g dt and never consumes the rhs channel that P2G
+//      fills (P2G.hpp:120-123), so the rhs term is restated here in GridVelocityWithRhs.
+//   5. ApplyBoundaryConditionOnGridBlocks with six analytic planes (GridOp.hpp:113-164,
+//      geometry/Collider.h:80-110, geometry/AnalyticLevelSet.h:11-43)
+//   6. G2PTransfer (simulation/transfer/G2P.hpp:43-84)
+// Stress and plasticity are evaluated inside P2G on a local copy of F exactly as the
+// reference does ("ref-verbatim"): the projected F is not written back, logJp is.
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "zensim/omp/execution/ExecutionPolicy.hpp"
+#include "zensim/simulation/sparsity/SparsityOp.hpp"
+#include "zensim/simulation/transfer/P2G.hpp"
+#include "zensim/simulation/transfer/G2P.hpp"
+#include "zensim/geometry/SparseLevelSet.hpp"
+#include "zensim/simulation/grid/GridOp.hpp"
+#include "zensim/geometry/AnalyticLevelSet.h"
+#include "zensim/geometry/Collider.h"
+
+namespace {
+
+  using namespace zs;
+  using table_t = HashTable<i32, 3, int>;
+  using grids_t = Grids<f32, 3, 8>;
+  using particles_t = Particles<f32, 3>;
+
+  // Restated grid update: v = (mv + rhs) * (1/m) + g dt on cells with m != 0.
+  template <execspace_e space> struct GridVelocityWithRhs {
+    using view_t = GridsView<space, grids_t>;
+    GridVelocityWithRhs(wrapv<space>, grids_t &g, float dt, vec<float, 3> grav)
+        : grids{proxy<space>(g)}, dt{dt}, grav{grav} {}
+    void operator()(typename grids_t::size_type blockid,
+                    typename grids_t::cell_index_type cellid) noexcept {
+      auto block = grids[blockid];
+      float mass = block(0, cellid);
+      if (mass != 0.f) {
+        mass = 1.f / mass;
+        vec<float, 3> vel{};
+        for (int d = 0; d != 3; ++d)
+          vel[d] = (block(1 + d, cellid) + block(4 + d, cellid)) * mass + grav[d] * dt;
+        for (int d = 0; d != 3; ++d) block(1 + d, cellid) = vel[d];
+      }
+    }
+    view_t grids;
+    float dt;
+    vec<float, 3> grav;
+  };
+
+  using plane_t = AnalyticLevelSet<analytic_geometry_e::Plane, float, 3>;
+
+}  // namespace
+
+extern "C" {
+
+struct zsref_params {
+  int model;          // 0 fixed-corotated, 1 Drucker-Prager sand
+  int policy;         // 0 seq_exec, 1 omp_exec
+  int threads;        // omp threads; <= 0 selects zpc's default (hardware_concurrency - 1)
+  int order;          // 0 keep the table's insertion order, 1 canonical ascending (bx,by,bz)
+  int wall_type;      // 0 sticky, 1 slip, 2 separate
+  int wall_cells;     // wall thickness in cells (planes at wall_cells*dx from each face)
+  int table_expected; // expected entry count given to HashTable (capacity next_2pow(n)*16)
+  int volume_correction;
+  float dx, dt, gx, gy, gz;
+  float E, nu, volume;
+  float friction_deg, cohesion, beta;
+};
+
+// Runs nsteps substeps in place on SoA host arrays (x,v: n*3; C,F: n*9 column-major).
+// Grid output (optional, out_keys may be NULL): active block keys (i32*3 each) in table
+// index order and per block 512 cells x 4 channels (m, vx, vy, vz) after the boundary
+// conditions of the last substep, channel-major inside a block.
+// Returns 0 on success, 1 if the grid output capacity is too small, 2 if the table is full.
+int zsref_run(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
+              float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
+              float *out_grid, double *out_seconds) {
+  constexpr auto host = execspace_e::host;
+  constexpr auto omp = execspace_e::openmp;
+  particles_t pars{(size_t)n, memsrc_e::host, -1};
+  pars.addAttr("m", attrib_e::scalar);
+  pars.addAttr("v", attrib_e::vector);
+  pars.addAttr("C", attrib_e::matrix);
+  pars.addAttr("F", attrib_e::matrix);
+  pars.addAttr("logJp", attrib_e::scalar);
+  std::memcpy((float *)pars.getAttrAddress("m"), m, sizeof(float) * n);
+  std::memcpy((float *)pars.getAttrAddress("x"), x, sizeof(float) * 3 * n);
+  std::memcpy((float *)pars.getAttrAddress("v"), v, sizeof(float) * 3 * n);
+  std::memcpy((float *)pars.getAttrAddress("C"), C, sizeof(float) * 9 * n);
+  std::memcpy((float *)pars.getAttrAddress("F"), F, sizeof(float) * 9 * n);
+  std::memcpy((float *)pars.getAttrAddress("logJp"), logJp, sizeof(float) * n);
+
+  table_t table{(size_t)std::max(p->table_expected, 1), memsrc_e::host, -1};
+  grids_t grids{{{"m", 1}, {"v", 3}, {"rhs", 3}}, p->dx, (size_t)table._tableSize,
+                memsrc_e::host, -1};
+
+  FixedCorotatedConfig fc{};
+  fc.E = p->E;
+  fc.nu = p->nu;
+  fc.volume = p->volume;
+  DruckerPragerConfig dp{};
+  dp.E = p->E;
+  dp.nu = p->nu;
+  dp.volume = p->volume;
+  dp.fa = p->friction_deg;
+  dp.cohesion = p->cohesion;
+  dp.beta = p->beta;
+  dp.volumeCorrection = p->volume_correction != 0;
+  {
+    // ConstitutiveModel.hpp:752 default: sqrt(2/3) * 2 sin(phi) / (3 - sin(phi))
+    float sin_phi = (float)std::sin((double)p->friction_deg / 180.0 * 3.14159265358979323846);
+    dp.yieldSurface = 0.816496580927726f * 2.f * sin_phi / (3.f - sin_phi);
+  }
+
+  std::vector<Collider<plane_t>> walls;
+  {
+    const float lo = p->wall_cells * p->dx, hi = 1.f - p->wall_cells * p->dx;
+    collider_e ct = p->wall_type == 0 ? collider_e::Sticky
+                    : p->wall_type == 1 ? collider_e::Slip
+                                        : collider_e::Separate;
+    for (int d = 0; d != 3; ++d) {
+      vec<float, 3> o{0.f, 0.f, 0.f}, nrm{0.f, 0.f, 0.f};
+      o[d] = lo;
+      nrm[d] = 1.f;
+      walls.emplace_back(plane_t{o, nrm}, ct);
+      o[d] = hi;
+      nrm[d] = -1.f;
+      walls.emplace_back(plane_t{o, nrm}, ct);
+    }
+  }
+  const vec<float, 3> grav{p->gx, p->gy, p->gz};
+  int status = 0;
+
+  auto run = [&](auto pol, auto tag) {
+    constexpr auto space = decltype(tag)::value;
+    auto t0 = std::chrono::steady_clock::now();
+    for (int step = 0; step != nsteps; ++step) {
+      pol(range(table._tableSize), CleanSparsity{wrapv<space>{}, table});
+      pol(range((size_t)n),
+          ComputeSparsity{wrapv<space>{}, p->dx, 8, table, pars.attrVector("x")});
+      int nparblocks = table.size();
+      pol(range((size_t)nparblocks),
+          EnlargeSparsity{wrapv<space>{}, table, vec<int, 3>{0, 0, 0}, vec<int, 3>{2, 2, 2}});
+      int nb = table.size();
+      if (nb >= table._tableSize - 20) {
+        status = 2;
+        return;
+      }
+      if (p->order == 1) {
+        auto *keys = table._activeKeys.data();
+        std::sort(keys, keys + nb, [](const auto &a, const auto &b) {
+          for (int d = 0; d != 3; ++d)
+            if (a[d] != b[d]) return a[d] < b[d];
+          return false;
+        });
+        pol(range(table._tableSize),
+            ResetHashTable{proxy<space>(table), false});
+        pol(range((size_t)nb), ReinsertHashTable{proxy<space>(table)});
+      }
+      pol(Collapse{(size_t)nb, (size_t)512}, CleanGridBlocks{wrapv<space>{}, grids});
+      if (p->model == 0)
+        pol(range((size_t)n), P2GTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{},
+                                          p->dt, fc, pars, table, grids});
+      else
+        pol(range((size_t)n), P2GTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{},
+                                          p->dt, dp, pars, table, grids});
+      pol(Collapse{(size_t)nb, (size_t)512},
+          GridVelocityWithRhs<space>{wrapv<space>{}, grids, p->dt, grav});
+      for (auto &w : walls)
+        pol(Collapse{(size_t)nb, (size_t)512},
+            ApplyBoundaryConditionOnGridBlocks{wrapv<space>{}, w, table, grids});
+      if (p->model == 0)
+        pol(range((size_t)n), G2PTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{},
+                                          p->dt, fc, grids, table, pars});
+      else
+        pol(range((size_t)n), G2PTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{},
+                                          p->dt, dp, grids, table, pars});
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (out_seconds) *out_seconds = std::chrono::duration<double>(t1 - t0).count();
+  };
+
+  if (p->policy == 0)
+    run(seq_exec(), wrapv<host>{});
+  else {
+    auto pol = omp_exec();
+    if (p->threads > 0) pol = OmpExecutionPolicy{}.threads(p->threads);
+    run(pol, wrapv<omp>{});
+  }
+  if (status) return status;
+
+  std::memcpy(x, (float *)pars.getAttrAddress("x"), sizeof(float) * 3 * n);
+  std::memcpy(v, (float *)pars.getAttrAddress("v"), sizeof(float) * 3 * n);
+  std::memcpy(C, (float *)pars.getAttrAddress("C"), sizeof(float) * 9 * n);
+  std::memcpy(F, (float *)pars.getAttrAddress("F"), sizeof(float) * 9 * n);
+  std::memcpy(logJp, (float *)pars.getAttrAddress("logJp"), sizeof(float) * n);
+
+  const int nb = table.size();
+  if (out_nblocks) *out_nblocks = nb;
+  if (out_keys) {
+    if (nb > cap_blocks) return 1;
+    auto tv = proxy<host>(grids);
+    for (int b = 0; b != nb; ++b) {
+      auto key = table._activeKeys[b];
+      for (int d = 0; d != 3; ++d) out_keys[b * 3 + d] = key[d];
+      auto block = tv[b];
+      for (int c = 0; c != 4; ++c)
+        for (int cell = 0; cell != 512; ++cell)
+          out_grid[((size_t)b * 4 + c) * 512 + cell] = block(c, cell);
+    }
+  }
+  return 0;
+}
+
+// Reference-verbatim stress of one particle, for unit parity of the constitutive code
+// (physics/ConstitutiveModel_Vol_dP.hpp:10-46 and :241-325).  PF and F are column-major.
+void zsref_stress(int model, float volume, float E, float nu, float friction_deg,
+                  float cohesion, float beta, int volume_correction, float *F, float *logJp,
+                  float *PF) {
+  auto [mu, lambda] = lame_parameters(E, nu);
+  vec<float, 9> f{}, pf{};
+  for (int i = 0; i != 9; ++i) f[i] = F[i];
+  if (model == 0)
+    compute_stress_fixedcorotated(volume, mu, lambda, f, pf);
+  else {
+    float sin_phi = (float)std::sin((double)friction_deg / 180.0 * 3.14159265358979323846);
+    float ys = 0.816496580927726f * 2.f * sin_phi / (3.f - sin_phi);
+    compute_stress_sand(volume, mu, lambda, cohesion, beta, ys, volume_correction != 0, *logJp,
+                        f, pf);
+    for (int i = 0; i != 9; ++i) F[i] = f[i];
+  }
+  for (int i = 0; i != 9; ++i) PF[i] = pf[i];
+}
+
+// The reference's float 3x3 SVD (math/matrix/SVD.hpp:15-1025), A column-major.
+void zsref_svd(const float *A, float *U, float *S, float *V) {
+  math::svd_3d(A[0], A[3], A[6], A[1], A[4], A[7], A[2], A[5], A[8], U[0], U[3], U[6], U[1],
+               U[4], U[7], U[2], U[5], U[8], S[0], S[1], S[2], V[0], V[3], V[6], V[1], V[4],
+               V[7], V[2], V[5], V[8]);
+}
+
+// Block keys of a HashTable after inserting the given particle positions in order with
+// seq_exec (ComputeSparsity + EnlargeSparsity), in the table's own insertion order.
+// Also reports, for every key, the table slot it landed in.
+int zsref_activate(int n, const float *x, float dx, int table_expected, int cap,
+                   int *out_nblocks, int *out_nparblocks, int *out_keys, int *out_slots,
+                   int *out_table_size) {
+  constexpr auto host = execspace_e::host;
+  particles_t pars{(size_t)n, memsrc_e::host, -1};
+  std::memcpy((float *)pars.getAttrAddress("x"), x, sizeof(float) * 3 * n);
+  table_t table{(size_t)std::max(table_expected, 1), memsrc_e::host, -1};
+  auto pol = seq_exec();
+  pol(range(table._tableSize), CleanSparsity{wrapv<host>{}, table});
+  pol(range((size_t)n), ComputeSparsity{wrapv<host>{}, dx, 8, table, pars.attrVector("x")});
+  int npb = table.size();
+  pol(range((size_t)npb),
+      EnlargeSparsity{wrapv<host>{}, table, vec<int, 3>{0, 0, 0}, vec<int, 3>{2, 2, 2}});
+  int nb = table.size();
+  *out_nblocks = nb;
+  *out_nparblocks = npb;
+  *out_table_size = table._tableSize;
+  if (nb > cap) return 1;
+  auto view = proxy<host>(table);
+  for (int b = 0; b != nb; ++b) {
+    auto key = table._activeKeys[b];
+    for (int d = 0; d != 3; ++d) out_keys[b * 3 + d] = key[d];
+    out_slots[b] = view.entry(key);
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,134 @@
+"""Test infrastructure: runs the reference's own MPM path (oracle/_ref/zsref_cli, compiled from
+the zpc sources by oracle/build_ref.sh) in a subprocess, exchanging raw little-endian files.
+
+The reference's host runtime is run in its own process because, loaded into a Python process,
+it intermittently blocked on a futex before its first operator launch; the same calls from a
+plain C++ process never did.  Every call has a timeout and is retried once.
+"""
+from __future__ import annotations
+
+import os
+import struct
+import subprocess
+import tempfile
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+CLI = HERE / "_ref" / "zsref_cli"
+
+POLICY_SEQ, POLICY_OMP = 0, 1
+
+
+def available() -> bool:
+    return CLI.exists()
+
+
+def _run(request: bytes, timeout: float) -> bytes:
+    if not CLI.exists():
+        raise FileNotFoundError(f"{CLI} not built (oracle/build_ref.sh needs the reference sources)")
+    last = None
+    for _attempt in range(2):
+        with tempfile.TemporaryDirectory() as td:
+            req = os.path.join(td, "req.bin")
+            rep = os.path.join(td, "rep.bin")
+            with open(req, "wb") as f:
+                f.write(request)
+            try:
+                r = subprocess.run([str(CLI), req, rep], capture_output=True, timeout=timeout)
+            except subprocess.TimeoutExpired as e:
+                last = e
+                continue
+            if r.returncode != 0:
+                raise RuntimeError(f"zsref_cli failed: {r.stderr.decode(errors='replace')}")
+            with open(rep, "rb") as f:
+                return f.read()
+    raise RuntimeError(f"zsref_cli timed out twice: {last}")
+
+
+def _params_bytes(spec, policy: int, threads: int, order: int, table_expected: int) -> bytes:
+    m = spec.material
+    ints = [m.model, policy, threads, order, spec.wall_type, spec.wall_cells, table_expected,
+            m.volume_correction]
+    floats = [spec.dx, spec.dt, *spec.gravity, m.E, m.nu, spec.volume, m.friction_deg, m.cohesion,
+              m.beta]
+    return struct.pack("<8i11f", *ints, *floats)
+
+
+@dataclass
+class RefResult:
+    status: int
+    seconds: float
+    x: np.ndarray
+    v: np.ndarray
+    C: np.ndarray
+    F: np.ndarray
+    logJp: np.ndarray
+    keys: np.ndarray
+    grid: np.ndarray
+
+
+def run(spec, particles, nsteps: int, policy: int = POLICY_SEQ, threads: int = 0, order: int = 1,
+        table_expected: int | None = None, cap_blocks: int = 1 << 15,
+        timeout: float = 600.0) -> RefResult:
+    n = particles.n
+    if table_expected is None:
+        table_expected = max(n // 512, 64)
+    req = struct.pack("<i", 1) + _params_bytes(spec, policy, threads, order, table_expected)
+    req += struct.pack("<3i", n, nsteps, cap_blocks)
+    for a in (particles.m, particles.x, particles.v, particles.C, particles.F, particles.plastic):
+        req += np.ascontiguousarray(a, dtype="<f4").tobytes()
+    rep = _run(req, timeout)
+    status, nb = struct.unpack_from("<2i", rep, 0)
+    secs = struct.unpack_from("<d", rep, 8)[0]
+    off = 16
+    out = []
+    for cnt, shape in ((3 * n, (n, 3)), (3 * n, (n, 3)), (9 * n, (n, 9)), (9 * n, (n, 9)), (n, (n,))):
+        out.append(np.frombuffer(rep, "<f4", cnt, off).reshape(shape).copy())
+        off += 4 * cnt
+    keys = np.zeros((0, 3), np.int32)
+    grid = np.zeros((0, 4, 512), np.float32)
+    if status == 0 and cap_blocks:
+        keys = np.frombuffer(rep, "<i4", 3 * nb, off).reshape(nb, 3).copy()
+        off += 12 * nb
+        grid = np.frombuffer(rep, "<f4", nb * 2048, off).reshape(nb, 4, 512).copy()
+    return RefResult(status, secs, *out, keys, grid)
+
+
+def activate(x: np.ndarray, dx: float, table_expected: int, cap: int = 1 << 16, timeout: float = 120.0):
+    x = np.ascontiguousarray(x, dtype="<f4")
+    req = struct.pack("<iifii", 2, len(x), dx, table_expected, cap) + x.tobytes()
+    rep = _run(req, timeout)
+    st, nb, npb, ts = struct.unpack_from("<4i", rep, 0)
+    if st != 0:
+        raise RuntimeError(f"zsref activate failed: {st}")
+    keys = np.frombuffer(rep, "<i4", 3 * nb, 16).reshape(nb, 3).copy()
+    slots = np.frombuffer(rep, "<i4", nb, 16 + 12 * nb).copy()
+    return keys, slots, npb, ts
+
+
+def stress(spec, F: np.ndarray, logJp: np.ndarray, timeout: float = 120.0):
+    """Reference compute_stress_* on a batch: returns (PF, F_projected, logJp_new)."""
+    m = spec.material
+    F = np.ascontiguousarray(F.reshape(-1, 9), dtype="<f4")
+    cnt = len(F)
+    req = struct.pack("<iii6fi", 3, cnt, m.model, spec.volume, m.E, m.nu, m.friction_deg, m.cohesion,
+                      m.beta, m.volume_correction)
+    req += F.tobytes() + np.ascontiguousarray(logJp, dtype="<f4").tobytes()
+    rep = _run(req, timeout)
+    PF = np.frombuffer(rep, "<f4", 9 * cnt, 0).reshape(cnt, 9).copy()
+    Fo = np.frombuffer(rep, "<f4", 9 * cnt, 36 * cnt).reshape(cnt, 9).copy()
+    lj = np.frombuffer(rep, "<f4", cnt, 72 * cnt).copy()
+    return PF, Fo, lj
+
+
+def svd(A: np.ndarray, timeout: float = 120.0):
+    A = np.ascontiguousarray(A.reshape(-1, 9), dtype="<f4")
+    cnt = len(A)
+    rep = _run(struct.pack("<ii", 4, cnt) + A.tobytes(), timeout)
+    U = np.frombuffer(rep, "<f4", 9 * cnt, 0).reshape(cnt, 9).copy()
+    S = np.frombuffer(rep, "<f4", 3 * cnt, 36 * cnt).reshape(cnt, 3).copy()
+    V = np.frombuffer(rep, "<f4", 9 * cnt, 48 * cnt).reshape(cnt, 9).copy()
+    return U, S, V

@@ -1,0 +1,674 @@
+// Host runtime of libzsmpm.so: the C ABI declared in include/zsmpm.h.
+//
+// A scene owns every device buffer of one MPM system (particles double-buffered in binned
+// order, the HashTable<i32,3,int>-layout block table, the sparse grid of 8^3 blocks and
+// the binning scratch).  Stages enqueue kernels on the caller's stream; zsmpm_run replays
+// a CUDA graph of two substeps (the particle buffers alternate between them).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "zsmpm.h"
+#include "zsmpm_internal.h"
+
+using namespace zsmpm;
+
+struct zsmpm_scene {
+  zsmpm_scene_desc desc{};
+  int device = 0;
+  scene_device dev{};
+  particle_buffers bufs[2];
+  int cur = 0;
+  bool uploaded = false;
+  bool binned = false;  // src[] valid for the current particle order
+  cudaStream_t last_stream = nullptr;
+  // graphs of two consecutive substeps, one per starting buffer parity
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaStream_t graph_stream = nullptr;
+  // stage timing
+  bool timing = false;
+  cudaEvent_t ev[6] = {};
+  float stage_ms[5] = {};
+  std::vector<void *> allocations;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+zsmpm_status fail(zsmpm_status st, const std::string &msg) {
+  g_error = msg;
+  return st;
+}
+
+zsmpm_status cuda_fail(cudaError_t e, const char *what) {
+  return fail(ZSMPM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define ZS_TRY(expr, what)                        \
+  do {                                            \
+    cudaError_t e__ = (expr);                     \
+    if (e__ != cudaSuccess) return cuda_fail(e__, what); \
+  } while (0)
+
+template <class T> zsmpm_status dev_alloc(zsmpm_scene *s, T **p, size_t count, const char *what) {
+  void *ptr = nullptr;
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&ptr, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  s->allocations.push_back(ptr);
+  *p = static_cast<T *>(ptr);
+  return ZSMPM_OK;
+}
+
+#define ZS_ALLOC(ptr, count, what)                             \
+  do {                                                         \
+    zsmpm_status st__ = dev_alloc(s, &(ptr), (count), (what)); \
+    if (st__ != ZSMPM_OK) return st__;                         \
+  } while (0)
+
+int64_t next_2pow(int64_t n) {
+  int64_t p = 1;
+  while (p < n) p <<= 1;
+  return p;
+}
+
+material_dev make_material(const zsmpm_material &m) {
+  material_dev d{};
+  d.model = m.model;
+  d.mode = m.model == ZSMPM_SNOW ? 0 : m.plasticity_mode;
+  d.volume_correction = m.volume_correction;
+  // ConstitutiveModel.hpp:34-38 (mu evaluated through the double literal 0.5)
+  d.mu = (float)(0.5 * (double)m.E / (double)(1.f + m.nu));
+  d.lambda = m.E * m.nu / ((1.f + m.nu) * (1.f - 2.f * m.nu));
+  d.volume = m.volume;
+  d.cohesion = m.cohesion;
+  d.beta = m.beta;
+  const float sin_phi = (float)std::sin((double)m.friction_deg / 180.0 * 3.14159265358979323846);
+  d.yield_surface = 0.816496580927726f * 2.f * sin_phi / (3.f - sin_phi);
+  d.hardening = m.hardening;
+  d.theta_c = m.theta_c;
+  d.theta_s = m.theta_s;
+  return d;
+}
+
+cudaStream_t as_stream(void *st) { return static_cast<cudaStream_t>(st); }
+
+zsmpm_status check_scene(zsmpm_scene *s, bool need_particles) {
+  if (!s) return fail(ZSMPM_ERR_INVALID_ARG, "scene is null");
+  if (need_particles && !s->uploaded) return fail(ZSMPM_ERR_NOT_READY, "no particles uploaded");
+  cudaError_t e = cudaSetDevice(s->device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  return ZSMPM_OK;
+}
+
+void bind_buffers(zsmpm_scene *s) {
+  s->dev.cur = s->bufs[s->cur];
+  s->dev.nxt = s->bufs[s->cur ^ 1];
+}
+
+zsmpm_status status_from_word(int w) {
+  if (w == 0) return ZSMPM_OK;
+  std::string msg = "device status:";
+  zsmpm_status st = ZSMPM_ERR_CAPACITY;
+  if (w & kStatusOutOfDomain) {
+    msg += " particle position NaN/Inf or outside the block-key range;";
+    st = ZSMPM_ERR_OUT_OF_DOMAIN;
+  }
+  if (w & kStatusTableFull) {
+    msg += " hash table full;";
+    st = ZSMPM_ERR_TABLE_FULL;
+  }
+  if (w & kStatusCapacity) msg += " block capacity exceeded;";
+  if (w & kStatusBitmap) msg += " active-block bounding box too large;";
+  if (w & kStatusMissingBlock) msg += " particle stencil outside its block neighbourhood;";
+  if (w & kStatusTimeout) {
+    msg += " bounded wait gave up;";
+    st = ZSMPM_ERR_TIMEOUT;
+  }
+  return fail(st, msg);
+}
+
+zsmpm_status allocate_particles(zsmpm_scene *s, int64_t cap) {
+  const bool plastic = s->desc.material.model != ZSMPM_FIXED_COROTATED;
+  for (int k = 0; k < 2; ++k) {
+    particle_buffers &b = s->bufs[k];
+    ZS_ALLOC(b.xm, cap, "alloc xm");
+    ZS_ALLOC(b.v, cap, "alloc v");
+    ZS_ALLOC(b.C, 9 * cap, "alloc C");
+    ZS_ALLOC(b.A, 9 * cap, "alloc A");
+    ZS_ALLOC(b.F, 9 * cap, "alloc F");
+    if (plastic) ZS_ALLOC(b.plastic, cap, "alloc plastic");
+    ZS_ALLOC(b.id, cap, "alloc id");
+  }
+  scene_device &d = s->dev;
+  ZS_ALLOC(d.key32, cap, "alloc key32");
+  ZS_ALLOC(d.rnk, cap, "alloc rnk");
+  ZS_ALLOC(d.tmp, cap, "alloc tmp");
+  ZS_ALLOC(d.src, cap, "alloc src");
+  return ZSMPM_OK;
+}
+
+zsmpm_status allocate_blocks(zsmpm_scene *s, int64_t n) {
+  scene_device &d = s->dev;
+  int64_t expected = s->desc.table_expected > 0 ? s->desc.table_expected : std::max<int64_t>(n / 512, 64);
+  const int64_t T = next_2pow(expected) * 16;
+  if (T > (int64_t)1 << 30) return fail(ZSMPM_ERR_CAPACITY, "hash table too large");
+  d.prm.table_size = (int)T;
+  d.prm.nb_cap = (int)std::min<int64_t>(T - 20, std::max<int64_t>(65536, n / 16));
+  d.prm.bitmap_cap = 1 << 23;  // 2^28 dense block positions
+  const int64_t nbc = d.prm.nb_cap;
+  ZS_ALLOC(d.pk, T, "alloc table pk");
+  ZS_ALLOC(d.tkeys, 3 * T, "alloc table keys");
+  ZS_ALLOC(d.tidx, T, "alloc table indices");
+  ZS_ALLOC(d.tstatus, T, "alloc table status");
+  ZS_ALLOC(d.active_keys, 3 * nbc, "alloc active keys");
+  ZS_ALLOC(d.view_cnt, 1, "alloc cnt");
+  ZS_ALLOC(d.ins_pk, nbc, "alloc ins_pk");
+  ZS_ALLOC(d.ins_slot, nbc, "alloc ins_slot");
+  ZS_ALLOC(d.blk_pk, nbc, "alloc blk_pk");
+  ZS_ALLOC(d.nbr, 8 * nbc, "alloc nbr");
+  ZS_ALLOC(d.bitmap, d.prm.bitmap_cap, "alloc bitmap");
+  ZS_ALLOC(d.word_prefix, (int64_t)d.prm.bitmap_cap + 1, "alloc word prefix");
+  ZS_ALLOC(d.ctr, kCtrCount, "alloc counters");
+  ZS_ALLOC(d.block_count, nbc, "alloc block count");
+  ZS_ALLOC(d.block_start, nbc + 1, "alloc block start");
+  ZS_ALLOC(d.cell_count, 512 * nbc, "alloc cell count");
+  ZS_ALLOC(d.cell_start, 512 * nbc, "alloc cell start");
+  ZS_ALLOC(d.scan_part, 2 * kScanCtas + 1, "alloc scan partials");
+  ZS_ALLOC(d.grid, (size_t)kGridChannels * 512 * nbc, "alloc grid");
+  ZS_TRY(cudaMemset(d.bitmap, 0, sizeof(uint32_t) * d.prm.bitmap_cap), "memset bitmap");
+  ZS_TRY(cudaMemset(d.ctr, 0, sizeof(int) * kCtrCount), "memset counters");
+  ZS_TRY(cudaMemset(d.block_count, 0, sizeof(int) * nbc), "memset block count");
+  ZS_TRY(cudaMemset(d.cell_count, 0, sizeof(int) * 512 * nbc), "memset cell count");
+  ZS_TRY(cudaMemset(d.view_cnt, 0, sizeof(int)), "memset cnt");
+  ZS_TRY(cudaMemset(d.tstatus, 0xff, sizeof(int) * T), "memset table status");
+  return ZSMPM_OK;
+}
+
+void release(zsmpm_scene *s) {
+  for (int k = 0; k < 2; ++k)
+    if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
+  for (auto &e : s->ev)
+    if (e) cudaEventDestroy(e);
+  for (void *p : s->allocations) cudaFree(p);
+  s->allocations.clear();
+}
+
+void invalidate_graphs(zsmpm_scene *s) {
+  for (int k = 0; k < 2; ++k)
+    if (s->graph[k]) {
+      cudaGraphExecDestroy(s->graph[k]);
+      s->graph[k] = nullptr;
+    }
+}
+
+zsmpm_status read_status(zsmpm_scene *s) {
+  int w = 0;
+  ZS_TRY(cudaMemcpy(&w, &s->dev.ctr[kCtrStatus], sizeof(int), cudaMemcpyDeviceToHost), "read status");
+  if (w) {
+    // report once, then clear so that the next call starts clean
+    cudaMemset(&s->dev.ctr[kCtrStatus], 0, sizeof(int));
+  }
+  return status_from_word(w);
+}
+
+zsmpm_status substep_enqueue(zsmpm_scene *s, cudaStream_t st) {
+  bind_buffers(s);
+  if (s->timing) cudaEventRecord(s->ev[0], st);
+  ZS_TRY(launch_activate(s->dev, st), "activate");
+  if (s->timing) cudaEventRecord(s->ev[1], st);
+  ZS_TRY(launch_bin(s->dev, st), "bin");
+  if (s->timing) cudaEventRecord(s->ev[2], st);
+  ZS_TRY(launch_p2g(s->dev, st), "p2g");
+  if (s->timing) cudaEventRecord(s->ev[3], st);
+  ZS_TRY(launch_grid_update(s->dev, st), "grid update");
+  if (s->timing) cudaEventRecord(s->ev[4], st);
+  ZS_TRY(launch_g2p(s->dev, st), "g2p");
+  if (s->timing) cudaEventRecord(s->ev[5], st);
+  s->cur ^= 1;
+  bind_buffers(s);
+  return ZSMPM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ZSMPM_API const char *zsmpm_last_error_string(void) { return g_error.c_str(); }
+ZSMPM_API const char *zsmpm_version(void) { return "zsmpm-b200 0.1 (sm_100a)"; }
+
+ZSMPM_API int zsmpm_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_create(const zsmpm_scene_desc *desc, zsmpm_scene **out) {
+  if (!desc || !out) return fail(ZSMPM_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (!(desc->dx > 0.f) || !(desc->dt > 0.f)) return fail(ZSMPM_ERR_INVALID_ARG, "dx and dt must be > 0");
+  if (desc->material.model < 0 || desc->material.model > 2)
+    return fail(ZSMPM_ERR_INVALID_ARG, "unknown material model");
+  if (desc->wall_type < 0 || desc->wall_type > 3) return fail(ZSMPM_ERR_INVALID_ARG, "unknown wall type");
+  if (desc->block_order != ZSMPM_BLOCK_ORDER_SORTED)
+    return fail(ZSMPM_ERR_INVALID_ARG, "only ZSMPM_BLOCK_ORDER_SORTED is implemented by the device path");
+  if (zsmpm_device_count() <= 0) return fail(ZSMPM_ERR_NO_DEVICE, "no CUDA device visible");
+  auto *s = new zsmpm_scene();
+  s->desc = *desc;
+  s->device = desc->device;
+  cudaError_t e = cudaSetDevice(s->device);
+  if (e != cudaSuccess) {
+    delete s;
+    return cuda_fail(e, "cudaSetDevice");
+  }
+  scene_params &p = s->dev.prm;
+  p.dx = desc->dx;
+  p.inv_dx = 1.f / desc->dx;
+  p.dt = desc->dt;
+  p.kappa = desc->dt * (4.f * p.inv_dx * p.inv_dx);  // dt * D_inv (P2G.hpp:52, :104)
+  p.four_over_dx = 4.f * p.inv_dx;
+  for (int d = 0; d < 3; ++d) p.gravity[d] = desc->gravity[d];
+  p.wall_type = desc->wall_type;
+  p.wall_cells = desc->wall_cells;
+  p.mat = make_material(desc->material);
+  for (auto &ev : s->ev) cudaEventCreate(&ev);
+  *out = s;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_destroy(zsmpm_scene *s) {
+  if (!s) return ZSMPM_OK;
+  cudaSetDevice(s->device);
+  cudaDeviceSynchronize();
+  release(s);
+  delete s;
+  return ZSMPM_OK;
+}
+
+static zsmpm_status prepare_upload(zsmpm_scene *s, int64_t n) {
+  if (n <= 0 || n > (int64_t)0x7fffffff) return fail(ZSMPM_ERR_INVALID_ARG, "particle count out of range");
+  if (!s->uploaded) {
+    int64_t cap = s->desc.max_particles > 0 ? s->desc.max_particles : n;
+    if (cap < n) return fail(ZSMPM_ERR_CAPACITY, "more particles than max_particles");
+    zsmpm_status st = allocate_particles(s, cap);
+    if (st != ZSMPM_OK) return st;
+    st = allocate_blocks(s, cap);
+    if (st != ZSMPM_OK) return st;
+    s->dev.prm.cap = (int)cap;
+  } else if (n > s->dev.prm.cap) {
+    return fail(ZSMPM_ERR_CAPACITY, "more particles than the scene's capacity");
+  }
+  s->dev.prm.n = (int)n;
+  s->cur = 0;
+  bind_buffers(s);
+  invalidate_graphs(s);
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_upload(zsmpm_scene *s, const zsmpm_particle_arrays *p, int64_t n,
+                                          int32_t on_device, void *stream) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (!p || !p->m || !p->x) return fail(ZSMPM_ERR_INVALID_ARG, "m and x are required");
+  st = prepare_upload(s, n);
+  if (st != ZSMPM_OK) return st;
+  cudaStream_t cs = as_stream(stream);
+  const float *dm = p->m, *dx = p->x, *dv = p->v, *dC = p->C, *dF = p->F, *dpl = p->plastic;
+  std::vector<void *> staging;
+  if (!on_device) {
+    auto stage = [&](const float *h, size_t count, const float **d) -> cudaError_t {
+      if (!h) {
+        *d = nullptr;
+        return cudaSuccess;
+      }
+      void *ptr = nullptr;
+      cudaError_t e = cudaMalloc(&ptr, count * sizeof(float));
+      if (e != cudaSuccess) return e;
+      staging.push_back(ptr);
+      e = cudaMemcpyAsync(ptr, h, count * sizeof(float), cudaMemcpyHostToDevice, cs);
+      *d = static_cast<const float *>(ptr);
+      return e;
+    };
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = stage(p->m, n, &dm);
+    if (e == cudaSuccess) e = stage(p->x, 3 * n, &dx);
+    if (e == cudaSuccess) e = stage(p->v, 3 * n, &dv);
+    if (e == cudaSuccess) e = stage(p->C, 9 * n, &dC);
+    if (e == cudaSuccess) e = stage(p->F, 9 * n, &dF);
+    if (e == cudaSuccess) e = stage(p->plastic, n, &dpl);
+    if (e != cudaSuccess) {
+      cudaStreamSynchronize(cs);
+      for (void *q : staging) cudaFree(q);
+      return cuda_fail(e, "upload staging");
+    }
+  }
+  cudaError_t e = launch_import(s->dev, dm, dx, dv, dC, dF, dpl, (int)n, cs);
+  if (e == cudaSuccess) e = launch_prime(s->dev, cs);
+  if (!staging.empty()) {
+    cudaError_t e2 = cudaStreamSynchronize(cs);
+    for (void *q : staging) cudaFree(q);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "upload");
+  s->uploaded = true;
+  s->binned = false;
+  s->last_stream = cs;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_upload_tilevector(zsmpm_scene *s, const zsmpm_tilevector_view *tv,
+                                                     int64_t n, void *stream) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (!tv || !tv->base || tv->lane_width != 32 || tv->off_m < 0 || tv->off_x < 0)
+    return fail(ZSMPM_ERR_INVALID_ARG, "tile vector view needs base, lane_width 32, m and x");
+  st = prepare_upload(s, n);
+  if (st != ZSMPM_OK) return st;
+  cudaStream_t cs = as_stream(stream);
+  cudaError_t e = launch_import_tilevector(s->dev, tv->base, tv->num_channels, tv->off_m, tv->off_x,
+                                           tv->off_v, tv->off_C, tv->off_F, tv->off_plastic, (int)n, cs);
+  if (e == cudaSuccess) e = launch_prime(s->dev, cs);
+  if (e != cudaSuccess) return cuda_fail(e, "upload tilevector");
+  s->uploaded = true;
+  s->binned = false;
+  s->last_stream = cs;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_download(zsmpm_scene *s, zsmpm_particle_arrays *p, int32_t on_device,
+                                            void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!p) return fail(ZSMPM_ERR_INVALID_ARG, "null particle arrays");
+  cudaStream_t cs = as_stream(stream);
+  bind_buffers(s);
+  const int64_t n = s->dev.prm.n;
+  if (on_device) {
+    ZS_TRY(launch_export(s->dev, p->m, p->x, p->v, p->C, p->F, p->plastic, cs), "download");
+    return ZSMPM_OK;
+  }
+  float *dbuf = nullptr;
+  ZS_TRY(cudaMalloc(&dbuf, sizeof(float) * 26 * n), "download staging");
+  float *dm = dbuf, *dx = dm + n, *dv = dx + 3 * n, *dC = dv + 3 * n, *dF = dC + 9 * n, *dpl = dF + 9 * n;
+  cudaError_t e = launch_export(s->dev, p->m ? dm : nullptr, p->x ? dx : nullptr, p->v ? dv : nullptr,
+                                p->C ? dC : nullptr, p->F ? dF : nullptr, p->plastic ? dpl : nullptr, cs);
+  auto get = [&](float *h, const float *d, size_t count) {
+    if (h && e == cudaSuccess) e = cudaMemcpyAsync(h, d, count * sizeof(float), cudaMemcpyDeviceToHost, cs);
+  };
+  get(p->m, dm, n);
+  get(p->x, dx, 3 * n);
+  get(p->v, dv, 3 * n);
+  get(p->C, dC, 9 * n);
+  get(p->F, dF, 9 * n);
+  get(p->plastic, dpl, n);
+  cudaError_t e2 = cudaStreamSynchronize(cs);
+  cudaFree(dbuf);
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess) return cuda_fail(e, "download");
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_download_tilevector(zsmpm_scene *s, const zsmpm_tilevector_view *tv,
+                                                       void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!tv || !tv->base || tv->lane_width != 32) return fail(ZSMPM_ERR_INVALID_ARG, "bad tile vector view");
+  bind_buffers(s);
+  ZS_TRY(launch_export_tilevector(s->dev, tv->base, tv->num_channels, tv->off_m, tv->off_x, tv->off_v,
+                                  tv->off_C, tv->off_F, tv->off_plastic, as_stream(stream)),
+         "download tilevector");
+  return ZSMPM_OK;
+}
+
+ZSMPM_API int64_t zsmpm_scene_num_particles(const zsmpm_scene *s) { return s ? s->dev.prm.n : 0; }
+
+ZSMPM_API zsmpm_status zsmpm_scene_status(zsmpm_scene *s) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (!s->uploaded) return ZSMPM_OK;
+  ZS_TRY(cudaStreamSynchronize(s->last_stream), "synchronize");
+  return read_status(s);
+}
+
+ZSMPM_API zsmpm_status zsmpm_activate_blocks(zsmpm_scene *s, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  bind_buffers(s);
+  ZS_TRY(launch_activate(s->dev, as_stream(stream)), "activate");
+  s->binned = false;
+  s->last_stream = as_stream(stream);
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_bin_particles(zsmpm_scene *s, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  bind_buffers(s);
+  ZS_TRY(launch_bin(s->dev, as_stream(stream)), "bin");
+  s->binned = true;
+  s->last_stream = as_stream(stream);
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_p2g(zsmpm_scene *s, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!s->binned) return fail(ZSMPM_ERR_NOT_READY, "p2g needs zsmpm_activate_blocks and zsmpm_bin_particles first");
+  bind_buffers(s);
+  ZS_TRY(launch_p2g(s->dev, as_stream(stream)), "p2g");
+  s->last_stream = as_stream(stream);
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_grid_update(zsmpm_scene *s, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!s->binned) return fail(ZSMPM_ERR_NOT_READY, "grid update needs an activated grid");
+  bind_buffers(s);
+  ZS_TRY(launch_grid_update(s->dev, as_stream(stream)), "grid update");
+  s->last_stream = as_stream(stream);
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_g2p(zsmpm_scene *s, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!s->binned) return fail(ZSMPM_ERR_NOT_READY, "g2p needs a binned, updated grid");
+  bind_buffers(s);
+  ZS_TRY(launch_g2p(s->dev, as_stream(stream)), "g2p");
+  s->cur ^= 1;
+  bind_buffers(s);
+  s->binned = false;
+  s->last_stream = as_stream(stream);
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_substep(zsmpm_scene *s, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  st = substep_enqueue(s, as_stream(stream));
+  if (st != ZSMPM_OK) return st;
+  s->binned = false;
+  s->last_stream = as_stream(stream);
+  if (s->timing) {
+    ZS_TRY(cudaEventSynchronize(s->ev[5]), "stage timing");
+    for (int k = 0; k < 5; ++k) cudaEventElapsedTime(&s->stage_ms[k], s->ev[k], s->ev[k + 1]);
+  }
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_run(zsmpm_scene *s, int32_t nsteps, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (nsteps < 0) return fail(ZSMPM_ERR_INVALID_ARG, "nsteps < 0");
+  cudaStream_t cs = as_stream(stream);
+  const bool timing = s->timing;
+  s->timing = false;
+  // capture the pair of substeps starting from the current parity once, on a private
+  // stream (capture is not allowed on the legacy default stream)
+  const int parity = s->cur;
+  if (nsteps >= 2 && !s->graph[parity]) {
+    if (!s->graph_stream) ZS_TRY(cudaStreamCreateWithFlags(&s->graph_stream, cudaStreamNonBlocking), "graph stream");
+    ZS_TRY(cudaStreamBeginCapture(s->graph_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    zsmpm_status a = substep_enqueue(s, s->graph_stream);
+    zsmpm_status b = a == ZSMPM_OK ? substep_enqueue(s, s->graph_stream) : a;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->graph_stream, &g);
+    s->cur = parity;  // capture enqueued nothing; restore the parity it advanced
+    bind_buffers(s);
+    if (a != ZSMPM_OK || b != ZSMPM_OK) {
+      if (g) cudaGraphDestroy(g);
+      s->timing = timing;
+      return a != ZSMPM_OK ? a : b;
+    }
+    if (e != cudaSuccess) {
+      s->timing = timing;
+      return cuda_fail(e, "end capture");
+    }
+    e = cudaGraphInstantiate(&s->graph[parity], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      s->timing = timing;
+      return cuda_fail(e, "graph instantiate");
+    }
+  }
+  int done = 0;
+  for (; done + 2 <= nsteps; done += 2) {
+    cudaError_t e = cudaGraphLaunch(s->graph[parity], cs);
+    if (e != cudaSuccess) {
+      s->timing = timing;
+      return cuda_fail(e, "graph launch");
+    }
+  }
+  // the pair leaves the parity unchanged
+  if (done < nsteps) {
+    st = substep_enqueue(s, cs);
+    if (st != ZSMPM_OK) {
+      s->timing = timing;
+      return st;
+    }
+  }
+  s->timing = timing;
+  s->binned = false;
+  s->last_stream = cs;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_get_table_view(zsmpm_scene *s, zsmpm_table_view *out) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!out) return fail(ZSMPM_ERR_INVALID_ARG, "null view");
+  out->keys = s->dev.tkeys;
+  out->indices = s->dev.tidx;
+  out->status = s->dev.tstatus;
+  out->active_keys = s->dev.active_keys;
+  out->cnt = s->dev.view_cnt;
+  out->table_size = s->dev.prm.table_size;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_num_blocks(zsmpm_scene *s, int32_t *out) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!out) return fail(ZSMPM_ERR_INVALID_ARG, "null output");
+  ZS_TRY(cudaStreamSynchronize(s->last_stream), "synchronize");
+  ZS_TRY(cudaMemcpy(out, s->dev.view_cnt, sizeof(int), cudaMemcpyDeviceToHost), "read block count");
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_get_grid_view(zsmpm_scene *s, zsmpm_grid_view *out) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!out) return fail(ZSMPM_ERR_INVALID_ARG, "null view");
+  int nb = 0;
+  st = zsmpm_num_blocks(s, &nb);
+  if (st != ZSMPM_OK) return st;
+  out->base = s->dev.grid;
+  out->num_channels = kGridChannels;
+  out->num_blocks = nb;
+  out->keys = s->dev.active_keys;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_download_grid(zsmpm_scene *s, int32_t *keys, float *grid, int32_t cap_blocks,
+                                           int32_t *out_nblocks) {
+  int nb = 0;
+  zsmpm_status st = zsmpm_num_blocks(s, &nb);
+  if (st != ZSMPM_OK) return st;
+  if (out_nblocks) *out_nblocks = nb;
+  if (nb > cap_blocks) return fail(ZSMPM_ERR_CAPACITY, "grid output capacity too small");
+  if (keys) ZS_TRY(cudaMemcpy(keys, s->dev.active_keys, sizeof(int) * 3 * nb, cudaMemcpyDeviceToHost), "copy keys");
+  if (grid)
+    ZS_TRY(cudaMemcpy(grid, s->dev.grid, sizeof(float) * kGridChannels * 512 * (size_t)nb, cudaMemcpyDeviceToHost),
+           "copy grid");
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_download_binning(zsmpm_scene *s, int32_t *order, int32_t *block_start,
+                                              int32_t cap_blocks) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!s->binned) return fail(ZSMPM_ERR_NOT_READY, "call zsmpm_bin_particles first");
+  int nb = 0;
+  st = zsmpm_num_blocks(s, &nb);
+  if (st != ZSMPM_OK) return st;
+  if (nb > cap_blocks) return fail(ZSMPM_ERR_CAPACITY, "block_start capacity too small");
+  const int n = s->dev.prm.n;
+  bind_buffers(s);
+  if (order) {
+    int *d = nullptr;
+    ZS_TRY(cudaMalloc(&d, sizeof(int) * n), "binning staging");
+    cudaError_t e = launch_export_order(s->dev, d, s->last_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->last_stream);
+    if (e == cudaSuccess) e = cudaMemcpy(order, d, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "download binning");
+  }
+  if (block_start)
+    ZS_TRY(cudaMemcpy(block_start, s->dev.block_start, sizeof(int) * (nb + 1), cudaMemcpyDeviceToHost),
+           "copy block start");
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_set_stage_timing(zsmpm_scene *s, int32_t enabled) {
+  if (!s) return fail(ZSMPM_ERR_INVALID_ARG, "scene is null");
+  s->timing = enabled != 0;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_stage_times(zsmpm_scene *s, float *ms, int32_t count) {
+  if (!s || !ms) return fail(ZSMPM_ERR_INVALID_ARG, "null argument");
+  for (int k = 0; k < count && k < 5; ++k) ms[k] = s->stage_ms[k];
+  return ZSMPM_OK;
+}
+
+ZSMPM_API int32_t zsmpm_kernels_per_substep(const zsmpm_scene *) { return kernels_per_substep(); }
+
+ZSMPM_API zsmpm_status zsmpm_svd3(const float *A, float *U, float *S, float *V, int64_t count, void *stream) {
+  if (count < 0 || (count > 0 && (!A || !U || !S || !V))) return fail(ZSMPM_ERR_INVALID_ARG, "bad svd arguments");
+  if (count == 0) return ZSMPM_OK;
+  ZS_TRY(launch_svd_batch(A, U, S, V, count, as_stream(stream)), "svd");
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_constitutive(const zsmpm_material *mat, float *F, float *plastic, float *tau,
+                                          int64_t count, void *stream) {
+  if (!mat || count < 0 || (count > 0 && (!F || !tau))) return fail(ZSMPM_ERR_INVALID_ARG, "bad arguments");
+  if (mat->model != ZSMPM_FIXED_COROTATED && count > 0 && !plastic)
+    return fail(ZSMPM_ERR_INVALID_ARG, "plastic state required for this model");
+  if (count == 0) return ZSMPM_OK;
+  ZS_TRY(launch_constitutive_batch(make_material(*mat), F, plastic, tau, count, as_stream(stream)),
+         "constitutive");
+  return ZSMPM_OK;
+}
+
+}  // extern "C"

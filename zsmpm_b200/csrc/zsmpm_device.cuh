@@ -1,0 +1,368 @@
+// Device-side math of the MPM substep: packed block keys, the reference's hash, the 3x3
+// SVD, the constitutive updates and warp/CTA helpers.  Everything here is __device__ code
+// for sm_100a; host code sees only the constants.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace zsmpm {
+
+// ---------------------------------------------------------------- constants / layout
+constexpr int kSide = 8;                 // block side (cells)
+constexpr int kBlockCells = 512;         // 8^3
+constexpr int kGridChannels = 4;         // m, p.x/v.x, p.y/v.y, p.z/v.z
+constexpr int kHalo = 12;                // halo side, cells [8b, 8b+12) per axis
+constexpr int kHaloCells = kHalo * kHalo * kHalo;
+constexpr uint64_t kEmptyKey = ~0ull;
+constexpr int kKeyBias = 1 << 20;        // packed block coordinate bias (21 bits each)
+constexpr int kKeyLimit = (1 << 20) - 4; // |block coordinate| must stay below this
+
+// device status word bits (OR-ed), surfaced as zsmpm_status by the host
+enum : int {
+  kStatusTableFull = 1 << 0,
+  kStatusCapacity = 1 << 1,
+  kStatusOutOfDomain = 1 << 2,
+  kStatusMissingBlock = 1 << 3,
+  kStatusTimeout = 1 << 4,
+  kStatusBitmap = 1 << 5,
+};
+
+// Block keys travel packed into 63 bits: (bx+2^20)<<42 | (by+2^20)<<21 | (bz+2^20).
+// Packed order equals lexicographic (bx, by, bz) order.
+__host__ __device__ __forceinline__ uint64_t pack_key(int bx, int by, int bz) {
+  return ((uint64_t)(uint32_t)(bx + kKeyBias) << 42) | ((uint64_t)(uint32_t)(by + kKeyBias) << 21) |
+         (uint64_t)(uint32_t)(bz + kKeyBias);
+}
+__host__ __device__ __forceinline__ int3 unpack_key(uint64_t k) {
+  return make_int3((int)((k >> 42) & 0x1fffff) - kKeyBias, (int)((k >> 21) & 0x1fffff) - kKeyBias,
+                   (int)(k & 0x1fffff) - kKeyBias);
+}
+
+// The reference's HashTable home slot (container/HashTable.hpp:493-500 with
+// math/Hash.hpp:17-27): 64-bit hash_combine over the three coordinates, truncated to i32,
+// then (h % T + T) % T.
+__host__ __device__ __forceinline__ int home_slot(int bx, int by, int bz, int table_size) {
+  uint64_t seed = (uint64_t)(int64_t)bx;
+  seed ^= ((uint64_t)(int64_t)by + 0x9e3779b97f4a7c15ull + (seed << 12) + (seed >> 4));
+  seed ^= ((uint64_t)(int64_t)bz + 0x9e3779b97f4a7c15ull + (seed << 12) + (seed >> 4));
+  const int h = (int)(uint32_t)seed;
+  return (h % table_size + table_size) % table_size;
+}
+
+// floor division by the block side for the stencil-origin cell, written as the reference
+// does in ComputeSparsity (SparsityOp.hpp:75-77)
+__host__ __device__ __forceinline__ int block_of_cell(int c) { return (c + (c < 0 ? -7 : 0)) / 8; }
+
+// ---------------------------------------------------------------- small matrix helpers
+struct mat3 {
+  float m[9];  // column-major, m[3*c + r]
+};
+
+// ---------------------------------------------------------------- 3x3 SVD
+// McAdams et al. 2011 ("Computing the singular value decomposition of 3x3 matrices with
+// minimal branching and elementary floating point operations"), the algorithm of the
+// reference's math::svd_3d (math/matrix/SVD.hpp:15-1025): four sweeps of approximate
+// Givens Jacobi conjugations of A^T A accumulated as a quaternion, column sort with sign
+// fix, Givens QR.  Same steps and constants; the reciprocal square roots use the SFU
+// (rsqrtf), as the reference's CUDA build does with __frsqrt_rn.
+namespace svd_detail {
+constexpr float kTiny = 1.e-20f;
+constexpr float kSmall = 1.e-12f;
+constexpr float kFourGammaSq = 5.8284273147583007813f;
+__device__ __forceinline__ float sin_pi8() { return __int_as_float(1053028117); }
+__device__ __forceinline__ float cos_pi8() { return __int_as_float(1064076127); }
+
+__device__ __forceinline__ void conjugate(float &pp, float &qq, float &rr, float &pq, float &rp,
+                                          float &rq, float &qs, float &qk, float &qi,
+                                          float &qj) {
+  float sh = pq * 0.5f;
+  float t5 = pp - qq;
+  const bool big = sh * sh >= kTiny;
+  sh = big ? sh : 0.f;
+  float ch = big ? t5 : 1.f;
+  float sh2 = sh * sh, ch2 = ch * ch;
+  const float r = rsqrtf(sh2 + ch2);
+  sh *= r;
+  ch *= r;
+  if (ch2 <= kFourGammaSq * sh2) {
+    sh = sin_pi8();
+    ch = cos_pi8();
+  }
+  sh2 = sh * sh;
+  ch2 = ch * ch;
+  const float c = ch2 - sh2;
+  const float s = 2.f * ch * sh;
+  const float scale = sh2 + ch2;
+  rr = rr * scale * scale;
+  rp *= scale;
+  rq *= scale;
+  const float rp0 = rp, rq0 = rq;
+  rp = c * rp0 + s * rq0;
+  rq = c * rq0 - s * rp0;
+  const float s2 = s * s, c2 = c * c;
+  const float pp0 = pp, qq0 = qq, pq0 = pq;
+  const float cs = c * s;
+  const float two_pq_cs = 2.f * pq0 * cs;
+  pp = pp0 * c2 + qq0 * s2 + two_pq_cs;
+  qq = qq0 * c2 + pp0 * s2 - two_pq_cs;
+  pq = pq0 * (c2 - s2) - t5 * cs;
+  const float a = sh * qi, b = sh * qj, k = sh * qk, w = sh * qs;
+  qs = ch * qs - k;
+  qk = ch * qk + w;
+  qi = ch * qi + b;
+  qj = ch * qj - a;
+}
+
+__device__ __forceinline__ float refined_rsqrt(float x) {
+  const float y = rsqrtf(x);
+  return y + 0.5f * y - x * (0.5f * y * y * y);
+}
+
+__device__ __forceinline__ void givens_qr(float a[3][3], float u[3][3], int p, int q, int col) {
+  const float apc = a[p][col], aqc = a[q][col];
+  float sh = (aqc * aqc >= kSmall) ? aqc : 0.f;
+  float ch = fmaxf(fmaxf(-apc, apc), kSmall);
+  const bool pos = apc >= 0.f;
+  {
+    const float n2 = ch * ch + sh * sh;
+    ch = ch + refined_rsqrt(n2) * n2;
+  }
+  if (!pos) {
+    const float t = ch;
+    ch = sh;
+    sh = t;
+  }
+  {
+    const float r = refined_rsqrt(ch * ch + sh * sh);
+    ch *= r;
+    sh *= r;
+  }
+  const float c = ch * ch - sh * sh;
+  const float s = 2.f * sh * ch;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float x1 = a[p][k], x2 = a[q][k];
+    a[p][k] = c * x1 + s * x2;
+    a[q][k] = c * x2 - s * x1;
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const float x1 = u[r][p], x2 = u[r][q];
+    u[r][p] = c * x1 + s * x2;
+    u[r][q] = c * x2 - s * x1;
+  }
+}
+
+__device__ __forceinline__ void swap_cols(float a[3][3], float v[3][3], float rho[3], int i, int j,
+                                          int neg) {
+  if (rho[i] < rho[j]) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      float t = a[r][i];
+      a[r][i] = a[r][j];
+      a[r][j] = t;
+      t = v[r][i];
+      v[r][i] = v[r][j];
+      v[r][j] = t;
+    }
+    const float t = rho[i];
+    rho[i] = rho[j];
+    rho[j] = t;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      a[r][neg] = -a[r][neg];
+      v[r][neg] = -v[r][neg];
+    }
+  }
+}
+}  // namespace svd_detail
+
+// A (column-major) = U diag(S) V^T; U, V rotations; S sorted by magnitude, S[2] may be < 0.
+__device__ __forceinline__ void svd3(const float *A, float *U, float *S, float *V) {
+  using namespace svd_detail;
+  float a[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a[r][c] = A[3 * c + r];
+  float s11 = a[0][0] * a[0][0] + a[1][0] * a[1][0] + a[2][0] * a[2][0];
+  float s21 = a[0][1] * a[0][0] + a[1][1] * a[1][0] + a[2][1] * a[2][0];
+  float s31 = a[0][2] * a[0][0] + a[1][2] * a[1][0] + a[2][2] * a[2][0];
+  float s22 = a[0][1] * a[0][1] + a[1][1] * a[1][1] + a[2][1] * a[2][1];
+  float s32 = a[0][2] * a[0][1] + a[1][2] * a[1][1] + a[2][2] * a[2][1];
+  float s33 = a[0][2] * a[0][2] + a[1][2] * a[1][2] + a[2][2] * a[2][2];
+  float qs = 1.f, qx = 0.f, qy = 0.f, qz = 0.f;
+#pragma unroll
+  for (int sweep = 0; sweep < 4; ++sweep) {
+    conjugate(s11, s22, s33, s21, s31, s32, qs, qz, qx, qy);
+    conjugate(s22, s33, s11, s32, s21, s31, qs, qx, qy, qz);
+    conjugate(s33, s11, s22, s31, s32, s21, qs, qy, qz, qx);
+  }
+  {
+    const float r = refined_rsqrt(qs * qs + qx * qx + qy * qy + qz * qz);
+    qs *= r;
+    qx *= r;
+    qy *= r;
+    qz *= r;
+  }
+  float v[3][3];
+  {
+    const float xx = qx * qx, yy = qy * qy, zz = qz * qz, ww = qs * qs;
+    v[0][0] = ww + xx - yy - zz;
+    v[1][1] = ww - xx + yy - zz;
+    v[2][2] = ww - xx - yy + zz;
+    const float x2 = qx + qx, y2 = qy + qy, z2 = qz + qz;
+    const float wx = qs * x2, wy = qs * y2, wz = qs * z2;
+    const float xy = qy * x2, yz = qz * y2, zx = qx * z2;
+    v[0][1] = xy - wz;
+    v[1][2] = yz - wx;
+    v[2][0] = zx - wy;
+    v[1][0] = xy + wz;
+    v[2][1] = yz + wx;
+    v[0][2] = zx + wy;
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const float a0 = a[r][0], a1 = a[r][1], a2 = a[r][2];
+    a[r][0] = v[0][0] * a0 + v[1][0] * a1 + v[2][0] * a2;
+    a[r][1] = v[0][1] * a0 + v[1][1] * a1 + v[2][1] * a2;
+    a[r][2] = v[0][2] * a0 + v[1][2] * a1 + v[2][2] * a2;
+  }
+  float rho[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) rho[c] = a[0][c] * a[0][c] + a[1][c] * a[1][c] + a[2][c] * a[2][c];
+  swap_cols(a, v, rho, 0, 1, 1);
+  swap_cols(a, v, rho, 0, 2, 0);
+  swap_cols(a, v, rho, 1, 2, 2);
+  float u[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
+  givens_qr(a, u, 0, 1, 0);
+  givens_qr(a, u, 0, 2, 0);
+  givens_qr(a, u, 1, 2, 1);
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      U[3 * c + r] = u[r][c];
+      V[3 * c + r] = v[r][c];
+    }
+  S[0] = a[0][0];
+  S[1] = a[1][1];
+  S[2] = a[2][2];
+}
+
+// ---------------------------------------------------------------- constitutive models
+struct material_dev {
+  int model;            // 0 FC, 1 DP, 2 snow
+  int mode;             // 0 committed, 1 reference ordering
+  int volume_correction;
+  float mu, lambda, volume;
+  float cohesion, beta, yield_surface;
+  float hardening, theta_c, theta_s;
+};
+
+// out[3c+r] = sum_k M[3k+r] d[k] N[3k+c]
+__device__ __forceinline__ void mul_diag_t(float *out, const float *M, const float *d,
+                                           const float *N) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      out[3 * c + r] = M[r] * d[0] * N[c] + M[3 + r] * d[1] * N[3 + c] + M[6 + r] * d[2] * N[6 + c];
+}
+
+// Kirchhoff stress tau = V0 P F^T for an isotropic model with F = U diag(S) V^T and
+// principal first Piola stress Ph: P F^T = U diag(Ph * S) U^T.
+__device__ __forceinline__ void kirchhoff(float *tau, const float *U, const float *Ph,
+                                          const float *S, float volume) {
+  const float d[3] = {Ph[0] * S[0] * volume, Ph[1] * S[1] * volume, Ph[2] * S[2] * volume};
+  mul_diag_t(tau, U, d, U);
+}
+
+// Fixed corotated principal stress (ConstitutiveModel_Vol_dP.hpp:17-23)
+__device__ __forceinline__ void fc_principal(float mu, float lambda, const float *S, float *Ph) {
+  const float J = S[0] * S[1] * S[2];
+  const float smu = 2.f * mu, sl = lambda * (J - 1.f);
+  Ph[0] = smu * (S[0] - 1.f) + sl * (S[1] * S[2]);
+  Ph[1] = smu * (S[1] - 1.f) + sl * (S[0] * S[2]);
+  Ph[2] = smu * (S[2] - 1.f) + sl * (S[0] * S[1]);
+}
+
+// Return map + stress.  F: trial deformation in, F after the model's projection out
+// (the projected F is what the reference's stress functions leave in their F argument);
+// plastic: logJp (DP) or Jp (snow); tau out.  Reference ordering keeps F unchanged.
+__device__ __forceinline__ void constitutive(const material_dev &mat, float *F, float &plastic,
+                                             float *tau) {
+  float U[9], S[3], V[9];
+  svd3(F, U, S, V);
+  if (mat.model == 0) {
+    float Ph[3];
+    fc_principal(mat.mu, mat.lambda, S, Ph);
+    kirchhoff(tau, U, Ph, S, mat.volume);
+    return;
+  }
+  float Ns[3], logNs[3];
+  if (mat.model == 1) {
+    // compute_stress_sand (ConstitutiveModel_Vol_dP.hpp:241-325)
+    float eps[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) eps[i] = logf(fmaxf(fabsf(S[i]), 1e-4f)) - mat.cohesion;
+    const float sum_eps = eps[0] + eps[1] + eps[2];
+    const float tr = sum_eps + plastic;
+    float eh[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) eh[i] = eps[i] - tr / 3.f;
+    const float ehn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2]);
+    const float smu = 2.f * mat.mu;
+    if (tr >= 0.f) {
+      const float e = expf(mat.cohesion);
+      Ns[0] = Ns[1] = Ns[2] = e;
+      if (mat.volume_correction) plastic = mat.beta * sum_eps + plastic;
+    } else if (mat.mu != 0.f) {
+      plastic = 0.f;
+      const float dg = ehn + (3.f * mat.lambda + smu) / smu * tr * mat.yield_surface;
+      const float f = dg <= 0.f ? 0.f : dg / ehn;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) Ns[i] = expf(eps[i] - f * eh[i] + mat.cohesion);
+    } else {
+      Ns[0] = Ns[1] = Ns[2] = 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) logNs[i] = logf(Ns[i]);
+    const float trl = logNs[0] + logNs[1] + logNs[2];
+    // P F_new^T = U diag(Ph * Ns) U^T with Ph = (2 mu log Ns + lambda tr log Ns) / Ns
+    float PhNs[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) PhNs[i] = (smu * logNs[i] + mat.lambda * trl) * mat.volume;
+    mul_diag_t(tau, U, PhNs, U);
+  } else {
+    // snow: SnowPlasticity::do_project_sigma (SnowPlasticity.hpp:24-32) committed to F,
+    // Jp accumulated, then fixed corotated with hardened Lame parameters
+    const float J = S[0] * S[1] * S[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      Ns[i] = fmaxf(fminf(S[i], 1.f + mat.theta_s), 1.f - mat.theta_c);
+    const float Jc = Ns[0] * Ns[1] * Ns[2];
+    plastic = plastic * (J / fmaxf(Jc, 1e-6f));
+    const float e = expf(mat.hardening * (1.f - plastic));
+    float Ph[3];
+    fc_principal(mat.mu * e, mat.lambda * e, Ns, Ph);
+    kirchhoff(tau, U, Ph, Ns, mat.volume);
+  }
+  if (mat.mode == 0) mul_diag_t(F, U, Ns, V);
+}
+
+// ---------------------------------------------------------------- warp helpers
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// vectorised global reduction of four consecutive floats (16-byte aligned address)
+__device__ __forceinline__ void red_add_v4(float *addr, float a, float b, float c, float d) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b),
+               "f"(c), "f"(d)
+               : "memory");
+}
+
+}  // namespace zsmpm

@@ -1,0 +1,109 @@
+// Internal host/device interface between the C ABI layer (zsmpm_api.cu) and the kernels
+// (zsmpm_kernels.cu).  Not part of the public ABI.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "zsmpm_device.cuh"
+
+namespace zsmpm {
+
+// One particle buffer set.  Vectors are float4 (x,y,z,m) / (vx,vy,vz,0); 3x3 matrices are
+// stored component-major (component k of particle i at M[k*cap + i]) so that a warp's
+// loads of one component are contiguous.
+struct particle_buffers {
+  float4 *xm = nullptr;
+  float4 *v = nullptr;
+  float *C = nullptr;
+  float *A = nullptr;  // affine momentum m C - (4 dt / dx^2) tau, consumed by P2G
+  float *F = nullptr;
+  float *plastic = nullptr;  // logJp (DP) or Jp (snow); null for fixed corotated
+  int *id = nullptr;         // upload index
+};
+
+// Device counters (int32), zeroed at the start of every substep except the status word.
+enum counter_slot : int {
+  kCtrParticleBlocks = 0,  // blocks inserted from particles (insertion indices [0, npb))
+  kCtrEnlarged = 1,        // blocks inserted by the enlargement
+  kCtrBlocks = 2,          // total active blocks of this substep
+  kCtrStatus = 3,          // sticky status bits (kStatus*)
+  kCtrBoxLo = 4,           // 3 ints: bounding box of particle blocks
+  kCtrBoxHi = 7,           // 3 ints
+  kCtrWords = 10,          // bitmap words in use
+  kCtrWork = 11,           // 8 work counters for persistent kernels
+  kCtrCount = 24
+};
+enum work_slot : int { kWorkCellStart = 0, kWorkFinalize = 1, kWorkP2G = 2, kWorkG2P = 3, kWorkGrid = 4 };
+
+struct scene_params {
+  int n;          // particles
+  int cap;        // particle capacity (matrix component stride)
+  int nb_cap;     // block capacity
+  int table_size; // hash table slots (power of two)
+  int bitmap_cap; // bitmap words available
+  float dx, inv_dx, dt, kappa, four_over_dx;
+  float gravity[3];
+  int wall_type, wall_cells;
+  material_dev mat;
+};
+
+struct scene_device {
+  scene_params prm;
+  particle_buffers cur, nxt;
+  // hash table (HashTableView-compatible arrays + packed keys used for CAS/probing)
+  uint64_t *pk = nullptr;
+  int *tkeys = nullptr;   // [T][3]
+  int *tidx = nullptr;    // [T]
+  int *tstatus = nullptr; // [T]
+  int *active_keys = nullptr; // [nb_cap][3] sorted keys (view)
+  int *view_cnt = nullptr;    // active block count (view)
+  uint64_t *ins_pk = nullptr; // [nb_cap] keys by insertion index
+  int *ins_slot = nullptr;    // [nb_cap]
+  uint64_t *blk_pk = nullptr; // [nb_cap] keys by final block index
+  int *nbr = nullptr;         // [nb_cap][8]
+  uint32_t *bitmap = nullptr; // [bitmap_cap]
+  int *word_prefix = nullptr; // [bitmap_cap]
+  int *ctr = nullptr;         // [kCtrCount]
+  // binning
+  int *block_count = nullptr; // [nb_cap]
+  int *block_start = nullptr; // [nb_cap + 1]
+  int *cell_count = nullptr;  // [nb_cap * 512]
+  int *cell_start = nullptr;  // [nb_cap * 512]
+  uint32_t *key32 = nullptr;  // [cap]
+  int *rnk = nullptr;         // [cap]
+  int *tmp = nullptr;         // [cap]
+  int *src = nullptr;         // [cap] slot -> index in cur
+  int *scan_part = nullptr;   // [2 * kScanCtas + 1]
+  float *grid = nullptr;      // [nb_cap][4][512]
+};
+
+constexpr int kScanCtas = 256;
+
+// launchers (all asynchronous on `st`)
+cudaError_t launch_activate(scene_device &s, cudaStream_t st);
+cudaError_t launch_bin(scene_device &s, cudaStream_t st);
+cudaError_t launch_p2g(scene_device &s, cudaStream_t st);
+cudaError_t launch_grid_update(scene_device &s, cudaStream_t st);
+cudaError_t launch_g2p(scene_device &s, cudaStream_t st);
+int kernels_per_substep();
+
+// upload / download helpers: staging is AoS (x: 3n, C/F: 9n), see zsmpm_particle_arrays
+cudaError_t launch_import(scene_device &s, const float *m, const float *x, const float *v,
+                          const float *C, const float *F, const float *plastic, int n,
+                          cudaStream_t st);
+cudaError_t launch_import_tilevector(scene_device &s, const float *base, int nchn, int off_m,
+                                     int off_x, int off_v, int off_C, int off_F, int off_pl,
+                                     int n, cudaStream_t st);
+cudaError_t launch_prime(scene_device &s, cudaStream_t st);
+cudaError_t launch_export(const scene_device &s, float *m, float *x, float *v, float *C,
+                          float *F, float *plastic, cudaStream_t st);
+cudaError_t launch_export_tilevector(const scene_device &s, float *base, int nchn, int off_m,
+                                     int off_x, int off_v, int off_C, int off_F, int off_pl,
+                                     cudaStream_t st);
+cudaError_t launch_export_order(const scene_device &s, int *order, cudaStream_t st);
+cudaError_t launch_svd_batch(const float *A, float *U, float *S, float *V, long long count,
+                             cudaStream_t st);
+cudaError_t launch_constitutive_batch(const material_dev &mat, float *F, float *plastic,
+                                      float *tau, long long count, cudaStream_t st);
+
+}  // namespace zsmpm

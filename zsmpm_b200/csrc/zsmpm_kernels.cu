@@ -1,0 +1,1001 @@
+// sm_100a kernels of the explicit MLS/APIC MPM substep.
+//
+// Pipeline of one substep (all launches have fixed shapes and read their sizes from
+// device counters, so a substep can be captured in a CUDA graph):
+//   activation  k_begin, k_insert_particle_blocks, k_enlarge, k_bitmap_prepare,
+//               k_bitmap_set, scan(3), k_assign_ranks, k_neighbors
+//   binning     k_bin_count, scan(3), k_cell_start, k_bin_scatter, k_bin_finalize
+//   transfer    k_p2g, k_grid_update, k_g2p
+// Reference operators replaced: SparsityOp.hpp:41-112 (activation), SparsityOp.hpp:115-196
+// (binning), P2G.hpp:45-127, GridOp.hpp:54-164, G2P.hpp:43-84 (paths inside include/zensim).
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "zsmpm_device.cuh"
+#include "zsmpm_internal.h"
+
+namespace zsmpm {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ void set_status(int *ctr, int bit) { atomicOr(&ctr[kCtrStatus], bit); }
+
+__device__ __forceinline__ int grid_threads() { return gridDim.x * blockDim.x; }
+
+// ----------------------------------------------------------------- hash table
+// Insert with the reference's home slot and stride-127 linear probing
+// (HashTable.hpp:356-374).  The slot is claimed by a 64-bit CAS on the packed key instead
+// of the reference's per-slot spin lock, so no thread ever waits on another.
+// Returns the insertion index when this call inserted the key, -1 when it existed, -2 when
+// the table is full.
+__device__ int table_insert(const scene_device &s, uint64_t key, int3 k, int *counter,
+                            int index_base) {
+  const int T = s.prm.table_size;
+  int slot = home_slot(k.x, k.y, k.z, T);
+  for (int probe = 0; probe < T; ++probe) {
+    const unsigned long long prev =
+        atomicCAS((unsigned long long *)&s.pk[slot], (unsigned long long)kEmptyKey,
+                  (unsigned long long)key);
+    if (prev == kEmptyKey) {
+      const int idx = index_base + atomicAdd(counter, 1);
+      s.tkeys[3 * slot + 0] = k.x;
+      s.tkeys[3 * slot + 1] = k.y;
+      s.tkeys[3 * slot + 2] = k.z;
+      if (idx < s.prm.nb_cap) {
+        s.ins_pk[idx] = key;
+        s.ins_slot[idx] = slot;
+      } else {
+        set_status(s.ctr, kStatusCapacity);
+      }
+      s.tidx[slot] = idx;
+      return idx;
+    }
+    if (prev == key) return -1;
+    slot = (slot + 127) & (T - 1);
+  }
+  set_status(s.ctr, kStatusTableFull);
+  return -2;
+}
+
+// HashTable::query (HashTable.hpp:444-456): index of the key or -1.
+__device__ int table_query(const scene_device &s, uint64_t key, int3 k) {
+  const int T = s.prm.table_size;
+  int slot = home_slot(k.x, k.y, k.z, T);
+  for (int probe = 0; probe < T; ++probe) {
+    const uint64_t p = s.pk[slot];
+    if (p == key) return s.tidx[slot];
+    if (p == kEmptyKey) return -1;
+    slot = (slot + 127) & (T - 1);
+  }
+  return -1;
+}
+
+// Stencil-origin cell and block of a position exactly as ComputeSparsity computes them
+// (SparsityOp.hpp:70-77): c = floor(x * (1/dx) + 0.5) - 2, block = floor_div(c, 8).
+// Returns false for NaN/Inf or positions beyond the packed key range.
+__device__ __forceinline__ bool cell_of(const scene_params &p, float4 x, int3 &c, int3 &b) {
+  const float fx = x.x * p.inv_dx + 0.5f, fy = x.y * p.inv_dx + 0.5f, fz = x.z * p.inv_dx + 0.5f;
+  const float lim = (float)(kKeyLimit * 8);
+  if (!(fabsf(fx) < lim && fabsf(fy) < lim && fabsf(fz) < lim)) return false;
+  c = make_int3((int)floorf(fx) - 2, (int)floorf(fy) - 2, (int)floorf(fz) - 2);
+  b = make_int3(block_of_cell(c.x), block_of_cell(c.y), block_of_cell(c.z));
+  return true;
+}
+
+// ----------------------------------------------------------------- CTA scan helpers
+template <int NT>
+__device__ __forceinline__ int cta_exclusive_scan(int v, int &total, int *smem /* >= NT/32 + 1 */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) smem[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < NT / 32 ? smem[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < NT / 32) smem[lane] = w;
+    if (lane == NT / 32 - 1) smem[NT / 32] = w;
+  }
+  __syncthreads();
+  const int incl = x + (warp > 0 ? smem[warp - 1] : 0);
+  total = smem[NT / 32];
+  __syncthreads();
+  return incl - v;
+}
+
+// ----------------------------------------------------------------- device-wide scan
+// Three-phase exclusive scan over n values produced by Load(i) (n read from device memory
+// at *n_ptr), kScanCtas CTAs x kThreads.  out[n] receives the total.
+struct load_popc {
+  const uint32_t *w;
+  __device__ int operator()(int i) const { return __popc(w[i]); }
+};
+struct load_int {
+  const int *a;
+  __device__ int operator()(int i) const { return a[i]; }
+};
+
+template <class Load>
+__global__ void __launch_bounds__(kThreads) k_scan_reduce(Load ld, const int *n_ptr, int *part) {
+  __shared__ int sm[kThreads / 32 + 1];
+  const int n = *n_ptr;
+  const int chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int lo = min(n, (int)blockIdx.x * chunk), hi = min(n, lo + chunk);
+  int acc = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) acc += ld(i);
+  int total;
+  cta_exclusive_scan<kThreads>(acc, total, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kThreads) k_scan_partials(int *part, int parts) {
+  __shared__ int sm[kThreads / 32 + 1];
+  const int v = threadIdx.x < parts ? part[threadIdx.x] : 0;
+  int total;
+  const int ex = cta_exclusive_scan<kThreads>(v, total, sm);
+  if (threadIdx.x < parts) part[threadIdx.x] = ex;
+  if (threadIdx.x == 0) part[parts] = total;
+}
+
+template <class Load>
+__global__ void __launch_bounds__(kThreads) k_scan_down(Load ld, const int *n_ptr, const int *part,
+                                                         int *out) {
+  __shared__ int sm[kThreads / 32 + 1];
+  const int n = *n_ptr;
+  const int chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int lo = min(n, (int)blockIdx.x * chunk), hi = min(n, lo + chunk);
+  int run = part[blockIdx.x];
+  for (int base = lo; base < hi; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int v = i < hi ? ld(i) : 0;
+    int total;
+    const int ex = cta_exclusive_scan<kThreads>(v, total, sm);
+    if (i < hi) out[i] = run + ex;
+    run += total;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = part[gridDim.x];
+}
+
+template <class Load>
+cudaError_t device_scan(Load ld, const int *n_ptr, int *part, int *out, cudaStream_t st) {
+  k_scan_reduce<<<kScanCtas, kThreads, 0, st>>>(ld, n_ptr, part);
+  k_scan_partials<<<1, kThreads, 0, st>>>(part, kScanCtas);
+  k_scan_down<<<kScanCtas, kThreads, 0, st>>>(ld, n_ptr, part, out);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------- activation
+// Resets the hash table (CleanSparsity, SparsityOp.hpp:41-55) and the per-substep counters.
+__global__ void __launch_bounds__(kThreads) k_begin(scene_device s) {
+  const int T = s.prm.table_size;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += grid_threads()) {
+    s.pk[i] = kEmptyKey;
+    s.tkeys[3 * i + 0] = 0x7fffffff;
+    s.tkeys[3 * i + 1] = 0x7fffffff;
+    s.tkeys[3 * i + 2] = 0x7fffffff;
+    s.tidx[i] = -1;
+    s.tstatus[i] = -1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < kCtrCount) {
+    const int t = threadIdx.x;
+    if (t == kCtrStatus) return;
+    int v = 0;
+    if (t >= kCtrBoxLo && t < kCtrBoxLo + 3) v = 0x7fffffff;
+    if (t >= kCtrBoxHi && t < kCtrBoxHi + 3) v = -0x7fffffff;
+    s.ctr[t] = v;
+  }
+}
+
+// ComputeSparsity (SparsityOp.hpp:58-86): one insert per distinct block key of a warp.
+__global__ void __launch_bounds__(kThreads) k_insert_particle_blocks(scene_device s) {
+  const int lane = threadIdx.x & 31;
+  const int n = s.prm.n;
+  int3 lo = make_int3(0x7fffffff, 0x7fffffff, 0x7fffffff);
+  int3 hi = make_int3(-0x7fffffff, -0x7fffffff, -0x7fffffff);
+  const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warps = grid_threads() >> 5;
+  for (int base = warp_global * 32; base < n; base += warps * 32) {
+    const int i = base + lane;
+    uint64_t key = kEmptyKey - 1 - lane;  // distinct per lane when invalid
+    int3 c, b = make_int3(0, 0, 0);
+    bool valid = false;
+    if (i < n) {
+      if (cell_of(s.prm, s.cur.xm[i], c, b)) {
+        key = pack_key(b.x, b.y, b.z);
+        valid = true;
+      } else {
+        set_status(s.ctr, kStatusOutOfDomain);
+      }
+    }
+    const unsigned peers = __match_any_sync(kFull, key);
+    if (valid && lane == __ffs(peers) - 1) {
+      table_insert(s, key, b, &s.ctr[kCtrParticleBlocks], 0);
+      lo = make_int3(min(lo.x, b.x), min(lo.y, b.y), min(lo.z, b.z));
+      hi = make_int3(max(hi.x, b.x), max(hi.y, b.y), max(hi.z, b.z));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo.x = min(lo.x, __shfl_xor_sync(kFull, lo.x, o));
+    lo.y = min(lo.y, __shfl_xor_sync(kFull, lo.y, o));
+    lo.z = min(lo.z, __shfl_xor_sync(kFull, lo.z, o));
+    hi.x = max(hi.x, __shfl_xor_sync(kFull, hi.x, o));
+    hi.y = max(hi.y, __shfl_xor_sync(kFull, hi.y, o));
+    hi.z = max(hi.z, __shfl_xor_sync(kFull, hi.z, o));
+  }
+  if (lane == 0 && lo.x != 0x7fffffff) {
+    atomicMin(&s.ctr[kCtrBoxLo + 0], lo.x);
+    atomicMin(&s.ctr[kCtrBoxLo + 1], lo.y);
+    atomicMin(&s.ctr[kCtrBoxLo + 2], lo.z);
+    atomicMax(&s.ctr[kCtrBoxHi + 0], hi.x);
+    atomicMax(&s.ctr[kCtrBoxHi + 1], hi.y);
+    atomicMax(&s.ctr[kCtrBoxHi + 2], hi.z);
+  }
+}
+
+// EnlargeSparsity{lo=0, hi=2} (SparsityOp.hpp:88-112): the +{0,1}^3 neighbours of every
+// particle block, so that the 3x3x3 stencil of every particle lands in active blocks.
+__global__ void __launch_bounds__(kThreads) k_enlarge(scene_device s) {
+  const int npb = min(s.ctr[kCtrParticleBlocks], s.prm.nb_cap);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npb * 7; t += grid_threads()) {
+    const int i = t / 7, o = t % 7 + 1;
+    const int3 k = unpack_key(s.ins_pk[i]);
+    const int3 nk = make_int3(k.x + (o >> 2), k.y + ((o >> 1) & 1), k.z + (o & 1));
+    table_insert(s, pack_key(nk.x, nk.y, nk.z), nk, &s.ctr[kCtrEnlarged], npb);
+  }
+}
+
+// Total block count, capacity checks and the dense bounding box of the bitmap that ranks
+// the blocks in ascending (bx, by, bz) order.
+__global__ void k_bitmap_prepare(scene_device s) {
+  if (threadIdx.x != 0) return;
+  int nb = s.ctr[kCtrParticleBlocks] + s.ctr[kCtrEnlarged];
+  if (nb >= s.prm.table_size - 20) set_status(s.ctr, kStatusTableFull);  // HashTable.hpp:369
+  if (nb > s.prm.nb_cap) {
+    set_status(s.ctr, kStatusCapacity);
+    nb = s.prm.nb_cap;
+  }
+  s.ctr[kCtrBlocks] = nb;
+  *s.view_cnt = nb;
+  int words = 0;
+  if (nb > 0) {
+    const long long ex = (long long)s.ctr[kCtrBoxHi + 0] - s.ctr[kCtrBoxLo + 0] + 2;
+    const long long ey = (long long)s.ctr[kCtrBoxHi + 1] - s.ctr[kCtrBoxLo + 1] + 2;
+    const long long ez = (long long)s.ctr[kCtrBoxHi + 2] - s.ctr[kCtrBoxLo + 2] + 2;
+    const long long vol = ex * ey * ez;
+    const long long w = (vol + 31) / 32;
+    if (w > s.prm.bitmap_cap) {
+      set_status(s.ctr, kStatusBitmap);
+      s.ctr[kCtrBlocks] = 0;
+      *s.view_cnt = 0;
+    } else {
+      words = (int)w;
+    }
+  }
+  s.ctr[kCtrWords] = words;
+}
+
+__device__ __forceinline__ long long dense_id(const scene_device &s, int3 k) {
+  const long long ey = (long long)s.ctr[kCtrBoxHi + 1] - s.ctr[kCtrBoxLo + 1] + 2;
+  const long long ez = (long long)s.ctr[kCtrBoxHi + 2] - s.ctr[kCtrBoxLo + 2] + 2;
+  return (((long long)k.x - s.ctr[kCtrBoxLo + 0]) * ey + ((long long)k.y - s.ctr[kCtrBoxLo + 1])) * ez +
+         ((long long)k.z - s.ctr[kCtrBoxLo + 2]);
+}
+
+__global__ void __launch_bounds__(kThreads) k_bitmap_set(scene_device s) {
+  const int nb = s.ctr[kCtrWords] > 0 ? s.ctr[kCtrBlocks] : 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += grid_threads()) {
+    const long long d = dense_id(s, unpack_key(s.ins_pk[i]));
+    atomicOr(&s.bitmap[d >> 5], 1u << (d & 31));
+  }
+}
+
+// rank = number of active keys below this one; index == rank from here on
+__global__ void __launch_bounds__(kThreads) k_assign_ranks(scene_device s) {
+  const int nb = s.ctr[kCtrWords] > 0 ? s.ctr[kCtrBlocks] : 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += grid_threads()) {
+    const uint64_t key = s.ins_pk[i];
+    const int3 k = unpack_key(key);
+    const long long d = dense_id(s, k);
+    const uint32_t w = s.bitmap[d >> 5];
+    const int rank = s.word_prefix[d >> 5] + __popc(w & ((1u << (d & 31)) - 1u));
+    s.tidx[s.ins_slot[i]] = rank;
+    s.blk_pk[rank] = key;
+    s.active_keys[3 * rank + 0] = k.x;
+    s.active_keys[3 * rank + 1] = k.y;
+    s.active_keys[3 * rank + 2] = k.z;
+  }
+}
+
+// neighbour table b + {0,1}^3 (index dx*4 + dy*2 + dz); clears the bitmap for next time
+__global__ void __launch_bounds__(kThreads) k_neighbors(scene_device s) {
+  const int nb = s.ctr[kCtrBlocks];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb * 8; t += grid_threads()) {
+    const int b = t >> 3, o = t & 7;
+    const int3 k = unpack_key(s.blk_pk[b]);
+    const int3 nk = make_int3(k.x + (o >> 2), k.y + ((o >> 1) & 1), k.z + (o & 1));
+    s.nbr[t] = table_query(s, pack_key(nk.x, nk.y, nk.z), nk);
+  }
+  const int words = s.ctr[kCtrWords];
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += grid_threads()) s.bitmap[w] = 0u;
+}
+
+// ----------------------------------------------------------------- binning
+// Per particle: its block index and stencil-origin cell; counts per cell (rank within the
+// cell from the atomic) and per block (warp-aggregated).
+__global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
+  const int lane = threadIdx.x & 31;
+  const int n = s.prm.n;
+  const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warps = grid_threads() >> 5;
+  for (int base = warp_global * 32; base < n; base += warps * 32) {
+    const int i = base + lane;
+    uint64_t key = kEmptyKey - 1 - lane;
+    int3 c = make_int3(0, 0, 0), b = make_int3(0, 0, 0);
+    bool valid = false;
+    if (i < n && cell_of(s.prm, s.cur.xm[i], c, b)) {
+      key = pack_key(b.x, b.y, b.z);
+      valid = true;
+    }
+    const unsigned peers = __match_any_sync(kFull, key);
+    const int leader = __ffs(peers) - 1;
+    int blk = -1;
+    if (valid && lane == leader) blk = table_query(s, key, b);
+    blk = __shfl_sync(kFull, blk, leader);
+    if (valid && blk < 0) set_status(s.ctr, kStatusMissingBlock);
+    const bool ok = valid && blk >= 0;
+    // block counts, one atomic per distinct block of the warp
+    const unsigned bpeers = __match_any_sync(kFull, ok ? blk : -1 - lane);
+    if (ok && lane == __ffs(bpeers) - 1) atomicAdd(&s.block_count[blk], __popc(bpeers));
+    if (i < n) {
+      if (ok) {
+        const int cell = ((c.x - 8 * b.x) << 6) | ((c.y - 8 * b.y) << 3) | (c.z - 8 * b.z);
+        const uint32_t k32 = (uint32_t)blk * 512u + (uint32_t)cell;
+        s.key32[i] = k32;
+        s.rnk[i] = atomicAdd(&s.cell_count[k32], 1);
+      } else {
+        s.key32[i] = 0xffffffffu;
+        s.rnk[i] = 0;
+      }
+    }
+  }
+}
+
+// Persistent per-block CTA loop helper.
+__device__ __forceinline__ int grab_block(int *counter, int *s_b) {
+  __syncthreads();
+  if (threadIdx.x == 0) *s_b = atomicAdd(counter, 1);
+  __syncthreads();
+  return *s_b;
+}
+
+// cell-major offsets of every cell's particle list
+__global__ void __launch_bounds__(512) k_cell_start(scene_device s) {
+  __shared__ int sm[512 / 32 + 1];
+  __shared__ int s_b;
+  const int nb = s.ctr[kCtrBlocks];
+  for (;;) {
+    const int b = grab_block(&s.ctr[kCtrWork + kWorkCellStart], &s_b);
+    if (b >= nb) break;
+    const int c = s.cell_count[b * 512 + threadIdx.x];
+    int total;
+    const int ex = cta_exclusive_scan<512>(c, total, sm);
+    s.cell_start[b * 512 + threadIdx.x] = s.block_start[b] + ex;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_bin_scatter(scene_device s) {
+  const int n = s.prm.n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += grid_threads()) {
+    const uint32_t k = s.key32[i];
+    if (k == 0xffffffffu) continue;
+    s.tmp[s.cell_start[k] + s.rnk[i]] = i;
+  }
+}
+
+// Final particle order of a block: rows r = 0, 1, ... each holding the r-th particle (by
+// upload index) of every cell with more than r particles, cells ascending.  Consecutive
+// slots therefore sit in distinct cells.  Also zeroes the block's grid, counts for the
+// next substep.
+__global__ void __launch_bounds__(512) k_bin_finalize(scene_device s) {
+  constexpr int kMaxList = 24;
+  __shared__ int sm[512 / 32 + 1];
+  __shared__ int s_b, s_max;
+  const int nb = s.ctr[kCtrBlocks];
+  const int t = threadIdx.x;
+  for (;;) {
+    const int b = grab_block(&s.ctr[kCtrWork + kWorkFinalize], &s_b);
+    if (b >= nb) break;
+    if (t == 0) s_max = 0;
+    const int c = s.cell_count[b * 512 + t];
+    const int cs = s.cell_start[b * 512 + t];
+    s.cell_count[b * 512 + t] = 0;
+    int li[kMaxList], lid[kMaxList];
+    if (c <= kMaxList) {
+      for (int r = 0; r < c; ++r) {
+        const int i = s.tmp[cs + r];
+        const int id = s.cur.id[i];
+        int q = r;
+        while (q > 0 && lid[q - 1] > id) {
+          lid[q] = lid[q - 1];
+          li[q] = li[q - 1];
+          --q;
+        }
+        lid[q] = id;
+        li[q] = i;
+      }
+    } else {
+      // long lists (strongly compressed cells): insertion sort in place in global memory
+      for (int r = 1; r < c; ++r) {
+        const int i = s.tmp[cs + r];
+        const int id = s.cur.id[i];
+        int q = r;
+        while (q > 0 && s.cur.id[s.tmp[cs + q - 1]] > id) {
+          s.tmp[cs + q] = s.tmp[cs + q - 1];
+          --q;
+        }
+        s.tmp[cs + q] = i;
+      }
+    }
+    __syncthreads();
+    atomicMax(&s_max, c);
+    __syncthreads();
+    const int maxc = s_max;
+    const int bs = s.block_start[b];
+    int row = 0;
+    for (int r = 0; r < maxc; ++r) {
+      const int flag = c > r ? 1 : 0;
+      int total;
+      const int ex = cta_exclusive_scan<512>(flag, total, sm);
+      if (flag) s.src[bs + row + ex] = c <= kMaxList ? li[r] : s.tmp[cs + r];
+      row += total;
+    }
+    float4 *g = reinterpret_cast<float4 *>(s.grid + (size_t)b * kGridChannels * 512);
+    g[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (t == 0) s.block_count[b] = 0;
+  }
+}
+
+// ----------------------------------------------------------------- P2G
+// One CTA per block (persistent): scatter the block's particles into a 12^3 halo of the
+// grid in shared memory (cells [8b, 8b+12) per axis, covering b and its +1 neighbours),
+// then flush the halo with 16-byte vector reductions into the 8 neighbour blocks.
+// Grid channels: m and p = sum W (m v + A (x_i - x_p)), which is the reference's
+// mv + rhs (P2G.hpp:108-125) with A = m C - (4 dt/dx^2) tau precomputed by G2P.
+__global__ void __launch_bounds__(kThreads) k_p2g(scene_device s) {
+  __shared__ float sh[kGridChannels][kHalo][kHalo][kHalo];
+  __shared__ int s_b;
+  const scene_params &p = s.prm;
+  const int nb = s.ctr[kCtrBlocks];
+  float *shf = &sh[0][0][0][0];
+  for (;;) {
+    const int b = grab_block(&s.ctr[kCtrWork + kWorkP2G], &s_b);
+    if (b >= nb) break;
+    const int start = s.block_start[b], end = s.block_start[b + 1];
+    if (start == end) continue;
+    for (int q = threadIdx.x; q < kGridChannels * kHaloCells; q += blockDim.x) shf[q] = 0.f;
+    __syncthreads();
+    const int3 bk = unpack_key(s.blk_pk[b]);
+    const int ox = bk.x * 8, oy = bk.y * 8, oz = bk.z * 8;
+    for (int slot = start + threadIdx.x; slot < end; slot += blockDim.x) {
+      const int i = s.src[slot];
+      const float4 xm = s.cur.xm[i];
+      const float4 vv = s.cur.v[i];
+      float A[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) A[k] = s.cur.A[(size_t)k * p.cap + i];
+      const float X[3] = {__fdiv_rn(xm.x, p.dx), __fdiv_rn(xm.y, p.dx), __fdiv_rn(xm.z, p.dx)};
+      int hb[3];
+      float w[3][3], lp[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float base = floorf(X[d] - 0.5f);
+        const float f = X[d] - base;
+        hb[d] = (int)base - (d == 0 ? ox : d == 1 ? oy : oz);
+        w[d][0] = 0.5f * (1.5f - f) * (1.5f - f);
+        const float f1 = f - 1.f;
+        w[d][1] = 0.75f - f1 * f1;
+        const float f2 = 0.5f + f1;
+        w[d][2] = 0.5f * f2 * f2;
+        lp[d] = f * p.dx;
+      }
+      if (hb[0] < 0 || hb[0] > kHalo - 3 || hb[1] < 0 || hb[1] > kHalo - 3 || hb[2] < 0 ||
+          hb[2] > kHalo - 3) {
+        set_status(s.ctr, kStatusMissingBlock);
+        continue;
+      }
+      const float m = xm.w;
+      // value at node offset (i,j,k): q + i*ax + j*ay + k*az
+      float q[3], ax[3], ay[3], az[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        q[d] = m * (d == 0 ? vv.x : d == 1 ? vv.y : vv.z) - (A[d] * lp[0] + A[3 + d] * lp[1] + A[6 + d] * lp[2]);
+        ax[d] = A[d] * p.dx;
+        ay[d] = A[3 + d] * p.dx;
+        az[d] = A[6 + d] * p.dx;
+      }
+#pragma unroll
+      for (int ii = 0; ii < 3; ++ii) {
+        float qi[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) qi[d] = q[d] + (float)ii * ax[d];
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+          float qij[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) qij[d] = qi[d] + (float)jj * ay[d];
+          const float wij = w[0][ii] * w[1][jj];
+          const int hrow = ((hb[0] + ii) * kHalo + (hb[1] + jj)) * kHalo + hb[2];
+#pragma unroll
+          for (int kk = 0; kk < 3; ++kk) {
+            const float W = wij * w[2][kk];
+            const int h = hrow + kk;
+            atomicAdd(&shf[0 * kHaloCells + h], W * m);
+            atomicAdd(&shf[1 * kHaloCells + h], W * (qij[0] + (float)kk * az[0]));
+            atomicAdd(&shf[2 * kHaloCells + h], W * (qij[1] + (float)kk * az[1]));
+            atomicAdd(&shf[3 * kHaloCells + h], W * (qij[2] + (float)kk * az[2]));
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // flush: items (ch, hx, hy, quad) over 4 x 12 x 12 x 3
+    for (int it = threadIdx.x; it < kGridChannels * kHalo * kHalo * 3; it += blockDim.x) {
+      const int quad = it % 3, hy = (it / 3) % kHalo, hx = (it / (3 * kHalo)) % kHalo,
+                ch = it / (3 * kHalo * kHalo);
+      const float *src4 = &sh[ch][hx][hy][quad * 4];
+      const float a0 = src4[0], a1 = src4[1], a2 = src4[2], a3 = src4[3];
+      if (a0 == 0.f && a1 == 0.f && a2 == 0.f && a3 == 0.f) continue;
+      const int t = (hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0);
+      const int tb = s.nbr[b * 8 + t];
+      if (tb < 0) {
+        set_status(s.ctr, kStatusMissingBlock);
+        continue;
+      }
+      const int cell = ((hx & 7) << 6) | ((hy & 7) << 3) | ((quad * 4) & 7);
+      red_add_v4(s.grid + ((size_t)tb * kGridChannels + ch) * 512 + cell, a0, a1, a2, a3);
+    }
+  }
+}
+
+// ----------------------------------------------------------------- grid update
+// ComputeGridBlockVelocity with the rhs term (v = (mv + rhs)/m + g dt; GridOp.hpp:93-99
+// restated) and ApplyBoundaryConditionOnGridBlocks with six planes wall_cells*dx inside
+// the unit box (GridOp.hpp:136-161, Collider.h:98-105).
+__device__ __forceinline__ void apply_walls(const scene_params &p, const float pos[3], float v[3]) {
+  if (p.wall_type == 3) return;
+  const float lo = (float)p.wall_cells * p.dx, hi = 1.f - (float)p.wall_cells * p.dx;
+#pragma unroll
+  for (int w = 0; w < 6; ++w) {
+    const int axis = w >> 1;
+    const float sgn = (w & 1) ? -1.f : 1.f;
+    const float sd = sgn * (pos[axis] - ((w & 1) ? hi : lo));
+    if (!(sd < 0.f)) continue;
+    if (p.wall_type == 0) {
+      v[0] = v[1] = v[2] = 0.f;
+    } else {
+      const float proj = sgn * v[axis];
+      if (p.wall_type == 1 || proj < 0.f) v[axis] = v[axis] - proj * sgn;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_grid_update(scene_device s) {
+  const scene_params &p = s.prm;
+  const int nb = s.ctr[kCtrBlocks];
+  const long long total = (long long)nb * 512;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += grid_threads()) {
+    const int b = (int)(t >> 9), cell = (int)(t & 511);
+    float *g = s.grid + (size_t)b * kGridChannels * 512 + cell;
+    const float m = g[0];
+    if (m == 0.f) continue;
+    const float inv = 1.f / m;
+    float v[3] = {g[512] * inv + p.gravity[0] * p.dt, g[1024] * inv + p.gravity[1] * p.dt,
+                  g[1536] * inv + p.gravity[2] * p.dt};
+    if (m > 0.f) {
+      const int3 k = unpack_key(s.blk_pk[b]);
+      const float pos[3] = {((float)k.x * 8.f + (float)(cell >> 6)) * p.dx,
+                            ((float)k.y * 8.f + (float)((cell >> 3) & 7)) * p.dx,
+                            ((float)k.z * 8.f + (float)(cell & 7)) * p.dx};
+      apply_walls(p, pos, v);
+    }
+    g[512] = v[0];
+    g[1024] = v[1];
+    g[1536] = v[2];
+  }
+}
+
+// ----------------------------------------------------------------- G2P
+// One CTA per block (persistent): stage the 12^3 halo of grid velocities in shared memory,
+// then per particle gather v and C (G2P.hpp:56-66), advect, update F = (I + dt C) F
+// (G2P.hpp:76-78), run the constitutive update and write the particle to its binned slot
+// in the next buffer set, so that storage order follows the binning of this substep.
+__global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
+  __shared__ float sv[3][kHalo][kHalo][kHalo];
+  __shared__ int s_b;
+  const scene_params &p = s.prm;
+  const int nb = s.ctr[kCtrBlocks];
+  float *svf = &sv[0][0][0][0];
+  for (;;) {
+    const int b = grab_block(&s.ctr[kCtrWork + kWorkG2P], &s_b);
+    if (b >= nb) break;
+    const int start = s.block_start[b], end = s.block_start[b + 1];
+    if (start == end) continue;
+    // halo load: items (ch, hx, hy, quad) over 3 x 12 x 12 x 3, 16-byte loads
+    for (int it = threadIdx.x; it < 3 * kHalo * kHalo * 3; it += blockDim.x) {
+      const int quad = it % 3, hy = (it / 3) % kHalo, hx = (it / (3 * kHalo)) % kHalo,
+                ch = it / (3 * kHalo * kHalo);
+      const int t = (hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0);
+      const int tb = s.nbr[b * 8 + t];
+      float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (tb >= 0) {
+        const int cell = ((hx & 7) << 6) | ((hy & 7) << 3) | ((quad * 4) & 7);
+        val = *reinterpret_cast<const float4 *>(s.grid + ((size_t)tb * kGridChannels + 1 + ch) * 512 + cell);
+      }
+      float *dst = &sv[ch][hx][hy][quad * 4];
+      dst[0] = val.x;
+      dst[1] = val.y;
+      dst[2] = val.z;
+      dst[3] = val.w;
+    }
+    __syncthreads();
+    const int3 bk = unpack_key(s.blk_pk[b]);
+    const int org[3] = {bk.x * 8, bk.y * 8, bk.z * 8};
+    for (int slot = start + threadIdx.x; slot < end; slot += blockDim.x) {
+      const int i = s.src[slot];
+      float4 xm = s.cur.xm[i];
+      float F[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) F[k] = s.cur.F[(size_t)k * p.cap + i];
+      float pl = s.cur.plastic ? s.cur.plastic[i] : 0.f;
+      const int id = s.cur.id[i];
+      const float X[3] = {__fdiv_rn(xm.x, p.dx), __fdiv_rn(xm.y, p.dx), __fdiv_rn(xm.z, p.dx)};
+      int hb[3];
+      float w[3][3], f[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float base = floorf(X[d] - 0.5f);
+        f[d] = X[d] - base;
+        hb[d] = (int)base - org[d];
+        w[d][0] = 0.5f * (1.5f - f[d]) * (1.5f - f[d]);
+        const float f1 = f[d] - 1.f;
+        w[d][1] = 0.75f - f1 * f1;
+        const float f2 = 0.5f + f1;
+        w[d][2] = 0.5f * f2 * f2;
+      }
+      const bool inside = hb[0] >= 0 && hb[0] <= kHalo - 3 && hb[1] >= 0 && hb[1] <= kHalo - 3 &&
+                          hb[2] >= 0 && hb[2] <= kHalo - 3;
+      if (!inside) set_status(s.ctr, kStatusMissingBlock);
+      float vel[3] = {0.f, 0.f, 0.f};
+      float B[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // sum W v (node - f)^T
+      if (inside) {
+#pragma unroll
+        for (int ii = 0; ii < 3; ++ii) {
+          const float dxi = (float)ii - f[0];
+#pragma unroll
+          for (int jj = 0; jj < 3; ++jj) {
+            const float dyj = (float)jj - f[1];
+            const float wij = w[0][ii] * w[1][jj];
+            const int hrow = ((hb[0] + ii) * kHalo + (hb[1] + jj)) * kHalo + hb[2];
+            // separable accumulation over k: s0 = sum_k wz v, s1 = sum_k wz (k - fz) v
+            float s0[3] = {0.f, 0.f, 0.f}, s1[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+              const float wz = w[2][kk], wzd = wz * ((float)kk - f[2]);
+              const int h = hrow + kk;
+              const float vx = svf[h], vy = svf[kHaloCells + h], vz = svf[2 * kHaloCells + h];
+              s0[0] += wz * vx;
+              s0[1] += wz * vy;
+              s0[2] += wz * vz;
+              s1[0] += wzd * vx;
+              s1[1] += wzd * vy;
+              s1[2] += wzd * vz;
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const float a = wij * s0[d];
+              vel[d] += a;
+              B[d] += a * dxi;
+              B[3 + d] += a * dyj;
+              B[6 + d] += wij * s1[d];
+            }
+          }
+        }
+      }
+      float C[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) C[k] = B[k] * p.four_over_dx;
+      xm.x += vel[0] * p.dt;
+      xm.y += vel[1] * p.dt;
+      xm.z += vel[2] * p.dt;
+      // F <- (I + dt C) F
+      float Fn[9];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+          Fn[3 * c + r] = F[3 * c + r] + p.dt * (C[r] * F[3 * c] + C[3 + r] * F[3 * c + 1] + C[6 + r] * F[3 * c + 2]);
+      float tau[9];
+      constitutive(p.mat, Fn, pl, tau);
+      const size_t cap = (size_t)p.cap;
+      s.nxt.xm[slot] = xm;
+      s.nxt.v[slot] = make_float4(vel[0], vel[1], vel[2], 0.f);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        s.nxt.C[k * cap + slot] = C[k];
+        s.nxt.A[k * cap + slot] = xm.w * C[k] - p.kappa * tau[k];
+        s.nxt.F[k * cap + slot] = Fn[k];
+      }
+      if (s.nxt.plastic) s.nxt.plastic[slot] = pl;
+      s.nxt.id[slot] = id;
+    }
+  }
+}
+
+// ----------------------------------------------------------------- import / export
+__global__ void k_import(scene_device s, const float *m, const float *x, const float *v,
+                         const float *C, const float *F, const float *pl, int n) {
+  const size_t cap = (size_t)s.prm.cap;
+  const float plastic_default = s.prm.mat.model == 2 ? 1.f : 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += grid_threads()) {
+    s.cur.xm[i] = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], m[i]);
+    s.cur.v[i] = v ? make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      s.cur.C[k * cap + i] = C ? C[9 * (size_t)i + k] : 0.f;
+      s.cur.F[k * cap + i] = F ? F[9 * (size_t)i + k] : ((k & 3) == 0 ? 1.f : 0.f);
+    }
+    if (s.cur.plastic) s.cur.plastic[i] = pl ? pl[i] : plastic_default;
+    s.cur.id[i] = i;
+  }
+}
+
+__global__ void k_import_tv(scene_device s, const float *base, int nchn, int om, int ox, int ov,
+                            int oC, int oF, int opl, int n) {
+  const size_t cap = (size_t)s.prm.cap;
+  const float plastic_default = s.prm.mat.model == 2 ? 1.f : 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += grid_threads()) {
+    const size_t tile = (size_t)(i / 32) * nchn * 32 + (i % 32);
+    auto at = [&](int chn) { return base[tile + (size_t)chn * 32]; };
+    s.cur.xm[i] = make_float4(at(ox), at(ox + 1), at(ox + 2), at(om));
+    s.cur.v[i] = ov >= 0 ? make_float4(at(ov), at(ov + 1), at(ov + 2), 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      s.cur.C[k * cap + i] = oC >= 0 ? at(oC + k) : 0.f;
+      s.cur.F[k * cap + i] = oF >= 0 ? at(oF + k) : ((k & 3) == 0 ? 1.f : 0.f);
+    }
+    if (s.cur.plastic) s.cur.plastic[i] = opl >= 0 ? at(opl) : plastic_default;
+    s.cur.id[i] = i;
+  }
+}
+
+// stress of the stored state; A = m C - kappa tau (what the previous G2P would have written)
+__global__ void k_prime(scene_device s) {
+  const size_t cap = (size_t)s.prm.cap;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s.prm.n; i += grid_threads()) {
+    float F[9], tau[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) F[k] = s.cur.F[k * cap + i];
+    float pl = s.cur.plastic ? s.cur.plastic[i] : 0.f;
+    constitutive(s.prm.mat, F, pl, tau);
+    const float m = s.cur.xm[i].w;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      s.cur.F[k * cap + i] = F[k];
+      s.cur.A[k * cap + i] = m * s.cur.C[k * cap + i] - s.prm.kappa * tau[k];
+    }
+    if (s.cur.plastic) s.cur.plastic[i] = pl;
+  }
+}
+
+__global__ void k_export(scene_device s, float *m, float *x, float *v, float *C, float *F, float *pl) {
+  const size_t cap = (size_t)s.prm.cap;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s.prm.n; i += grid_threads()) {
+    const int o = s.cur.id[i];
+    const float4 xm = s.cur.xm[i], vv = s.cur.v[i];
+    if (m) m[o] = xm.w;
+    if (x) {
+      x[3 * (size_t)o] = xm.x;
+      x[3 * (size_t)o + 1] = xm.y;
+      x[3 * (size_t)o + 2] = xm.z;
+    }
+    if (v) {
+      v[3 * (size_t)o] = vv.x;
+      v[3 * (size_t)o + 1] = vv.y;
+      v[3 * (size_t)o + 2] = vv.z;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      if (C) C[9 * (size_t)o + k] = s.cur.C[k * cap + i];
+      if (F) F[9 * (size_t)o + k] = s.cur.F[k * cap + i];
+    }
+    if (pl) pl[o] = s.cur.plastic ? s.cur.plastic[i] : 0.f;
+  }
+}
+
+__global__ void k_export_tv(scene_device s, float *base, int nchn, int om, int ox, int ov, int oC,
+                            int oF, int opl) {
+  const size_t cap = (size_t)s.prm.cap;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s.prm.n; i += grid_threads()) {
+    const int o = s.cur.id[i];
+    const size_t tile = (size_t)(o / 32) * nchn * 32 + (o % 32);
+    auto at = [&](int chn) -> float & { return base[tile + (size_t)chn * 32]; };
+    const float4 xm = s.cur.xm[i], vv = s.cur.v[i];
+    if (om >= 0) at(om) = xm.w;
+    if (ox >= 0) {
+      at(ox) = xm.x;
+      at(ox + 1) = xm.y;
+      at(ox + 2) = xm.z;
+    }
+    if (ov >= 0) {
+      at(ov) = vv.x;
+      at(ov + 1) = vv.y;
+      at(ov + 2) = vv.z;
+    }
+    for (int k = 0; k < 9; ++k) {
+      if (oC >= 0) at(oC + k) = s.cur.C[k * cap + i];
+      if (oF >= 0) at(oF + k) = s.cur.F[k * cap + i];
+    }
+    if (opl >= 0) at(opl) = s.cur.plastic ? s.cur.plastic[i] : 0.f;
+  }
+}
+
+__global__ void k_export_order(scene_device s, int *order) {
+  // order[slot] = upload id of the particle that the binning placed in `slot`
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < s.prm.n; t += grid_threads())
+    order[t] = s.cur.id[s.src[t]];
+}
+
+__global__ void k_svd_batch(const float *A, float *U, float *S, float *V, long long count) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count; i += grid_threads()) {
+    float a[9], u[9], sg[3], v[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k] = A[9 * i + k];
+    svd3(a, u, sg, v);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      U[9 * i + k] = u[k];
+      V[9 * i + k] = v[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) S[3 * i + k] = sg[k];
+  }
+}
+
+__global__ void k_constitutive_batch(material_dev mat, float *F, float *pl, float *tau, long long count) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count; i += grid_threads()) {
+    float f[9], t[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = F[9 * i + k];
+    float p = pl ? pl[i] : 0.f;
+    constitutive(mat, f, p, t);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      F[9 * i + k] = f[k];
+      tau[9 * i + k] = t[k];
+    }
+    if (pl) pl[i] = p;
+  }
+}
+
+int g_num_sms = 0;
+int num_sms() {
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------- launchers
+cudaError_t launch_activate(scene_device &s, cudaStream_t st) {
+  const int sm = num_sms();
+  k_begin<<<sm * 4, kThreads, 0, st>>>(s);
+  k_insert_particle_blocks<<<sm * 8, kThreads, 0, st>>>(s);
+  k_enlarge<<<sm * 2, kThreads, 0, st>>>(s);
+  k_bitmap_prepare<<<1, 32, 0, st>>>(s);
+  k_bitmap_set<<<sm * 2, kThreads, 0, st>>>(s);
+  cudaError_t e = device_scan(load_popc{s.bitmap}, &s.ctr[kCtrWords], s.scan_part, s.word_prefix, st);
+  if (e != cudaSuccess) return e;
+  k_assign_ranks<<<sm * 2, kThreads, 0, st>>>(s);
+  k_neighbors<<<sm * 2, kThreads, 0, st>>>(s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
+  const int sm = num_sms();
+  k_bin_count<<<sm * 8, kThreads, 0, st>>>(s);
+  cudaError_t e = device_scan(load_int{s.block_count}, &s.ctr[kCtrBlocks], s.scan_part, s.block_start, st);
+  if (e != cudaSuccess) return e;
+  k_cell_start<<<sm * 2, 512, 0, st>>>(s);
+  k_bin_scatter<<<sm * 8, kThreads, 0, st>>>(s);
+  k_bin_finalize<<<sm * 2, 512, 0, st>>>(s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p2g(scene_device &s, cudaStream_t st) {
+  k_p2g<<<num_sms() * 3, kThreads, 0, st>>>(s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grid_update(scene_device &s, cudaStream_t st) {
+  k_grid_update<<<num_sms() * 8, kThreads, 0, st>>>(s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_g2p(scene_device &s, cudaStream_t st) {
+  k_g2p<<<num_sms() * 2, kThreads, 0, st>>>(s);
+  return cudaGetLastError();
+}
+
+// k_begin, insert, enlarge, prepare, set, 3 scans, ranks, neighbours; count, 3 scans,
+// cell_start, scatter, finalize; p2g; grid update; g2p
+int kernels_per_substep() { return 10 + 7 + 3; }
+
+cudaError_t launch_import(scene_device &s, const float *m, const float *x, const float *v,
+                          const float *C, const float *F, const float *plastic, int n,
+                          cudaStream_t st) {
+  k_import<<<num_sms() * 4, kThreads, 0, st>>>(s, m, x, v, C, F, plastic, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_import_tilevector(scene_device &s, const float *base, int nchn, int off_m,
+                                     int off_x, int off_v, int off_C, int off_F, int off_pl,
+                                     int n, cudaStream_t st) {
+  k_import_tv<<<num_sms() * 4, kThreads, 0, st>>>(s, base, nchn, off_m, off_x, off_v, off_C, off_F,
+                                                  off_pl, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prime(scene_device &s, cudaStream_t st) {
+  k_prime<<<num_sms() * 4, kThreads, 0, st>>>(s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export(const scene_device &s, float *m, float *x, float *v, float *C,
+                          float *F, float *plastic, cudaStream_t st) {
+  k_export<<<num_sms() * 4, kThreads, 0, st>>>(s, m, x, v, C, F, plastic);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export_tilevector(const scene_device &s, float *base, int nchn, int off_m,
+                                     int off_x, int off_v, int off_C, int off_F, int off_pl,
+                                     cudaStream_t st) {
+  k_export_tv<<<num_sms() * 4, kThreads, 0, st>>>(s, base, nchn, off_m, off_x, off_v, off_C, off_F,
+                                                  off_pl);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export_order(const scene_device &s, int *order, cudaStream_t st) {
+  k_export_order<<<num_sms() * 4, kThreads, 0, st>>>(s, order);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_svd_batch(const float *A, float *U, float *S, float *V, long long count,
+                             cudaStream_t st) {
+  k_svd_batch<<<num_sms() * 4, kThreads, 0, st>>>(A, U, S, V, count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_constitutive_batch(const material_dev &mat, float *F, float *plastic,
+                                      float *tau, long long count, cudaStream_t st) {
+  k_constitutive_batch<<<num_sms() * 4, kThreads, 0, st>>>(mat, F, plastic, tau, count);
+  return cudaGetLastError();
+}
+
+}  // namespace zsmpm
