@@ -1,0 +1,358 @@
+"""Benchmark: MPM particle-substeps per second of the explicit MLS/APIC substep on one B200.
+
+Workload (default): the Drucker-Prager two-box scene -- boxes [0.1,0.45]x[0.1,0.6]x[0.1,0.9]
+and [0.55,0.9]x[0.1,0.4]x[0.1,0.9] at dx=1/256 with 8 jittered particles per cell
+(30,089,900 particles from the geometry), E=3.5e5, nu=0.3, rho=2200, friction 30 deg,
+second box moving at (-1,0,0) m/s, slip walls, dt=5e-5.  A step is one full substep
+(activation, binning, P2G, grid update, G2P with SVD + return map).  Inputs (4.4 GB of
+particle state) are larger than the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--scene dp|fc|snow16m]
+
+Under torchrun every rank runs an independent replica (the path has no exchange step) and
+rank 0 prints one JSON line; time is the max over ranks of CUDA-event time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MPM particle-substeps/sec on 1 B200, learned vs plain closure at stated error"
+UNIT = "particle-substeps/s"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+
+
+def hbm_peak():
+    try:
+        return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def scene_for(name: str):
+    from zsmpm_b200 import scenes
+    if name == "dp":
+        return scenes.config2(), "dp_two_boxes_dx256_8ppc"
+    if name == "dp128":
+        return scenes.config2(dx=1 / 128), "dp_two_boxes_dx128_8ppc"
+    if name == "fc":
+        return scenes.config1(), "fc_cube_dx128_8ppc"
+    if name == "snow16m":
+        return scenes.config5_16m(), "snow_sphere_slab_dx295_4ppc"
+    raise SystemExit(f"unknown scene {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.file:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(parts)
+            except ValueError:
+                pass
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, val in zip(names, r[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def g2p_algorithmic_bytes(n: int, nb: int, plastic: bool) -> int:
+    """G2P per launch: per particle reads slot index 4, x|m 16, F 36, id 4 (+ plastic 4) and
+    writes x|m 16, v 16, C 36, A 36, F 36, id 4 (+ plastic 4); per active block reads the
+    3-channel velocity halo, 12 B per cell of the block (halo reads beyond the block come
+    from neighbours that are counted as their own blocks)."""
+    per_particle = 4 + 16 + 36 + 4 + 16 + 16 + 36 + 36 + 36 + 4 + (8 if plastic else 0)
+    return n * per_particle + nb * 512 * 12
+
+
+def substep_algorithmic_bytes(n: int, nb: int, plastic: bool) -> int:
+    """Whole substep, the survey's accounting (unfused P2G / grid / G2P): P2G reads x, v, C,
+    m, tau (100 B), G2P reads x, F and writes x, v, C, F, tau (180 B, +8 for plastic state),
+    binning 16 B, grid 72 B per active cell."""
+    return n * (100 + 180 + (8 if plastic else 0) + 16) + nb * 512 * 72
+
+
+def cpu_baseline_sample(spec, p, max_particles: int):
+    """A spatial slab of the workload (all particles with z below a cut), keeping density."""
+    from zsmpm_b200.scenes import Particles
+    z = p.x[:, 2]
+    if p.n <= max_particles:
+        return p, "full scene"
+    cut = float(np.quantile(z, max_particles / p.n))
+    idx = np.nonzero(z < cut)[0]
+    return p.subset(idx), f"slab z < {cut:.4f} of the workload ({len(idx)} particles)"
+
+
+def run_reference_arm(args, spec, workload, n_full):
+    from oracle import reference
+    from zsmpm_b200 import scenes
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    if not reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/zsref_cli not built "
+                          "(the reference sources were not present when build() ran)"}))
+        return 0
+    p = scenes.generate(spec)
+    sample, desc = cpu_baseline_sample(spec, p, args.ref_particles)
+    threads = os.cpu_count() or 1
+    # warm-up (separate process run), then K timed substeps on the sample
+    reference.run(spec, sample, max(args.warmup, 1), policy=reference.POLICY_OMP, threads=threads,
+                  cap_blocks=0, timeout=1800)
+    r = reference.run(spec, sample, args.steps, policy=reference.POLICY_OMP, threads=threads,
+                      cap_blocks=0, timeout=3600)
+    value = sample.n * args.steps / r.seconds
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * r.seconds / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": workload, "particles": n_full, "sample_particles": sample.n,
+                       "parallelism": "omp", "policy": "zs::omp_exec"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scene", default="dp", choices=["dp", "dp128", "fc", "snow16m"])
+    ap.add_argument("--ref-particles", type=int, default=1_500_000)
+    ap.add_argument("--ref-steps", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+
+    spec, workload = scene_for(args.scene)
+    from zsmpm_b200 import scenes
+    if args.impl == "reference":
+        return run_reference_arm(args, spec, workload, scenes.count_particles(spec))
+
+    ws, rank, local = dist_setup()
+    import torch
+
+    import zsmpm_b200 as zs
+    torch.cuda.set_device(local)
+    p = scenes.generate(spec)
+    n = p.n
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    plastic = spec.material.model != zs.FIXED_COROTATED
+
+    # pinned host copies of the inputs for the end-to-end leg
+    pinned = {k: torch.from_numpy(getattr(p, k)).pin_memory() for k in ("m", "x", "v", "C", "F", "plastic")}
+    out_x = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    out_v = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    h2d_bytes = sum(t.numel() * 4 for t in pinned.values())
+    d2h_bytes = (out_x.numel() + out_v.numel()) * 4 + 4
+
+    sc = zs.Scene(spec, device=local)
+    lib = zs._abi.lib()
+
+    def upload_pinned():
+        arrs = zs._abi.ParticleArrays(**{k: C.c_void_p(t.data_ptr()) for k, t in pinned.items()})
+        zs._abi.check(lib.zsmpm_scene_upload(sc.handle, C.byref(arrs), n, 0, C.c_void_p(sptr)), "upload")
+        sc.n = n
+
+    def download_xv():
+        arrs = zs._abi.ParticleArrays(x=C.c_void_p(out_x.data_ptr()), v=C.c_void_p(out_v.data_ptr()))
+        zs._abi.check(lib.zsmpm_scene_download(sc.handle, C.byref(arrs), 0, C.c_void_p(sptr)), "download")
+
+    # ---------------------------------------------------------------- device-resident leg
+    upload_pinned()
+    torch.cuda.synchronize()
+    sc.run(args.warmup, stream=sptr)
+    sc.status()
+    torch.cuda.synchronize()
+    barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sc.run(args.steps, stream=sptr)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    sc.status()
+    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(ms, ws)
+    barrier(ws)
+    value = n * args.steps * ws / (ms * 1e-3)
+    nb = sc.num_blocks()
+
+    # ---------------------------------------------------------------- per-stage timing pass
+    sc.set_stage_timing(True)
+    stage = np.zeros(5)
+    reps = min(args.steps, 8)
+    for _ in range(reps):
+        sc.substep(stream=sptr)
+        stage += np.array(sc.stage_times())
+    sc.set_stage_timing(False)
+    stage /= reps
+    sc.status()
+    peak, peak_kind = hbm_peak()
+    g2p_bytes = g2p_algorithmic_bytes(n, nb, plastic)
+    g2p_gbs = g2p_bytes / (stage[4] * 1e-3) / 1e9
+
+    # ---------------------------------------------------------------- end-to-end leg
+    torch.cuda.synchronize()
+    barrier(ws)
+    t0 = time.perf_counter()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    upload_pinned()
+    sc.run(args.steps, stream=sptr)
+    download_xv()
+    f1.record(stream)
+    sc.status()  # device -> host status word
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), ws)
+    wall = time.perf_counter() - t0
+    e2e = n * args.steps * ws / (e2e_ms * 1e-3)
+
+    # ---------------------------------------------------------------- CPU baseline (rank 0, N=1)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import reference
+            if reference.available():
+                sample, desc = cpu_baseline_sample(spec, p, args.ref_particles)
+                threads = os.cpu_count() or 1
+                r = reference.run(spec, sample, args.ref_steps, policy=reference.POLICY_OMP,
+                                  threads=threads, cap_blocks=0, timeout=900)
+                cpu = {"value": sample.n * args.ref_steps / r.seconds, "unit": UNIT, "cores": threads,
+                       "kind": "reference", "sample": f"{desc}, {args.ref_steps} substeps, zs::omp_exec"}
+            else:
+                cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                       "sample": "unavailable: oracle/_ref/zsref_cli not built"}
+        except Exception as exc:  # report, never fail the GPU line
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
+
+    total_bytes = substep_algorithmic_bytes(n, nb, plastic)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload, "particles": n, "active_blocks": nb,
+                       "dx": spec.dx, "ppc": spec.ppc, "dt": spec.dt, "material": "drucker_prager"
+                       if spec.material.model == zs.DRUCKER_PRAGER else
+                       ("snow" if spec.material.model == zs.SNOW else "fixed_corotated"),
+                       "closure": "plain", "parallelism": f"replicas{ws}",
+                       "l2": "inputs larger than L2 (particle state 4+ GB)",
+                       "substep_graph": "CUDA graph of 2 substeps"},
+            "roofline": {"bound": "hbm", "kernel": "k_g2p", "achieved": g2p_gbs, "peak": peak,
+                         "unit": "GB/s", "frac": g2p_gbs / peak, "traffic": None,
+                         "peak_kind": f"{peak_kind} copy bandwidth",
+                         "algorithmic_bytes_per_launch": g2p_bytes, "launch_ms": stage[4]},
+            "stage_ms": {"activate": stage[0], "bin": stage[1], "p2g": stage[2], "grid_update": stage[3],
+                         "g2p": stage[4]},
+            "substep_roofline": {"algorithmic_bytes_per_substep": total_bytes,
+                                 "achieved_gbs": total_bytes / (ms / args.steps * 1e-3) / 1e9,
+                                 "frac": total_bytes / (ms / args.steps * 1e-3) / 1e9 / peak},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes / args.steps,
+                    "d2h_bytes_per_step": d2h_bytes / args.steps, "wall_s": wall,
+                    "what": "upload from pinned host, K substeps, download x and v, status read"},
+            "gpu_launches": sc.kernels_per_substep() * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    sc.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -12,7 +12,7 @@
 #define SFX _f32
 #define R_LOG logf
 #define R_EXP expf
-#define R_SQRT sqrtf
+#define R_SQRT oracle_ref_sqrtf
 #define R_FLOOR floorf
 #define OR_SVD oracle_svd_f32
 #include "oracle_sim.h"

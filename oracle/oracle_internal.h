@@ -22,5 +22,6 @@ int32_t oracle_table_query(const oracle_table *t, const int32_t k[3]);
 void oracle_block_of(const float x[3], float dxinv, int32_t out[3]);
 int oracle_activate_table(oracle_table *t, int n, const float *x, float dx, int *nparblocks);
 void oracle_table_canonicalize(oracle_table *t);
+float oracle_ref_sqrtf(float arg);
 
 #endif

@@ -368,6 +368,43 @@ void oracle_svd_f32(const float *A, float *U, float *S, float *V) {
   S[2] = a[2][2];
 }
 
+/* ------------------------------------------------- the reference's float square root */
+/* zs::math::sqrt(float) (math/MathUtils.h:258-326): a bit-trick reciprocal square root
+ * (Lomont's constant 0x5f375a86, two Newton steps), two more Newton steps on the scaled
+ * argument, one correction step, then rescaling.  compute_stress_sand uses it for the norm
+ * of the deviatoric log strain (ConstitutiveModel_Vol_dP.hpp:263-265). */
+static float ref_q_rsqrt(float number) {
+  fbits b;
+  float x2 = number * 0.5f, y;
+  b.f = number;
+  b.u = 0x5f375a86u - (b.u >> 1);
+  y = b.f;
+  y = y * (1.5f - (x2 * y * y));
+  y = y * (1.5f - (x2 * y * y));
+  return y;
+}
+
+float oracle_ref_sqrtf(float arg) {
+  const float scale_in = 0x1.0p+26f, scale_out = 0x1.0p-13f;
+  fbits inf;
+  inf.u = 0x7f800000u;
+  if (arg < 0.0f) {
+    fbits q;
+    q.u = 0x7fffffffu;
+    return q.f;
+  } else if (arg == 0.0f || !(fabsf(arg) < inf.f)) {
+    return arg + arg;
+  }
+  arg = arg * scale_in;
+  float rsq = ref_q_rsqrt(arg);
+  rsq = ((-0.5f * arg * rsq) * rsq + 0.5f) * rsq + rsq;
+  rsq = ((-0.5f * arg * rsq) * rsq + 0.5f) * rsq + rsq;
+  float sqt = rsq * arg;
+  float err = sqt * -sqt + arg;
+  sqt = (0.5f * rsq * err + sqt);
+  return sqt * scale_out;
+}
+
 /* ---------------------------------------------------------------- FP64 SVD */
 
 static double det3d(const double m[3][3]) {

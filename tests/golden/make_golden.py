@@ -1,0 +1,73 @@
+"""Generates the golden fixtures in tests/golden/ by running the REFERENCE's own MPM path
+(oracle/_ref/zsref_cli, compiled from the zpc sources by oracle/build_ref.sh).
+
+The reference ships no MPM tests or golden data, so these fixtures are outputs of the
+reference itself on seeded synthetic inputs:
+  ref_substep_fc.npz / ref_substep_dp.npz   5 substeps, sequential policy, canonical block
+                                            order: inputs, particle outputs, active keys, grid
+  ref_svd.npz                               math::svd_3d on 256 matrices
+  ref_stress.npz                            compute_stress_fixedcorotated / _sand on 256 F
+  ref_activation.npz                        ComputeSparsity + EnlargeSparsity keys and slots
+Run:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+
+from oracle import reference  # noqa: E402
+from zsmpm_b200 import scenes  # noqa: E402
+
+
+def random_F(rng, n, spread):
+    q = rng.normal(size=(2, n, 4))
+    q /= np.linalg.norm(q, axis=2, keepdims=True)
+
+    def rot(q):
+        w, x, y, z = q.T
+        return np.stack([1 - 2 * (y * y + z * z), 2 * (x * y + w * z), 2 * (x * z - w * y),
+                         2 * (x * y - w * z), 1 - 2 * (x * x + z * z), 2 * (y * z + w * x),
+                         2 * (x * z + w * y), 2 * (y * z - w * x), 1 - 2 * (x * x + y * y)], 1).reshape(-1, 3, 3)
+    s = np.exp(rng.uniform(-spread, spread, size=(n, 3)))
+    A = rot(q[0]) @ (s[:, :, None] * np.eye(3)) @ rot(q[1])
+    return np.ascontiguousarray(A.transpose(0, 2, 1).reshape(n, 9)).astype(np.float32)
+
+
+def main() -> None:
+    if not reference.available():
+        raise SystemExit("oracle/_ref/zsref_cli is missing: run oracle/build_ref.sh first")
+    for model, name in ((0, "fc"), (1, "dp")):
+        spec = scenes.small_scene(model=model, mode=1, velocity=(0.4, -0.3, 0.2))
+        p = scenes.generate(spec)
+        r = reference.run(spec, p, 5, policy=reference.POLICY_SEQ)
+        assert r.status == 0
+        np.savez_compressed(HERE / f"ref_substep_{name}.npz", m=p.m, x0=p.x, v0=p.v, C0=p.C, F0=p.F,
+                            plastic0=p.plastic, x=r.x, v=r.v, C=r.C, F=r.F, logJp=r.logJp,
+                            keys=r.keys, grid=r.grid, steps=5, model=model)
+    rng = np.random.default_rng(42)
+    A = np.concatenate([random_F(rng, 192, 0.5), random_F(rng, 64, 0.02)])
+    U, S, V = reference.svd(A)
+    np.savez_compressed(HERE / "ref_svd.npz", A=A, U=U, S=S, V=V)
+    spec_dp = scenes.small_scene(model=1, mode=1)
+    F = random_F(rng, 256, 0.2)
+    lj = rng.uniform(-0.05, 0.05, 256).astype(np.float32)
+    PF_dp, F_dp, lj_dp = reference.stress(spec_dp, F, lj)
+    spec_fc = scenes.small_scene(model=0)
+    PF_fc, _, _ = reference.stress(spec_fc, F, np.zeros(256, np.float32))
+    np.savez_compressed(HERE / "ref_stress.npz", F=F, logJp=lj, PF_fc=PF_fc, PF_dp=PF_dp, F_dp=F_dp,
+                        logJp_dp=lj_dp)
+    spec = scenes.small_scene(model=0, n_side=0.25, velocity=(0, 0, 0), ppc=1, seed=3)
+    p = scenes.generate(spec)
+    keys, slots, npb, ts = reference.activate(p.x, spec.dx, 64)
+    np.savez_compressed(HERE / "ref_activation.npz", x=p.x, dx=spec.dx, expected=64, keys=keys,
+                        slots=slots, nparblocks=npb, table_size=ts)
+    print("wrote", sorted(f.name for f in HERE.glob("*.npz")))
+
+
+if __name__ == "__main__":
+    main()

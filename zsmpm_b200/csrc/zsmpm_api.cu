@@ -160,7 +160,7 @@ zsmpm_status allocate_blocks(zsmpm_scene *s, int64_t n) {
   const int64_t T = next_2pow(expected) * 16;
   if (T > (int64_t)1 << 30) return fail(ZSMPM_ERR_CAPACITY, "hash table too large");
   d.prm.table_size = (int)T;
-  d.prm.nb_cap = (int)std::min<int64_t>(T - 20, std::max<int64_t>(65536, n / 16));
+  d.prm.nb_cap = (int)std::max<int64_t>(1, std::min<int64_t>(T - 20, std::max<int64_t>(65536, n / 16)));
   d.prm.bitmap_cap = 1 << 23;  // 2^28 dense block positions
   const int64_t nbc = d.prm.nb_cap;
   ZS_ALLOC(d.pk, T, "alloc table pk");

@@ -47,10 +47,12 @@ __device__ int table_insert(const scene_device &s, uint64_t key, int3 k, int *co
       if (idx < s.prm.nb_cap) {
         s.ins_pk[idx] = key;
         s.ins_slot[idx] = slot;
+        s.tidx[slot] = idx;
       } else {
+        // beyond the block capacity: keep the key unqueryable so no kernel indexes past it
         set_status(s.ctr, kStatusCapacity);
+        s.tidx[slot] = -1;
       }
-      s.tidx[slot] = idx;
       return idx;
     }
     if (prev == key) return -1;
@@ -337,6 +339,7 @@ __global__ void __launch_bounds__(kThreads) k_neighbors(scene_device s) {
 __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
   const int lane = threadIdx.x & 31;
   const int n = s.prm.n;
+  const int nb = s.ctr[kCtrBlocks];
   const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int warps = grid_threads() >> 5;
   for (int base = warp_global * 32; base < n; base += warps * 32) {
@@ -353,8 +356,8 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
     int blk = -1;
     if (valid && lane == leader) blk = table_query(s, key, b);
     blk = __shfl_sync(kFull, blk, leader);
-    if (valid && blk < 0) set_status(s.ctr, kStatusMissingBlock);
-    const bool ok = valid && blk >= 0;
+    if (valid && (blk < 0 || blk >= nb)) set_status(s.ctr, kStatusMissingBlock);
+    const bool ok = valid && blk >= 0 && blk < nb;
     // block counts, one atomic per distinct block of the warp
     const unsigned bpeers = __match_any_sync(kFull, ok ? blk : -1 - lane);
     if (ok && lane == __ffs(bpeers) - 1) atomicAdd(&s.block_count[blk], __popc(bpeers));
