@@ -234,6 +234,27 @@ ZSMPM_API zsmpm_status zsmpm_svd3(const float *A, float *U, float *S, float *V, 
 ZSMPM_API zsmpm_status zsmpm_constitutive(const zsmpm_material *mat, float *F, float *plastic,
                                           float *tau, int64_t count, void *stream);
 
+/* ---- allocation-free variant --------------------------------------------------- */
+/* Block activation without any device allocation.  No counterpart in the reference: it is
+ * for callers that cannot call cudaMalloc at this point -- hosts whose own memory pool has
+ * already reserved the GPU, code running while a CUDA graph is being captured, plug-in or
+ * real-time loops that forbid allocation after start-up.  Same result as
+ * zsmpm_activate_blocks: the active block keys of the particles at x (device pointer,
+ * 3 floats per particle as in zs::Particles "x") after the +{0,1}^3 enlargement, ascending
+ * by (bx, by, bz), written to keys_out (device, cap_blocks x 3 int32), and their count to
+ * *count_out (device int32), or a negative code: -1 table, block or bounding-box limit
+ * reached, -2 more than cap_blocks blocks, -3 a position is NaN/Inf or out of range.
+ * Its scratch is one fixed array of about 3 MB in device memory, held on every GPU that
+ * loads the library until the process exits; it limits a call to 1,048,576 particles
+ * (larger n is rejected with ZSMPM_ERR_CAPACITY), 32,748 active blocks and an active-block
+ * bounding box of 2^21 positions.  The first call on a device looks up the array's device
+ * address with that device current, so make that first call before any stream capture.
+ * All calls share the array and each overwrites the last one's contents; calls whose work
+ * overlaps on the GPU race and give undefined results. */
+ZSMPM_API zsmpm_status zsmpm_activate_blocks_noalloc(const float *x, int64_t n, float dx,
+                                                     int32_t *keys_out, int32_t cap_blocks,
+                                                     int32_t *count_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -92,6 +92,7 @@ SIGNATURES = {
     "zsmpm_kernels_per_substep": (C.c_int32, [_P]),
     "zsmpm_svd3": (_S, [_P, _P, _P, _P, C.c_int64, _P]),
     "zsmpm_constitutive": (_S, [C.POINTER(Material), _P, _P, _P, C.c_int64, _P]),
+    "zsmpm_activate_blocks_noalloc": (_S, [_P, C.c_int64, C.c_float, _P, C.c_int32, _P, _P]),
 }
 
 _lib = None

@@ -238,6 +238,12 @@ zsmpm_status substep_enqueue(zsmpm_scene *s, cudaStream_t st) {
 
 }  // namespace
 
+namespace zsmpm {
+int record_error(int status, const char *message) {
+  return (int)fail((zsmpm_status)status, message ? message : "");
+}
+}  // namespace zsmpm
+
 extern "C" {
 
 ZSMPM_API const char *zsmpm_last_error_string(void) { return g_error.c_str(); }

@@ -101,6 +101,12 @@ cudaError_t launch_export_tilevector(const scene_device &s, float *base, int nch
                                      int off_x, int off_v, int off_C, int off_F, int off_pl,
                                      cudaStream_t st);
 cudaError_t launch_export_order(const scene_device &s, int *order, cudaStream_t st);
+// block activation of AoS positions into a caller-provided scene_device view (used by the
+// allocation-free entry point); writes the sorted keys and the count (or a negative code)
+cudaError_t launch_activate_static(scene_device &s, const float *x, int *keys_out, int cap,
+                                   int *count_out, cudaStream_t st);
+// records the calling thread's error message (read back by zsmpm_last_error_string)
+int record_error(int status, const char *message);
 cudaError_t launch_svd_batch(const float *A, float *U, float *S, float *V, long long count,
                              cudaStream_t st);
 cudaError_t launch_constitutive_batch(const material_dev &mat, float *F, float *plastic,

@@ -892,6 +892,82 @@ __global__ void k_constitutive_batch(material_dev mat, float *F, float *pl, floa
   }
 }
 
+// ----------------------------------------------------------------- allocation-free activation
+// Kernels used only by zsmpm_activate_blocks_noalloc (zsmpm_static.cu): particle positions
+// come as the reference's Particles "x" layout (3 floats per particle) instead of the
+// scene's float4 buffer, and the result is copied out to the caller's arrays.
+
+// Zeroes the bitmap and the status word of the static scratch before a call.
+__global__ void __launch_bounds__(kThreads) k_static_reset(scene_device s) {
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < s.prm.bitmap_cap; w += grid_threads())
+    s.bitmap[w] = 0u;
+  if (blockIdx.x == 0 && threadIdx.x == 0) s.ctr[kCtrStatus] = 0;
+}
+
+// ComputeSparsity over AoS positions, one insert per distinct block key of a warp.
+__global__ void __launch_bounds__(kThreads) k_insert_aos(scene_device s, const float *x) {
+  const int lane = threadIdx.x & 31;
+  const int n = s.prm.n;
+  int3 lo = make_int3(0x7fffffff, 0x7fffffff, 0x7fffffff);
+  int3 hi = make_int3(-0x7fffffff, -0x7fffffff, -0x7fffffff);
+  const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warps = grid_threads() >> 5;
+  for (int base = warp_global * 32; base < n; base += warps * 32) {
+    const int i = base + lane;
+    uint64_t key = kEmptyKey - 1 - lane;
+    int3 c, b = make_int3(0, 0, 0);
+    bool valid = false;
+    if (i < n) {
+      const float4 pos = make_float4(x[3 * (size_t)i], x[3 * (size_t)i + 1], x[3 * (size_t)i + 2], 0.f);
+      if (cell_of(s.prm, pos, c, b)) {
+        key = pack_key(b.x, b.y, b.z);
+        valid = true;
+      } else {
+        set_status(s.ctr, kStatusOutOfDomain);
+      }
+    }
+    const unsigned peers = __match_any_sync(kFull, key);
+    if (valid && lane == __ffs(peers) - 1) {
+      table_insert(s, key, b, &s.ctr[kCtrParticleBlocks], 0);
+      lo = make_int3(min(lo.x, b.x), min(lo.y, b.y), min(lo.z, b.z));
+      hi = make_int3(max(hi.x, b.x), max(hi.y, b.y), max(hi.z, b.z));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo.x = min(lo.x, __shfl_xor_sync(kFull, lo.x, o));
+    lo.y = min(lo.y, __shfl_xor_sync(kFull, lo.y, o));
+    lo.z = min(lo.z, __shfl_xor_sync(kFull, lo.z, o));
+    hi.x = max(hi.x, __shfl_xor_sync(kFull, hi.x, o));
+    hi.y = max(hi.y, __shfl_xor_sync(kFull, hi.y, o));
+    hi.z = max(hi.z, __shfl_xor_sync(kFull, hi.z, o));
+  }
+  if (lane == 0 && lo.x != 0x7fffffff) {
+    atomicMin(&s.ctr[kCtrBoxLo + 0], lo.x);
+    atomicMin(&s.ctr[kCtrBoxLo + 1], lo.y);
+    atomicMin(&s.ctr[kCtrBoxLo + 2], lo.z);
+    atomicMax(&s.ctr[kCtrBoxHi + 0], hi.x);
+    atomicMax(&s.ctr[kCtrBoxHi + 1], hi.y);
+    atomicMax(&s.ctr[kCtrBoxHi + 2], hi.z);
+  }
+}
+
+// Copies the sorted keys out; count_out = block count, or -1 (table full / capacity /
+// bounding box), -2 (more blocks than cap), -3 (a position was NaN/Inf or out of range).
+__global__ void __launch_bounds__(kThreads) k_export_keys(scene_device s, int *keys_out, int cap,
+                                                           int *count_out) {
+  const int st = s.ctr[kCtrStatus];
+  const int nb = s.ctr[kCtrBlocks];
+  int code = nb;
+  if (st & kStatusOutOfDomain) code = -3;
+  else if (st & (kStatusTableFull | kStatusCapacity | kStatusBitmap)) code = -1;
+  else if (nb > cap) code = -2;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *count_out = code;
+  if (code < 0) return;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * nb; t += grid_threads())
+    keys_out[t] = s.active_keys[t];
+}
+
 int g_num_sms = 0;
 int num_sms() {
   if (g_num_sms == 0) {
@@ -986,6 +1062,22 @@ cudaError_t launch_export_tilevector(const scene_device &s, float *base, int nch
 
 cudaError_t launch_export_order(const scene_device &s, int *order, cudaStream_t st) {
   k_export_order<<<num_sms() * 4, kThreads, 0, st>>>(s, order);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_activate_static(scene_device &s, const float *x, int *keys_out, int cap,
+                                   int *count_out, cudaStream_t st) {
+  const int sm = num_sms();
+  k_static_reset<<<sm, kThreads, 0, st>>>(s);
+  k_begin<<<sm * 4, kThreads, 0, st>>>(s);
+  k_insert_aos<<<sm * 8, kThreads, 0, st>>>(s, x);
+  k_enlarge<<<sm * 2, kThreads, 0, st>>>(s);
+  k_bitmap_prepare<<<1, 32, 0, st>>>(s);
+  k_bitmap_set<<<sm * 2, kThreads, 0, st>>>(s);
+  cudaError_t e = device_scan(load_popc{s.bitmap}, &s.ctr[kCtrWords], s.scan_part, s.word_prefix, st);
+  if (e != cudaSuccess) return e;
+  k_assign_ranks<<<sm * 2, kThreads, 0, st>>>(s);
+  k_export_keys<<<sm, kThreads, 0, st>>>(s, keys_out, cap, count_out);
   return cudaGetLastError();
 }
 
