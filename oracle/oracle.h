@@ -82,9 +82,8 @@ int oracle_activate(int n, const float *x, float dx, int table_expected, int cap
 int32_t oracle_hash_slot(int32_t kx, int32_t ky, int32_t kz, int32_t table_size);
 
 /* Particle binning order of the CUDA path, restated: given per-particle block ranks and
- * local stencil cells (0..511), returns order[] (slot -> particle index) sorted by
- * (block, rank within cell, cell) with particles of one cell kept in index order, plus
- * block_start[nblocks+1]. */
+ * local stencil cells (0..511), returns order[] (slot -> particle index), a stable sort by
+ * (block, cell), plus block_start[nblocks+1]. */
 void oracle_bin_order(int n, int nblocks, const int32_t *block, const int32_t *cell,
                       int32_t *order, int32_t *block_start);
 

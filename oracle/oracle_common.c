@@ -175,41 +175,21 @@ int oracle_activate(int n, const float *x, float dx, int table_expected, int cap
   return st;
 }
 
-/* Binning order of the CUDA path: particles grouped by block; inside a block, by rank
- * within their stencil cell first and by cell second, so that consecutive particles sit in
- * distinct cells; particles of one cell keep increasing index order. */
+/* Binning order of the CUDA path: particles grouped by block, then by stencil-origin cell
+ * ascending, particles of one cell in increasing index order (a stable sort by
+ * (block, cell)); block_start[b] is the first slot of block b. */
 void oracle_bin_order(int n, int nblocks, const int32_t *block, const int32_t *cell,
                       int32_t *order, int32_t *block_start) {
   const size_t ncells = (size_t)nblocks * 512;
-  int32_t *cnt = (int32_t *)calloc(ncells, sizeof(int32_t));
-  int32_t *first = (int32_t *)malloc(sizeof(int32_t) * (ncells + 1));
-  int32_t *members = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
-  for (int i = 0; i != n; ++i) cnt[(size_t)block[i] * 512 + cell[i]]++;
-  /* cell-major lists of particle indices, each list in increasing index order */
-  first[0] = 0;
-  for (size_t k = 0; k != ncells; ++k) first[k + 1] = first[k] + cnt[k];
-  {
-    int32_t *fill = (int32_t *)calloc(ncells, sizeof(int32_t));
-    for (int i = 0; i != n; ++i) {
-      size_t k = (size_t)block[i] * 512 + cell[i];
-      members[first[k] + fill[k]++] = i;
-    }
-    free(fill);
+  int32_t *first = (int32_t *)calloc(ncells + 1, sizeof(int32_t));
+  int32_t *fill = (int32_t *)calloc(ncells, sizeof(int32_t));
+  for (int i = 0; i != n; ++i) first[(size_t)block[i] * 512 + cell[i] + 1]++;
+  for (size_t k = 0; k != ncells; ++k) first[k + 1] += first[k];
+  for (int i = 0; i != n; ++i) {
+    size_t k = (size_t)block[i] * 512 + cell[i];
+    order[first[k] + fill[k]++] = i;
   }
-  /* emit row r (the r-th particle of every cell holding more than r) cell by cell */
-  block_start[0] = 0;
-  int32_t s = 0;
-  for (int b = 0; b != nblocks; ++b) {
-    const int32_t *c = &cnt[(size_t)b * 512];
-    int32_t maxc = 0;
-    for (int k = 0; k != 512; ++k)
-      if (c[k] > maxc) maxc = c[k];
-    for (int32_t r = 0; r != maxc; ++r)
-      for (int k = 0; k != 512; ++k)
-        if (c[k] > r) order[s++] = members[first[(size_t)b * 512 + k] + r];
-    block_start[b + 1] = s;
-  }
-  free(members);
+  for (int b = 0; b <= nblocks; ++b) block_start[b] = first[(size_t)b * 512];
+  free(fill);
   free(first);
-  free(cnt);
 }

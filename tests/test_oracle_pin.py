@@ -105,24 +105,16 @@ def test_hash_slot_formula():
 
 
 def test_bin_order_definition():
-    """Rows of (rank within cell, cell): consecutive slots of a block sit in distinct cells."""
+    """A stable sort by (block, cell): cells ascending inside a block, indices ascending in a cell."""
     from oracle import restated
     rng = np.random.default_rng(3)
     n = 5000
     block = rng.integers(0, 4, n).astype(np.int32)
-    cell = rng.integers(0, 64, n).astype(np.int32)
+    cell = rng.integers(0, 512, n).astype(np.int32)
     order, bstart = restated.bin_order(block, cell, 4)
-    assert sorted(order.tolist()) == list(range(n))
-    for b in range(4):
-        seg = order[bstart[b]:bstart[b + 1]]
-        assert np.all(block[seg] == b)
-        rank = {}
-        keys = []
-        for i in np.sort(seg):
-            rank[i] = rank.get(("c", cell[i]), 0)
-            rank[("c", cell[i])] = rank[i] + 1
-        keys = [(rank[i], cell[i]) for i in seg]
-        assert keys == sorted(keys)
+    expected = np.lexsort((np.arange(n), cell, block))
+    assert np.array_equal(order, expected)
+    assert np.array_equal(bstart, np.searchsorted(block[expected], np.arange(5)))
 
 
 @pytest.mark.slow

@@ -287,6 +287,12 @@ ZSMPM_API zsmpm_status zsmpm_scene_create(const zsmpm_scene_desc *desc, zsmpm_sc
   p.wall_cells = desc->wall_cells;
   p.mat = make_material(desc->material);
   for (auto &ev : s->ev) cudaEventCreate(&ev);
+  e = prepare_kernels();
+  if (e != cudaSuccess) {
+    release(s);
+    delete s;
+    return cuda_fail(e, "kernel attributes");
+  }
   *out = s;
   return ZSMPM_OK;
 }

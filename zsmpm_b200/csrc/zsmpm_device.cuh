@@ -313,21 +313,26 @@ __device__ __forceinline__ void constitutive(const material_dev &mat, float *F, 
     for (int i = 0; i < 3; ++i) eh[i] = eps[i] - tr / 3.f;
     const float ehn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2]);
     const float smu = 2.f * mat.mu;
+    // the projected log-strain is the exponent itself; the reference takes log(exp(H)),
+    // which differs from H only by the rounding of expf and logf
     if (tr >= 0.f) {
       const float e = expf(mat.cohesion);
       Ns[0] = Ns[1] = Ns[2] = e;
+      logNs[0] = logNs[1] = logNs[2] = mat.cohesion;
       if (mat.volume_correction) plastic = mat.beta * sum_eps + plastic;
     } else if (mat.mu != 0.f) {
       plastic = 0.f;
       const float dg = ehn + (3.f * mat.lambda + smu) / smu * tr * mat.yield_surface;
       const float f = dg <= 0.f ? 0.f : dg / ehn;
 #pragma unroll
-      for (int i = 0; i < 3; ++i) Ns[i] = expf(eps[i] - f * eh[i] + mat.cohesion);
+      for (int i = 0; i < 3; ++i) {
+        logNs[i] = eps[i] - f * eh[i] + mat.cohesion;
+        Ns[i] = expf(logNs[i]);
+      }
     } else {
       Ns[0] = Ns[1] = Ns[2] = 0.f;
+      logNs[0] = logNs[1] = logNs[2] = 0.f;
     }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) logNs[i] = logf(Ns[i]);
     const float trl = logNs[0] + logNs[1] + logNs[2];
     // P F_new^T = U diag(Ph * Ns) U^T with Ph = (2 mu log Ns + lambda tr log Ns) / Ns
     float PhNs[3];

@@ -79,6 +79,8 @@ struct scene_device {
 
 constexpr int kScanCtas = 256;
 
+// sets per-device kernel attributes (dynamic shared memory sizes); call with the device current
+cudaError_t prepare_kernels();
 // launchers (all asynchronous on `st`)
 cudaError_t launch_activate(scene_device &s, cudaStream_t st);
 cudaError_t launch_bin(scene_device &s, cudaStream_t st);

@@ -407,25 +407,22 @@ __global__ void __launch_bounds__(kThreads) k_bin_scatter(scene_device s) {
   }
 }
 
-// Final particle order of a block: rows r = 0, 1, ... each holding the r-th particle (by
-// upload index) of every cell with more than r particles, cells ascending.  Consecutive
-// slots therefore sit in distinct cells.  Also zeroes the block's grid, counts for the
-// next substep.
+// Final particle order of a block: cells ascending, the particles of a cell in increasing
+// upload index (a stable sort by (block, cell)).  Also zeroes the block's grid and the
+// counts for the next substep.
 __global__ void __launch_bounds__(512) k_bin_finalize(scene_device s) {
   constexpr int kMaxList = 24;
-  __shared__ int sm[512 / 32 + 1];
-  __shared__ int s_b, s_max;
+  __shared__ int s_b;
   const int nb = s.ctr[kCtrBlocks];
   const int t = threadIdx.x;
   for (;;) {
     const int b = grab_block(&s.ctr[kCtrWork + kWorkFinalize], &s_b);
     if (b >= nb) break;
-    if (t == 0) s_max = 0;
     const int c = s.cell_count[b * 512 + t];
     const int cs = s.cell_start[b * 512 + t];
     s.cell_count[b * 512 + t] = 0;
-    int li[kMaxList], lid[kMaxList];
     if (c <= kMaxList) {
+      int li[kMaxList], lid[kMaxList];
       for (int r = 0; r < c; ++r) {
         const int i = s.tmp[cs + r];
         const int id = s.cur.id[i];
@@ -438,6 +435,7 @@ __global__ void __launch_bounds__(512) k_bin_finalize(scene_device s) {
         lid[q] = id;
         li[q] = i;
       }
+      for (int r = 0; r < c; ++r) s.src[cs + r] = li[r];
     } else {
       // long lists (strongly compressed cells): insertion sort in place in global memory
       for (int r = 1; r < c; ++r) {
@@ -450,19 +448,7 @@ __global__ void __launch_bounds__(512) k_bin_finalize(scene_device s) {
         }
         s.tmp[cs + q] = i;
       }
-    }
-    __syncthreads();
-    atomicMax(&s_max, c);
-    __syncthreads();
-    const int maxc = s_max;
-    const int bs = s.block_start[b];
-    int row = 0;
-    for (int r = 0; r < maxc; ++r) {
-      const int flag = c > r ? 1 : 0;
-      int total;
-      const int ex = cta_exclusive_scan<512>(flag, total, sm);
-      if (flag) s.src[bs + row + ex] = c <= kMaxList ? li[r] : s.tmp[cs + r];
-      row += total;
+      for (int r = 0; r < c; ++r) s.src[cs + r] = s.tmp[cs + r];
     }
     float4 *g = reinterpret_cast<float4 *>(s.grid + (size_t)b * kGridChannels * 512);
     g[t] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -471,97 +457,204 @@ __global__ void __launch_bounds__(512) k_bin_finalize(scene_device s) {
 }
 
 // ----------------------------------------------------------------- P2G
-// One CTA per block (persistent): scatter the block's particles into a 12^3 halo of the
-// grid in shared memory (cells [8b, 8b+12) per axis, covering b and its +1 neighbours),
-// then flush the halo with 16-byte vector reductions into the 8 neighbour blocks.
-// Grid channels: m and p = sum W (m v + A (x_i - x_p)), which is the reference's
-// mv + rhs (P2G.hpp:108-125) with A = m C - (4 dt/dx^2) tau precomputed by G2P.
-__global__ void __launch_bounds__(kThreads) k_p2g(scene_device s) {
-  __shared__ float sh[kGridChannels][kHalo][kHalo][kHalo];
-  __shared__ int s_b;
+// One CTA per block (persistent).  The block's 512 cells are processed in chunks of 64:
+//  1. the CTA gathers the chunk's particles and stages, per particle, its 3x3 B-spline
+//     weights, m and the affine terms (q, A dx) in shared memory, laid out [field][rank][cell]
+//     so that lanes reading one rank of consecutive cells hit consecutive banks;
+//  2. one thread per (cell, channel) sums the cell's particles into 27 registers -- all
+//     particles of a cell share the same 27 stencil nodes -- and adds them to a 12^3 halo of
+//     the grid in shared memory (cells [8b, 8b+12) per axis: b and its +1 neighbours).
+// The halo is flushed with 16-byte vector reductions into the 8 neighbour blocks.  Grid
+// channels: m and p = sum W (m v + A (x_i - x_p)), the reference's mv + rhs
+// (P2G.hpp:108-125) with A = m C - (4 dt/dx^2) tau precomputed by G2P.
+constexpr int kP2GChunk = 64;     // cells per chunk
+constexpr int kP2GRanks = 12;     // particles per cell staged per chunk (more go direct)
+constexpr int kP2GFields = 22;    // w[9], m, q[3], ax[3], ay[3], az[3]
+constexpr int kP2GRow = kP2GChunk + 1;  // padded row: rank r of cell c in bank (r + c) % 32
+constexpr int kP2GThreads = 256;  // 4 channels x 64 cells
+
+struct p2g_particle {
+  float m, w[3][3], q[3], ax[3], ay[3], az[3];
+  int hb[3];
+};
+
+__device__ __forceinline__ void p2g_prepare(const scene_device &s, int i, int ox, int oy, int oz,
+                                            p2g_particle &pp) {
   const scene_params &p = s.prm;
+  const float4 xm = s.cur.xm[i];
+  const float4 vv = s.cur.v[i];
+  float A[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) A[k] = s.cur.A[(size_t)k * p.cap + i];
+  const float X[3] = {__fdiv_rn(xm.x, p.dx), __fdiv_rn(xm.y, p.dx), __fdiv_rn(xm.z, p.dx)};
+  float lp[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float base = floorf(X[d] - 0.5f);
+    const float f = X[d] - base;
+    pp.hb[d] = (int)base - (d == 0 ? ox : d == 1 ? oy : oz);
+    pp.w[d][0] = 0.5f * (1.5f - f) * (1.5f - f);
+    const float f1 = f - 1.f;
+    pp.w[d][1] = 0.75f - f1 * f1;
+    const float f2 = 0.5f + f1;
+    pp.w[d][2] = 0.5f * f2 * f2;
+    lp[d] = f * p.dx;
+  }
+  pp.m = xm.w;
+  const float vel[3] = {vv.x, vv.y, vv.z};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    pp.q[d] = pp.m * vel[d] - (A[d] * lp[0] + A[3 + d] * lp[1] + A[6 + d] * lp[2]);
+    pp.ax[d] = A[d] * p.dx;
+    pp.ay[d] = A[3 + d] * p.dx;
+    pp.az[d] = A[6 + d] * p.dx;
+  }
+}
+
+// all 27 nodes x 4 channels of one particle straight into the shared halo
+__device__ __forceinline__ void p2g_direct(float *shf, const p2g_particle &pp, int *ctr) {
+  if (pp.hb[0] < 0 || pp.hb[0] > kHalo - 3 || pp.hb[1] < 0 || pp.hb[1] > kHalo - 3 || pp.hb[2] < 0 ||
+      pp.hb[2] > kHalo - 3) {
+    set_status(ctr, kStatusMissingBlock);
+    return;
+  }
+  for (int ii = 0; ii < 3; ++ii)
+    for (int jj = 0; jj < 3; ++jj)
+      for (int kk = 0; kk < 3; ++kk) {
+        const float W = pp.w[0][ii] * pp.w[1][jj] * pp.w[2][kk];
+        const int h = ((pp.hb[0] + ii) * kHalo + (pp.hb[1] + jj)) * kHalo + pp.hb[2] + kk;
+        atomicAdd(&shf[h], W * pp.m);
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          atomicAdd(&shf[(1 + d) * kHaloCells + h],
+                    W * (pp.q[d] + (float)ii * pp.ax[d] + (float)jj * pp.ay[d] + (float)kk * pp.az[d]));
+      }
+}
+
+constexpr size_t kP2GSmemBytes =
+    sizeof(float) * (kGridChannels * kHaloCells + kP2GFields * kP2GRanks * kP2GRow) +
+    sizeof(int) * (kP2GChunk + 1);
+
+__global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
+  extern __shared__ float p2g_smem[];
+  float *sh = p2g_smem;
+  auto stg = reinterpret_cast<float(*)[kP2GRanks][kP2GRow]>(p2g_smem + kGridChannels * kHaloCells);
+  int *s_cs = reinterpret_cast<int *>(p2g_smem + kGridChannels * kHaloCells +
+                                      kP2GFields * kP2GRanks * kP2GRow);
+  __shared__ int s_b;
   const int nb = s.ctr[kCtrBlocks];
-  float *shf = &sh[0][0][0][0];
+  const int t = threadIdx.x;
+  const int my_cell = t & (kP2GChunk - 1), my_ch = t >> 6;
   for (;;) {
     const int b = grab_block(&s.ctr[kCtrWork + kWorkP2G], &s_b);
     if (b >= nb) break;
     const int start = s.block_start[b], end = s.block_start[b + 1];
     if (start == end) continue;
-    for (int q = threadIdx.x; q < kGridChannels * kHaloCells; q += blockDim.x) shf[q] = 0.f;
-    __syncthreads();
+    for (int q = t; q < kGridChannels * kHaloCells; q += blockDim.x) sh[q] = 0.f;
     const int3 bk = unpack_key(s.blk_pk[b]);
     const int ox = bk.x * 8, oy = bk.y * 8, oz = bk.z * 8;
-    for (int slot = start + threadIdx.x; slot < end; slot += blockDim.x) {
-      const int i = s.src[slot];
-      const float4 xm = s.cur.xm[i];
-      const float4 vv = s.cur.v[i];
-      float A[9];
+    for (int chunk = 0; chunk < 512 / kP2GChunk; ++chunk) {
+      const int cell0 = chunk * kP2GChunk;
+      __syncthreads();  // previous chunk's staging fully consumed (and halo zeroed)
+      if (t <= kP2GChunk) s_cs[t] = cell0 + t < 512 ? s.cell_start[b * 512 + cell0 + t] : end;
+      __syncthreads();
+      // ---- phase 1: consecutive threads take consecutive slots (coalesced gathers)
+      const int c0 = s_cs[0], c1 = s_cs[kP2GChunk];
+      for (int slot = c0 + t; slot < c1; slot += blockDim.x) {
+        int lo = 0, hi = kP2GChunk;  // last cell whose start is <= slot
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (s_cs[mid] <= slot) lo = mid;
+          else hi = mid;
+        }
+        const int cl = lo, r = slot - s_cs[lo], cell = cell0 + cl;
+        const int ex = (cell >> 6) + 1, ey = ((cell >> 3) & 7) + 1, ez = (cell & 7) + 1;
+        p2g_particle pp;
+        p2g_prepare(s, s.src[slot], ox, oy, oz, pp);
+        if (r >= kP2GRanks || pp.hb[0] != ex || pp.hb[1] != ey || pp.hb[2] != ez) {
+          // beyond the staged ranks, or a stencil origin that rounding moved off the
+          // cell: scatter this particle directly and stage a zero-mass stand-in
+          p2g_direct(sh, pp, s.ctr);
+          if (r < kP2GRanks)
+            for (int f = 0; f < kP2GFields; ++f) stg[f][r][cl] = 0.f;
+          continue;
+        }
 #pragma unroll
-      for (int k = 0; k < 9; ++k) A[k] = s.cur.A[(size_t)k * p.cap + i];
-      const float X[3] = {__fdiv_rn(xm.x, p.dx), __fdiv_rn(xm.y, p.dx), __fdiv_rn(xm.z, p.dx)};
-      int hb[3];
-      float w[3][3], lp[3];
+        for (int a = 0; a < 3; ++a)
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const float base = floorf(X[d] - 0.5f);
-        const float f = X[d] - base;
-        hb[d] = (int)base - (d == 0 ? ox : d == 1 ? oy : oz);
-        w[d][0] = 0.5f * (1.5f - f) * (1.5f - f);
-        const float f1 = f - 1.f;
-        w[d][1] = 0.75f - f1 * f1;
-        const float f2 = 0.5f + f1;
-        w[d][2] = 0.5f * f2 * f2;
-        lp[d] = f * p.dx;
+          for (int c = 0; c < 3; ++c) stg[3 * a + c][r][cl] = pp.w[a][c];
+        stg[9][r][cl] = pp.m;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          stg[10 + d][r][cl] = pp.q[d];
+          stg[13 + d][r][cl] = pp.ax[d];
+          stg[16 + d][r][cl] = pp.ay[d];
+          stg[19 + d][r][cl] = pp.az[d];
+        }
       }
-      if (hb[0] < 0 || hb[0] > kHalo - 3 || hb[1] < 0 || hb[1] > kHalo - 3 || hb[2] < 0 ||
-          hb[2] > kHalo - 3) {
-        set_status(s.ctr, kStatusMissingBlock);
-        continue;
-      }
-      const float m = xm.w;
-      // value at node offset (i,j,k): q + i*ax + j*ay + k*az
-      float q[3], ax[3], ay[3], az[3];
+      __syncthreads();
+      // ---- phase 2: thread (cell, channel) sums the staged particles of its cell
+      {
+        const int cnt = min(s_cs[my_cell + 1] - s_cs[my_cell], kP2GRanks);
+        if (cnt > 0) {
+          float acc[27];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        q[d] = m * (d == 0 ? vv.x : d == 1 ? vv.y : vv.z) - (A[d] * lp[0] + A[3 + d] * lp[1] + A[6 + d] * lp[2]);
-        ax[d] = A[d] * p.dx;
-        ay[d] = A[3 + d] * p.dx;
-        az[d] = A[6 + d] * p.dx;
-      }
+          for (int n = 0; n < 27; ++n) acc[n] = 0.f;
+          const int d = my_ch - 1;  // p channel index, -1 for mass
+          for (int r = 0; r < cnt; ++r) {
+            float w[3][3];
 #pragma unroll
-      for (int ii = 0; ii < 3; ++ii) {
-        float qi[3];
+            for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int d = 0; d < 3; ++d) qi[d] = q[d] + (float)ii * ax[d];
+              for (int c = 0; c < 3; ++c) w[a][c] = stg[3 * a + c][r][my_cell];
+            float q, ax, ay, az;
+            if (my_ch == 0) {
+              q = stg[9][r][my_cell];
+              ax = ay = az = 0.f;
+            } else {
+              q = stg[10 + d][r][my_cell];
+              ax = stg[13 + d][r][my_cell];
+              ay = stg[16 + d][r][my_cell];
+              az = stg[19 + d][r][my_cell];
+            }
 #pragma unroll
-        for (int jj = 0; jj < 3; ++jj) {
-          float qij[3];
+            for (int ii = 0; ii < 3; ++ii) {
+              const float qi = q + (float)ii * ax;
 #pragma unroll
-          for (int d = 0; d < 3; ++d) qij[d] = qi[d] + (float)jj * ay[d];
-          const float wij = w[0][ii] * w[1][jj];
-          const int hrow = ((hb[0] + ii) * kHalo + (hb[1] + jj)) * kHalo + hb[2];
+              for (int jj = 0; jj < 3; ++jj) {
+                const float qij = qi + (float)jj * ay;
+                const float wij = w[0][ii] * w[1][jj];
 #pragma unroll
-          for (int kk = 0; kk < 3; ++kk) {
-            const float W = wij * w[2][kk];
-            const int h = hrow + kk;
-            atomicAdd(&shf[0 * kHaloCells + h], W * m);
-            atomicAdd(&shf[1 * kHaloCells + h], W * (qij[0] + (float)kk * az[0]));
-            atomicAdd(&shf[2 * kHaloCells + h], W * (qij[1] + (float)kk * az[1]));
-            atomicAdd(&shf[3 * kHaloCells + h], W * (qij[2] + (float)kk * az[2]));
+                for (int kk = 0; kk < 3; ++kk) {
+                  const int n = (ii * 3 + jj) * 3 + kk;
+                  acc[n] = fmaf(wij * w[2][kk], qij + (float)kk * az, acc[n]);
+                }
+              }
+            }
           }
+          const int cell = cell0 + my_cell;
+          const int ex = (cell >> 6) + 1, ey = ((cell >> 3) & 7) + 1, ez = (cell & 7) + 1;
+          float *dst = sh + my_ch * kHaloCells;
+#pragma unroll
+          for (int ii = 0; ii < 3; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+              for (int kk = 0; kk < 3; ++kk)
+                atomicAdd(&dst[((ex + ii) * kHalo + (ey + jj)) * kHalo + ez + kk], acc[(ii * 3 + jj) * 3 + kk]);
         }
       }
     }
     __syncthreads();
     // flush: items (ch, hx, hy, quad) over 4 x 12 x 12 x 3
-    for (int it = threadIdx.x; it < kGridChannels * kHalo * kHalo * 3; it += blockDim.x) {
+    for (int it = t; it < kGridChannels * kHalo * kHalo * 3; it += blockDim.x) {
       const int quad = it % 3, hy = (it / 3) % kHalo, hx = (it / (3 * kHalo)) % kHalo,
                 ch = it / (3 * kHalo * kHalo);
-      const float *src4 = &sh[ch][hx][hy][quad * 4];
+      const float *src4 = &sh[((ch * kHalo + hx) * kHalo + hy) * kHalo + quad * 4];
       const float a0 = src4[0], a1 = src4[1], a2 = src4[2], a3 = src4[3];
       if (a0 == 0.f && a1 == 0.f && a2 == 0.f && a3 == 0.f) continue;
-      const int t = (hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0);
-      const int tb = s.nbr[b * 8 + t];
+      const int tt = (hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0);
+      const int tb = s.nbr[b * 8 + tt];
       if (tb < 0) {
         set_status(s.ctr, kStatusMissingBlock);
         continue;
@@ -1007,8 +1100,14 @@ cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// per-device kernel attributes; called once per scene with its device current, before any
+// capture of its launches
+cudaError_t prepare_kernels() {
+  return cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
+}
+
 cudaError_t launch_p2g(scene_device &s, cudaStream_t st) {
-  k_p2g<<<num_sms() * 3, kThreads, 0, st>>>(s);
+  k_p2g<<<num_sms() * 2, kP2GThreads, kP2GSmemBytes, st>>>(s);
   return cudaGetLastError();
 }
 
