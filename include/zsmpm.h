@@ -234,6 +234,76 @@ ZSMPM_API zsmpm_status zsmpm_svd3(const float *A, float *U, float *S, float *V, 
 ZSMPM_API zsmpm_status zsmpm_constitutive(const zsmpm_material *mat, float *F, float *plastic,
                                           float *tau, int64_t count, void *stream);
 
+/* ---- learned return-mapping closure -------------------------------------------- */
+/* An MLP 6 -> 64 -> 64 -> 64 -> 6 (SiLU) that replaces the return-mapping branch of the
+ * constitutive update inside G2P (ConstitutiveModel_Vol_dP.hpp:241-325 for Drucker-Prager,
+ * SnowPlasticity.hpp:24-32 for snow).  Inputs: the log singular values of the trial F (sorted
+ * as the SVD returns them) and three material/state features (Drucker-Prager: friction angle
+ * in degrees, cohesion as a log-strain shift, logJp; snow: theta_c, theta_s, log Jp).
+ * Outputs: projected minus trial log strain (3) and principal Kirchhoff stress (3).  Trained
+ * on the GPU by this library's own forward/backward/Adam kernels on pairs generated by the
+ * plain return map; inference inside G2P runs in BF16 on tensor cores with FP32 accumulation,
+ * falls back to the plain return map per particle whose inputs leave the training hull
+ * (per-feature min/max), and audits a sample of particles against the plain map.  No
+ * counterpart in the reference. */
+typedef struct zsmpm_closure zsmpm_closure;
+
+typedef struct {
+  int32_t model;            /* zsmpm_model: ZSMPM_DRUCKER_PRAGER or ZSMPM_SNOW */
+  float params[9158];       /* FP32 weights: W1[64][6] b1 W2[64][64] b2 W3[64][64] b3 W4[6][64] b4 */
+  float in_mean[6], in_inv_std[6];  /* input normalisation (x - mean) * inv_std */
+  float in_min[6], in_max[6];       /* training hull of the raw inputs */
+  float out_scale[6];               /* outputs are network outputs times out_scale */
+} zsmpm_closure_state;
+
+typedef struct {
+  int64_t audited;          /* particles checked against the plain return map */
+  double mean_rel_error;    /* mean of |tau_mlp - tau_plain| / (|tau_plain| + 1e-4 (3 lambda + 2 mu)) */
+  double max_rel_error;
+  double agg_rel_error;     /* sqrt(sum |dtau|^2 / sum |tau_plain|^2) over the audited particles */
+  int64_t fallbacks;        /* particle updates outside the hull that used the plain map */
+} zsmpm_closure_audit;
+
+ZSMPM_API zsmpm_status zsmpm_closure_create(const zsmpm_material *mat, int32_t device, zsmpm_closure **out);
+ZSMPM_API zsmpm_status zsmpm_closure_destroy(zsmpm_closure *c);
+/* Training set: n_random random trial states (log singular values uniform in
+ * [log 0.5, log 2]; Drucker-Prager friction 20-45 deg, cohesion 0-100 Pa mapped to a
+ * log-strain shift by 1/(3 lambda + 2 mu), zero for a quarter of the samples, logJp zero for
+ * half of them and else uniform in [0, 0.2]; snow theta_c 0.015-0.035, theta_s 0.005-0.01,
+ * log Jp in [-0.3, 0.3]) plus n_logged raw feature rows (device pointer, 6 floats each, e.g.
+ * from zsmpm_scene_set_state_log); targets from the plain return map.  Sets the input
+ * normalisation and the training hull (per-feature min/max of the training inputs). */
+ZSMPM_API zsmpm_status zsmpm_closure_build_dataset(zsmpm_closure *c, int64_t n_random, uint64_t seed,
+                                                   const float *logged, int64_t n_logged, void *stream);
+/* Adam on the mean squared error of normalised outputs, batches of `batch` samples;
+ * loss_out (host, `epochs` floats, optional) receives each epoch's mean loss. */
+ZSMPM_API zsmpm_status zsmpm_closure_train(zsmpm_closure *c, int32_t epochs, int32_t batch, float lr,
+                                           uint64_t seed, float *loss_out, void *stream);
+/* Loss and its gradient (mean over n samples) by the training kernels, for gradient checks:
+ * x, y raw device rows [n][6]; grad device [9158]; loss device [1]. */
+ZSMPM_API zsmpm_status zsmpm_closure_loss_grad(zsmpm_closure *c, const float *x, const float *y, int64_t n,
+                                               float *grad, float *loss, void *stream);
+/* Network outputs (unscaled D and tau) of raw feature rows (device [n][6]); bf16 != 0 runs
+ * the tensor-core forward that G2P uses, else an FP32 forward of the master weights. */
+ZSMPM_API zsmpm_status zsmpm_closure_infer(zsmpm_closure *c, const float *x, float *y, int64_t n, int32_t bf16,
+                                           void *stream);
+/* The plain return map's (D, tau) for raw feature rows (device [n][6]). */
+ZSMPM_API zsmpm_status zsmpm_closure_targets(zsmpm_closure *c, const float *x, float *y, int64_t n, void *stream);
+ZSMPM_API zsmpm_status zsmpm_closure_get_state(zsmpm_closure *c, zsmpm_closure_state *out);
+ZSMPM_API zsmpm_status zsmpm_closure_set_state(zsmpm_closure *c, const zsmpm_closure_state *in);
+/* Attach a trained closure to a scene (NULL detaches; the scene keeps the closure's device
+ * pointers, so destroy the closure only after detaching it); audit_period N checks one
+ * particle in N per substep against the plain map (0 = no audit).  Needs the committed
+ * plasticity ordering. */
+ZSMPM_API zsmpm_status zsmpm_scene_set_closure(zsmpm_scene *s, zsmpm_closure *c, int32_t audit_period);
+/* Audit totals since the closure was attached or the last reset (synchronises). */
+ZSMPM_API zsmpm_status zsmpm_scene_closure_audit(zsmpm_scene *s, zsmpm_closure_audit *out, int32_t reset);
+/* Log the raw closure features of the trial state of one particle in `period` per substep into
+ * buffer (device, cap x 6) during G2P; period 0 stops logging.  Resets the count. */
+ZSMPM_API zsmpm_status zsmpm_scene_set_state_log(zsmpm_scene *s, float *buffer, int64_t cap, int32_t period);
+/* Rows logged so far (at most cap; synchronises). */
+ZSMPM_API zsmpm_status zsmpm_scene_state_log_count(zsmpm_scene *s, int64_t *count_out);
+
 /* ---- allocation-free variant --------------------------------------------------- */
 /* Block activation without any device allocation.  No counterpart in the reference: it is
  * for callers that cannot call cudaMalloc at this point -- hosts whose own memory pool has

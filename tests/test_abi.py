@@ -44,14 +44,19 @@ def test_struct_layouts_match_header(zs, tmp_path):
                      "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu\\n\","
                      "sizeof(zsmpm_material), sizeof(zsmpm_scene_desc), offsetof(zsmpm_scene_desc, material),"
                      "offsetof(zsmpm_scene_desc, max_particles), sizeof(zsmpm_particle_arrays),"
-                     "sizeof(zsmpm_tilevector_view), sizeof(zsmpm_table_view));return 0;}\n")
+                     "sizeof(zsmpm_tilevector_view), sizeof(zsmpm_table_view));"
+                     "printf(\"%zu %zu %zu %zu\\n\", sizeof(zsmpm_closure_state),"
+                     "offsetof(zsmpm_closure_state, in_mean), sizeof(zsmpm_closure_audit),"
+                     "offsetof(zsmpm_closure_audit, fallbacks));return 0;}\n")
     exe = tmp_path / "probe"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(probe), "-o", str(exe)], check=True)
     vals = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()))
     a = zs._abi
     assert vals == [C.sizeof(a.Material), C.sizeof(a.SceneDesc), a.SceneDesc.material.offset,
                     a.SceneDesc.max_particles.offset, C.sizeof(a.ParticleArrays),
-                    C.sizeof(a.TileVectorView), C.sizeof(a.TableView)]
+                    C.sizeof(a.TileVectorView), C.sizeof(a.TableView),
+                    C.sizeof(a.ClosureState), a.ClosureState.in_mean.offset, C.sizeof(a.ClosureAudit),
+                    a.ClosureAudit.fallbacks.offset]
 
 
 def test_host_side_argument_checks_without_gpu(zs):
@@ -67,6 +72,12 @@ def test_host_side_argument_checks_without_gpu(zs):
     assert lib.zsmpm_scene_create(C.byref(desc), C.byref(h)) == zs._abi.ERR_INVALID_ARG
     assert lib.zsmpm_svd3(None, None, None, None, -1, None) == zs._abi.ERR_INVALID_ARG
     assert lib.zsmpm_scene_destroy(None) == zs._abi.OK
+    mat = zs._abi.Material(model=zs.FIXED_COROTATED)
+    c = C.c_void_p()
+    # the closure replaces a return map, which the elastic model does not have
+    assert lib.zsmpm_closure_create(C.byref(mat), 0, C.byref(c)) == zs._abi.ERR_INVALID_ARG
+    assert lib.zsmpm_closure_train(None, 1, 32, C.c_float(1e-3), 0, None, None) == zs._abi.ERR_INVALID_ARG
+    assert lib.zsmpm_closure_destroy(None) == zs._abi.OK
     assert lib.zsmpm_version().startswith(b"zsmpm")
 
 

@@ -59,6 +59,21 @@ class GridView(C.Structure):
                 ("keys", C.c_void_p)]
 
 
+MLP_PARAMS = 9158  # 6 -> 64 -> 64 -> 64 -> 6
+
+
+class ClosureState(C.Structure):
+    _fields_ = [("model", C.c_int32), ("params", C.c_float * MLP_PARAMS),
+                ("in_mean", C.c_float * 6), ("in_inv_std", C.c_float * 6),
+                ("in_min", C.c_float * 6), ("in_max", C.c_float * 6), ("out_scale", C.c_float * 6)]
+
+
+class ClosureAudit(C.Structure):
+    _fields_ = [("audited", C.c_int64), ("mean_rel_error", C.c_double),
+                ("max_rel_error", C.c_double), ("agg_rel_error", C.c_double),
+                ("fallbacks", C.c_int64)]
+
+
 _P = C.c_void_p
 _S = C.c_int  # zsmpm_status
 
@@ -92,6 +107,19 @@ SIGNATURES = {
     "zsmpm_kernels_per_substep": (C.c_int32, [_P]),
     "zsmpm_svd3": (_S, [_P, _P, _P, _P, C.c_int64, _P]),
     "zsmpm_constitutive": (_S, [C.POINTER(Material), _P, _P, _P, C.c_int64, _P]),
+    "zsmpm_closure_create": (_S, [C.POINTER(Material), C.c_int32, C.POINTER(_P)]),
+    "zsmpm_closure_destroy": (_S, [_P]),
+    "zsmpm_closure_build_dataset": (_S, [_P, C.c_int64, C.c_uint64, _P, C.c_int64, _P]),
+    "zsmpm_closure_train": (_S, [_P, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _P, _P]),
+    "zsmpm_closure_loss_grad": (_S, [_P, _P, _P, C.c_int64, _P, _P, _P]),
+    "zsmpm_closure_infer": (_S, [_P, _P, _P, C.c_int64, C.c_int32, _P]),
+    "zsmpm_closure_targets": (_S, [_P, _P, _P, C.c_int64, _P]),
+    "zsmpm_closure_get_state": (_S, [_P, C.POINTER(ClosureState)]),
+    "zsmpm_closure_set_state": (_S, [_P, C.POINTER(ClosureState)]),
+    "zsmpm_scene_set_closure": (_S, [_P, _P, C.c_int32]),
+    "zsmpm_scene_closure_audit": (_S, [_P, C.POINTER(ClosureAudit), C.c_int32]),
+    "zsmpm_scene_set_state_log": (_S, [_P, _P, C.c_int64, C.c_int32]),
+    "zsmpm_scene_state_log_count": (_S, [_P, C.POINTER(C.c_int64)]),
     "zsmpm_activate_blocks_noalloc": (_S, [_P, C.c_int64, C.c_float, _P, C.c_int32, _P, _P]),
 }
 

@@ -35,6 +35,8 @@ struct zsmpm_scene {
   cudaEvent_t ev[6] = {};
   float stage_ms[5] = {};
   std::vector<void *> allocations;
+  double *audit = nullptr;                  // closure audit accumulators (device, 8 doubles)
+  unsigned long long *log_count = nullptr;  // trial-state log counter (device)
 };
 
 namespace {
@@ -94,6 +96,7 @@ material_dev make_material(const zsmpm_material &m) {
   d.hardening = m.hardening;
   d.theta_c = m.theta_c;
   d.theta_s = m.theta_s;
+  d.friction_deg = m.friction_deg;
   return d;
 }
 
@@ -664,6 +667,88 @@ ZSMPM_API zsmpm_status zsmpm_stage_times(zsmpm_scene *s, float *ms, int32_t coun
 }
 
 ZSMPM_API int32_t zsmpm_kernels_per_substep(const zsmpm_scene *) { return kernels_per_substep(); }
+
+ZSMPM_API zsmpm_status zsmpm_scene_set_closure(zsmpm_scene *s, zsmpm_closure *c, int32_t audit_period) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (audit_period < 0) return fail(ZSMPM_ERR_INVALID_ARG, "audit_period < 0");
+  if (!c) {
+    invalidate_graphs(s);
+    s->dev.aux.learned = 0;
+    return ZSMPM_OK;
+  }
+  closure_dev cd{};
+  if (!closure_device_view(c, &cd)) return fail(ZSMPM_ERR_NOT_READY, "closure has no dataset or state yet");
+  if (cd.model != s->desc.material.model)
+    return fail(ZSMPM_ERR_INVALID_ARG, "closure was built for another material model");
+  if (s->desc.material.plasticity_mode != ZSMPM_PLASTICITY_COMMITTED && s->desc.material.model != ZSMPM_SNOW)
+    return fail(ZSMPM_ERR_INVALID_ARG, "the learned closure runs in the committed plasticity ordering");
+  if (!s->audit) {
+    double *a = nullptr;
+    ZS_TRY(cudaMalloc(&a, sizeof(double) * 8), "alloc audit");
+    s->allocations.push_back(a);
+    s->audit = a;
+    ZS_TRY(cudaMemset(s->audit, 0, sizeof(double) * 8), "memset audit");
+  }
+  invalidate_graphs(s);
+  cd.audit = s->audit;
+  cd.audit_period = audit_period;
+  s->dev.aux.cd = cd;
+  s->dev.aux.learned = 1;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_closure_audit(zsmpm_scene *s, zsmpm_closure_audit *out, int32_t reset) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (!out) return fail(ZSMPM_ERR_INVALID_ARG, "null output");
+  std::memset(out, 0, sizeof(*out));
+  if (!s->audit) return ZSMPM_OK;
+  if (s->last_stream) ZS_TRY(cudaStreamSynchronize(s->last_stream), "synchronize");
+  ZS_TRY(cudaDeviceSynchronize(), "synchronize");
+  double h[8];
+  ZS_TRY(cudaMemcpy(h, s->audit, sizeof(h), cudaMemcpyDeviceToHost), "read audit");
+  out->audited = (int64_t)h[0];
+  out->mean_rel_error = h[0] > 0 ? h[1] / h[0] : 0.0;
+  out->max_rel_error = h[2];
+  out->agg_rel_error = h[4] > 0 ? std::sqrt(h[3] / h[4]) : 0.0;
+  out->fallbacks = (int64_t)h[5];
+  if (reset) ZS_TRY(cudaMemset(s->audit, 0, sizeof(h)), "reset audit");
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_set_state_log(zsmpm_scene *s, float *buffer, int64_t cap, int32_t period) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (period < 0 || (period > 0 && (!buffer || cap < 1))) return fail(ZSMPM_ERR_INVALID_ARG, "bad log arguments");
+  if (!s->log_count) {
+    unsigned long long *c = nullptr;
+    ZS_TRY(cudaMalloc(&c, sizeof(unsigned long long)), "alloc log counter");
+    s->allocations.push_back(c);
+    s->log_count = c;
+  }
+  invalidate_graphs(s);
+  ZS_TRY(cudaMemset(s->log_count, 0, sizeof(unsigned long long)), "reset log counter");
+  s->dev.aux.log_buf = period > 0 ? buffer : nullptr;
+  s->dev.aux.log_cap = period > 0 ? cap : 0;
+  s->dev.aux.log_period = period;
+  s->dev.aux.log_count = s->log_count;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_state_log_count(zsmpm_scene *s, int64_t *count_out) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (!count_out) return fail(ZSMPM_ERR_INVALID_ARG, "null output");
+  *count_out = 0;
+  if (!s->log_count) return ZSMPM_OK;
+  if (s->last_stream) ZS_TRY(cudaStreamSynchronize(s->last_stream), "synchronize");
+  ZS_TRY(cudaDeviceSynchronize(), "synchronize");
+  unsigned long long c = 0;
+  ZS_TRY(cudaMemcpy(&c, s->log_count, sizeof(c), cudaMemcpyDeviceToHost), "read log counter");
+  *count_out = (int64_t)std::min<unsigned long long>(c, (unsigned long long)std::max<int64_t>(s->dev.aux.log_cap, 0));
+  return ZSMPM_OK;
+}
 
 ZSMPM_API zsmpm_status zsmpm_svd3(const float *A, float *U, float *S, float *V, int64_t count, void *stream) {
   if (count < 0 || (count > 0 && (!A || !U || !S || !V))) return fail(ZSMPM_ERR_INVALID_ARG, "bad svd arguments");

@@ -258,6 +258,7 @@ struct material_dev {
   float mu, lambda, volume;
   float cohesion, beta, yield_surface;
   float hardening, theta_c, theta_s;
+  float friction_deg;   // Drucker-Prager friction angle (a feature of the learned closure)
 };
 
 // out[3c+r] = sum_k M[3k+r] d[k] N[3k+c]

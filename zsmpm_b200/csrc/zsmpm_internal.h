@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 
 #include "zsmpm_device.cuh"
+#include "zsmpm_mlp.cuh"
+
+struct zsmpm_closure;
 
 namespace zsmpm {
 
@@ -21,7 +24,8 @@ struct particle_buffers {
   int *id = nullptr;         // upload index
 };
 
-// Device counters (int32), zeroed at the start of every substep except the status word.
+// Device counters (int32), zeroed at the start of every substep except the status word and
+// the substep counter.
 enum counter_slot : int {
   kCtrParticleBlocks = 0,  // blocks inserted from particles (insertion indices [0, npb))
   kCtrEnlarged = 1,        // blocks inserted by the enlargement
@@ -31,6 +35,7 @@ enum counter_slot : int {
   kCtrBoxHi = 7,           // 3 ints
   kCtrWords = 10,          // bitmap words in use
   kCtrWork = 11,           // 8 work counters for persistent kernels
+  kCtrSubstep = 20,        // substeps begun since the scene was created (audit/log sampling)
   kCtrCount = 24
 };
 enum work_slot : int { kWorkCellStart = 0, kWorkFinalize = 1, kWorkP2G = 2, kWorkG2P = 3, kWorkGrid = 4 };
@@ -47,8 +52,19 @@ struct scene_params {
   material_dev mat;
 };
 
+// G2P options beside the plain path: the learned closure and the trial-state log.
+struct g2p_aux {
+  int learned = 0;            // 1: G2P runs the closure's MLP in place of the return map
+  closure_dev cd{};           // its weights, normalisation, hull and audit accumulators
+  float *log_buf = nullptr;   // [log_cap][6] raw closure features of sampled particles
+  long long log_cap = 0;
+  int log_period = 0;         // one particle in log_period per substep (0 = off)
+  unsigned long long *log_count = nullptr;
+};
+
 struct scene_device {
   scene_params prm;
+  g2p_aux aux;
   particle_buffers cur, nxt;
   // hash table (HashTableView-compatible arrays + packed keys used for CAS/probing)
   uint64_t *pk = nullptr;
@@ -107,6 +123,8 @@ cudaError_t launch_export_order(const scene_device &s, int *order, cudaStream_t 
 // allocation-free entry point); writes the sorted keys and the count (or a negative code)
 cudaError_t launch_activate_static(scene_device &s, const float *x, int *keys_out, int cap,
                                    int *count_out, cudaStream_t st);
+// the device view of a closure that has a dataset or a loaded state (false otherwise)
+bool closure_device_view(const zsmpm_closure *c, closure_dev *out);
 // records the calling thread's error message (read back by zsmpm_last_error_string)
 int record_error(int status, const char *message);
 cudaError_t launch_svd_batch(const float *A, float *U, float *S, float *V, long long count,

@@ -192,6 +192,10 @@ __global__ void __launch_bounds__(kThreads) k_begin(scene_device s) {
   if (blockIdx.x == 0 && threadIdx.x < kCtrCount) {
     const int t = threadIdx.x;
     if (t == kCtrStatus) return;
+    if (t == kCtrSubstep) {
+      s.ctr[t] += 1;
+      return;
+    }
     int v = 0;
     if (t >= kCtrBoxLo && t < kCtrBoxLo + 3) v = 0x7fffffff;
     if (t >= kCtrBoxHi && t < kCtrBoxHi + 3) v = -0x7fffffff;
@@ -717,12 +721,132 @@ __global__ void __launch_bounds__(kThreads) k_grid_update(scene_device s) {
 // then per particle gather v and C (G2P.hpp:56-66), advect, update F = (I + dt C) F
 // (G2P.hpp:76-78), run the constitutive update and write the particle to its binned slot
 // in the next buffer set, so that storage order follows the binning of this substep.
+// Particles are taken 32 per warp; with the learned closure the whole warp steps together
+// (lanes past the block's end run on a copy of its first particle and write nothing), so
+// that the tensor-core MLP runs across the warp.
+
+// trial-state features of the closure: log singular values and the model's three
+// material/state features
+__device__ __forceinline__ void closure_features(const material_dev &mat, const float *S, float plastic,
+                                                 float *feat) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) feat[i] = logf(fmaxf(fabsf(S[i]), 1e-4f));
+  if (mat.model == 1) {
+    feat[3] = mat.friction_deg;
+    feat[4] = mat.cohesion;
+    feat[5] = plastic;
+  } else {
+    feat[3] = mat.theta_c;
+    feat[4] = mat.theta_s;
+    feat[5] = logf(plastic);
+  }
+}
+
+__device__ __forceinline__ principal_result plain_principal(const material_dev &mat, const float *S,
+                                                            const float *l, float plastic) {
+  if (mat.model == 1)
+    return dp_principal(mat.mu, mat.lambda, mat.cohesion, mat.beta, mat.volume_correction, mat.yield_surface, l,
+                        plastic);
+  return snow_principal(mat.mu, mat.lambda, mat.hardening, mat.theta_c, mat.theta_s, S, plastic);
+}
+
+// The learned constitutive update (committed ordering).  Warp-collective: every lane of the
+// warp calls it.  Inactive lanes compute on their copy and record nothing.
+__device__ __forceinline__ void learned_constitutive(const material_dev &mat, const closure_dev &cd,
+                                                     const uint2 *frag, const float *bias, __nv_bfloat16 *xs,
+                                                     float *ys, float *F, float &plastic, float *tau, bool active,
+                                                     int id, int substep) {
+  float U[9], S[3], V[9];
+  svd3(F, U, S, V);
+  float feat[6];
+  closure_features(mat, S, plastic, feat);
+  bool in_hull = true;
+  float in[kMlpIn];
+  net_scale ns;
+  closure_inputs(cd.model, cd.kappa, cd.hardening, feat, in, ns);
+#pragma unroll
+  for (int k = 0; k < kMlpIn; ++k) {
+    in_hull = in_hull && feat[k] >= cd.in_min[k] && feat[k] <= cd.in_max[k];
+    in[k] = (in[k] - cd.in_mean[k]) * cd.in_inv_std[k];
+  }
+  float out[kMlpOut];
+  mlp_forward_warp(in, out, frag, bias, xs, ys);
+#pragma unroll
+  for (int k = 0; k < kMlpOut; ++k) out[k] *= cd.out_scale[k];
+  float y[6];
+  closure_from_net(ns, out, y);
+  float tp[3], Ns[3], pl_new;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    tp[i] = y[3 + i];
+    Ns[i] = expf(feat[i] + y[i]);
+  }
+  // the plastic state follows the branch the projection took, which the projected strain shows
+  if (mat.model == 1) {
+    const float sum_eps = feat[0] + feat[1] + feat[2] - 3.f * mat.cohesion;
+    const float tr = sum_eps + plastic;
+    pl_new = tr >= 0.f ? (mat.volume_correction ? mat.beta * sum_eps + plastic : plastic) : 0.f;
+  } else {
+    pl_new = plastic * (S[0] * S[1] * S[2] / fmaxf(Ns[0] * Ns[1] * Ns[2], 1e-6f));
+  }
+  const bool audit = active && cd.audit_period > 0 &&
+                     ((unsigned)id * 2654435761u + (unsigned)substep * 40503u) % (unsigned)cd.audit_period == 0u;
+  if (!in_hull || audit) {
+    const principal_result r = plain_principal(mat, S, feat, plastic);
+    if (audit) {
+      float d2 = 0.f, t2 = 0.f;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        d2 += (tp[i] - r.tau[i]) * (tp[i] - r.tau[i]);
+        t2 += r.tau[i] * r.tau[i];
+      }
+      const float floor_stress = 1e-4f * (3.f * mat.lambda + 2.f * mat.mu);
+      const float rel = sqrtf(d2) / (sqrtf(t2) + floor_stress);
+      // non-negative doubles order like their bit patterns, so the max is an integer max
+      atomicAdd(&cd.audit[0], 1.0);
+      atomicAdd(&cd.audit[1], (double)rel);
+      atomicMax(reinterpret_cast<unsigned long long *>(&cd.audit[2]),
+                (unsigned long long)__double_as_longlong((double)rel));
+      atomicAdd(&cd.audit[3], (double)d2);
+      atomicAdd(&cd.audit[4], (double)t2);
+    }
+    if (!in_hull) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        tp[i] = r.tau[i];
+        Ns[i] = r.Ns[i];
+      }
+      pl_new = r.plastic;
+      if (active) atomicAdd(&cd.audit[5], 1.0);
+    }
+  }
+  plastic = pl_new;
+  const float d[3] = {tp[0] * mat.volume, tp[1] * mat.volume, tp[2] * mat.volume};
+  mul_diag_t(tau, U, d, U);
+  mul_diag_t(F, U, Ns, V);
+}
+
+constexpr size_t kG2PSmemPlain = sizeof(float) * 3 * kHaloCells;
+constexpr size_t kG2PSmemLearned = kG2PSmemPlain + sizeof(uint2) * kFragTotal + sizeof(float) * kBiasTotal +
+                                   (kThreads / 32) * (32 * 16 * sizeof(__nv_bfloat16) + 32 * 8 * sizeof(float));
+
+template <bool kLearned>
 __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
-  __shared__ float sv[3][kHalo][kHalo][kHalo];
+  extern __shared__ __align__(16) float g2p_smem[];
+  float *svf = g2p_smem;
   __shared__ int s_b;
   const scene_params &p = s.prm;
   const int nb = s.ctr[kCtrBlocks];
-  float *svf = &sv[0][0][0][0];
+  const int substep = s.ctr[kCtrSubstep];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint2 *sfrag = reinterpret_cast<uint2 *>(g2p_smem + 3 * kHaloCells);
+  float *sbias = reinterpret_cast<float *>(sfrag + kFragTotal);
+  __nv_bfloat16 *sxs = reinterpret_cast<__nv_bfloat16 *>(sbias + kBiasTotal);
+  float *sys = reinterpret_cast<float *>(sxs + (kThreads / 32) * 32 * 16);
+  if (kLearned) {
+    for (int i = threadIdx.x; i < kFragTotal; i += blockDim.x) sfrag[i] = s.aux.cd.frag[i];
+    for (int i = threadIdx.x; i < kBiasTotal; i += blockDim.x) sbias[i] = s.aux.cd.bias[i];
+  }
   for (;;) {
     const int b = grab_block(&s.ctr[kCtrWork + kWorkG2P], &s_b);
     if (b >= nb) break;
@@ -739,7 +863,7 @@ __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
         const int cell = ((hx & 7) << 6) | ((hy & 7) << 3) | ((quad * 4) & 7);
         val = *reinterpret_cast<const float4 *>(s.grid + ((size_t)tb * kGridChannels + 1 + ch) * 512 + cell);
       }
-      float *dst = &sv[ch][hx][hy][quad * 4];
+      float *dst = svf + ((ch * kHalo + hx) * kHalo + hy) * kHalo + quad * 4;
       dst[0] = val.x;
       dst[1] = val.y;
       dst[2] = val.z;
@@ -748,8 +872,11 @@ __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
     __syncthreads();
     const int3 bk = unpack_key(s.blk_pk[b]);
     const int org[3] = {bk.x * 8, bk.y * 8, bk.z * 8};
-    for (int slot = start + threadIdx.x; slot < end; slot += blockDim.x) {
-      const int i = s.src[slot];
+    for (int base = start + warp * 32; base < end; base += blockDim.x) {
+      const int slot = base + lane;
+      const bool active = slot < end;
+      if (!kLearned && !active) break;
+      const int i = s.src[active ? slot : start];
       float4 xm = s.cur.xm[i];
       float F[9];
 #pragma unroll
@@ -761,9 +888,9 @@ __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
       float w[3][3], f[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const float base = floorf(X[d] - 0.5f);
-        f[d] = X[d] - base;
-        hb[d] = (int)base - org[d];
+        const float bs = floorf(X[d] - 0.5f);
+        f[d] = X[d] - bs;
+        hb[d] = (int)bs - org[d];
         w[d][0] = 0.5f * (1.5f - f[d]) * (1.5f - f[d]);
         const float f1 = f[d] - 1.f;
         w[d][1] = 0.75f - f1 * f1;
@@ -772,7 +899,7 @@ __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
       }
       const bool inside = hb[0] >= 0 && hb[0] <= kHalo - 3 && hb[1] >= 0 && hb[1] <= kHalo - 3 &&
                           hb[2] >= 0 && hb[2] <= kHalo - 3;
-      if (!inside) set_status(s.ctr, kStatusMissingBlock);
+      if (active && !inside) set_status(s.ctr, kStatusMissingBlock);
       float vel[3] = {0.f, 0.f, 0.f};
       float B[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // sum W v (node - f)^T
       if (inside) {
@@ -822,8 +949,23 @@ __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
 #pragma unroll
         for (int r = 0; r < 3; ++r)
           Fn[3 * c + r] = F[3 * c + r] + p.dt * (C[r] * F[3 * c] + C[3 + r] * F[3 * c + 1] + C[6 + r] * F[3 * c + 2]);
+      // trial-state log for the closure's training set
+      if (s.aux.log_period > 0 && active && p.mat.model != 0 &&
+          ((unsigned)id + (unsigned)substep) % (unsigned)s.aux.log_period == 0u) {
+        float U[9], S[3], V[9], feat[6];
+        svd3(Fn, U, S, V);
+        closure_features(p.mat, S, pl, feat);
+        const unsigned long long k = atomicAdd(s.aux.log_count, 1ull);
+        if ((long long)k < s.aux.log_cap)
+          for (int q = 0; q < 6; ++q) s.aux.log_buf[6 * k + q] = feat[q];
+      }
       float tau[9];
-      constitutive(p.mat, Fn, pl, tau);
+      if (kLearned)
+        learned_constitutive(p.mat, s.aux.cd, sfrag, sbias, sxs + warp * 32 * 16, sys + warp * 32 * 8, Fn, pl, tau,
+                             active, id, substep);
+      else
+        constitutive(p.mat, Fn, pl, tau);
+      if (!active) continue;
       const size_t cap = (size_t)p.cap;
       s.nxt.xm[slot] = xm;
       s.nxt.v[slot] = make_float4(vel[0], vel[1], vel[2], 0.f);
@@ -1103,7 +1245,9 @@ cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
 // per-device kernel attributes; called once per scene with its device current, before any
 // capture of its launches
 cudaError_t prepare_kernels() {
-  return cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
+  cudaError_t e = cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kG2PSmemLearned);
 }
 
 cudaError_t launch_p2g(scene_device &s, cudaStream_t st) {
@@ -1117,7 +1261,10 @@ cudaError_t launch_grid_update(scene_device &s, cudaStream_t st) {
 }
 
 cudaError_t launch_g2p(scene_device &s, cudaStream_t st) {
-  k_g2p<<<num_sms() * 2, kThreads, 0, st>>>(s);
+  if (s.aux.learned)
+    k_g2p<true><<<num_sms() * 2, kThreads, kG2PSmemLearned, st>>>(s);
+  else
+    k_g2p<false><<<num_sms() * 2, kThreads, kG2PSmemPlain, st>>>(s);
   return cudaGetLastError();
 }
 
