@@ -157,6 +157,68 @@ def substep_algorithmic_bytes(n: int, nb: int, plastic: bool) -> int:
     return n * (100 + 180 + (8 if plastic else 0) + 16) + nb * 512 * 72
 
 
+def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms):
+    """The same workload with the learned closure in G2P.  The closure is trained on the GPU
+    (this library's forward/backward/Adam kernels) on random trial states plus trial states
+    logged from a few plain substeps of this scene, then the scene is re-uploaded, warmed up and
+    timed like the plain leg with one particle in 100 audited per substep."""
+    import torch
+
+    from zsmpm_b200 import closure as cl
+    # trial states from the plain path
+    upload_pinned()
+    period = max(1, -(-n * 4 // args.train_logged))
+    buf = torch.empty((args.train_logged, 6), dtype=torch.float32, device="cuda")
+    cl.set_state_log(sc, buf, period)
+    sc.run(4, stream=sptr)
+    n_log = cl.state_log_count(sc)
+    cl.set_state_log(sc, None, 0)
+    torch.cuda.synchronize()
+    c = cl.Closure(spec.material, spec.volume, device=torch.cuda.current_device())
+    t0 = time.perf_counter()
+    c.build_dataset(args.train_random, seed=7, logged=buf[:n_log].contiguous())
+    schedule = ((6, 4096, 2e-3), (6, 4096, 5e-4), (4, 8192, 1e-4))
+    losses = c.fit(schedule)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    # timed leg from the initial state
+    upload_pinned()
+    cl.attach(sc, c, audit_period=100)
+    sc.run(args.warmup, stream=sptr)
+    sc.status()
+    cl.audit(sc, reset=True)
+    torch.cuda.synchronize()
+    barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sc.run(args.steps, stream=sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sc.status()
+    lms = max_over_ranks(e0.elapsed_time(e1), ws)
+    a = cl.audit(sc)
+    sc.set_stage_timing(True)
+    g2p = 0.0
+    reps = min(args.steps, 8)
+    for _ in range(reps):
+        sc.substep(stream=sptr)
+        g2p += sc.stage_times()[4]
+    sc.set_stage_timing(False)
+    sc.status()
+    cl.attach(sc, None)
+    c.close()
+    value = n * args.steps * ws / (lms * 1e-3)
+    return {"value": value, "unit": UNIT, "ms_per_step": lms / args.steps,
+            "vs_plain": (plain_ms * args.steps) / lms, "g2p_ms": g2p / reps,
+            "audit": {"period": 100, **a,
+                      "what": "principal Kirchhoff stress of audited particles vs the plain return map; "
+                              "rel = |dtau| / (|tau| + 1e-4 (3 lambda + 2 mu)); agg = sqrt(sum|dtau|^2/sum|tau|^2)"},
+            "training": {"random_states": args.train_random, "logged_states": n_log,
+                         "epochs": sum(e for e, _, _ in schedule), "seconds": train_s,
+                         "first_loss": float(losses[0]), "final_loss": float(losses[-1])},
+            "inference": "BF16 mma.sync m16n8k16, FP32 accumulation, fused in G2P"}
+
+
 def cpu_baseline_sample(spec, p, max_particles: int):
     """A spatial slab of the workload (all particles with z below a cut), keeping density."""
     from zsmpm_b200.scenes import Particles
@@ -210,6 +272,9 @@ def main(argv=None):
     ap.add_argument("--ref-particles", type=int, default=1_500_000)
     ap.add_argument("--ref-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-closure leg")
+    ap.add_argument("--train-random", type=int, default=1_500_000)
+    ap.add_argument("--train-logged", type=int, default=500_000)
     args = ap.parse_args(argv)
 
     spec, workload = scene_for(args.scene)
@@ -299,6 +364,11 @@ def main(argv=None):
     wall = time.perf_counter() - t0
     e2e = n * args.steps * ws / (e2e_ms * 1e-3)
 
+    # ---------------------------------------------------------------- learned-closure leg
+    learned = None
+    if plastic and not args.no_learned:
+        learned = learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, ms / args.steps)
+
     # ---------------------------------------------------------------- CPU baseline (rank 0, N=1)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -345,6 +415,7 @@ def main(argv=None):
             "gpu_launches": sc.kernels_per_substep() * args.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "learned": learned,
         }
         print(json.dumps(line))
     sc.close()

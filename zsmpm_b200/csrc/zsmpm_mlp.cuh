@@ -205,50 +205,43 @@ __device__ __forceinline__ uint32_t silu_bf16x2(uint32_t x) {
   return y;
 }
 
-// One hidden layer of N=64 outputs for both 16-row tiles: acc = X W^T + b.
+// One hidden layer of N=64 outputs for one 16-row tile: acc = X W^T + b.
 template <int KS>
-__device__ __forceinline__ void mlp_layer64(const uint32_t (&a)[2][KS][4], const uint2 *frag,
-                                            const float *bias, float (&acc)[2][8][4], int lane) {
+__device__ __forceinline__ void mlp_layer64(const uint32_t (&a)[KS][4], const uint2 *frag, const float *bias,
+                                            float (&acc)[8][4], int lane) {
   const int t = lane & 3;
 #pragma unroll
   for (int nt = 0; nt < 8; ++nt) {
     const float b0 = bias[nt * 8 + 2 * t], b1 = bias[nt * 8 + 2 * t + 1];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-      acc[mt][nt][0] = b0;
-      acc[mt][nt][1] = b1;
-      acc[mt][nt][2] = b0;
-      acc[mt][nt][3] = b1;
-    }
+    acc[nt][0] = b0;
+    acc[nt][1] = b1;
+    acc[nt][2] = b0;
+    acc[nt][3] = b1;
   }
 #pragma unroll
   for (int ks = 0; ks < KS; ++ks)
 #pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      const uint2 b = frag[(ks * 8 + nt) * 32 + lane];
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt) mma_bf16_16816(acc[mt][nt], a[mt][ks], b);
-    }
+    for (int nt = 0; nt < 8; ++nt) mma_bf16_16816(acc[nt], a[ks], frag[(ks * 8 + nt) * 32 + lane]);
 }
 
-// Accumulator tiles of a 64-wide layer -> SiLU -> A fragments (K = 64, 4 slices) of the next.
+// Accumulator tile of a 64-wide layer -> SiLU -> A fragments (K = 64, 4 slices) of the next.
 // The C fragment of n-tiles (2ks, 2ks+1) holds exactly the A fragment of k-slice ks, so the
 // activations never leave registers.
-__device__ __forceinline__ void mlp_activate(const float (&acc)[2][8][4], uint32_t (&a)[2][4][4]) {
+__device__ __forceinline__ void mlp_activate(const float (&acc)[8][4], uint32_t (&a)[4][4]) {
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-    for (int ks = 0; ks < 4; ++ks) {
-      a[mt][ks][0] = silu_bf16x2(pack_bf16x2(acc[mt][2 * ks][0], acc[mt][2 * ks][1]));
-      a[mt][ks][1] = silu_bf16x2(pack_bf16x2(acc[mt][2 * ks][2], acc[mt][2 * ks][3]));
-      a[mt][ks][2] = silu_bf16x2(pack_bf16x2(acc[mt][2 * ks + 1][0], acc[mt][2 * ks + 1][1]));
-      a[mt][ks][3] = silu_bf16x2(pack_bf16x2(acc[mt][2 * ks + 1][2], acc[mt][2 * ks + 1][3]));
-    }
+  for (int ks = 0; ks < 4; ++ks) {
+    a[ks][0] = silu_bf16x2(pack_bf16x2(acc[2 * ks][0], acc[2 * ks][1]));
+    a[ks][1] = silu_bf16x2(pack_bf16x2(acc[2 * ks][2], acc[2 * ks][3]));
+    a[ks][2] = silu_bf16x2(pack_bf16x2(acc[2 * ks + 1][0], acc[2 * ks + 1][1]));
+    a[ks][3] = silu_bf16x2(pack_bf16x2(acc[2 * ks + 1][2], acc[2 * ks + 1][3]));
+  }
 }
 
 // Forward pass for the 32 particles of a warp.  in[6] are this lane's normalised features,
 // out[6] receives this lane's outputs (normalised units).  xs (32 x 16 bf16) and ys
 // (32 x 8 float) are per-warp shared scratch.  Every lane of the warp must call this together.
+// The two 16-row tiles run one after the other, so that one tile's accumulators (32 floats)
+// and activations (16 words) are live at a time.
 __device__ __forceinline__ void mlp_forward_warp(const float (&in)[kMlpIn], float (&out)[kMlpOut],
                                                  const uint2 *frag, const float *bias,
                                                  __nv_bfloat16 *xs, float *ys) {
@@ -257,50 +250,36 @@ __device__ __forceinline__ void mlp_forward_warp(const float (&in)[kMlpIn], floa
 #pragma unroll
   for (int k = 0; k < 16; ++k) xs[lane * 16 + k] = __float2bfloat16_rn(k < kMlpIn ? in[k] : 0.f);
   __syncwarp();
-  uint32_t a1[2][1][4];
   const uint32_t *xw = reinterpret_cast<const uint32_t *>(xs);  // 8 words per row
-#pragma unroll
+#pragma unroll 1
   for (int mt = 0; mt < 2; ++mt) {
     const int r0 = mt * 16 + g, r1 = r0 + 8;
-    a1[mt][0][0] = xw[r0 * 8 + t];
-    a1[mt][0][1] = xw[r1 * 8 + t];
-    a1[mt][0][2] = xw[r0 * 8 + 4 + t];
-    a1[mt][0][3] = xw[r1 * 8 + 4 + t];
-  }
-  float acc[2][8][4];
-  uint32_t ah[2][4][4];
-  mlp_layer64<1>(a1, frag + kFragOff1, bias, acc, lane);
-  mlp_activate(acc, ah);
-  mlp_layer64<4>(ah, frag + kFragOff2, bias + 64, acc, lane);
-  mlp_activate(acc, ah);
-  mlp_layer64<4>(ah, frag + kFragOff3, bias + 128, acc, lane);
-  mlp_activate(acc, ah);
-  // output layer, N = 8 (6 used)
-  float o[2][4];
-  {
+    uint32_t a1[1][4];
+    a1[0][0] = xw[r0 * 8 + t];
+    a1[0][1] = xw[r1 * 8 + t];
+    a1[0][2] = xw[r0 * 8 + 4 + t];
+    a1[0][3] = xw[r1 * 8 + 4 + t];
+    float acc[8][4];
+    uint32_t ah[4][4];
+    mlp_layer64<1>(a1, frag + kFragOff1, bias, acc, lane);
+    mlp_activate(acc, ah);
+    mlp_layer64<4>(ah, frag + kFragOff2, bias + 64, acc, lane);
+    mlp_activate(acc, ah);
+    mlp_layer64<4>(ah, frag + kFragOff3, bias + 128, acc, lane);
+    mlp_activate(acc, ah);
+    // output layer, N = 8 (6 used)
+    float o[4];
     const float b0 = bias[192 + 2 * t], b1 = bias[192 + 2 * t + 1];
+    o[0] = b0;
+    o[1] = b1;
+    o[2] = b0;
+    o[3] = b1;
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-      o[mt][0] = b0;
-      o[mt][1] = b1;
-      o[mt][2] = b0;
-      o[mt][3] = b1;
-    }
-#pragma unroll
-    for (int ks = 0; ks < 4; ++ks) {
-      const uint2 b = frag[kFragOff4 + ks * 32 + lane];
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt) mma_bf16_16816(o[mt], ah[mt][ks], b);
-    }
-  }
-  __syncwarp();
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
-    const int r0 = mt * 16 + g, r1 = r0 + 8;
-    ys[r0 * 8 + 2 * t] = o[mt][0];
-    ys[r0 * 8 + 2 * t + 1] = o[mt][1];
-    ys[r1 * 8 + 2 * t] = o[mt][2];
-    ys[r1 * 8 + 2 * t + 1] = o[mt][3];
+    for (int ks = 0; ks < 4; ++ks) mma_bf16_16816(o, ah[ks], frag[kFragOff4 + ks * 32 + lane]);
+    ys[r0 * 8 + 2 * t] = o[0];
+    ys[r0 * 8 + 2 * t + 1] = o[1];
+    ys[r1 * 8 + 2 * t] = o[2];
+    ys[r1 * 8 + 2 * t + 1] = o[3];
   }
   __syncwarp();
 #pragma unroll
