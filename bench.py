@@ -7,7 +7,12 @@ second box moving at (-1,0,0) m/s, slip walls, dt=5e-5.  A step is one full subs
 (activation, binning, P2G, grid update, G2P with SVD + return map).  Inputs (4.4 GB of
 particle state) are larger than the 126 MB L2, so no flush is needed between steps.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--scene dp|fc|snow16m]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--scene dp|dp128|fc|snow16m|batch256]
+
+--scene batch256 runs the batched workload: 256 independent scenes (15,386,080 particles,
+per-scene counts log-uniform in [4k, 200k], half fixed corotated, half Drucker-Prager) advanced
+together, one launch per stage.  Launch shapes are picked by the library's autotuner first.
 
 Under torchrun every rank runs an independent replica (the path has no exchange step) and
 rank 0 prints one JSON line; time is the max over ranks of CUDA-event time.
@@ -52,7 +57,19 @@ def scene_for(name: str):
         return scenes.config1(), "fc_cube_dx128_8ppc"
     if name == "snow16m":
         return scenes.config5_16m(), "snow_sphere_slab_dx295_4ppc"
+    if name == "batch256":
+        from zsmpm_b200 import batch
+        return batch.config4(), "batch_256_scenes_dx128_8ppc"
     raise SystemExit(f"unknown scene {name}")
+
+
+def generate_workload(spec):
+    """(concatenated particles, per-scene Particles list or None)."""
+    from zsmpm_b200 import batch, scenes
+    if isinstance(spec, list):
+        parts = batch.generate_all(spec)
+        return batch._concat(parts), parts
+    return scenes.generate(spec), None
 
 
 class ClockSampler:
@@ -230,9 +247,35 @@ def cpu_baseline_sample(spec, p, max_particles: int):
     return p.subset(idx), f"slab z < {cut:.4f} of the workload ({len(idx)} particles)"
 
 
+def reference_cpu_rate(spec, p, parts, steps, warmup, max_particles, threads, timeout):
+    """Particle-substeps/s of the reference's omp_exec path (oracle/_ref) on a bounded sample:
+    a z-slab of a single scene, or the first scenes of a batch (each its own system, as the
+    reference advances them one after another) up to max_particles."""
+    from oracle import reference
+    if parts is None:
+        sample, desc = cpu_baseline_sample(spec, p, max_particles)
+        jobs = [(spec, sample)]
+    else:
+        jobs, total = [], 0
+        for sp, q in zip(spec, parts):
+            if total and total + q.n > max_particles:
+                break
+            jobs.append((sp, q))
+            total += q.n
+        desc = f"the first {len(jobs)} of {len(spec)} scenes ({total} particles), run one after another"
+    if warmup:
+        sp0, q0 = jobs[0]
+        reference.run(sp0, q0, warmup, policy=reference.POLICY_OMP, threads=threads, cap_blocks=0, timeout=timeout)
+    seconds, work = 0.0, 0
+    for sp, q in jobs:
+        r = reference.run(sp, q, steps, policy=reference.POLICY_OMP, threads=threads, cap_blocks=0, timeout=timeout)
+        seconds += r.seconds
+        work += q.n * steps
+    return work / seconds, desc
+
+
 def run_reference_arm(args, spec, workload, n_full):
     from oracle import reference
-    from zsmpm_b200 import scenes
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -240,21 +283,16 @@ def run_reference_arm(args, spec, workload, n_full):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/zsref_cli not built "
                           "(the reference sources were not present when build() ran)"}))
         return 0
-    p = scenes.generate(spec)
-    sample, desc = cpu_baseline_sample(spec, p, args.ref_particles)
+    p, parts = generate_workload(spec)
     threads = os.cpu_count() or 1
-    # warm-up (separate process run), then K timed substeps on the sample
-    reference.run(spec, sample, max(args.warmup, 1), policy=reference.POLICY_OMP, threads=threads,
-                  cap_blocks=0, timeout=1800)
-    r = reference.run(spec, sample, args.steps, policy=reference.POLICY_OMP, threads=threads,
-                      cap_blocks=0, timeout=3600)
-    value = sample.n * args.steps / r.seconds
+    value, desc = reference_cpu_rate(spec, p, parts, args.steps, max(args.warmup, 1), args.ref_particles,
+                                     threads, 3600)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * r.seconds / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": workload, "particles": n_full, "sample_particles": sample.n,
-                       "parallelism": "omp", "policy": "zs::omp_exec"},
+            "config": {"workload": workload, "particles": n_full, "parallelism": "omp",
+                       "policy": "zs::omp_exec"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -268,11 +306,12 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scene", default="dp", choices=["dp", "dp128", "fc", "snow16m"])
+    ap.add_argument("--scene", default="dp", choices=["dp", "dp128", "fc", "snow16m", "batch256"])
     ap.add_argument("--ref-particles", type=int, default=1_500_000)
     ap.add_argument("--ref-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-closure leg")
+    ap.add_argument("--no-autotune", action="store_true", help="default launch shapes")
     ap.add_argument("--train-random", type=int, default=1_500_000)
     ap.add_argument("--train-logged", type=int, default=500_000)
     args = ap.parse_args(argv)
@@ -280,18 +319,21 @@ def main(argv=None):
     spec, workload = scene_for(args.scene)
     from zsmpm_b200 import scenes
     if args.impl == "reference":
-        return run_reference_arm(args, spec, workload, scenes.count_particles(spec))
+        n_full = (sum(scenes.count_particles(sp) for sp in spec) if isinstance(spec, list)
+                  else scenes.count_particles(spec))
+        return run_reference_arm(args, spec, workload, n_full)
 
     ws, rank, local = dist_setup()
     import torch
 
     import zsmpm_b200 as zs
     torch.cuda.set_device(local)
-    p = scenes.generate(spec)
+    p, parts = generate_workload(spec)
     n = p.n
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
-    plastic = spec.material.model != zs.FIXED_COROTATED
+    specs = spec if isinstance(spec, list) else [spec]
+    plastic = any(sp.material.model != zs.FIXED_COROTATED for sp in specs)
 
     # pinned host copies of the inputs for the end-to-end leg
     pinned = {k: torch.from_numpy(getattr(p, k)).pin_memory() for k in ("m", "x", "v", "C", "F", "plastic")}
@@ -300,17 +342,29 @@ def main(argv=None):
     h2d_bytes = sum(t.numel() * 4 for t in pinned.values())
     d2h_bytes = (out_x.numel() + out_v.numel()) * 4 + 4
 
-    sc = zs.Scene(spec, device=local)
     lib = zs._abi.lib()
+    if parts is None:
+        sc = zs.Scene(spec, device=local)
+    else:
+        from zsmpm_b200 import batch
+        sc = batch.Batch(spec, device=local)
+        counts = (C.c_int64 * len(parts))(*[q.n for q in parts])
 
     def upload_pinned():
         arrs = zs._abi.ParticleArrays(**{k: C.c_void_p(t.data_ptr()) for k, t in pinned.items()})
-        zs._abi.check(lib.zsmpm_scene_upload(sc.handle, C.byref(arrs), n, 0, C.c_void_p(sptr)), "upload")
+        if parts is None:
+            zs._abi.check(lib.zsmpm_scene_upload(sc.handle, C.byref(arrs), n, 0, C.c_void_p(sptr)), "upload")
+        else:
+            zs._abi.check(lib.zsmpm_batch_upload(sc.handle, C.byref(arrs), counts, 0, C.c_void_p(sptr)), "upload")
         sc.n = n
 
     def download_xv():
         arrs = zs._abi.ParticleArrays(x=C.c_void_p(out_x.data_ptr()), v=C.c_void_p(out_v.data_ptr()))
         zs._abi.check(lib.zsmpm_scene_download(sc.handle, C.byref(arrs), 0, C.c_void_p(sptr)), "download")
+
+    # ---------------------------------------------------------------- launch shapes
+    upload_pinned()
+    tuning = sc.autotune(trials=2, stream=sptr) if not args.no_autotune else None
 
     # ---------------------------------------------------------------- device-resident leg
     upload_pinned()
@@ -366,7 +420,7 @@ def main(argv=None):
 
     # ---------------------------------------------------------------- learned-closure leg
     learned = None
-    if plastic and not args.no_learned:
+    if plastic and parts is None and not args.no_learned:
         learned = learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, ms / args.steps)
 
     # ---------------------------------------------------------------- CPU baseline (rank 0, N=1)
@@ -375,11 +429,9 @@ def main(argv=None):
         try:
             from oracle import reference
             if reference.available():
-                sample, desc = cpu_baseline_sample(spec, p, args.ref_particles)
                 threads = os.cpu_count() or 1
-                r = reference.run(spec, sample, args.ref_steps, policy=reference.POLICY_OMP,
-                                  threads=threads, cap_blocks=0, timeout=900)
-                cpu = {"value": sample.n * args.ref_steps / r.seconds, "unit": UNIT, "cores": threads,
+                rate, desc = reference_cpu_rate(spec, p, parts, args.ref_steps, 0, args.ref_particles, threads, 900)
+                cpu = {"value": rate, "unit": UNIT, "cores": threads,
                        "kind": "reference", "sample": f"{desc}, {args.ref_steps} substeps, zs::omp_exec"}
             else:
                 cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
@@ -393,11 +445,12 @@ def main(argv=None):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload, "particles": n, "active_blocks": nb,
-                       "dx": spec.dx, "ppc": spec.ppc, "dt": spec.dt, "material": "drucker_prager"
-                       if spec.material.model == zs.DRUCKER_PRAGER else
-                       ("snow" if spec.material.model == zs.SNOW else "fixed_corotated"),
-                       "closure": "plain", "parallelism": f"replicas{ws}",
+            "config": {"workload": workload, "particles": n, "active_blocks": nb, "scenes": len(specs),
+                       "dx": specs[0].dx, "ppc": specs[0].ppc, "dt": specs[0].dt,
+                       "material": "mixed fixed_corotated / drucker_prager" if len(specs) > 1 else
+                       ("drucker_prager" if specs[0].material.model == zs.DRUCKER_PRAGER else
+                        ("snow" if specs[0].material.model == zs.SNOW else "fixed_corotated")),
+                       "closure": "plain", "parallelism": f"replicas{ws}", "launch_shapes": tuning,
                        "l2": "inputs larger than L2 (particle state 4+ GB)",
                        "substep_graph": "CUDA graph of 2 substeps"},
             "roofline": {"bound": "hbm", "kernel": "k_g2p", "achieved": g2p_gbs, "peak": peak,

@@ -121,7 +121,7 @@ typedef struct {
                                (SparsityCompute.tpp:11-14); capacity next_2pow(n)*16 */
   int32_t block_order;      /* zsmpm_block_order */
   int32_t device;           /* CUDA device ordinal */
-  int32_t threads_per_cta;  /* 0 = autotuned/default; else 128, 256 or 512 */
+  int32_t threads_per_cta;  /* G2P CTA size: 0 = default (256) or the autotuner's pick; 128 or 256 */
 } zsmpm_scene_desc;
 
 /* Particle arrays in the reference's zs::Particles<f32,3> layout: one array per attribute,
@@ -203,8 +203,9 @@ ZSMPM_API zsmpm_status zsmpm_grid_update(zsmpm_scene *scene, void *stream);
 ZSMPM_API zsmpm_status zsmpm_g2p(zsmpm_scene *scene, void *stream);
 /* One full substep (activate, bin, P2G, grid update + walls, G2P). */
 ZSMPM_API zsmpm_status zsmpm_substep(zsmpm_scene *scene, void *stream);
-/* nsteps substeps replayed from a CUDA graph of one substep (captured on first use);
- * checks the device status word once at the end. */
+/* nsteps substeps, replayed from a CUDA graph of two substeps (captured on first use per
+ * buffer parity; an odd last substep is launched directly).  Asynchronous: capacity and
+ * domain errors collect in the device status word, which zsmpm_scene_status reads. */
 ZSMPM_API zsmpm_status zsmpm_run(zsmpm_scene *scene, int32_t nsteps, void *stream);
 
 /* ---- views and diagnostics ------------------------------------------------------- */
@@ -233,6 +234,39 @@ ZSMPM_API zsmpm_status zsmpm_svd3(const float *A, float *U, float *S, float *V, 
  * plastic (in/out) and tau = V0 P F^T (out). */
 ZSMPM_API zsmpm_status zsmpm_constitutive(const zsmpm_material *mat, float *F, float *plastic,
                                           float *tau, int64_t count, void *stream);
+
+/* ---- batched scenes ------------------------------------------------------------ */
+/* Many independent MPM systems advanced together: every stage is one launch over the blocks
+ * of all scenes, and zsmpm_run replays one CUDA graph for the whole batch.  The scenes share
+ * dx, dt, gravity and walls (desc; walls in each scene's own [0,1]^3) and have a material
+ * each.  Particle positions stay in scene coordinates; scene s's block keys are offset by 32
+ * blocks per axis times its slot (s & 7, (s >> 3) & 7, s >> 6), so the scenes never share a
+ * block.  Limits: 1/dx <= 176, at most 65,536 scenes, each scene's particles inside
+ * [-4 * 8 dx, 27 * 8 dx) per axis (else ZSMPM_ERR_OUT_OF_DOMAIN).  Drucker-Prager scenes run
+ * the committed plasticity ordering.  No counterpart in the reference, which advances one
+ * system per launch sequence. */
+ZSMPM_API zsmpm_status zsmpm_batch_create(const zsmpm_scene_desc *desc, const zsmpm_material *materials,
+                                          int32_t nscenes, zsmpm_scene **out);
+/* Particles of all scenes concatenated in scene order, counts[nscenes] per scene.  Downloads
+ * (zsmpm_scene_download) return them in the same order.  Other scene calls (run, substep,
+ * stages, status, download, views, timing, autotune) work on a batch as on one scene. */
+ZSMPM_API zsmpm_status zsmpm_batch_upload(zsmpm_scene *s, const zsmpm_particle_arrays *p, const int64_t *counts,
+                                          int32_t on_device, void *stream);
+ZSMPM_API zsmpm_status zsmpm_batch_num_scenes(const zsmpm_scene *s, int32_t *out);
+
+/* ---- launch-shape autotuner ----------------------------------------------------- */
+typedef struct {
+  int32_t g2p_threads;      /* G2P CTA size: 128 or 256 (0 = default 256) */
+  int32_t g2p_ctas_per_sm;  /* persistent G2P CTAs per SM, 1-4 (0 = default 2) */
+  int32_t p2g_ctas_per_sm;  /* persistent P2G CTAs per SM, 1-2 (0 = default 2) */
+  float g2p_ms, p2g_ms;     /* stage times of the chosen shapes (autotune output) */
+} zsmpm_tuning;
+
+/* Times G2P over CTA size x CTAs per SM and P2G over CTAs per SM on the uploaded particles
+ * (one untimed and `trials` timed substeps per candidate; this advances the simulation by
+ * those substeps), keeps the fastest of each and returns them in *out (optional). */
+ZSMPM_API zsmpm_status zsmpm_autotune(zsmpm_scene *s, int32_t trials, zsmpm_tuning *out, void *stream);
+ZSMPM_API zsmpm_status zsmpm_set_tuning(zsmpm_scene *s, const zsmpm_tuning *t);
 
 /* ---- learned return-mapping closure -------------------------------------------- */
 /* An MLP 6 -> 64 -> 64 -> 64 -> 6 (SiLU) that replaces the return-mapping branch of the

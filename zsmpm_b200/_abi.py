@@ -59,6 +59,11 @@ class GridView(C.Structure):
                 ("keys", C.c_void_p)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("g2p_threads", C.c_int32), ("g2p_ctas_per_sm", C.c_int32), ("p2g_ctas_per_sm", C.c_int32),
+                ("g2p_ms", C.c_float), ("p2g_ms", C.c_float)]
+
+
 MLP_PARAMS = 9158  # 6 -> 64 -> 64 -> 64 -> 6
 
 
@@ -107,6 +112,11 @@ SIGNATURES = {
     "zsmpm_kernels_per_substep": (C.c_int32, [_P]),
     "zsmpm_svd3": (_S, [_P, _P, _P, _P, C.c_int64, _P]),
     "zsmpm_constitutive": (_S, [C.POINTER(Material), _P, _P, _P, C.c_int64, _P]),
+    "zsmpm_batch_create": (_S, [C.POINTER(SceneDesc), C.POINTER(Material), C.c_int32, C.POINTER(_P)]),
+    "zsmpm_batch_upload": (_S, [_P, C.POINTER(ParticleArrays), _P, C.c_int32, _P]),
+    "zsmpm_batch_num_scenes": (_S, [_P, C.POINTER(C.c_int32)]),
+    "zsmpm_autotune": (_S, [_P, C.c_int32, C.POINTER(Tuning), _P]),
+    "zsmpm_set_tuning": (_S, [_P, C.POINTER(Tuning)]),
     "zsmpm_closure_create": (_S, [C.POINTER(Material), C.c_int32, C.POINTER(_P)]),
     "zsmpm_closure_destroy": (_S, [_P]),
     "zsmpm_closure_build_dataset": (_S, [_P, C.c_int64, C.c_uint64, _P, C.c_int64, _P]),

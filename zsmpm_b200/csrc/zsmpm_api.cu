@@ -36,6 +36,10 @@ struct zsmpm_scene {
   float stage_ms[5] = {};
   std::vector<void *> allocations;
   double *audit = nullptr;                  // closure audit accumulators (device, 8 doubles)
+  // batched scenes
+  int nscenes = 0;                          // 0: a single scene
+  bool any_plastic = false;
+  std::vector<int64_t> counts;              // particles of each scene (last upload)
   unsigned long long *log_count = nullptr;  // trial-state log counter (device)
 };
 
@@ -138,7 +142,7 @@ zsmpm_status status_from_word(int w) {
 }
 
 zsmpm_status allocate_particles(zsmpm_scene *s, int64_t cap) {
-  const bool plastic = s->desc.material.model != ZSMPM_FIXED_COROTATED;
+  const bool plastic = s->desc.material.model != ZSMPM_FIXED_COROTATED || s->any_plastic;
   for (int k = 0; k < 2; ++k) {
     particle_buffers &b = s->bufs[k];
     ZS_ALLOC(b.xm, cap, "alloc xm");
@@ -148,6 +152,7 @@ zsmpm_status allocate_particles(zsmpm_scene *s, int64_t cap) {
     ZS_ALLOC(b.F, 9 * cap, "alloc F");
     if (plastic) ZS_ALLOC(b.plastic, cap, "alloc plastic");
     ZS_ALLOC(b.id, cap, "alloc id");
+    if (s->nscenes > 0) ZS_ALLOC(b.sid, cap, "alloc scene ids");
   }
   scene_device &d = s->dev;
   ZS_ALLOC(d.key32, cap, "alloc key32");
@@ -268,6 +273,8 @@ ZSMPM_API zsmpm_status zsmpm_scene_create(const zsmpm_scene_desc *desc, zsmpm_sc
   if (desc->material.model < 0 || desc->material.model > 2)
     return fail(ZSMPM_ERR_INVALID_ARG, "unknown material model");
   if (desc->wall_type < 0 || desc->wall_type > 3) return fail(ZSMPM_ERR_INVALID_ARG, "unknown wall type");
+  if (desc->threads_per_cta != 0 && desc->threads_per_cta != 128 && desc->threads_per_cta != 256)
+    return fail(ZSMPM_ERR_INVALID_ARG, "threads_per_cta must be 0, 128 or 256");
   if (desc->block_order != ZSMPM_BLOCK_ORDER_SORTED)
     return fail(ZSMPM_ERR_INVALID_ARG, "only ZSMPM_BLOCK_ORDER_SORTED is implemented by the device path");
   if (zsmpm_device_count() <= 0) return fail(ZSMPM_ERR_NO_DEVICE, "no CUDA device visible");
@@ -289,6 +296,7 @@ ZSMPM_API zsmpm_status zsmpm_scene_create(const zsmpm_scene_desc *desc, zsmpm_sc
   p.wall_type = desc->wall_type;
   p.wall_cells = desc->wall_cells;
   p.mat = make_material(desc->material);
+  p.g2p_threads = desc->threads_per_cta;
   for (auto &ev : s->ev) cudaEventCreate(&ev);
   e = prepare_kernels();
   if (e != cudaSuccess) {
@@ -329,10 +337,20 @@ static zsmpm_status prepare_upload(zsmpm_scene *s, int64_t n) {
   return ZSMPM_OK;
 }
 
+static zsmpm_status upload_arrays(zsmpm_scene *s, const zsmpm_particle_arrays *p, int64_t n, int32_t on_device,
+                                  void *stream);
+
 ZSMPM_API zsmpm_status zsmpm_scene_upload(zsmpm_scene *s, const zsmpm_particle_arrays *p, int64_t n,
                                           int32_t on_device, void *stream) {
   zsmpm_status st = check_scene(s, false);
   if (st != ZSMPM_OK) return st;
+  if (s->nscenes > 0) return fail(ZSMPM_ERR_INVALID_ARG, "a batch takes zsmpm_batch_upload");
+  return upload_arrays(s, p, n, on_device, stream);
+}
+
+static zsmpm_status upload_arrays(zsmpm_scene *s, const zsmpm_particle_arrays *p, int64_t n, int32_t on_device,
+                                  void *stream) {
+  zsmpm_status st = ZSMPM_OK;
   if (!p || !p->m || !p->x) return fail(ZSMPM_ERR_INVALID_ARG, "m and x are required");
   st = prepare_upload(s, n);
   if (st != ZSMPM_OK) return st;
@@ -386,6 +404,7 @@ ZSMPM_API zsmpm_status zsmpm_scene_upload_tilevector(zsmpm_scene *s, const zsmpm
   if (st != ZSMPM_OK) return st;
   if (!tv || !tv->base || tv->lane_width != 32 || tv->off_m < 0 || tv->off_x < 0)
     return fail(ZSMPM_ERR_INVALID_ARG, "tile vector view needs base, lane_width 32, m and x");
+  if (s->nscenes > 0) return fail(ZSMPM_ERR_INVALID_ARG, "a batch takes zsmpm_batch_upload");
   st = prepare_upload(s, n);
   if (st != ZSMPM_OK) return st;
   cudaStream_t cs = as_stream(stream);
@@ -677,6 +696,7 @@ ZSMPM_API zsmpm_status zsmpm_scene_set_closure(zsmpm_scene *s, zsmpm_closure *c,
     s->dev.aux.learned = 0;
     return ZSMPM_OK;
   }
+  if (s->nscenes > 0) return fail(ZSMPM_ERR_INVALID_ARG, "the learned closure runs on single scenes");
   closure_dev cd{};
   if (!closure_device_view(c, &cd)) return fail(ZSMPM_ERR_NOT_READY, "closure has no dataset or state yet");
   if (cd.model != s->desc.material.model)
@@ -721,6 +741,7 @@ ZSMPM_API zsmpm_status zsmpm_scene_set_state_log(zsmpm_scene *s, float *buffer, 
   zsmpm_status st = check_scene(s, false);
   if (st != ZSMPM_OK) return st;
   if (period < 0 || (period > 0 && (!buffer || cap < 1))) return fail(ZSMPM_ERR_INVALID_ARG, "bad log arguments");
+  if (period > 0 && s->nscenes > 0) return fail(ZSMPM_ERR_INVALID_ARG, "the state log runs on single scenes");
   if (!s->log_count) {
     unsigned long long *c = nullptr;
     ZS_TRY(cudaMalloc(&c, sizeof(unsigned long long)), "alloc log counter");
@@ -747,6 +768,159 @@ ZSMPM_API zsmpm_status zsmpm_scene_state_log_count(zsmpm_scene *s, int64_t *coun
   unsigned long long c = 0;
   ZS_TRY(cudaMemcpy(&c, s->log_count, sizeof(c), cudaMemcpyDeviceToHost), "read log counter");
   *count_out = (int64_t)std::min<unsigned long long>(c, (unsigned long long)std::max<int64_t>(s->dev.aux.log_cap, 0));
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_batch_create(const zsmpm_scene_desc *desc, const zsmpm_material *materials,
+                                          int32_t nscenes, zsmpm_scene **out) {
+  if (!desc || !materials || !out) return fail(ZSMPM_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (nscenes < 1 || nscenes > kBatchMaxScenes) return fail(ZSMPM_ERR_INVALID_ARG, "nscenes out of range");
+  if (!(desc->dx > 0.f) || 1.f / desc->dx > 8.f * (kBatchSlot - kBatchMargin - 2))
+    return fail(ZSMPM_ERR_INVALID_ARG, "batched scenes need 1/dx <= 176 (a scene's [0,1]^3 fits its key slot)");
+  bool plastic = false;
+  for (int k = 0; k < nscenes; ++k) {
+    const zsmpm_material &m = materials[k];
+    if (m.model < 0 || m.model > 2) return fail(ZSMPM_ERR_INVALID_ARG, "unknown material model in batch");
+    if (m.model == ZSMPM_DRUCKER_PRAGER && m.plasticity_mode != ZSMPM_PLASTICITY_COMMITTED)
+      return fail(ZSMPM_ERR_INVALID_ARG, "batched scenes run the committed plasticity ordering");
+    plastic = plastic || m.model != ZSMPM_FIXED_COROTATED;
+  }
+  zsmpm_scene_desc d = *desc;
+  d.material = materials[0];
+  zsmpm_scene *s = nullptr;
+  zsmpm_status st = zsmpm_scene_create(&d, &s);
+  if (st != ZSMPM_OK) return st;
+  s->nscenes = nscenes;
+  s->any_plastic = plastic;
+  std::vector<material_dev> mats(nscenes);
+  for (int k = 0; k < nscenes; ++k) mats[k] = make_material(materials[k]);
+  material_dev *dm = nullptr;
+  int *ds = nullptr;
+  cudaError_t e = cudaMalloc(&dm, sizeof(material_dev) * nscenes);
+  if (e == cudaSuccess) s->allocations.push_back(dm);
+  if (e == cudaSuccess) e = cudaMalloc(&ds, sizeof(int) * (nscenes + 1));
+  if (e == cudaSuccess) s->allocations.push_back(ds);
+  if (e == cudaSuccess) e = cudaMemcpy(dm, mats.data(), sizeof(material_dev) * nscenes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    zsmpm_scene_destroy(s);
+    return cuda_fail(e, "batch materials");
+  }
+  s->dev.prm.batch = 1;
+  s->dev.prm.nscenes = nscenes;
+  s->dev.prm.mats = dm;
+  s->dev.prm.scene_start = ds;
+  *out = s;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_batch_upload(zsmpm_scene *s, const zsmpm_particle_arrays *p, const int64_t *counts,
+                                          int32_t on_device, void *stream) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (s->nscenes < 1) return fail(ZSMPM_ERR_INVALID_ARG, "not a batch (zsmpm_batch_create)");
+  if (!counts) return fail(ZSMPM_ERR_INVALID_ARG, "null counts");
+  std::vector<int> start(s->nscenes + 1, 0);
+  int64_t n = 0;
+  for (int k = 0; k < s->nscenes; ++k) {
+    if (counts[k] < 0) return fail(ZSMPM_ERR_INVALID_ARG, "negative scene particle count");
+    n += counts[k];
+    if (n > (int64_t)0x7fffffff) return fail(ZSMPM_ERR_INVALID_ARG, "particle count out of range");
+    start[k + 1] = (int)n;
+  }
+  ZS_TRY(cudaMemcpy(const_cast<int *>(s->dev.prm.scene_start), start.data(), sizeof(int) * start.size(),
+                    cudaMemcpyHostToDevice),
+         "scene starts");
+  s->counts.assign(counts, counts + s->nscenes);
+  return upload_arrays(s, p, n, on_device, stream);
+}
+
+ZSMPM_API zsmpm_status zsmpm_batch_num_scenes(const zsmpm_scene *s, int32_t *out) {
+  if (!s || !out) return fail(ZSMPM_ERR_INVALID_ARG, "null argument");
+  *out = s->nscenes;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_autotune(zsmpm_scene *s, int32_t trials, zsmpm_tuning *out, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (trials < 1) return fail(ZSMPM_ERR_INVALID_ARG, "trials < 1");
+  cudaStream_t cs = as_stream(stream);
+  scene_params &p = s->dev.prm;
+  const bool was_timing = s->timing;
+  s->timing = true;
+  invalidate_graphs(s);
+  // time one stage under a launch shape: one untimed substep, then `trials` timed ones
+  auto time_stage = [&](int stage, float *ms) -> zsmpm_status {
+    float total = 0.f;
+    for (int r = 0; r <= trials; ++r) {
+      zsmpm_status q = substep_enqueue(s, cs);
+      if (q != ZSMPM_OK) return q;
+      ZS_TRY(cudaStreamSynchronize(cs), "tune sync");
+      float t = 0.f;
+      ZS_TRY(cudaEventElapsedTime(&t, s->ev[stage], s->ev[stage + 1]), "tune timing");
+      if (r > 0) total += t;
+    }
+    *ms = total / trials;
+    return read_status(s);
+  };
+  zsmpm_tuning best{};
+  // G2P: CTA size x CTAs per SM (each CTA owns one block at a time)
+  float best_g2p = 3.4e38f;
+  const int g2p_threads[2] = {256, 128};
+  const int g2p_per_sm[4] = {1, 2, 3, 4};
+  for (int a : g2p_threads)
+    for (int b : g2p_per_sm) {
+      if (s->dev.aux.learned && (a != 256 || b > 2)) continue;  // learned G2P: 256 threads, <= 2 per SM
+      p.g2p_threads = a;
+      p.g2p_ctas_per_sm = b;
+      float ms = 0.f;
+      st = time_stage(4, &ms);
+      if (st != ZSMPM_OK) break;
+      if (ms < best_g2p) {
+        best_g2p = ms;
+        best.g2p_threads = a;
+        best.g2p_ctas_per_sm = b;
+      }
+    }
+  float best_p2g = 3.4e38f;
+  if (st == ZSMPM_OK)
+    for (int b : {1, 2}) {
+      p.p2g_ctas_per_sm = b;
+      float ms = 0.f;
+      st = time_stage(2, &ms);
+      if (st != ZSMPM_OK) break;
+      if (ms < best_p2g) {
+        best_p2g = ms;
+        best.p2g_ctas_per_sm = b;
+      }
+    }
+  s->timing = was_timing;
+  if (st != ZSMPM_OK) return st;
+  p.g2p_threads = best.g2p_threads;
+  p.g2p_ctas_per_sm = best.g2p_ctas_per_sm;
+  p.p2g_ctas_per_sm = best.p2g_ctas_per_sm;
+  best.g2p_ms = best_g2p;
+  best.p2g_ms = best_p2g;
+  invalidate_graphs(s);
+  s->last_stream = cs;
+  if (out) *out = best;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_set_tuning(zsmpm_scene *s, const zsmpm_tuning *t) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (!t) return fail(ZSMPM_ERR_INVALID_ARG, "null tuning");
+  if ((t->g2p_threads != 0 && t->g2p_threads != 128 && t->g2p_threads != 256) || t->g2p_ctas_per_sm < 0 ||
+      t->g2p_ctas_per_sm > 4 || t->p2g_ctas_per_sm < 0 || t->p2g_ctas_per_sm > 2)
+    return fail(ZSMPM_ERR_INVALID_ARG, "tuning out of range");
+  if (s->dev.aux.learned && t->g2p_threads == 128)
+    return fail(ZSMPM_ERR_INVALID_ARG, "the learned G2P runs 256-thread CTAs");
+  s->dev.prm.g2p_threads = t->g2p_threads;
+  s->dev.prm.g2p_ctas_per_sm = t->g2p_ctas_per_sm;
+  s->dev.prm.p2g_ctas_per_sm = t->p2g_ctas_per_sm;
+  invalidate_graphs(s);
   return ZSMPM_OK;
 }
 

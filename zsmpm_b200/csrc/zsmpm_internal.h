@@ -22,7 +22,15 @@ struct particle_buffers {
   float *F = nullptr;
   float *plastic = nullptr;  // logJp (DP) or Jp (snow); null for fixed corotated
   int *id = nullptr;         // upload index
+  int *sid = nullptr;        // scene of the particle (batched scenes only)
 };
+
+// Batched scenes share one key space: scene s owns a slot of kBatchSlot blocks per axis at
+// slot coordinates (s & 7, (s >> 3) & 7, s >> 6); its particles keep local positions and its
+// blocks lie in [-kBatchMargin, kBatchSlot - kBatchMargin) per axis before the slot offset.
+constexpr int kBatchSlot = 32;
+constexpr int kBatchMargin = 4;
+constexpr int kBatchMaxScenes = 1 << 16;
 
 // Device counters (int32), zeroed at the start of every substep except the status word and
 // the substep counter.
@@ -50,6 +58,14 @@ struct scene_params {
   float gravity[3];
   int wall_type, wall_cells;
   material_dev mat;
+  // batched scenes
+  int batch;                        // 1: particles carry a scene id, keys carry the scene slot
+  int nscenes;
+  const material_dev *mats;         // [nscenes] per-scene materials (device)
+  const int *scene_start;           // [nscenes + 1] upload-index ranges of the scenes (device)
+  // launch shapes (set by the autotuner; 0 = default)
+  int g2p_threads;                  // 128 or 256
+  int g2p_ctas_per_sm, p2g_ctas_per_sm;
 };
 
 // G2P options beside the plain path: the learned closure and the trial-state log.

@@ -87,6 +87,35 @@ __device__ __forceinline__ bool cell_of(const scene_params &p, float4 x, int3 &c
   return true;
 }
 
+// Batched scenes: the slot of a scene, the slot coordinate of a key component (keys of a
+// scene lie in [32 slot - 4, 32 slot + 28)), and the scene-local block of a key.
+__device__ __forceinline__ int3 slot_of_scene(int sc) { return make_int3(sc & 7, (sc >> 3) & 7, sc >> 6); }
+__device__ __forceinline__ int slot_coord(int k) { return (k + kBatchMargin) / kBatchSlot; }
+__device__ __forceinline__ int scene_of_key(int3 k) {
+  return slot_coord(k.x) + 8 * slot_coord(k.y) + 64 * slot_coord(k.z);
+}
+__device__ __forceinline__ int3 local_block(const scene_params &p, int3 k) {
+  if (!p.batch) return k;
+  return make_int3(k.x - kBatchSlot * slot_coord(k.x), k.y - kBatchSlot * slot_coord(k.y),
+                   k.z - kBatchSlot * slot_coord(k.z));
+}
+
+// Cell and block of particle i in the scene's key space: cell_of, then for batched scenes a
+// check that the local block leaves room for the +1 enlargement inside the slot, and the
+// slot offset.
+__device__ __forceinline__ bool particle_cell(const scene_device &s, int i, float4 x, int3 &c, int3 &b) {
+  if (!cell_of(s.prm, x, c, b)) return false;
+  if (s.prm.batch) {
+    const int hi = kBatchSlot - kBatchMargin - 1;
+    if (b.x < -kBatchMargin || b.x >= hi || b.y < -kBatchMargin || b.y >= hi || b.z < -kBatchMargin || b.z >= hi)
+      return false;
+    const int3 o = slot_of_scene(s.cur.sid[i]);
+    b = make_int3(b.x + kBatchSlot * o.x, b.y + kBatchSlot * o.y, b.z + kBatchSlot * o.z);
+    c = make_int3(c.x + 8 * kBatchSlot * o.x, c.y + 8 * kBatchSlot * o.y, c.z + 8 * kBatchSlot * o.z);
+  }
+  return true;
+}
+
 // ----------------------------------------------------------------- CTA scan helpers
 template <int NT>
 __device__ __forceinline__ int cta_exclusive_scan(int v, int &total, int *smem /* >= NT/32 + 1 */) {
@@ -217,7 +246,7 @@ __global__ void __launch_bounds__(kThreads) k_insert_particle_blocks(scene_devic
     int3 c, b = make_int3(0, 0, 0);
     bool valid = false;
     if (i < n) {
-      if (cell_of(s.prm, s.cur.xm[i], c, b)) {
+      if (particle_cell(s, i, s.cur.xm[i], c, b)) {
         key = pack_key(b.x, b.y, b.z);
         valid = true;
       } else {
@@ -351,7 +380,7 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
     uint64_t key = kEmptyKey - 1 - lane;
     int3 c = make_int3(0, 0, 0), b = make_int3(0, 0, 0);
     bool valid = false;
-    if (i < n && cell_of(s.prm, s.cur.xm[i], c, b)) {
+    if (i < n && particle_cell(s, i, s.cur.xm[i], c, b)) {
       key = pack_key(b.x, b.y, b.z);
       valid = true;
     }
@@ -555,7 +584,7 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
     const int start = s.block_start[b], end = s.block_start[b + 1];
     if (start == end) continue;
     for (int q = t; q < kGridChannels * kHaloCells; q += blockDim.x) sh[q] = 0.f;
-    const int3 bk = unpack_key(s.blk_pk[b]);
+    const int3 bk = local_block(s.prm, unpack_key(s.blk_pk[b]));
     const int ox = bk.x * 8, oy = bk.y * 8, oz = bk.z * 8;
     for (int chunk = 0; chunk < 512 / kP2GChunk; ++chunk) {
       const int cell0 = chunk * kP2GChunk;
@@ -704,7 +733,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_update(scene_device s) {
     float v[3] = {g[512] * inv + p.gravity[0] * p.dt, g[1024] * inv + p.gravity[1] * p.dt,
                   g[1536] * inv + p.gravity[2] * p.dt};
     if (m > 0.f) {
-      const int3 k = unpack_key(s.blk_pk[b]);
+      const int3 k = local_block(p, unpack_key(s.blk_pk[b]));
       const float pos[3] = {((float)k.x * 8.f + (float)(cell >> 6)) * p.dx,
                             ((float)k.y * 8.f + (float)((cell >> 3) & 7)) * p.dx,
                             ((float)k.z * 8.f + (float)(cell & 7)) * p.dx};
@@ -830,11 +859,15 @@ constexpr size_t kG2PSmemPlain = sizeof(float) * 3 * kHaloCells;
 constexpr size_t kG2PSmemLearned = kG2PSmemPlain + sizeof(uint2) * kFragTotal + sizeof(float) * kBiasTotal +
                                    (kThreads / 32) * (32 * 16 * sizeof(__nv_bfloat16) + 32 * 8 * sizeof(float));
 
-template <bool kLearned>
-__global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
+// kLearned: the closure's MLP replaces the return map (256 threads only); kBatch: batched
+// scenes (per-block scene material, scene-local block origin); NT threads per CTA.
+template <bool kLearned, bool kBatch, int NT>
+__global__ void __launch_bounds__(NT) k_g2p(scene_device s) {
+  static_assert(!kLearned || (NT == kThreads && !kBatch), "learned G2P runs single scenes at 256 threads");
   extern __shared__ __align__(16) float g2p_smem[];
   float *svf = g2p_smem;
   __shared__ int s_b;
+  __shared__ material_dev s_mat;
   const scene_params &p = s.prm;
   const int nb = s.ctr[kCtrBlocks];
   const int substep = s.ctr[kCtrSubstep];
@@ -852,8 +885,10 @@ __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
     if (b >= nb) break;
     const int start = s.block_start[b], end = s.block_start[b + 1];
     if (start == end) continue;
+    const int3 gk = unpack_key(s.blk_pk[b]);
+    if (kBatch && threadIdx.x == 0) s_mat = p.mats[scene_of_key(gk)];
     // halo load: items (ch, hx, hy, quad) over 3 x 12 x 12 x 3, 16-byte loads
-    for (int it = threadIdx.x; it < 3 * kHalo * kHalo * 3; it += blockDim.x) {
+    for (int it = threadIdx.x; it < 3 * kHalo * kHalo * 3; it += NT) {
       const int quad = it % 3, hy = (it / 3) % kHalo, hx = (it / (3 * kHalo)) % kHalo,
                 ch = it / (3 * kHalo * kHalo);
       const int t = (hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0);
@@ -870,9 +905,9 @@ __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
       dst[3] = val.w;
     }
     __syncthreads();
-    const int3 bk = unpack_key(s.blk_pk[b]);
+    const int3 bk = kBatch ? local_block(p, gk) : gk;
     const int org[3] = {bk.x * 8, bk.y * 8, bk.z * 8};
-    for (int base = start + warp * 32; base < end; base += blockDim.x) {
+    for (int base = start + warp * 32; base < end; base += NT) {
       const int slot = base + lane;
       const bool active = slot < end;
       if (!kLearned && !active) break;
@@ -950,7 +985,7 @@ __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
         for (int r = 0; r < 3; ++r)
           Fn[3 * c + r] = F[3 * c + r] + p.dt * (C[r] * F[3 * c] + C[3 + r] * F[3 * c + 1] + C[6 + r] * F[3 * c + 2]);
       // trial-state log for the closure's training set
-      if (s.aux.log_period > 0 && active && p.mat.model != 0 &&
+      if (!kBatch && s.aux.log_period > 0 && active && p.mat.model != 0 &&
           ((unsigned)id + (unsigned)substep) % (unsigned)s.aux.log_period == 0u) {
         float U[9], S[3], V[9], feat[6];
         svd3(Fn, U, S, V);
@@ -963,6 +998,8 @@ __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
       if (kLearned)
         learned_constitutive(p.mat, s.aux.cd, sfrag, sbias, sxs + warp * 32 * 16, sys + warp * 32 * 8, Fn, pl, tau,
                              active, id, substep);
+      else if (kBatch)
+        constitutive(s_mat, Fn, pl, tau);
       else
         constitutive(p.mat, Fn, pl, tau);
       if (!active) continue;
@@ -977,16 +1014,34 @@ __global__ void __launch_bounds__(kThreads) k_g2p(scene_device s) {
       }
       if (s.nxt.plastic) s.nxt.plastic[slot] = pl;
       s.nxt.id[slot] = id;
+      if (kBatch) s.nxt.sid[slot] = s.cur.sid[i];
     }
   }
 }
 
 // ----------------------------------------------------------------- import / export
+// scene of upload index i: the last scene whose start is <= i
+__device__ __forceinline__ int scene_of_index(const scene_params &p, int i) {
+  int lo = 0, hi = p.nscenes;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (p.scene_start[mid] <= i) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 __global__ void k_import(scene_device s, const float *m, const float *x, const float *v,
                          const float *C, const float *F, const float *pl, int n) {
   const size_t cap = (size_t)s.prm.cap;
-  const float plastic_default = s.prm.mat.model == 2 ? 1.f : 0.f;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += grid_threads()) {
+    int model = s.prm.mat.model;
+    if (s.prm.batch) {
+      const int sc = scene_of_index(s.prm, i);
+      s.cur.sid[i] = sc;
+      model = s.prm.mats[sc].model;
+    }
+    const float plastic_default = model == 2 ? 1.f : 0.f;
     s.cur.xm[i] = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], m[i]);
     s.cur.v[i] = v ? make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
@@ -1026,7 +1081,10 @@ __global__ void k_prime(scene_device s) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) F[k] = s.cur.F[k * cap + i];
     float pl = s.cur.plastic ? s.cur.plastic[i] : 0.f;
-    constitutive(s.prm.mat, F, pl, tau);
+    if (s.prm.batch)
+      constitutive(s.prm.mats[s.cur.sid[i]], F, pl, tau);
+    else
+      constitutive(s.prm.mat, F, pl, tau);
     const float m = s.cur.xm[i].w;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
@@ -1247,11 +1305,13 @@ cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
 cudaError_t prepare_kernels() {
   cudaError_t e = cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kG2PSmemLearned);
+  return cudaFuncSetAttribute(k_g2p<true, false, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)kG2PSmemLearned);
 }
 
 cudaError_t launch_p2g(scene_device &s, cudaStream_t st) {
-  k_p2g<<<num_sms() * 2, kP2GThreads, kP2GSmemBytes, st>>>(s);
+  const int per_sm = s.prm.p2g_ctas_per_sm > 0 ? s.prm.p2g_ctas_per_sm : 2;
+  k_p2g<<<num_sms() * per_sm, kP2GThreads, kP2GSmemBytes, st>>>(s);
   return cudaGetLastError();
 }
 
@@ -1261,10 +1321,17 @@ cudaError_t launch_grid_update(scene_device &s, cudaStream_t st) {
 }
 
 cudaError_t launch_g2p(scene_device &s, cudaStream_t st) {
+  const int per_sm = s.prm.g2p_ctas_per_sm > 0 ? s.prm.g2p_ctas_per_sm : 2;
+  const int grid = num_sms() * per_sm;
+  const bool small = s.prm.g2p_threads == 128;
   if (s.aux.learned)
-    k_g2p<true><<<num_sms() * 2, kThreads, kG2PSmemLearned, st>>>(s);
+    k_g2p<true, false, kThreads><<<grid, kThreads, kG2PSmemLearned, st>>>(s);
+  else if (s.prm.batch)
+    small ? k_g2p<false, true, 128><<<grid, 128, kG2PSmemPlain, st>>>(s)
+          : k_g2p<false, true, kThreads><<<grid, kThreads, kG2PSmemPlain, st>>>(s);
   else
-    k_g2p<false><<<num_sms() * 2, kThreads, kG2PSmemPlain, st>>>(s);
+    small ? k_g2p<false, false, 128><<<grid, 128, kG2PSmemPlain, st>>>(s)
+          : k_g2p<false, false, kThreads><<<grid, kThreads, kG2PSmemPlain, st>>>(s);
   return cudaGetLastError();
 }
 
