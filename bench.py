@@ -130,32 +130,15 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def dist_setup():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    return ws, rank, local
-
-
 def max_over_ranks(x: float, ws: int) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from zsmpm_b200 import replicas
+    return replicas.max_over_ranks(x) if ws > 1 else x
 
 
 def barrier(ws: int):
+    from zsmpm_b200 import replicas
     if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+        replicas.barrier()
 
 
 def g2p_algorithmic_bytes(n: int, nb: int, plastic: bool) -> int:
@@ -323,7 +306,8 @@ def main(argv=None):
                   else scenes.count_particles(spec))
         return run_reference_arm(args, spec, workload, n_full)
 
-    ws, rank, local = dist_setup()
+    from zsmpm_b200 import replicas
+    ws, rank, local = replicas.init("nccl")
     import torch
 
     import zsmpm_b200 as zs
@@ -472,9 +456,7 @@ def main(argv=None):
         }
         print(json.dumps(line))
     sc.close()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finish()
     return 0
 
 
