@@ -141,6 +141,16 @@ def barrier(ws: int):
         replicas.barrier()
 
 
+# DRAM bytes (read + write) per particle of one k_g2p launch, from ncu captures of the same
+# kernel (dram__bytes_read.sum + dram__bytes_write.sum over the particles of the launch):
+#   two-box sand scene: captured at dx = 1/128 (3.7 M particles; the 30 M workload is scaled by
+#   the particle count, traffic grows in proportion): 743.7 MB / 3,703,824
+#   256-scene batch: captured at full size: 3.467 GB / 15,386,080
+G2P_TRAFFIC_PER_PARTICLE = {"dp_two_boxes_dx256_8ppc": 743.66e6 / 3703824,
+                            "dp_two_boxes_dx128_8ppc": 743.66e6 / 3703824,
+                            "batch_256_scenes_dx128_8ppc": 3.4673e9 / 15386080}
+
+
 def g2p_algorithmic_bytes(n: int, nb: int, plastic: bool) -> int:
     """G2P per launch: per particle reads slot index 4, x|m 16, F 36, id 4 (+ plastic 4) and
     writes x|m 16, v 16, C 36, A 36, F 36, id 4 (+ plastic 4); per active block reads the
@@ -438,7 +448,11 @@ def main(argv=None):
                        "l2": "inputs larger than L2 (particle state 4+ GB)",
                        "substep_graph": "CUDA graph of 2 substeps"},
             "roofline": {"bound": "hbm", "kernel": "k_g2p", "achieved": g2p_gbs, "peak": peak,
-                         "unit": "GB/s", "frac": g2p_gbs / peak, "traffic": None,
+                         "unit": "GB/s", "frac": g2p_gbs / peak,
+                         "traffic": (G2P_TRAFFIC_PER_PARTICLE[workload] * n if workload in G2P_TRAFFIC_PER_PARTICLE
+                                     else None),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per particle of a "
+                                           "k_g2p launch (profiles/), times this launch's particles",
                          "peak_kind": f"{peak_kind} copy bandwidth",
                          "algorithmic_bytes_per_launch": g2p_bytes, "launch_ms": stage[4]},
             "stage_ms": {"activate": stage[0], "bin": stage[1], "p2g": stage[2], "grid_update": stage[3],

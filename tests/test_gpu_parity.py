@@ -230,6 +230,14 @@ def test_substep_matches_reference_cpu_path(zs, gpu, model):
     e_gpu = rel_l2(g.v, o64.v)
     e_cpu = rel_l2(base.v, o64.v)
     assert e_gpu < max(2 * e_cpu, 1e-6)
+    m64, p64 = grid_mass_momentum(o64.keys, o64.grid)
+    print(f"\nparity model {model}: GPU vs reference CPU: x {rel_l2(g.x, base.x):.2e} v {rel_l2(g.v, base.v):.2e} "
+          f"F {rel_l2(g.F, base.F):.2e} F-I {rel_l2(g.F - eye, base.F - eye):.2e} mass {abs(mg - mb) / mb:.2e} "
+          f"momentum {np.linalg.norm(pg - pb) / np.linalg.norm(pb):.2e} | vs FP64: GPU x {rel_l2(g.x, o64.x):.2e} "
+          f"v {e_gpu:.2e} F {rel_l2(g.F, o64.F):.2e} mass {abs(mg - m64) / m64:.2e} "
+          f"momentum {np.linalg.norm(pg - p64) / np.linalg.norm(p64):.2e}; reference CPU x {rel_l2(base.x, o64.x):.2e} "
+          f"v {e_cpu:.2e} F {rel_l2(base.F, o64.F):.2e} mass {abs(mb - m64) / m64:.2e} "
+          f"momentum {np.linalg.norm(pb - p64) / np.linalg.norm(p64):.2e}")
     if model == 1:
         # the GPU keeps logJp one projection ahead (see zsmpm.h); advance the reference's
         _, _, lj = restated.stress(spec, base.F, base.plastic if ref is None else ref.logJp, mode=1)
