@@ -341,8 +341,8 @@ ZSMPM_API zsmpm_status zsmpm_scene_state_log_count(zsmpm_scene *s, int64_t *coun
 /* ---- allocation-free variant --------------------------------------------------- */
 /* Block activation without any device allocation.  No counterpart in the reference: it is
  * for callers that cannot call cudaMalloc at this point -- hosts whose own memory pool has
- * already reserved the GPU, code running while a CUDA graph is being captured, plug-in or
- * real-time loops that forbid allocation after start-up.  Same result as
+ * already reserved the GPU, plug-in or real-time loops that forbid allocation after
+ * start-up.  Same result as
  * zsmpm_activate_blocks: the active block keys of the particles at x (device pointer,
  * 3 floats per particle as in zs::Particles "x") after the +{0,1}^3 enlargement, ascending
  * by (bx, by, bz), written to keys_out (device, cap_blocks x 3 int32), and their count to

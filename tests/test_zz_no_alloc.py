@@ -2,8 +2,8 @@
 scene path's zsmpm_activate_blocks.
 
 That entry point exists for callers that cannot allocate device memory when they need block
-activation (a host whose pool already holds the GPU, code running under CUDA graph capture,
-plug-in loops that forbid allocation after start-up); its scratch is a fixed device array
+activation (a host whose pool already holds the GPU, plug-in loops that forbid allocation
+after start-up); its scratch is a fixed device array
 shared by all calls.  The keys are integers, so the comparison is exact.  Two calls in a row
 check that the shared scratch left by one call does not leak into the next.  This file is
 named to be collected last.

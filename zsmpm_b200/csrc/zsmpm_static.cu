@@ -2,9 +2,8 @@
 // ascending block order) that allocates nothing.
 //
 // Some callers cannot call cudaMalloc when they need this step: hosts whose own pool has
-// already reserved the GPU's memory, code that runs while a CUDA graph is being captured
-// (allocation is not a capturable operation), and plug-in or real-time loops that forbid
-// allocation after start-up.  For them the scratch of this entry point (hash table, dense
+// already reserved the GPU's memory, and plug-in or real-time loops that forbid allocation
+// after start-up.  For them the scratch of this entry point (hash table, dense
 // bitmap, scan partials, counters) lives in a fixed file-scope device array instead of
 // scene-owned buffers; the caller passes the inputs and the outputs.
 //
