@@ -257,7 +257,7 @@ ZSMPM_API zsmpm_status zsmpm_batch_num_scenes(const zsmpm_scene *s, int32_t *out
 /* ---- launch-shape autotuner ----------------------------------------------------- */
 typedef struct {
   int32_t g2p_threads;      /* G2P CTA size: 128 or 256 (0 = default 256) */
-  int32_t g2p_ctas_per_sm;  /* persistent G2P CTAs per SM, 1-4 (0 = default 2) */
+  int32_t g2p_ctas_per_sm;  /* persistent G2P CTAs per SM, 1-6 (0 = default: 3, learned 2) */
   int32_t p2g_ctas_per_sm;  /* persistent P2G CTAs per SM, 1-2 (0 = default 2) */
   float g2p_ms, p2g_ms;     /* stage times of the chosen shapes (autotune output) */
 } zsmpm_tuning;

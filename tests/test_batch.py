@@ -90,7 +90,7 @@ def test_autotune_picks_a_valid_shape_and_keeps_results(zs, gpu):
     a = batch.Batch(specs, parts)
     choice = a.autotune(trials=1)
     assert choice["g2p_threads"] in (128, 256)
-    assert 1 <= choice["g2p_ctas_per_sm"] <= 4 and 1 <= choice["p2g_ctas_per_sm"] <= 2
+    assert 1 <= choice["g2p_ctas_per_sm"] <= 6 and 1 <= choice["p2g_ctas_per_sm"] <= 2
     assert choice["g2p_ms"] > 0 and choice["p2g_ms"] > 0
     a.upload(parts)
     a.run(20)

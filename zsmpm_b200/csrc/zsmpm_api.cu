@@ -868,10 +868,11 @@ ZSMPM_API zsmpm_status zsmpm_autotune(zsmpm_scene *s, int32_t trials, zsmpm_tuni
   // G2P: CTA size x CTAs per SM (each CTA owns one block at a time)
   float best_g2p = 3.4e38f;
   const int g2p_threads[2] = {256, 128};
-  const int g2p_per_sm[4] = {1, 2, 3, 4};
+  const int g2p_per_sm[6] = {1, 2, 3, 4, 5, 6};
   for (int a : g2p_threads)
     for (int b : g2p_per_sm) {
       if (s->dev.aux.learned && (a != 256 || b > 2)) continue;  // learned G2P: 256 threads, <= 2 per SM
+      if (a == 256 && b > 4) continue;                          // beyond what stays resident
       p.g2p_threads = a;
       p.g2p_ctas_per_sm = b;
       float ms = 0.f;
@@ -913,7 +914,7 @@ ZSMPM_API zsmpm_status zsmpm_set_tuning(zsmpm_scene *s, const zsmpm_tuning *t) {
   if (st != ZSMPM_OK) return st;
   if (!t) return fail(ZSMPM_ERR_INVALID_ARG, "null tuning");
   if ((t->g2p_threads != 0 && t->g2p_threads != 128 && t->g2p_threads != 256) || t->g2p_ctas_per_sm < 0 ||
-      t->g2p_ctas_per_sm > 4 || t->p2g_ctas_per_sm < 0 || t->p2g_ctas_per_sm > 2)
+      t->g2p_ctas_per_sm > 6 || t->p2g_ctas_per_sm < 0 || t->p2g_ctas_per_sm > 2)
     return fail(ZSMPM_ERR_INVALID_ARG, "tuning out of range");
   if (s->dev.aux.learned && t->g2p_threads == 128)
     return fail(ZSMPM_ERR_INVALID_ARG, "the learned G2P runs 256-thread CTAs");

@@ -861,8 +861,12 @@ constexpr size_t kG2PSmemLearned = kG2PSmemPlain + sizeof(uint2) * kFragTotal + 
 
 // kLearned: the closure's MLP replaces the return map (256 threads only); kBatch: batched
 // scenes (per-block scene material, scene-local block origin); NT threads per CTA.
+// The plain variants are register-capped for 3 (256 threads) or 5 (128 threads) resident CTAs
+// per SM: the kernel is issue- and latency-bound, and the extra warps hide more latency than
+// the cap costs (2.41 -> 2.09 ms on the 30 M-particle sand scene, no spills).  The learned
+// variant is capped for 2 (128 registers; at 1 CTA per SM it takes 6.2 ms instead of 4.8).
 template <bool kLearned, bool kBatch, int NT>
-__global__ void __launch_bounds__(NT) k_g2p(scene_device s) {
+__global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(scene_device s) {
   static_assert(!kLearned || (NT == kThreads && !kBatch), "learned G2P runs single scenes at 256 threads");
   extern __shared__ __align__(16) float g2p_smem[];
   float *svf = g2p_smem;
@@ -1321,7 +1325,7 @@ cudaError_t launch_grid_update(scene_device &s, cudaStream_t st) {
 }
 
 cudaError_t launch_g2p(scene_device &s, cudaStream_t st) {
-  const int per_sm = s.prm.g2p_ctas_per_sm > 0 ? s.prm.g2p_ctas_per_sm : 2;
+  const int per_sm = s.prm.g2p_ctas_per_sm > 0 ? s.prm.g2p_ctas_per_sm : (s.aux.learned ? 2 : 3);
   const int grid = num_sms() * per_sm;
   const bool small = s.prm.g2p_threads == 128;
   if (s.aux.learned)
