@@ -165,6 +165,19 @@ typedef struct {
   int32_t *keys;        /* device, [num_blocks][3] */
 } zsmpm_grid_view;
 
+/* BhtViewLite<i32,3,int,16> fields (py_interop/BhtInstantiations.cpp:63-75; container/Bht.hpp),
+ * device pointers: the bucketed three-hash table that zpc's SparseGrid keeps its blocks in. */
+typedef struct {
+  int32_t *keys;        /* [table_size][4] storage keys (x, y, z, pad); bytes 0x3f when empty */
+  int32_t *indices;     /* [table_size] block index of the key, -1 when empty */
+  int32_t *status;      /* [table_size] slot lock, -1 (unlocked) */
+  int32_t *active_keys; /* [cnt][3] key of block index b */
+  int32_t *cnt;         /* number of keys */
+  int32_t *success;     /* build success flag, 1 */
+  int32_t table_size;
+  uint32_t hashers[6];  /* (hashx, hashy) of hf0, hf1, hf2 */
+} zsmpm_bht_view;
+
 typedef struct zsmpm_scene zsmpm_scene;
 
 ZSMPM_API const char *zsmpm_last_error_string(void);
@@ -211,6 +224,19 @@ ZSMPM_API zsmpm_status zsmpm_run(zsmpm_scene *scene, int32_t nsteps, void *strea
 /* ---- views and diagnostics ------------------------------------------------------- */
 ZSMPM_API zsmpm_status zsmpm_get_table_view(zsmpm_scene *scene, zsmpm_table_view *out);
 ZSMPM_API zsmpm_status zsmpm_get_grid_view(zsmpm_scene *scene, zsmpm_grid_view *out);
+/* The active blocks of the last activation as a bht<i32,3,int,16> (synchronises; rebuilt on
+ * every call, on the host): the table that the reference's host BHTView::insert
+ * (container/Bht.hpp:612-665) builds when the keys are inserted in ascending block order into
+ * a bht sized for max(blocks, 16) entries, so index == block index.  The view stays valid until the next call or
+ * the scene's destruction. */
+ZSMPM_API zsmpm_status zsmpm_get_bht_view(zsmpm_scene *scene, zsmpm_bht_view *out);
+/* The same table built on the host from keys[nkeys][3] in order, sized for `expected` entries
+ * (0: nkeys): table_keys [cap_slots][4], indices and status [cap_slots]; *table_size and the
+ * hasher parameters hashers[6] are set even when cap_slots is too small (then
+ * ZSMPM_ERR_CAPACITY).  No device needed. */
+ZSMPM_API zsmpm_status zsmpm_bht_build_host(const int32_t *keys, int32_t nkeys, int32_t expected,
+                                            int32_t *table_keys, int32_t *indices, int32_t *status,
+                                            int32_t cap_slots, int32_t *table_size, uint32_t *hashers);
 /* Number of active blocks of the last activation (synchronises). */
 ZSMPM_API zsmpm_status zsmpm_num_blocks(zsmpm_scene *scene, int32_t *out);
 /* Copies the active keys [nb][3] and the grid [nb][4][512] to host memory. */

@@ -16,6 +16,9 @@
 //     reply:     f32 PF[9*count], F[9*count], logJp[count]
 //   4 svd:       int32 count, f32 A[9*count]
 //     reply:     f32 U[9*count], S[3*count], V[9*count]
+//   5 bht:       int32 nkeys, int32 expected, int32 cap_slots, int32 keys[3*nkeys]
+//     reply:     int32 status, table_size, u32 hash[6], int32 cnt,
+//                then (status == 0) int32 keys[3*table_size], indices[table_size], status[table_size]
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -38,6 +41,8 @@ void zsref_svd(const float *A, float *U, float *S, float *V);
 int zsref_activate(int n, const float *x, float dx, int table_expected, int cap,
                    int *out_nblocks, int *out_nparblocks, int *out_keys, int *out_slots,
                    int *out_table_size);
+int zsref_bht(int nkeys, const int *keys, int expected, int cap_slots, int *out_table_size,
+              unsigned *out_hash, int *out_keys, int *out_indices, int *out_status, int *out_cnt);
 }
 
 namespace {
@@ -133,6 +138,23 @@ int main(int argc, char **argv) {
     wrv(PF.data(), PF.size());
     wrv(F.data(), F.size());
     wrv(lj.data(), lj.size());
+  } else if (cmd == 5) {
+    const int nk = rd<int32_t>(), expected = rd<int32_t>(), cap = rd<int32_t>();
+    std::vector<int> keys;
+    rdv(keys, 3 * (size_t)nk);
+    std::vector<int> tk(3 * (size_t)cap), ti(cap), tst(cap);
+    unsigned hash[6] = {};
+    int ts = 0, cnt = 0;
+    int st = zsref_bht(nk, keys.data(), expected, cap, &ts, hash, tk.data(), ti.data(), tst.data(), &cnt);
+    wr<int32_t>(st);
+    wr<int32_t>(ts);
+    wrv(hash, 6);
+    wr<int32_t>(cnt);
+    if (st == 0) {
+      wrv(tk.data(), 3 * (size_t)ts);
+      wrv(ti.data(), (size_t)ts);
+      wrv(tst.data(), (size_t)ts);
+    }
   } else if (cmd == 4) {
     const int count = rd<int32_t>();
     std::vector<float> A, U(9 * (size_t)count), S(3 * (size_t)count), V(9 * (size_t)count);

@@ -37,6 +37,7 @@
 #include "zensim/simulation/grid/GridOp.hpp"
 #include "zensim/geometry/AnalyticLevelSet.h"
 #include "zensim/geometry/Collider.h"
+#include "zensim/container/Bht.hpp"
 
 namespace {
 
@@ -286,6 +287,34 @@ int zsref_activate(int n, const float *x, float dx, int table_expected, int cap,
     for (int d = 0; d != 3; ++d) out_keys[b * 3 + d] = key[d];
     out_slots[b] = view.entry(key);
   }
+  return 0;
+}
+
+// A bht<i32,3,int,16> (container/Bht.hpp) built by the reference's own host insert
+// (BHTView::insert, Bht.hpp:612-665) from the given keys in the given order, default insertion
+// indices.  Outputs: table size, the three hashers' (hashx, hashy), and per slot the stored key
+// (x, y, z), index and status; cnt.  Returns 1 when cap_slots is too small.
+int zsref_bht(int nkeys, const int *keys, int expected, int cap_slots, int *out_table_size,
+              unsigned *out_hash, int *out_keys, int *out_indices, int *out_status, int *out_cnt) {
+  using bht_t = zs::bht<int, 3, int, 16>;
+  bht_t table{(size_t)std::max(expected, 1), memsrc_e::host, -1};
+  *out_table_size = (int)table._tableSize;
+  out_hash[0] = table._hf0._hashx;
+  out_hash[1] = table._hf0._hashy;
+  out_hash[2] = table._hf1._hashx;
+  out_hash[3] = table._hf1._hashy;
+  out_hash[4] = table._hf2._hashx;
+  out_hash[5] = table._hf2._hashy;
+  if ((int)table._tableSize > cap_slots) return 1;
+  auto v = view<execspace_e::host>(table);
+  for (int k = 0; k != nkeys; ++k) v.insert(vec<int, 3>{keys[3 * k], keys[3 * k + 1], keys[3 * k + 2]});
+  for (int i = 0; i != (int)table._tableSize; ++i) {
+    const auto &sk = table.self().keys[i];
+    for (int d = 0; d != 3; ++d) out_keys[3 * i + d] = sk.val[d];
+    out_indices[i] = table.self().indices[i];
+    out_status[i] = table.self().status[i];
+  }
+  *out_cnt = (int)table.size();
   return 0;
 }
 

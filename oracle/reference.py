@@ -109,6 +109,26 @@ def activate(x: np.ndarray, dx: float, table_expected: int, cap: int = 1 << 16, 
     return keys, slots, npb, ts
 
 
+def bht(keys: np.ndarray, expected: int, cap_slots: int = 1 << 20, timeout: float = 120.0) -> dict:
+    """The reference's bht<i32,3,int,16> (container/Bht.hpp) after its host insert of `keys` in
+    order: table size, hasher parameters, and per slot key, index and status."""
+    keys = np.ascontiguousarray(keys, dtype="<i4").reshape(-1, 3)
+    req = struct.pack("<iiii", 5, len(keys), expected, cap_slots) + keys.tobytes()
+    rep = _run(req, timeout)
+    st, ts = struct.unpack_from("<2i", rep, 0)
+    hash6 = np.frombuffer(rep, "<u4", 6, 8).copy()
+    cnt = struct.unpack_from("<i", rep, 32)[0]
+    if st != 0:
+        raise RuntimeError(f"zsref bht failed: {st}")
+    off = 36
+    tkeys = np.frombuffer(rep, "<i4", 3 * ts, off).reshape(ts, 3).copy()
+    off += 12 * ts
+    idx = np.frombuffer(rep, "<i4", ts, off).copy()
+    off += 4 * ts
+    status = np.frombuffer(rep, "<i4", ts, off).copy()
+    return {"table_size": ts, "hash": hash6, "cnt": cnt, "keys": tkeys, "indices": idx, "status": status}
+
+
 def stress(spec, F: np.ndarray, logJp: np.ndarray, timeout: float = 120.0):
     """Reference compute_stress_* on a batch: returns (PF, F_projected, logJp_new)."""
     m = spec.material

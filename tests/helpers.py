@@ -33,3 +33,13 @@ def aligned_grids(keys_a, grid_a, keys_b, grid_b):
     da, db = grid_by_key(keys_a, grid_a), grid_by_key(keys_b, grid_b)
     common = sorted(set(da) & set(db))
     return (np.stack([da[k] for k in common]), np.stack([db[k] for k in common]), set(da) ^ set(db))
+
+
+def d2h(ptr: int, shape, dtype) -> np.ndarray:
+    """Copies a device array of the library into host memory (cudaMemcpy, device->host)."""
+    import ctypes
+    out = np.empty(shape, dtype)
+    rt = ctypes.CDLL("libcudart.so.12")
+    rt.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    assert rt.cudaMemcpy(out.ctypes.data, ptr, out.nbytes, 2) == 0
+    return out

@@ -47,7 +47,9 @@ def test_struct_layouts_match_header(zs, tmp_path):
                      "sizeof(zsmpm_tilevector_view), sizeof(zsmpm_table_view));"
                      "printf(\"%zu %zu %zu %zu\\n\", sizeof(zsmpm_closure_state),"
                      "offsetof(zsmpm_closure_state, in_mean), sizeof(zsmpm_closure_audit),"
-                     "offsetof(zsmpm_closure_audit, fallbacks));return 0;}\n")
+                     "offsetof(zsmpm_closure_audit, fallbacks));"
+                     "printf(\"%zu %zu %zu\\n\", sizeof(zsmpm_bht_view), offsetof(zsmpm_bht_view, table_size),"
+                     "sizeof(zsmpm_tuning));return 0;}\n")
     exe = tmp_path / "probe"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(probe), "-o", str(exe)], check=True)
     vals = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()))
@@ -56,7 +58,8 @@ def test_struct_layouts_match_header(zs, tmp_path):
                     a.SceneDesc.max_particles.offset, C.sizeof(a.ParticleArrays),
                     C.sizeof(a.TileVectorView), C.sizeof(a.TableView),
                     C.sizeof(a.ClosureState), a.ClosureState.in_mean.offset, C.sizeof(a.ClosureAudit),
-                    a.ClosureAudit.fallbacks.offset]
+                    a.ClosureAudit.fallbacks.offset, C.sizeof(a.BhtView), a.BhtView.table_size.offset,
+                    C.sizeof(a.Tuning)]
 
 
 def test_host_side_argument_checks_without_gpu(zs):

@@ -31,6 +31,23 @@ __all__ = ["Scene", "ZsmpmError", "SceneSpec", "MaterialSpec", "Shape", "Particl
            "PLASTICITY_REFERENCE", "WALL_STICKY", "WALL_SLIP", "WALL_SEPARATE", "WALL_NONE"]
 
 
+def bht_build_host(keys: np.ndarray, expected: int = 0) -> dict:
+    """The bht<i32,3,int,16> layout of keys [n][3] inserted in order (host only)."""
+    keys = np.ascontiguousarray(keys, dtype=np.int32).reshape(-1, 3)
+    lib = _abi.lib()
+    size = C.c_int32()
+    hashers = (C.c_uint32 * 6)()
+    lib.zsmpm_bht_build_host(_ptr(keys), len(keys), expected, None, None, None, 0, C.byref(size), hashers)
+    n = size.value
+    tk = np.empty((n, 4), np.int32)
+    ti = np.empty(n, np.int32)
+    ts = np.empty(n, np.int32)
+    _abi.check(lib.zsmpm_bht_build_host(_ptr(keys), len(keys), expected, _ptr(tk), _ptr(ti), _ptr(ts), n,
+                                        C.byref(size), hashers), "bht_build_host")
+    return {"table_size": n, "hash": np.array(list(hashers), np.uint32), "keys": tk, "indices": ti,
+            "status": ts}
+
+
 def device_count() -> int:
     return int(_abi.lib().zsmpm_device_count())
 
@@ -185,6 +202,12 @@ class Scene:
         _abi.check(self._lib.zsmpm_download_binning(self._h, _ptr(order), _ptr(bstart), nb),
                    "download_binning")
         return order, bstart
+
+    def bht_view(self) -> _abi.BhtView:
+        """The active blocks as the reference's bht<i32,3,int,16> (device pointers)."""
+        v = _abi.BhtView()
+        _abi.check(self._lib.zsmpm_get_bht_view(self._h, C.byref(v)), "bht_view")
+        return v
 
     def table_view(self) -> _abi.TableView:
         tv = _abi.TableView()

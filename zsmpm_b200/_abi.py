@@ -59,6 +59,12 @@ class GridView(C.Structure):
                 ("keys", C.c_void_p)]
 
 
+class BhtView(C.Structure):
+    _fields_ = [("keys", C.c_void_p), ("indices", C.c_void_p), ("status", C.c_void_p),
+                ("active_keys", C.c_void_p), ("cnt", C.c_void_p), ("success", C.c_void_p),
+                ("table_size", C.c_int32), ("hashers", C.c_uint32 * 6)]
+
+
 class Tuning(C.Structure):
     _fields_ = [("g2p_threads", C.c_int32), ("g2p_ctas_per_sm", C.c_int32), ("p2g_ctas_per_sm", C.c_int32),
                 ("g2p_ms", C.c_float), ("p2g_ms", C.c_float)]
@@ -112,6 +118,8 @@ SIGNATURES = {
     "zsmpm_kernels_per_substep": (C.c_int32, [_P]),
     "zsmpm_svd3": (_S, [_P, _P, _P, _P, C.c_int64, _P]),
     "zsmpm_constitutive": (_S, [C.POINTER(Material), _P, _P, _P, C.c_int64, _P]),
+    "zsmpm_get_bht_view": (_S, [_P, C.POINTER(BhtView)]),
+    "zsmpm_bht_build_host": (_S, [_P, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32, C.POINTER(C.c_int32), _P]),
     "zsmpm_batch_create": (_S, [C.POINTER(SceneDesc), C.POINTER(Material), C.c_int32, C.POINTER(_P)]),
     "zsmpm_batch_upload": (_S, [_P, C.POINTER(ParticleArrays), _P, C.c_int32, _P]),
     "zsmpm_batch_num_scenes": (_S, [_P, C.POINTER(C.c_int32)]),

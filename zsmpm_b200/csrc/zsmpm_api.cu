@@ -40,6 +40,10 @@ struct zsmpm_scene {
   int nscenes = 0;                          // 0: a single scene
   bool any_plastic = false;
   std::vector<int64_t> counts;              // particles of each scene (last upload)
+  // bht layout of the active keys (zsmpm_get_bht_view), grown on demand
+  int32_t *bht_keys = nullptr, *bht_indices = nullptr, *bht_status = nullptr, *bht_active = nullptr,
+          *bht_cnt = nullptr;
+  int64_t bht_cap = 0;
   unsigned long long *log_count = nullptr;  // trial-state log counter (device)
 };
 
@@ -199,7 +203,16 @@ zsmpm_status allocate_blocks(zsmpm_scene *s, int64_t n) {
   return ZSMPM_OK;
 }
 
+void release_bht(zsmpm_scene *s) {
+  for (int32_t **p : {&s->bht_keys, &s->bht_indices, &s->bht_status, &s->bht_active, &s->bht_cnt}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  s->bht_cap = 0;
+}
+
 void release(zsmpm_scene *s) {
+  release_bht(s);
   for (int k = 0; k < 2; ++k)
     if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
   for (auto &e : s->ev)
@@ -768,6 +781,54 @@ ZSMPM_API zsmpm_status zsmpm_scene_state_log_count(zsmpm_scene *s, int64_t *coun
   unsigned long long c = 0;
   ZS_TRY(cudaMemcpy(&c, s->log_count, sizeof(c), cudaMemcpyDeviceToHost), "read log counter");
   *count_out = (int64_t)std::min<unsigned long long>(c, (unsigned long long)std::max<int64_t>(s->dev.aux.log_cap, 0));
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_get_bht_view(zsmpm_scene *s, zsmpm_bht_view *out) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!out) return fail(ZSMPM_ERR_INVALID_ARG, "null output");
+  if (s->last_stream) ZS_TRY(cudaStreamSynchronize(s->last_stream), "synchronize");
+  ZS_TRY(cudaDeviceSynchronize(), "synchronize");
+  int nb = 0;
+  ZS_TRY(cudaMemcpy(&nb, &s->dev.ctr[kCtrBlocks], sizeof(int), cudaMemcpyDeviceToHost), "read block count");
+  std::vector<int32_t> keys(3 * (size_t)std::max(nb, 1));
+  if (nb > 0)
+    ZS_TRY(cudaMemcpy(keys.data(), s->dev.active_keys, sizeof(int32_t) * 3 * nb, cudaMemcpyDeviceToHost),
+           "read active keys");
+  int32_t size = 0;
+  uint32_t hash[6] = {};
+  // sized for max(nb, 16) entries: below that the reference's proximity rule (an index at or
+  // above size - 20 fails) rejects even a single key
+  const int32_t expected = std::max(nb, 16);
+  zsmpm_bht_build_host(keys.data(), nb, expected, nullptr, nullptr, nullptr, 0, &size, hash);
+  std::vector<int32_t> tk(4 * (size_t)size), ti(size), ts(size);
+  st = zsmpm_bht_build_host(keys.data(), nb, expected, tk.data(), ti.data(), ts.data(), size, &size, hash);
+  if (st != ZSMPM_OK) return st;
+  if (size > s->bht_cap) {
+    release_bht(s);
+    ZS_TRY(cudaMalloc(&s->bht_keys, sizeof(int32_t) * 4 * (size_t)size), "alloc bht keys");
+    ZS_TRY(cudaMalloc(&s->bht_indices, sizeof(int32_t) * (size_t)size), "alloc bht indices");
+    ZS_TRY(cudaMalloc(&s->bht_status, sizeof(int32_t) * (size_t)size), "alloc bht status");
+    ZS_TRY(cudaMalloc(&s->bht_active, sizeof(int32_t) * 3 * (size_t)size), "alloc bht active keys");
+    ZS_TRY(cudaMalloc(&s->bht_cnt, sizeof(int32_t) * 2), "alloc bht count");
+    s->bht_cap = size;
+  }
+  const int32_t cs[2] = {nb, 1};  // cnt, build success
+  ZS_TRY(cudaMemcpy(s->bht_keys, tk.data(), sizeof(int32_t) * tk.size(), cudaMemcpyHostToDevice), "bht keys");
+  ZS_TRY(cudaMemcpy(s->bht_indices, ti.data(), sizeof(int32_t) * ti.size(), cudaMemcpyHostToDevice), "bht indices");
+  ZS_TRY(cudaMemcpy(s->bht_status, ts.data(), sizeof(int32_t) * ts.size(), cudaMemcpyHostToDevice), "bht status");
+  if (nb > 0)
+    ZS_TRY(cudaMemcpy(s->bht_active, keys.data(), sizeof(int32_t) * 3 * nb, cudaMemcpyHostToDevice), "bht active");
+  ZS_TRY(cudaMemcpy(s->bht_cnt, cs, sizeof(cs), cudaMemcpyHostToDevice), "bht count");
+  out->keys = s->bht_keys;
+  out->indices = s->bht_indices;
+  out->status = s->bht_status;
+  out->active_keys = s->bht_active;
+  out->cnt = s->bht_cnt;
+  out->success = s->bht_cnt + 1;
+  out->table_size = size;
+  for (int k = 0; k < 6; ++k) out->hashers[k] = hash[k];
   return ZSMPM_OK;
 }
 
