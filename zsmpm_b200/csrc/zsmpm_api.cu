@@ -44,6 +44,9 @@ struct zsmpm_scene {
   int32_t *bht_keys = nullptr, *bht_indices = nullptr, *bht_status = nullptr, *bht_active = nullptr,
           *bht_cnt = nullptr;
   int64_t bht_cap = 0;
+  // device staging for host-pointer uploads and downloads (AoS arrays), kept between calls
+  float *staging = nullptr;
+  size_t staging_floats = 0;
   unsigned long long *log_count = nullptr;  // trial-state log counter (device)
 };
 
@@ -145,6 +148,21 @@ zsmpm_status status_from_word(int w) {
   return fail(st, msg);
 }
 
+// the scene's staging buffer with room for `floats` floats (grown, never shrunk)
+cudaError_t staging_for(zsmpm_scene *s, size_t floats) {
+  if (floats <= s->staging_floats) return cudaSuccess;
+  if (s->staging) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return e;
+    cudaFree(s->staging);
+    s->staging = nullptr;
+    s->staging_floats = 0;
+  }
+  cudaError_t e = cudaMalloc(&s->staging, floats * sizeof(float));
+  if (e == cudaSuccess) s->staging_floats = floats;
+  return e;
+}
+
 zsmpm_status allocate_particles(zsmpm_scene *s, int64_t cap) {
   const bool plastic = s->desc.material.model != ZSMPM_FIXED_COROTATED || s->any_plastic;
   for (int k = 0; k < 2; ++k) {
@@ -213,6 +231,9 @@ void release_bht(zsmpm_scene *s) {
 
 void release(zsmpm_scene *s) {
   release_bht(s);
+  if (s->staging) cudaFree(s->staging);
+  s->staging = nullptr;
+  s->staging_floats = 0;
   for (int k = 0; k < 2; ++k)
     if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
   for (auto &e : s->ev)
@@ -369,20 +390,19 @@ static zsmpm_status upload_arrays(zsmpm_scene *s, const zsmpm_particle_arrays *p
   if (st != ZSMPM_OK) return st;
   cudaStream_t cs = as_stream(stream);
   const float *dm = p->m, *dx = p->x, *dv = p->v, *dC = p->C, *dF = p->F, *dpl = p->plastic;
-  std::vector<void *> staging;
   if (!on_device) {
+    // host arrays go through the scene's staging buffer (26 floats per particle at most)
+    ZS_TRY(staging_for(s, 26 * (size_t)n), "upload staging");
+    float *base = s->staging;
     auto stage = [&](const float *h, size_t count, const float **d) -> cudaError_t {
       if (!h) {
         *d = nullptr;
         return cudaSuccess;
       }
-      void *ptr = nullptr;
-      cudaError_t e = cudaMalloc(&ptr, count * sizeof(float));
-      if (e != cudaSuccess) return e;
-      staging.push_back(ptr);
-      e = cudaMemcpyAsync(ptr, h, count * sizeof(float), cudaMemcpyHostToDevice, cs);
-      *d = static_cast<const float *>(ptr);
-      return e;
+      float *dst = base;
+      base += count;
+      *d = dst;
+      return cudaMemcpyAsync(dst, h, count * sizeof(float), cudaMemcpyHostToDevice, cs);
     };
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = stage(p->m, n, &dm);
@@ -391,19 +411,12 @@ static zsmpm_status upload_arrays(zsmpm_scene *s, const zsmpm_particle_arrays *p
     if (e == cudaSuccess) e = stage(p->C, 9 * n, &dC);
     if (e == cudaSuccess) e = stage(p->F, 9 * n, &dF);
     if (e == cudaSuccess) e = stage(p->plastic, n, &dpl);
-    if (e != cudaSuccess) {
-      cudaStreamSynchronize(cs);
-      for (void *q : staging) cudaFree(q);
-      return cuda_fail(e, "upload staging");
-    }
+    if (e != cudaSuccess) return cuda_fail(e, "upload staging copy");
   }
   cudaError_t e = launch_import(s->dev, dm, dx, dv, dC, dF, dpl, (int)n, cs);
   if (e == cudaSuccess) e = launch_prime(s->dev, cs);
-  if (!staging.empty()) {
-    cudaError_t e2 = cudaStreamSynchronize(cs);
-    for (void *q : staging) cudaFree(q);
-    if (e == cudaSuccess) e = e2;
-  }
+  // host arrays may be reused once the call returns, and the staging buffer is free again
+  if (e == cudaSuccess && !on_device) e = cudaStreamSynchronize(cs);
   if (e != cudaSuccess) return cuda_fail(e, "upload");
   s->uploaded = true;
   s->binned = false;
@@ -443,8 +456,8 @@ ZSMPM_API zsmpm_status zsmpm_scene_download(zsmpm_scene *s, zsmpm_particle_array
     ZS_TRY(launch_export(s->dev, p->m, p->x, p->v, p->C, p->F, p->plastic, cs), "download");
     return ZSMPM_OK;
   }
-  float *dbuf = nullptr;
-  ZS_TRY(cudaMalloc(&dbuf, sizeof(float) * 26 * n), "download staging");
+  ZS_TRY(staging_for(s, 26 * (size_t)n), "download staging");
+  float *dbuf = s->staging;
   float *dm = dbuf, *dx = dm + n, *dv = dx + 3 * n, *dC = dv + 3 * n, *dF = dC + 9 * n, *dpl = dF + 9 * n;
   cudaError_t e = launch_export(s->dev, p->m ? dm : nullptr, p->x ? dx : nullptr, p->v ? dv : nullptr,
                                 p->C ? dC : nullptr, p->F ? dF : nullptr, p->plastic ? dpl : nullptr, cs);
@@ -458,7 +471,6 @@ ZSMPM_API zsmpm_status zsmpm_scene_download(zsmpm_scene *s, zsmpm_particle_array
   get(p->F, dF, 9 * n);
   get(p->plastic, dpl, n);
   cudaError_t e2 = cudaStreamSynchronize(cs);
-  cudaFree(dbuf);
   if (e == cudaSuccess) e = e2;
   if (e != cudaSuccess) return cuda_fail(e, "download");
   return ZSMPM_OK;
