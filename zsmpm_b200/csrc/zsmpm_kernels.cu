@@ -455,10 +455,13 @@ __global__ void __launch_bounds__(512) k_bin_finalize(scene_device s) {
     const int cs = s.cell_start[b * 512 + t];
     s.cell_count[b * 512 + t] = 0;
     if (c <= kMaxList) {
+      // two rounds of independent loads (the cell's particle list, then their upload ids),
+      // then an insertion sort of (id, index) pairs by id
       int li[kMaxList], lid[kMaxList];
-      for (int r = 0; r < c; ++r) {
-        const int i = s.tmp[cs + r];
-        const int id = s.cur.id[i];
+      for (int r = 0; r < c; ++r) li[r] = s.tmp[cs + r];
+      for (int r = 0; r < c; ++r) lid[r] = s.cur.id[li[r]];
+      for (int r = 1; r < c; ++r) {
+        const int i = li[r], id = lid[r];
         int q = r;
         while (q > 0 && lid[q - 1] > id) {
           lid[q] = lid[q - 1];
@@ -855,7 +858,8 @@ __device__ __forceinline__ void learned_constitutive(const material_dev &mat, co
   mul_diag_t(F, U, Ns, V);
 }
 
-constexpr size_t kG2PSmemPlain = sizeof(float) * 3 * kHaloCells;
+// the velocity halo, one float4 (vx, vy, vz, 0) per node so that a node is one 16-byte load
+constexpr size_t kG2PSmemPlain = sizeof(float4) * kHaloCells;
 constexpr size_t kG2PSmemLearned = kG2PSmemPlain + sizeof(uint2) * kFragTotal + sizeof(float) * kBiasTotal +
                                    (kThreads / 32) * (32 * 16 * sizeof(__nv_bfloat16) + 32 * 8 * sizeof(float));
 
@@ -869,14 +873,14 @@ template <bool kLearned, bool kBatch, int NT>
 __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(scene_device s) {
   static_assert(!kLearned || (NT == kThreads && !kBatch), "learned G2P runs single scenes at 256 threads");
   extern __shared__ __align__(16) float g2p_smem[];
-  float *svf = g2p_smem;
+  float4 *svf = reinterpret_cast<float4 *>(g2p_smem);
   __shared__ int s_b;
   __shared__ material_dev s_mat;
   const scene_params &p = s.prm;
   const int nb = s.ctr[kCtrBlocks];
   const int substep = s.ctr[kCtrSubstep];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint2 *sfrag = reinterpret_cast<uint2 *>(g2p_smem + 3 * kHaloCells);
+  uint2 *sfrag = reinterpret_cast<uint2 *>(g2p_smem + 4 * kHaloCells);
   float *sbias = reinterpret_cast<float *>(sfrag + kFragTotal);
   __nv_bfloat16 *sxs = reinterpret_cast<__nv_bfloat16 *>(sbias + kBiasTotal);
   float *sys = reinterpret_cast<float *>(sxs + (kThreads / 32) * 32 * 16);
@@ -891,22 +895,25 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
     if (start == end) continue;
     const int3 gk = unpack_key(s.blk_pk[b]);
     if (kBatch && threadIdx.x == 0) s_mat = p.mats[scene_of_key(gk)];
-    // halo load: items (ch, hx, hy, quad) over 3 x 12 x 12 x 3, 16-byte loads
-    for (int it = threadIdx.x; it < 3 * kHalo * kHalo * 3; it += NT) {
-      const int quad = it % 3, hy = (it / 3) % kHalo, hx = (it / (3 * kHalo)) % kHalo,
-                ch = it / (3 * kHalo * kHalo);
+    // halo load: items (hx, hy, quad) over 12 x 12 x 3; each reads four consecutive cells of
+    // the three velocity channels (16-byte loads) and writes four float4 nodes
+    for (int it = threadIdx.x; it < kHalo * kHalo * 3; it += NT) {
+      const int quad = it % 3, hy = (it / 3) % kHalo, hx = it / (3 * kHalo);
       const int t = (hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0);
       const int tb = s.nbr[b * 8 + t];
-      float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 vx = make_float4(0.f, 0.f, 0.f, 0.f), vy = vx, vz = vx;
       if (tb >= 0) {
         const int cell = ((hx & 7) << 6) | ((hy & 7) << 3) | ((quad * 4) & 7);
-        val = *reinterpret_cast<const float4 *>(s.grid + ((size_t)tb * kGridChannels + 1 + ch) * 512 + cell);
+        const float *g = s.grid + ((size_t)tb * kGridChannels + 1) * 512 + cell;
+        vx = *reinterpret_cast<const float4 *>(g);
+        vy = *reinterpret_cast<const float4 *>(g + 512);
+        vz = *reinterpret_cast<const float4 *>(g + 1024);
       }
-      float *dst = svf + ((ch * kHalo + hx) * kHalo + hy) * kHalo + quad * 4;
-      dst[0] = val.x;
-      dst[1] = val.y;
-      dst[2] = val.z;
-      dst[3] = val.w;
+      float4 *dst = svf + (hx * kHalo + hy) * kHalo + quad * 4;
+      dst[0] = make_float4(vx.x, vy.x, vz.x, 0.f);
+      dst[1] = make_float4(vx.y, vy.y, vz.y, 0.f);
+      dst[2] = make_float4(vx.z, vy.z, vz.z, 0.f);
+      dst[3] = make_float4(vx.w, vy.w, vz.w, 0.f);
     }
     __syncthreads();
     const int3 bk = kBatch ? local_block(p, gk) : gk;
@@ -956,7 +963,8 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
             for (int kk = 0; kk < 3; ++kk) {
               const float wz = w[2][kk], wzd = wz * ((float)kk - f[2]);
               const int h = hrow + kk;
-              const float vx = svf[h], vy = svf[kHaloCells + h], vz = svf[2 * kHaloCells + h];
+              const float4 node = svf[h];
+              const float vx = node.x, vy = node.y, vz = node.z;
               s0[0] += wz * vx;
               s0[1] += wz * vy;
               s0[2] += wz * vz;
