@@ -637,33 +637,53 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
 #pragma unroll
           for (int n = 0; n < 27; ++n) acc[n] = 0.f;
           const int d = my_ch - 1;  // p channel index, -1 for mass
-          for (int r = 0; r < cnt; ++r) {
-            float w[3][3];
+          if (my_ch == 0) {
+            // mass: W m (the warp is channel-uniform)
+            for (int r = 0; r < cnt; ++r) {
+              float w[3][3];
 #pragma unroll
-            for (int a = 0; a < 3; ++a)
+              for (int a = 0; a < 3; ++a)
 #pragma unroll
-              for (int c = 0; c < 3; ++c) w[a][c] = stg[3 * a + c][r][my_cell];
-            float q, ax, ay, az;
-            if (my_ch == 0) {
-              q = stg[9][r][my_cell];
-              ax = ay = az = 0.f;
-            } else {
-              q = stg[10 + d][r][my_cell];
-              ax = stg[13 + d][r][my_cell];
-              ay = stg[16 + d][r][my_cell];
-              az = stg[19 + d][r][my_cell];
+                for (int c = 0; c < 3; ++c) w[a][c] = stg[3 * a + c][r][my_cell];
+              const float m = stg[9][r][my_cell];
+#pragma unroll
+              for (int ii = 0; ii < 3; ++ii) {
+                const float wm = w[0][ii] * m;
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) {
+                  const float wij = wm * w[1][jj];
+#pragma unroll
+                  for (int kk = 0; kk < 3; ++kk) {
+                    const int n = (ii * 3 + jj) * 3 + kk;
+                    acc[n] = fmaf(wij, w[2][kk], acc[n]);
+                  }
+                }
+              }
             }
+          } else {
+            // momentum: W (q + ii ax + jj ay + kk az), in cell units of the node offset
+            for (int r = 0; r < cnt; ++r) {
+              float w[3][3];
 #pragma unroll
-            for (int ii = 0; ii < 3; ++ii) {
-              const float qi = q + (float)ii * ax;
+              for (int a = 0; a < 3; ++a)
 #pragma unroll
-              for (int jj = 0; jj < 3; ++jj) {
-                const float qij = qi + (float)jj * ay;
-                const float wij = w[0][ii] * w[1][jj];
+                for (int c = 0; c < 3; ++c) w[a][c] = stg[3 * a + c][r][my_cell];
+              const float q = stg[10 + d][r][my_cell];
+              const float ax = stg[13 + d][r][my_cell];
+              const float ay = stg[16 + d][r][my_cell];
+              const float az = stg[19 + d][r][my_cell];
 #pragma unroll
-                for (int kk = 0; kk < 3; ++kk) {
-                  const int n = (ii * 3 + jj) * 3 + kk;
-                  acc[n] = fmaf(wij * w[2][kk], qij + (float)kk * az, acc[n]);
+              for (int ii = 0; ii < 3; ++ii) {
+                const float qi = q + (float)ii * ax;
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) {
+                  const float qij = qi + (float)jj * ay;
+                  const float wij = w[0][ii] * w[1][jj];
+#pragma unroll
+                  for (int kk = 0; kk < 3; ++kk) {
+                    const int n = (ii * 3 + jj) * 3 + kk;
+                    acc[n] = fmaf(wij * w[2][kk], qij + (float)kk * az, acc[n]);
+                  }
                 }
               }
             }
