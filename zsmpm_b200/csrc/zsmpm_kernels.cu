@@ -569,7 +569,7 @@ __device__ __forceinline__ void p2g_direct(float *shf, const p2g_particle &pp, i
 
 constexpr size_t kP2GSmemBytes =
     sizeof(float) * (kGridChannels * kHaloCells + kP2GFields * kP2GRanks * kP2GRow) +
-    sizeof(int) * (kP2GChunk + 1);
+    sizeof(int) * 2 * (kP2GChunk + 1);
 
 __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
   extern __shared__ float p2g_smem[];
@@ -589,11 +589,14 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
     for (int q = t; q < kGridChannels * kHaloCells; q += blockDim.x) sh[q] = 0.f;
     const int3 bk = local_block(s.prm, unpack_key(s.blk_pk[b]));
     const int ox = bk.x * 8, oy = bk.y * 8, oz = bk.z * 8;
+    // cell starts of chunk k in s_cs0 + (k & 1) * (kP2GChunk + 1); the next chunk's are loaded
+    // during this chunk's phase 2, so a chunk needs two barriers
+    int *const s_cs0 = s_cs;
+    if (t <= kP2GChunk) s_cs0[t] = t < 512 ? s.cell_start[b * 512 + t] : end;
     for (int chunk = 0; chunk < 512 / kP2GChunk; ++chunk) {
       const int cell0 = chunk * kP2GChunk;
-      __syncthreads();  // previous chunk's staging fully consumed (and halo zeroed)
-      if (t <= kP2GChunk) s_cs[t] = cell0 + t < 512 ? s.cell_start[b * 512 + cell0 + t] : end;
-      __syncthreads();
+      __syncthreads();  // previous chunk's staging consumed, this chunk's starts loaded, halo zeroed
+      int *s_cs = s_cs0 + (chunk & 1) * (kP2GChunk + 1);
       // ---- phase 1: consecutive threads take consecutive slots (coalesced gathers)
       const int c0 = s_cs[0], c1 = s_cs[kP2GChunk];
       for (int slot = c0 + t; slot < c1; slot += blockDim.x) {
@@ -629,6 +632,10 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
         }
       }
       __syncthreads();
+      if (chunk + 1 < 512 / kP2GChunk && t <= kP2GChunk) {
+        const int nc = cell0 + kP2GChunk + t;
+        s_cs0[((chunk + 1) & 1) * (kP2GChunk + 1) + t] = nc < 512 ? s.cell_start[b * 512 + nc] : end;
+      }
       // ---- phase 2: thread (cell, channel) sums the staged particles of its cell
       {
         const int cnt = min(s_cs[my_cell + 1] - s_cs[my_cell], kP2GRanks);
