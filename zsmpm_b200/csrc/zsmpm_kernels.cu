@@ -508,6 +508,7 @@ constexpr int kP2GRanks = 12;     // particles per cell staged per chunk (more g
 constexpr int kP2GFields = 22;    // w[9], m, q[3], ax[3], ay[3], az[3]
 constexpr int kP2GRow = kP2GChunk + 1;  // padded row: rank r of cell c in bank (r + c) % 32
 constexpr int kP2GThreads = 256;  // 4 channels x 64 cells
+constexpr int kP2GMap = 1024;     // slots of a chunk mapped to their cell (more: binary search)
 
 struct p2g_particle {
   float m, w[3][3], q[3], ax[3], ay[3], az[3];
@@ -569,7 +570,7 @@ __device__ __forceinline__ void p2g_direct(float *shf, const p2g_particle &pp, i
 
 constexpr size_t kP2GSmemBytes =
     sizeof(float) * (kGridChannels * kHaloCells + kP2GFields * kP2GRanks * kP2GRow) +
-    sizeof(int) * 2 * (kP2GChunk + 1);
+    sizeof(int) * 2 * (kP2GChunk + 1) + sizeof(unsigned char) * 2 * kP2GMap;
 
 __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
   extern __shared__ float p2g_smem[];
@@ -592,19 +593,39 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
     // cell starts of chunk k in s_cs0 + (k & 1) * (kP2GChunk + 1); the next chunk's are loaded
     // during this chunk's phase 2, so a chunk needs two barriers
     int *const s_cs0 = s_cs;
+    unsigned char *const s_map0 = reinterpret_cast<unsigned char *>(s_cs0 + 2 * (kP2GChunk + 1));
+    // slot -> cell map of chunk k in s_map0 + (k & 1) * kP2GMap, written by the chunk's cell
+    // threads from the global cell starts
+    auto fill_map = [&](int chunk_to_fill) {
+      if (t < kP2GChunk) {
+        const int c = chunk_to_fill * kP2GChunk + t;
+        const int cs = s.cell_start[b * 512 + c];
+        const int ce = c + 1 < 512 ? s.cell_start[b * 512 + c + 1] : end;
+        const int base = s.cell_start[b * 512 + chunk_to_fill * kP2GChunk];
+        unsigned char *m = s_map0 + (chunk_to_fill & 1) * kP2GMap;
+        for (int q = cs - base; q < ce - base && q < kP2GMap; ++q) m[q] = (unsigned char)t;
+      }
+    };
     if (t <= kP2GChunk) s_cs0[t] = t < 512 ? s.cell_start[b * 512 + t] : end;
+    fill_map(0);
     for (int chunk = 0; chunk < 512 / kP2GChunk; ++chunk) {
       const int cell0 = chunk * kP2GChunk;
       __syncthreads();  // previous chunk's staging consumed, this chunk's starts loaded, halo zeroed
       int *s_cs = s_cs0 + (chunk & 1) * (kP2GChunk + 1);
       // ---- phase 1: consecutive threads take consecutive slots (coalesced gathers)
       const int c0 = s_cs[0], c1 = s_cs[kP2GChunk];
+      const unsigned char *s_map = s_map0 + (chunk & 1) * kP2GMap;
       for (int slot = c0 + t; slot < c1; slot += blockDim.x) {
-        int lo = 0, hi = kP2GChunk;  // last cell whose start is <= slot
-        while (hi - lo > 1) {
-          const int mid = (lo + hi) >> 1;
-          if (s_cs[mid] <= slot) lo = mid;
-          else hi = mid;
+        int lo = 0;  // the cell of this slot: the last cell whose start is <= slot
+        if (slot - c0 < kP2GMap) {
+          lo = s_map[slot - c0];
+        } else {
+          int hi = kP2GChunk;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_cs[mid] <= slot) lo = mid;
+            else hi = mid;
+          }
         }
         const int cl = lo, r = slot - s_cs[lo], cell = cell0 + cl;
         const int ex = (cell >> 6) + 1, ey = ((cell >> 3) & 7) + 1, ez = (cell & 7) + 1;
@@ -632,9 +653,12 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
         }
       }
       __syncthreads();
-      if (chunk + 1 < 512 / kP2GChunk && t <= kP2GChunk) {
-        const int nc = cell0 + kP2GChunk + t;
-        s_cs0[((chunk + 1) & 1) * (kP2GChunk + 1) + t] = nc < 512 ? s.cell_start[b * 512 + nc] : end;
+      if (chunk + 1 < 512 / kP2GChunk) {
+        if (t <= kP2GChunk) {
+          const int nc = cell0 + kP2GChunk + t;
+          s_cs0[((chunk + 1) & 1) * (kP2GChunk + 1) + t] = nc < 512 ? s.cell_start[b * 512 + nc] : end;
+        }
+        fill_map(chunk + 1);
       }
       // ---- phase 2: thread (cell, channel) sums the staged particles of its cell
       {
