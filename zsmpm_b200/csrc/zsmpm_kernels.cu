@@ -394,16 +394,18 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
     // block counts, one atomic per distinct block of the warp
     const unsigned bpeers = __match_any_sync(kFull, ok ? blk : -1 - lane);
     if (ok && lane == __ffs(bpeers) - 1) atomicAdd(&s.block_count[blk], __popc(bpeers));
+    // cell counts, one atomic per distinct cell of the warp (particles arrive in the previous
+    // binning's order, so a warp spans a few cells); ranks within the warp follow lane order
+    const int cell = ((c.x - 8 * b.x) << 6) | ((c.y - 8 * b.y) << 3) | (c.z - 8 * b.z);
+    const uint32_t k32 = ok ? (uint32_t)blk * 512u + (uint32_t)cell : 0xffffffffu - (uint32_t)lane;
+    const unsigned cpeers = __match_any_sync(kFull, k32);
+    const int cleader = __ffs(cpeers) - 1;
+    int cbase = 0;
+    if (ok && lane == cleader) cbase = atomicAdd(&s.cell_count[k32], __popc(cpeers));
+    cbase = __shfl_sync(kFull, cbase, cleader);
     if (i < n) {
-      if (ok) {
-        const int cell = ((c.x - 8 * b.x) << 6) | ((c.y - 8 * b.y) << 3) | (c.z - 8 * b.z);
-        const uint32_t k32 = (uint32_t)blk * 512u + (uint32_t)cell;
-        s.key32[i] = k32;
-        s.rnk[i] = atomicAdd(&s.cell_count[k32], 1);
-      } else {
-        s.key32[i] = 0xffffffffu;
-        s.rnk[i] = 0;
-      }
+      s.key32[i] = ok ? k32 : 0xffffffffu;
+      s.rnk[i] = ok ? cbase + __popc(cpeers & lanemask_lt()) : 0;
     }
   }
 }
