@@ -20,6 +20,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
+// Particle passes take kPass particles per thread per round: all loads first, so that several
+// are in flight per thread (the passes are bound by load latency, not bandwidth).
+constexpr int kPass = 4;
 
 __device__ __forceinline__ void set_status(int *ctr, int bit) { atomicOr(&ctr[kCtrStatus], bit); }
 
@@ -103,13 +106,14 @@ __device__ __forceinline__ int3 local_block(const scene_params &p, int3 k) {
 // Cell and block of particle i in the scene's key space: cell_of, then for batched scenes a
 // check that the local block leaves room for the +1 enlargement inside the slot, and the
 // slot offset.
-__device__ __forceinline__ bool particle_cell(const scene_device &s, int i, float4 x, int3 &c, int3 &b) {
+// sid: the particle's scene (batched scenes only)
+__device__ __forceinline__ bool particle_cell(const scene_device &s, int sid, float4 x, int3 &c, int3 &b) {
   if (!cell_of(s.prm, x, c, b)) return false;
   if (s.prm.batch) {
     const int hi = kBatchSlot - kBatchMargin - 1;
     if (b.x < -kBatchMargin || b.x >= hi || b.y < -kBatchMargin || b.y >= hi || b.z < -kBatchMargin || b.z >= hi)
       return false;
-    const int3 o = slot_of_scene(s.cur.sid[i]);
+    const int3 o = slot_of_scene(sid);
     b = make_int3(b.x + kBatchSlot * o.x, b.y + kBatchSlot * o.y, b.z + kBatchSlot * o.z);
     c = make_int3(c.x + 8 * kBatchSlot * o.x, c.y + 8 * kBatchSlot * o.y, c.z + 8 * kBatchSlot * o.z);
   }
@@ -240,24 +244,35 @@ __global__ void __launch_bounds__(kThreads) k_insert_particle_blocks(scene_devic
   int3 hi = make_int3(-0x7fffffff, -0x7fffffff, -0x7fffffff);
   const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int warps = grid_threads() >> 5;
-  for (int base = warp_global * 32; base < n; base += warps * 32) {
-    const int i = base + lane;
-    uint64_t key = kEmptyKey - 1 - lane;  // distinct per lane when invalid
-    int3 c, b = make_int3(0, 0, 0);
-    bool valid = false;
-    if (i < n) {
-      if (particle_cell(s, i, s.cur.xm[i], c, b)) {
-        key = pack_key(b.x, b.y, b.z);
-        valid = true;
-      } else {
-        set_status(s.ctr, kStatusOutOfDomain);
-      }
+  for (int base0 = warp_global * 32 * kPass; base0 < n; base0 += warps * 32 * kPass) {
+    float4 xs[kPass];
+    int sids[kPass];
+#pragma unroll
+    for (int u = 0; u < kPass; ++u) {
+      const int i = base0 + u * 32 + lane;
+      xs[u] = i < n ? s.cur.xm[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      sids[u] = (s.prm.batch && i < n) ? s.cur.sid[i] : 0;
     }
-    const unsigned peers = __match_any_sync(kFull, key);
-    if (valid && lane == __ffs(peers) - 1) {
-      table_insert(s, key, b, &s.ctr[kCtrParticleBlocks], 0);
-      lo = make_int3(min(lo.x, b.x), min(lo.y, b.y), min(lo.z, b.z));
-      hi = make_int3(max(hi.x, b.x), max(hi.y, b.y), max(hi.z, b.z));
+#pragma unroll
+    for (int u = 0; u < kPass; ++u) {
+      const int i = base0 + u * 32 + lane;
+      uint64_t key = kEmptyKey - 1 - lane;  // distinct per lane when invalid
+      int3 c, b = make_int3(0, 0, 0);
+      bool valid = false;
+      if (i < n) {
+        if (particle_cell(s, sids[u], xs[u], c, b)) {
+          key = pack_key(b.x, b.y, b.z);
+          valid = true;
+        } else {
+          set_status(s.ctr, kStatusOutOfDomain);
+        }
+      }
+      const unsigned peers = __match_any_sync(kFull, key);
+      if (valid && lane == __ffs(peers) - 1) {
+        table_insert(s, key, b, &s.ctr[kCtrParticleBlocks], 0);
+        lo = make_int3(min(lo.x, b.x), min(lo.y, b.y), min(lo.z, b.z));
+        hi = make_int3(max(hi.x, b.x), max(hi.y, b.y), max(hi.z, b.z));
+      }
     }
   }
 #pragma unroll
@@ -375,12 +390,22 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
   const int nb = s.ctr[kCtrBlocks];
   const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int warps = grid_threads() >> 5;
-  for (int base = warp_global * 32; base < n; base += warps * 32) {
-    const int i = base + lane;
+  for (int base0 = warp_global * 32 * kPass; base0 < n; base0 += warps * 32 * kPass) {
+   float4 xs[kPass];
+   int sids[kPass];
+#pragma unroll
+   for (int u = 0; u < kPass; ++u) {
+     const int i = base0 + u * 32 + lane;
+     xs[u] = i < n ? s.cur.xm[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+     sids[u] = (s.prm.batch && i < n) ? s.cur.sid[i] : 0;
+   }
+#pragma unroll
+   for (int u = 0; u < kPass; ++u) {
+    const int i = base0 + u * 32 + lane;
     uint64_t key = kEmptyKey - 1 - lane;
     int3 c = make_int3(0, 0, 0), b = make_int3(0, 0, 0);
     bool valid = false;
-    if (i < n && particle_cell(s, i, s.cur.xm[i], c, b)) {
+    if (i < n && particle_cell(s, sids[u], xs[u], c, b)) {
       key = pack_key(b.x, b.y, b.z);
       valid = true;
     }
@@ -407,6 +432,7 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
       s.key32[i] = ok ? k32 : 0xffffffffu;
       s.rnk[i] = ok ? cbase + __popc(cpeers & lanemask_lt()) : 0;
     }
+   }
   }
 }
 
@@ -435,10 +461,21 @@ __global__ void __launch_bounds__(512) k_cell_start(scene_device s) {
 
 __global__ void __launch_bounds__(kThreads) k_bin_scatter(scene_device s) {
   const int n = s.prm.n;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += grid_threads()) {
-    const uint32_t k = s.key32[i];
-    if (k == 0xffffffffu) continue;
-    s.tmp[s.cell_start[k] + s.rnk[i]] = i;
+  const int stride = grid_threads();
+  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += kPass * stride) {
+    uint32_t k[kPass];
+    int r[kPass], cs[kPass];
+#pragma unroll
+    for (int u = 0; u < kPass; ++u) {
+      const int i = i0 + u * stride;
+      k[u] = i < n ? s.key32[i] : 0xffffffffu;
+      r[u] = i < n ? s.rnk[i] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < kPass; ++u) cs[u] = k[u] != 0xffffffffu ? s.cell_start[k[u]] : 0;
+#pragma unroll
+    for (int u = 0; u < kPass; ++u)
+      if (k[u] != 0xffffffffu) s.tmp[cs[u] + r[u]] = i0 + u * stride;
   }
 }
 
