@@ -39,9 +39,12 @@ __device__ int table_insert(const scene_device &s, uint64_t key, int3 k, int *co
   const int T = s.prm.table_size;
   int slot = home_slot(k.x, k.y, k.z, T);
   for (int probe = 0; probe < T; ++probe) {
-    const unsigned long long prev =
-        atomicCAS((unsigned long long *)&s.pk[slot], (unsigned long long)kEmptyKey,
-                  (unsigned long long)key);
+    // most calls find their key already present (every warp of a block's particles asks):
+    // a plain load settles those without a contended atomic
+    unsigned long long prev = *reinterpret_cast<volatile unsigned long long *>(&s.pk[slot]);
+    if (prev == (unsigned long long)key) return -1;
+    if (prev == kEmptyKey)
+      prev = atomicCAS((unsigned long long *)&s.pk[slot], (unsigned long long)kEmptyKey, (unsigned long long)key);
     if (prev == kEmptyKey) {
       const int idx = index_base + atomicAdd(counter, 1);
       s.tkeys[3 * slot + 0] = k.x;
