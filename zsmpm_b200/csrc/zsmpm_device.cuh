@@ -178,6 +178,11 @@ __device__ __forceinline__ void swap_cols(float a[3][3], float v[3][3], float rh
 }  // namespace svd_detail
 
 // A (column-major) = U diag(S) V^T; U, V rotations; S sorted by magnitude, S[2] may be < 0.
+// kWarpEarlyExit: stop the Jacobi sweeps after the second or third once, for every lane of the
+// warp, the off-diagonal of A^T A is below 1e-7 of its diagonal (squared: 1e-14), where the
+// remaining sweeps only move the result by rounding.  Every lane of the warp must call it then.
+// The default runs the reference's four sweeps.
+template <bool kWarpEarlyExit = false>
 __device__ __forceinline__ void svd3(const float *A, float *U, float *S, float *V) {
   using namespace svd_detail;
   float a[3][3];
@@ -194,6 +199,11 @@ __device__ __forceinline__ void svd3(const float *A, float *U, float *S, float *
   float qs = 1.f, qx = 0.f, qy = 0.f, qz = 0.f;
 #pragma unroll
   for (int sweep = 0; sweep < 4; ++sweep) {
+    if (kWarpEarlyExit && sweep >= 2) {
+      const float off = s21 * s21 + s31 * s31 + s32 * s32;
+      const float diag = s11 * s11 + s22 * s22 + s33 * s33;
+      if (__all_sync(0xffffffffu, off <= 1e-14f * diag)) break;
+    }
     conjugate(s11, s22, s33, s21, s31, s32, qs, qz, qx, qy);
     conjugate(s22, s33, s11, s32, s21, s31, qs, qx, qy, qz);
     conjugate(s33, s11, s22, s31, s32, s21, qs, qy, qz, qx);
@@ -291,10 +301,11 @@ __device__ __forceinline__ void fc_principal(float mu, float lambda, const float
 // Return map + stress.  F: trial deformation in, F after the model's projection out
 // (the projected F is what the reference's stress functions leave in their F argument);
 // plastic: logJp (DP) or Jp (snow); tau out.  Reference ordering keeps F unchanged.
+template <bool kWarpEarlyExit = false>
 __device__ __forceinline__ void constitutive(const material_dev &mat, float *F, float &plastic,
                                              float *tau) {
   float U[9], S[3], V[9];
-  svd3(F, U, S, V);
+  svd3<kWarpEarlyExit>(F, U, S, V);
   if (mat.model == 0) {
     float Ph[3];
     fc_principal(mat.mu, mat.lambda, S, Ph);

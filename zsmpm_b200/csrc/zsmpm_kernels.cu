@@ -846,9 +846,9 @@ __global__ void __launch_bounds__(kThreads) k_grid_update(scene_device s) {
 // then per particle gather v and C (G2P.hpp:56-66), advect, update F = (I + dt C) F
 // (G2P.hpp:76-78), run the constitutive update and write the particle to its binned slot
 // in the next buffer set, so that storage order follows the binning of this substep.
-// Particles are taken 32 per warp; with the learned closure the whole warp steps together
-// (lanes past the block's end run on a copy of its first particle and write nothing), so
-// that the tensor-core MLP runs across the warp.
+// Particles are taken 32 per warp and the whole warp steps together (lanes past the block's
+// end run on a copy of its first particle and write nothing): the SVD's early exit is a
+// warp-wide vote, and the learned closure's tensor-core MLP runs across the warp.
 
 // trial-state features of the closure: log singular values and the model's three
 // material/state features
@@ -1013,8 +1013,9 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
     const int org[3] = {bk.x * 8, bk.y * 8, bk.z * 8};
     for (int base = start + warp * 32; base < end; base += NT) {
       const int slot = base + lane;
+      // every lane of the warp stays in the loop (lanes past the block's end work on a copy of
+      // its first particle and store nothing): the SVD's early exit is a warp-wide vote
       const bool active = slot < end;
-      if (!kLearned && !active) break;
       const int i = s.src[active ? slot : start];
       float4 xm = s.cur.xm[i];
       float F[9];
@@ -1104,9 +1105,9 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
         learned_constitutive(p.mat, s.aux.cd, sfrag, sbias, sxs + warp * 32 * 16, sys + warp * 32 * 8, Fn, pl, tau,
                              active, id, substep);
       else if (kBatch)
-        constitutive(s_mat, Fn, pl, tau);
+        constitutive<true>(s_mat, Fn, pl, tau);
       else
-        constitutive(p.mat, Fn, pl, tau);
+        constitutive<true>(p.mat, Fn, pl, tau);
       if (!active) continue;
       const size_t cap = (size_t)p.cap;
       s.nxt.xm[slot] = xm;
