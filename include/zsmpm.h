@@ -343,10 +343,16 @@ ZSMPM_API zsmpm_status zsmpm_closure_train(zsmpm_closure *c, int32_t epochs, int
  * x, y raw device rows [n][6]; grad device [9158]; loss device [1]. */
 ZSMPM_API zsmpm_status zsmpm_closure_loss_grad(zsmpm_closure *c, const float *x, const float *y, int64_t n,
                                                float *grad, float *loss, void *stream);
-/* Network outputs (unscaled D and tau) of raw feature rows (device [n][6]); bf16 != 0 runs
- * the tensor-core forward that G2P uses, else an FP32 forward of the master weights. */
+/* Network outputs (unscaled D and tau) of raw feature rows (device [n][6]).  bf16 selects the
+ * path: 0 an FP32 forward of the master weights; 1 the BF16 mma.sync forward that G2P runs
+ * (one warp per 32 rows, activations in registers); 2 a BF16 tcgen05 forward (5th-generation
+ * tensor cores: 128-row tiles per CTA, operands in shared memory, FP32 accumulators in tensor
+ * memory).  Asynchronous; zsmpm_closure_status reports a tcgen05 wait that gave up. */
 ZSMPM_API zsmpm_status zsmpm_closure_infer(zsmpm_closure *c, const float *x, float *y, int64_t n, int32_t bf16,
                                            void *stream);
+/* Synchronises the device and reports (then clears) a bounded tensor-core wait that gave up
+ * in zsmpm_closure_infer (ZSMPM_ERR_TIMEOUT). */
+ZSMPM_API zsmpm_status zsmpm_closure_status(zsmpm_closure *c);
 /* The plain return map's (D, tau) for raw feature rows (device [n][6]). */
 ZSMPM_API zsmpm_status zsmpm_closure_targets(zsmpm_closure *c, const float *x, float *y, int64_t n, void *stream);
 ZSMPM_API zsmpm_status zsmpm_closure_get_state(zsmpm_closure *c, zsmpm_closure_state *out);

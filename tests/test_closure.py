@@ -161,6 +161,36 @@ def test_inference_fp32_and_bf16_match_cpu_oracle(zs, gpu, model):
     c.close()
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("model", [DP, SNOW])
+def test_tcgen05_inference_matches_mma_sync_and_oracle(zs, gpu, model):
+    """The tcgen05 forward (BF16 operands in shared memory, FP32 accumulators in tensor memory)
+    against the mma.sync forward and the float64 oracle, on ragged row counts."""
+    import torch
+    spec, c = _closure(zs, model)
+    c.train(2, batch=2048, lr=1e-3)
+    st = c.state_arrays()
+    k, xi = _kappa(spec.material), spec.material.hardening
+    for n in (1, 128, 1000, 70001):
+        rows = random_rows(model, n, 21 + n, spec.material.E, spec.material.nu)
+        x = torch.from_numpy(rows).to(gpu)
+        ytc = c.infer(x, path="tcgen05").cpu().numpy().astype(np.float64)
+        c.status()
+        ymma = c.infer(x, path="mma_sync").cpu().numpy().astype(np.float64)
+        xin = mlp.inputs(model, rows, k, xi)[0]
+        ref = mlp.from_net(model, rows, mlp.forward(st["params"], (xin - st["in_mean"]) * st["in_inv_std"])
+                           * st["out_scale"], k, xi)
+        assert np.all(np.isfinite(ytc))
+        for lo in (0, 3):
+            scale = np.linalg.norm(ref[:, lo:lo + 3]) / np.sqrt(3) + 1e-30
+            for col in range(lo, lo + 3):
+                # BF16 operands and activations, FP32 accumulation: as the mma.sync path
+                assert np.linalg.norm(ytc[:, col] - ref[:, col]) <= 3e-2 * scale
+                # the two tensor-core paths round the same values; they differ by accumulation order
+                assert np.linalg.norm(ytc[:, col] - ymma[:, col]) <= 5e-3 * scale
+    c.close()
+
+
 def stress_errors(y, ref, mat):
     """Relative principal-stress error per row, floored at 1e-4 of the stress scale, and the
     aggregate sqrt(sum |dtau|^2 / sum |tau|^2)."""

@@ -132,6 +132,7 @@ SIGNATURES = {
     "zsmpm_closure_loss_grad": (_S, [_P, _P, _P, C.c_int64, _P, _P, _P]),
     "zsmpm_closure_infer": (_S, [_P, _P, _P, C.c_int64, C.c_int32, _P]),
     "zsmpm_closure_targets": (_S, [_P, _P, _P, C.c_int64, _P]),
+    "zsmpm_closure_status": (_S, [_P]),
     "zsmpm_closure_get_state": (_S, [_P, C.POINTER(ClosureState)]),
     "zsmpm_closure_set_state": (_S, [_P, C.POINTER(ClosureState)]),
     "zsmpm_scene_set_closure": (_S, [_P, _P, C.c_int32]),

@@ -96,12 +96,19 @@ class Closure:
                                                      _stream(stream)), "closure_loss_grad")
         return loss, grad
 
-    def infer(self, x, bf16: bool = True, stream=None):
+    def infer(self, x, bf16: bool = True, stream=None, path: str | None = None):
+        """Network outputs (D, tau) of raw rows x.  path: "fp32", "mma_sync" (the G2P forward)
+        or "tcgen05"; by default "mma_sync" when bf16 else "fp32"."""
         import torch
+        mode = {"fp32": 0, "mma_sync": 1, "tcgen05": 2}[path or ("mma_sync" if bf16 else "fp32")]
         y = torch.empty_like(x)
         _abi.check(self._lib.zsmpm_closure_infer(self._h, _rows(x, "x"), _rows(y, "y"), int(x.shape[0]),
-                                                 int(bool(bf16)), _stream(stream)), "closure_infer")
+                                                 mode, _stream(stream)), "closure_infer")
         return y
+
+    def status(self) -> None:
+        """Synchronises; raises if a bounded tensor-core wait of the tcgen05 path gave up."""
+        _abi.check(self._lib.zsmpm_closure_status(self._h), "closure_status")
 
     def targets(self, x, stream=None):
         """The plain return map's (D, tau) for raw rows x."""

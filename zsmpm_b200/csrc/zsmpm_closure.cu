@@ -26,6 +26,8 @@ struct zsmpm_closure {
   float *grad = nullptr;
   float *adam_m = nullptr, *adam_v = nullptr;
   uint2 *frag = nullptr;
+  uint4 *umma_w = nullptr;    // weights in the tcgen05 shared-memory layout (kTcWBytes)
+  int *tc_status = nullptr;   // bounded-wait failures of the tcgen05 inference
   float *bias = nullptr;
   double *audit = nullptr;    // audit accumulators until the closure is attached to a scene
   float *data_x = nullptr;    // raw features [n][6]
@@ -417,6 +419,240 @@ __global__ void k_closure_infer_fp32(closure_dev cd, const float *p, const float
   }
 }
 
+// ---------------------------------------------------------------- tcgen05 inference
+// The same network on the 5th-generation tensor cores: one CTA of 128 threads takes 128-row
+// tiles (one thread per row).  Per layer one elected thread issues tcgen05.mma (kind::f16,
+// BF16 operands from shared memory, FP32 accumulators in tensor memory, M = 128) and commits
+// it to an mbarrier; every thread then loads its row of the accumulator with tcgen05.ld,
+// adds the bias, applies SiLU in bf16x2 (as the mma.sync path does) and writes the next
+// layer's A tile back to shared memory.
+//
+// Shared-memory operands use the K-major layout without swizzle: 8-row x 16-byte core
+// matrices; element (r, k) of an R-row matrix at (k / 8) * (16 R) + (r / 8) * 128 + (r % 8) * 16
+// + (k % 8) * 2 bytes, so the stride between 8-row groups is 128 B and the stride between
+// 8-element K chunks is 16 R bytes (the descriptor's stride and leading byte offsets).
+constexpr int kTcRows = 128;
+constexpr int kTcW1 = 0;                         // 64 x 16
+constexpr int kTcW2 = kTcW1 + 64 * 16 * 2;       // 64 x 64
+constexpr int kTcW3 = kTcW2 + 64 * 64 * 2;       // 64 x 64
+constexpr int kTcW4 = kTcW3 + 64 * 64 * 2;       // 16 x 64 (6 rows used)
+constexpr int kTcA = kTcW4 + 16 * 64 * 2;        // 128 x 64 activations
+constexpr int kTcSmem = kTcA + kTcRows * 64 * 2;
+constexpr int kTcWBytes = kTcA;                  // the packed weights
+constexpr int kTcTmemCols = 64;
+constexpr long long kTcWaitLimit = 1ll << 22;    // try_wait rounds before giving up
+
+__host__ __device__ constexpr int umma_offset(int R, int r, int k) {
+  return (k >> 3) * (16 * R) + (r >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+// weights -> bf16 in the K-major layout (W[out][in]; zero padding to K = 16 and N = 16)
+__global__ void k_pack_umma(const float *p, __nv_bfloat16 *w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // element index over all four matrices
+  int base, R, K, layer, local;
+  if (i < 64 * 16) { layer = 0; base = kTcW1; R = 64; K = 16; local = i; }
+  else if (i < 64 * 16 + 4096) { layer = 1; base = kTcW2; R = 64; K = 64; local = i - 64 * 16; }
+  else if (i < 64 * 16 + 8192) { layer = 2; base = kTcW3; R = 64; K = 64; local = i - 64 * 16 - 4096; }
+  else if (i < 64 * 16 + 8192 + 16 * 64) { layer = 3; base = kTcW4; R = 16; K = 64; local = i - 64 * 16 - 8192; }
+  else return;
+  const int r = local / K, k = local % K;
+  float v = 0.f;
+  if (layer == 0) v = k < 6 ? p[kOffW1 + r * 6 + k] : 0.f;
+  else if (layer == 1) v = p[kOffW2 + r * 64 + k];
+  else if (layer == 2) v = p[kOffW3 + r * 64 + k];
+  else v = r < 6 ? p[kOffW4 + r * 64 + k] : 0.f;
+  w[(base + umma_offset(R, r, k)) / 2] = __float2bfloat16_rn(v);
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)(128u >> 4) << 32;  // 8-row groups 128 B apart
+  d |= (uint64_t)1 << 46;            // descriptor version of sm_100; no swizzle, base offset 0
+  return d;
+}
+
+// kind::f16 instruction descriptor: BF16 A and B (K-major), FP32 D, M = 128, N
+__device__ __forceinline__ uint32_t umma_idesc(int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p; \n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < kTcWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 64 columns of this thread's row of the accumulator
+__device__ __forceinline__ void tmem_ld64(uint32_t addr, float (&v)[64]) {
+  uint32_t r[64];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,"
+      "%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+        "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+        "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+        "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+        "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 64; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// one hidden layer's epilogue: bias + SiLU (bf16x2) of this thread's 64 accumulators into its
+// row of the A tile
+__device__ __forceinline__ void tc_hidden_epilogue(uint32_t tmem_row, const float *bias, unsigned char *a_tile,
+                                                   int row) {
+  float v[64];
+  tmem_ld64(tmem_row, v);
+#pragma unroll
+  for (int kc = 0; kc < 8; ++kc) {
+    uint4 q;
+    q.x = silu_bf16x2(pack_bf16x2(v[8 * kc + 0] + bias[8 * kc + 0], v[8 * kc + 1] + bias[8 * kc + 1]));
+    q.y = silu_bf16x2(pack_bf16x2(v[8 * kc + 2] + bias[8 * kc + 2], v[8 * kc + 3] + bias[8 * kc + 3]));
+    q.z = silu_bf16x2(pack_bf16x2(v[8 * kc + 4] + bias[8 * kc + 4], v[8 * kc + 5] + bias[8 * kc + 5]));
+    q.w = silu_bf16x2(pack_bf16x2(v[8 * kc + 6] + bias[8 * kc + 6], v[8 * kc + 7] + bias[8 * kc + 7]));
+    *reinterpret_cast<uint4 *>(a_tile + umma_offset(kTcRows, row, 8 * kc)) = q;
+  }
+}
+
+__global__ void __launch_bounds__(kTcRows) k_closure_infer_tc(closure_dev cd, const uint4 *wpack, const float *x,
+                                                              float *y, int64_t n, int *status) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t taddr_s;
+  __shared__ float sbias[kBiasTotal];
+  const int t = threadIdx.x, warp = t >> 5;
+  for (int i = t; i < kTcA / 16; i += kTcRows) reinterpret_cast<uint4 *>(tsm)[i] = wpack[i];
+  for (int i = t; i < kBiasTotal; i += kTcRows) sbias[i] = cd.bias[i];
+  const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (warp == 0) {
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&taddr_s);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kTcTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (t == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1));
+  async_proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = taddr_s;
+  const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 lanes
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(tsm);
+  unsigned char *a_tile = tsm + kTcA;
+  const uint32_t a_addr = sbase + kTcA;
+  const uint32_t id64 = umma_idesc(64), id16 = umma_idesc(16);
+  uint32_t parity = 0;
+  bool ok = true;
+  for (int64_t tile = blockIdx.x; tile * kTcRows < n; tile += gridDim.x) {
+    const int64_t row = tile * kTcRows + t;
+    // input row -> network inputs -> bf16 A tile (K = 16: 6 inputs and zeros)
+    float raw[6], in[kMlpIn];
+    net_scale ns;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) raw[k] = row < n ? x[6 * row + k] : (k == 3 ? 0.02f : k == 4 ? 0.0075f : 0.f);
+    closure_inputs(cd.model, cd.kappa, cd.hardening, raw, in, ns);
+#pragma unroll
+    for (int k = 0; k < kMlpIn; ++k) in[k] = (in[k] - cd.in_mean[k]) * cd.in_inv_std[k];
+    uint4 q0;
+    q0.x = pack_bf16x2(in[0], in[1]);
+    q0.y = pack_bf16x2(in[2], in[3]);
+    q0.z = pack_bf16x2(in[4], in[5]);
+    q0.w = 0u;
+    *reinterpret_cast<uint4 *>(a_tile + umma_offset(kTcRows, t, 0)) = q0;
+    *reinterpret_cast<uint4 *>(a_tile + umma_offset(kTcRows, t, 8)) = make_uint4(0u, 0u, 0u, 0u);
+    // four layers: MMA by one thread, completion through the mbarrier, epilogue by all
+#pragma unroll 1
+    for (int layer = 0; layer < 4 && ok; ++layer) {
+      async_proxy_fence();
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      if (t == 0) {
+        const int ksteps = layer == 0 ? 1 : 4;
+        const uint32_t w_off = layer == 0 ? kTcW1 : layer == 1 ? kTcW2 : layer == 2 ? kTcW3 : kTcW4;
+        const uint32_t w_rows = layer == 3 ? 16 : 64;
+        for (int ks = 0; ks < ksteps; ++ks)
+          umma_bf16(tmem, umma_desc(a_addr + 2 * ks * (16 * kTcRows), 16 * kTcRows),
+                    umma_desc(sbase + w_off + 2 * ks * (16 * w_rows), 16 * w_rows), layer == 3 ? id16 : id64,
+                    ks > 0 ? 1u : 0u);
+        umma_commit(bar);
+      }
+      const bool done = mbar_wait(bar, parity);
+      parity ^= 1u;
+      ok = __syncthreads_and(done) != 0;
+      if (!ok) break;
+      tc_fence_after();
+      if (layer < 3) {
+        tc_hidden_epilogue(tmem_row, sbias + 64 * layer, a_tile, t);
+      } else {
+        float o[16];
+        tmem_ld16(tmem_row, o);
+        float out[kMlpOut], yr[6];
+#pragma unroll
+        for (int k = 0; k < kMlpOut; ++k) out[k] = (o[k] + sbias[192 + k]) * cd.out_scale[k];
+        closure_from_net(ns, out, yr);
+        if (row < n)
+#pragma unroll
+          for (int k = 0; k < 6; ++k) y[6 * row + k] = yr[k];
+      }
+      tc_fence_before();
+    }
+    if (!ok) break;
+  }
+  // all tensor-memory reads are complete (tcgen05.ld waits) and no MMA is in flight unless a
+  // wait gave up; then one more bounded wait for it before the columns are freed
+  if (!ok) {
+    mbar_wait(bar, parity ^ 1u);  // the phase whose wait gave up (parity has moved past it)
+    if (t == 0) atomicOr(status, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
+}
+
 zsmpm_status cerr(zsmpm_status st, const std::string &m) { return (zsmpm_status)record_error(st, m.c_str()); }
 zsmpm_status ccuda(cudaError_t e, const char *what) {
   return cerr(ZSMPM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -479,6 +715,7 @@ norm_dev norm_of(const closure_dev &cd) {
 
 zsmpm_status pack(zsmpm_closure *c, cudaStream_t st) {
   k_pack_fragments<<<(kFragTotal + 255) / 256, 256, 0, st>>>(c->params, c->frag, c->bias);
+  k_pack_umma<<<(kTcWBytes / 2 + 255) / 256, 256, 0, st>>>(c->params, reinterpret_cast<__nv_bfloat16 *>(c->umma_w));
   CZ_TRY(cudaGetLastError(), "pack fragments");
   return ZSMPM_OK;
 }
@@ -529,6 +766,9 @@ ZSMPM_API zsmpm_status zsmpm_closure_create(const zsmpm_material *mat, int32_t d
   if (e == cudaSuccess) e = cudaMalloc(&c->adam_m, sizeof(float) * kMlpParams);
   if (e == cudaSuccess) e = cudaMalloc(&c->adam_v, sizeof(float) * kMlpParams);
   if (e == cudaSuccess) e = cudaMalloc(&c->frag, sizeof(uint2) * kFragTotal);
+  if (e == cudaSuccess) e = cudaMalloc(&c->umma_w, kTcWBytes);
+  if (e == cudaSuccess) e = cudaMalloc(&c->tc_status, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->tc_status, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&c->bias, sizeof(float) * kBiasTotal);
   if (e == cudaSuccess) e = cudaMalloc(&c->stats, sizeof(float) * 32);
   if (e == cudaSuccess) e = cudaMalloc(&c->loss, sizeof(float));
@@ -564,7 +804,8 @@ ZSMPM_API zsmpm_status zsmpm_closure_destroy(zsmpm_closure *c) {
   cudaDeviceSynchronize();
   for (void *p : {(void *)c->params, (void *)c->grad, (void *)c->adam_m, (void *)c->adam_v, (void *)c->frag,
                   (void *)c->bias, (void *)c->stats, (void *)c->loss, (void *)c->audit, (void *)c->data_x,
-                  (void *)c->data_y, (void *)c->data_xt, (void *)c->data_yt})
+                  (void *)c->data_y, (void *)c->data_xt, (void *)c->data_yt, (void *)c->umma_w,
+                  (void *)c->tc_status})
     if (p) cudaFree(p);
   delete c;
   return ZSMPM_OK;
@@ -713,7 +954,13 @@ ZSMPM_API zsmpm_status zsmpm_closure_infer(zsmpm_closure *c, const float *x, flo
   if (!c || !x || !y || n < 1) return cerr(ZSMPM_ERR_INVALID_ARG, "bad arguments");
   CZ_TRY(cudaSetDevice(c->device), "cudaSetDevice");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (bf16) {
+  if (bf16 == 2) {
+    const zsmpm_status ps = pack(c, st);
+    if (ps != ZSMPM_OK) return ps;
+    const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+    const int grid = (int)std::min<int64_t>(tiles, (int64_t)sms() * 4);
+    k_closure_infer_tc<<<grid, kTcRows, kTcSmem, st>>>(c->cd, c->umma_w, x, y, n, c->tc_status);
+  } else if (bf16) {
     const zsmpm_status ps = pack(c, st);
     if (ps != ZSMPM_OK) return ps;
     k_closure_infer_bf16<<<sms() * 4, kThreads, 0, st>>>(c->cd, x, y, n);
@@ -721,6 +968,19 @@ ZSMPM_API zsmpm_status zsmpm_closure_infer(zsmpm_closure *c, const float *x, flo
     k_closure_infer_fp32<<<sms() * 4, kThreads, 0, st>>>(c->cd, c->params, x, y, n);
   }
   CZ_TRY(cudaGetLastError(), "closure infer");
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_closure_status(zsmpm_closure *c) {
+  if (!c) return cerr(ZSMPM_ERR_INVALID_ARG, "null closure");
+  CZ_TRY(cudaSetDevice(c->device), "cudaSetDevice");
+  CZ_TRY(cudaDeviceSynchronize(), "synchronize");
+  int w = 0;
+  CZ_TRY(cudaMemcpy(&w, c->tc_status, sizeof(int), cudaMemcpyDeviceToHost), "read closure status");
+  if (w) {
+    cudaMemset(c->tc_status, 0, sizeof(int));
+    return cerr(ZSMPM_ERR_TIMEOUT, "a bounded wait for a tensor-core MMA gave up");
+  }
   return ZSMPM_OK;
 }
 

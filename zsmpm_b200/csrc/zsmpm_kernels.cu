@@ -882,7 +882,7 @@ __device__ __forceinline__ void learned_constitutive(const material_dev &mat, co
                                                      float *ys, float *F, float &plastic, float *tau, bool active,
                                                      int id, int substep) {
   float U[9], S[3], V[9];
-  svd3(F, U, S, V);
+  svd3<true>(F, U, S, V);
   float feat[6];
   closure_features(mat, S, plastic, feat);
   bool in_hull = true;
