@@ -216,6 +216,7 @@ def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms
     sc.set_stage_timing(False)
     sc.status()
     cl.attach(sc, None)
+    mlp = mlp_inference_leg(c, n_rows=min(n, 16_777_216))
     c.close()
     value = n * args.steps * ws / (lms * 1e-3)
     return {"value": value, "unit": UNIT, "ms_per_step": lms / args.steps,
@@ -226,7 +227,40 @@ def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms
             "training": {"random_states": args.train_random, "logged_states": n_log,
                          "epochs": sum(e for e, _, _ in schedule), "seconds": train_s,
                          "first_loss": float(losses[0]), "final_loss": float(losses[-1])},
-            "inference": "BF16 mma.sync m16n8k16, FP32 accumulation, fused in G2P"}
+            "inference": "BF16 mma.sync m16n8k16, FP32 accumulation, fused in G2P",
+            "mlp_inference": mlp}
+
+
+def mlp_inference_leg(c, n_rows: int, reps: int = 5) -> dict:
+    """The closure's network alone over n_rows feature rows, on both tensor-core paths: the
+    mma.sync forward that G2P fuses and the tcgen05 forward (tensor-memory accumulators).
+    17,920 FLOP per row (6-64-64-64-6); peak = measured dense BF16 (burst)."""
+    import torch
+    try:
+        peak = float(json.loads(PEAKS.read_text())["bf16_tflops"])
+        peak_kind = "measured"
+    except Exception:
+        peak, peak_kind = 1590.0, "fallback"
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.zeros((n_rows, 6), dtype=torch.float32, device="cuda")
+    x[:, :3] = (torch.rand((n_rows, 3), generator=g, device="cuda") - 0.5) * 0.02
+    x[:, :3] = torch.sort(x[:, :3], dim=1, descending=True).values
+    x[:, 3] = 30.0
+    out = {"rows": n_rows, "flop_per_row": 17920, "peak_tflops": peak, "peak_kind": peak_kind}
+    for path in ("mma_sync", "tcgen05"):
+        c.infer(x, path=path)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            c.infer(x, path=path)
+        e1.record()
+        torch.cuda.synchronize()
+        c.status()
+        ms = e0.elapsed_time(e1) / reps
+        tf = n_rows * 17920 / (ms * 1e-3) / 1e12
+        out[path] = {"ms": ms, "rows_per_s": n_rows / (ms * 1e-3), "tflops": tf, "frac_of_peak": tf / peak}
+    return out
 
 
 def cpu_baseline_sample(spec, p, max_particles: int):

@@ -958,7 +958,9 @@ ZSMPM_API zsmpm_status zsmpm_closure_infer(zsmpm_closure *c, const float *x, flo
     const zsmpm_status ps = pack(c, st);
     if (ps != ZSMPM_OK) return ps;
     const int64_t tiles = (n + kTcRows - 1) / kTcRows;
-    const int grid = (int)std::min<int64_t>(tiles, (int64_t)sms() * 4);
+    // six resident CTAs per SM (37.7 KB of shared memory and 64 tensor-memory columns each), so
+    // that six tiles' layer chains overlap on the SM's tensor core
+    const int grid = (int)std::min<int64_t>(tiles, (int64_t)sms() * 6);
     k_closure_infer_tc<<<grid, kTcRows, kTcSmem, st>>>(c->cd, c->umma_w, x, y, n, c->tc_status);
   } else if (bf16) {
     const zsmpm_status ps = pack(c, st);
