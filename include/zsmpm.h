@@ -261,6 +261,55 @@ ZSMPM_API zsmpm_status zsmpm_svd3(const float *A, float *U, float *S, float *V, 
 ZSMPM_API zsmpm_status zsmpm_constitutive(const zsmpm_material *mat, float *F, float *plastic,
                                           float *tau, int64_t count, void *stream);
 
+/* ---- the implicit system (simulation/mpm/ImplicitMPM.hpp) ---------------------------- */
+/* Grid dof vectors are device arrays of `ndofs` floats, node-major over the active blocks in
+ * canonical order: entry (block*512 + cell)*3 + d, cell = x*64 + y*8 + z inside the block.
+ * This is the layout of a dof_view<space, 3> over a zs::Vector<float> (types/View.h:77-168)
+ * that ImplicitMPMSystem's operators take.  ndofs must be at least 1536 * zsmpm_num_blocks;
+ * shorter vectors are not touched and leave ZSMPM_ERR_CAPACITY in the scene status.  Vectors
+ * must be 16-byte aligned.  All calls are asynchronous on `stream`; they need a binned scene
+ * (zsmpm_activate_blocks + zsmpm_bin_particles for the current positions), and all but
+ * zsmpm_g2p2g read the grid mass of a zsmpm_p2g of that activation.  Single scenes only. */
+
+/* G2P2GTransfer (simulation/transfer/G2P2G.hpp:49-142; replaces its launch in
+ * ImplicitMPM.hpp:51-53).  ADDS to f, per particle and stencil node,
+ * W (4/dx^2) (V0 P(F*) F*^T)(x_i - x_p), where F* = (I + dt C) F and C is gathered from the
+ * velocity field v; the particle state is not changed.  Fixed corotated, Drucker-Prager and
+ * snow. */
+ZSMPM_API zsmpm_status zsmpm_g2p2g(zsmpm_scene *scene, const float *v, float *f, int64_t ndofs,
+                                   float dt, void *stream);
+/* ImplicitMPMSystem::multiply (ImplicitMPM.hpp:34-61): out = 0, out += G2P2G(in), then where
+ * the node mass m > 0, out = (out dt^2 + m) in (ForceDtSqrPlusMass, :17-33). */
+ZSMPM_API zsmpm_status zsmpm_implicit_multiply(zsmpm_scene *scene, const float *in, float *out,
+                                               int64_t ndofs, float dt, void *stream);
+/* ImplicitMPMSystem::project (ImplicitMPM.hpp:99-124) with the scene's six walls
+ * (Projector, :63-97): nodes with m > 0 get the walls' collision response, others are 0. */
+ZSMPM_API zsmpm_status zsmpm_implicit_project(zsmpm_scene *scene, float *inout, int64_t ndofs,
+                                              void *stream);
+/* ImplicitMPMSystem::precondition (ImplicitMPM.hpp:139-153; DivPernodeMass, :126-137):
+ * out = in / m where m > 0; other entries of out are left unchanged. */
+ZSMPM_API zsmpm_status zsmpm_implicit_precondition(zsmpm_scene *scene, const float *in, float *out,
+                                                   int64_t ndofs, void *stream);
+
+/* ConjugateGradient<T, dim>'s settings (math/linear/ConjugateGradient.hpp:10-38). */
+typedef struct {
+  int32_t max_iters; /* maxIters (the reference's default: 1000) */
+  float tol;         /* tol (1e-6 for float) */
+  float rel_tol;     /* relTol (0.5); the loop stops once sqrt(r.q) <= min(rel_tol * its first value, tol) */
+} zsmpm_cg_options;
+
+/* ConjugateGradient::solve (ConjugateGradient.hpp:69-172) with the implicit system above as
+ * its matrix: x (in: initial guess; out: result) and b are dof vectors.  The iterations run on
+ * the device; their scalars stay in device memory, and the host reads the stopping flag once
+ * every 8 iterations.  opts may be null (the reference's defaults).  iters_out (host, may be
+ * null) receives the iteration count solve returns.  The call synchronises `stream`.  Its
+ * four scratch vectors are allocated on the first call and grown when ndofs grows.  Entries of
+ * the preconditioned residual that the reference leaves unwritten (nodes without mass) start
+ * at zero here. */
+ZSMPM_API zsmpm_status zsmpm_implicit_cg(zsmpm_scene *scene, float *x, const float *b, int64_t ndofs,
+                                         float dt, const zsmpm_cg_options *opts, int32_t *iters_out,
+                                         void *stream);
+
 /* ---- batched scenes ------------------------------------------------------------ */
 /* Many independent MPM systems advanced together: every stage is one launch over the blocks
  * of all scenes, and zsmpm_run replays one CUDA graph for the whole batch.  The scenes share

@@ -4,13 +4,19 @@
 # driven by oracle/ref_driver.cpp and oracle/ref_cli.cpp.  The output is the checker and the CPU baseline, never the product.
 #
 # zpc's CMake build needs the zpc_tpls submodule, which is not checked out, so the needed
-# translation units are compiled directly with g++.  Three reference headers do not parse
-# with g++ 13 because a dependent member template is called without the `template`
-# keyword; for those, patched copies are written under oracle/_ref/patched (searched before
-# the reference tree).  No patch touches arithmetic:
+# translation units are compiled directly with g++.  Four reference headers do not parse
+# with g++ 13 because a dependent member template is named without the `template`
+# keyword, and G2P2G.hpp calls the CUDA-only two-argument atomicAdd; for those, patched
+# copies are written under oracle/_ref/patched (searched before the reference tree).
+# No patch touches arithmetic:
 #   ZpcAsync.hpp                        _storage[i].data<T>()  -> .template data<T>()
 #   simulation/transfer/G2P.hpp         grid_block.pack<N>()   -> .template pack<N>()
 #   simulation/grid/GridOp.hpp          block.pack<N>()        -> .template pack<N>()
+#   types/View.h                        dof_detail::T_t        -> dof_detail::template T_t;
+#                                       typename integral_constant<..> -> integral_constant<..>
+#   simulation/transfer/G2P2G.hpp       atomicAdd(&r, v) -> atomic_add(wrapv<space>{}, &r, v),
+#                                       the exec-space atomic that P2G.hpp uses (a plain add
+#                                       under seq_exec)
 # Logging (plog) and magic_enum are replaced by the small shims in oracle/ref_shims.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -27,8 +33,15 @@ sed -E 's/(grid_block|block)\.pack</\1.template pack</g' \
   "$REF/zensim/simulation/transfer/G2P.hpp" > "$OUT/patched/zensim/simulation/transfer/G2P.hpp"
 sed -E 's/(grid_block|block)\.pack</\1.template pack</g' \
   "$REF/zensim/simulation/grid/GridOp.hpp" > "$OUT/patched/zensim/simulation/grid/GridOp.hpp"
-# relative includes of the patched copies ("Scheme.hpp", "../transfer/Scheme.hpp")
+mkdir -p "$OUT/patched/zensim/types"
+sed -E -e 's/= typename integral_constant</= integral_constant</' \
+  -e 's/dof_detail::(value_t|T_t|size_t|index_t|counter_t|dim_t|extent_t)/dof_detail::template \1/g' \
+  "$REF/zensim/types/View.h" > "$OUT/patched/zensim/types/View.h"
+sed -E 's/atomicAdd\(/atomic_add(wrapv<space>{}, /g' \
+  "$REF/zensim/simulation/transfer/G2P2G.hpp" > "$OUT/patched/zensim/simulation/transfer/G2P2G.hpp"
+# relative includes of the patched copies ("Scheme.hpp", "../transfer/Scheme.hpp", "Property.h")
 ln -sf "$REF/zensim/simulation/transfer/Scheme.hpp" "$OUT/patched/zensim/simulation/transfer/Scheme.hpp"
+ln -sf "$REF/zensim/types/Property.h" "$OUT/patched/zensim/types/Property.h"
 
 CXXFLAGS=(-std=c++17 -O2 -fPIC -fopenmp -ffp-contract=off -include cstdint -include utility
   -DZS_ENABLE_OPENMP=1 -DZS_ENABLE_CUDA=0 -DZS_ENABLE_MUSA=0 -DZS_ENABLE_SYCL=0

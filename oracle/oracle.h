@@ -21,6 +21,7 @@
  *   SVD (FP32)         math/matrix/SVD.hpp:15-1025 (McAdams et al. 2011 quaternion Jacobi)
  *   grid update        simulation/grid/GridOp.hpp:72-164, geometry/Collider.h:80-110
  *   G2P                simulation/transfer/G2P.hpp:43-84, math/matrix/MatrixUtils.h:136-146
+ *   G2P2G              simulation/transfer/G2P2G.hpp:49-142 (implicit force operator)
  * Matrices are column-major (M(i,j) = M[3j+i]) as in the reference.
  */
 #ifndef ZSMPM_ORACLE_H
@@ -59,6 +60,18 @@ int oracle_run_f32(const oracle_params *p, int n, const float *m, float *x, floa
 int oracle_run_f64(const oracle_params *p, int n, const double *m, double *x, double *v,
                    double *C, double *F, double *plastic, int nsteps, int cap_blocks,
                    int *out_nblocks, int *out_keys, double *out_grid);
+
+/* G2P2GTransfer, the implicit force operator (simulation/transfer/G2P2G.hpp:49-142): fout
+ * (zeroed first) receives sum_p W (4/dx^2) (V0 P(F*) F*^T)(x_i - x_p), F* = (I + dt C(vin)) F,
+ * with the particle state left unchanged.  vin and fout hold 1536 values per block, node-major
+ * [(block*512 + cell)*3 + d]; the blocks are keys[3*nb] in index order.  Returns 0, 2 when
+ * the table is full, 5 when a stencil node has no block. */
+int oracle_g2p2g_f32(const oracle_params *p, int n, const float *x, const float *F,
+                     const float *plastic, int nb, const int32_t *keys, const float *vin,
+                     float *fout);
+int oracle_g2p2g_f64(const oracle_params *p, int n, const double *x, const double *F,
+                     const double *plastic, int nb, const int32_t *keys, const double *vin,
+                     double *fout);
 
 /* McAdams 3x3 SVD in the reference's float operation order (A = U diag(S) V^T). */
 void oracle_svd_f32(const float *A, float *U, float *S, float *V);

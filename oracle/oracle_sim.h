@@ -397,6 +397,83 @@ int OR_NAME(oracle_run)(const oracle_params *p, int n, const R *m, R *x, R *v, R
   return status;
 }
 
+/* G2P2GTransfer (simulation/transfer/G2P2G.hpp:49-142), the implicit force operator: per
+ * particle, C from the velocity field vin, the trial F = (I + dt C) F (MatrixUtils.h:136-146),
+ * its stress on a copy of the state (:103-123; nothing is written back), then
+ * fout[node] += W (D_inv V0 P F^T)(x_i - x_p) (:125-140).  vin and fout are node-major over
+ * the given blocks, [(block*512 + cell)*3 + d], the layout of a dof_view<space, 3> over a
+ * Vector (types/View.h:77-168); block b of keys gets index b.  fout is zeroed first.  Returns
+ * 0, 2 when the table is full, 5 when a stencil node falls outside the blocks. */
+int OR_NAME(oracle_g2p2g)(const oracle_params *p, int n, const R *x, const R *F, const R *plastic,
+                          int nb, const int32_t *keys, const R *vin, R *fout) {
+  OR_NAME(cfg) cfg;
+  OR_NAME(make_cfg)(p, &cfg);
+  const R dx = cfg.dx, dt = cfg.dt;
+  const R dx_inv = (R)1 / dx;
+  const R D_inv = (R)4 * dx_inv * dx_inv;
+  oracle_table t;
+  if (oracle_table_init(&t, p->table_expected > nb ? p->table_expected : nb)) return 3;
+  int status = 0;
+  for (int b = 0; b != nb && !status; ++b)
+    if (oracle_table_insert(&t, &keys[3 * b], b) < 0) status = 2;
+  memset(fout, 0, sizeof(R) * 1536 * (size_t)(nb > 0 ? nb : 0));
+  for (int i = 0; i != n && !status; ++i) {
+    const R *xp = &x[3 * i];
+    R Cn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, contrib[9];
+    OR_NAME(arena) a;
+    OR_NAME(make_arena)(&a, dx, xp);
+    int32_t node[27];
+    for (int ii = 0; ii != 3; ++ii)
+      for (int jj = 0; jj != 3; ++jj)
+        for (int kk = 0; kk != 3; ++kk) {
+          int32_t coord[3] = {a.corner[0] + ii, a.corner[1] + jj, a.corner[2] + kk};
+          int32_t loc[3], bk[3];
+          for (int d = 0; d != 3; ++d) {
+            loc[d] = coord[d] & 7;
+            bk[d] = (coord[d] - loc[d]) / 8;
+          }
+          const int32_t blk = oracle_table_query(&t, bk);
+          const int q = (ii * 3 + jj) * 3 + kk;
+          if (blk < 0) {
+            status = 5;
+            node[q] = -1;
+            continue;
+          }
+          node[q] = blk * 512 + ((loc[0] << 6) | (loc[1] << 3) | loc[2]);
+          R xixp[3] = {(R)ii * dx - a.localPos[0], (R)jj * dx - a.localPos[1],
+                       (R)kk * dx - a.localPos[2]};
+          R W = a.w[0][ii] * a.w[1][jj] * a.w[2][kk];
+          const R *vi = &vin[(size_t)node[q] * 3];
+          for (int d = 0; d != 9; ++d) Cn[d] += W * vi[d % 3] * xixp[d / 3] * D_inv;
+        }
+    if (status) break;
+    R Fl[9], pl = plastic ? plastic[i] : (R)0;
+    {
+      R tmp[9];
+      const R *Fp = &F[9 * i];
+      for (int d = 0; d != 9; ++d) tmp[d] = Cn[d] * dt + ((d & 0x3) ? (R)0 : (R)1);
+      for (int c = 0; c != 3; ++c)
+        for (int r = 0; r != 3; ++r)
+          Fl[3 * c + r] = tmp[r] * Fp[3 * c] + tmp[3 + r] * Fp[3 * c + 1] + tmp[6 + r] * Fp[3 * c + 2];
+    }
+    OR_NAME(stress)(&cfg, Fl, &pl, contrib);
+    for (int d = 0; d != 9; ++d) contrib[d] = contrib[d] * D_inv;
+    for (int ii = 0; ii != 3; ++ii)
+      for (int jj = 0; jj != 3; ++jj)
+        for (int kk = 0; kk != 3; ++kk) {
+          const int q = (ii * 3 + jj) * 3 + kk;
+          R xixp[3] = {(R)ii * dx - a.localPos[0], (R)jj * dx - a.localPos[1],
+                       (R)kk * dx - a.localPos[2]};
+          R W = a.w[0][ii] * a.w[1][jj] * a.w[2][kk];
+          R *fi = &fout[(size_t)node[q] * 3];
+          for (int d = 0; d != 3; ++d)
+            fi[d] += W * (contrib[d] * xixp[0] + contrib[3 + d] * xixp[1] + contrib[6 + d] * xixp[2]);
+        }
+  }
+  oracle_table_free(&t);
+  return status;
+}
+
 #undef OR_NAME
 #undef OR_CAT
 #undef OR_CAT2

@@ -19,6 +19,14 @@
 //   5 bht:       int32 nkeys, int32 expected, int32 cap_slots, int32 keys[3*nkeys]
 //     reply:     int32 status, table_size, u32 hash[6], int32 cnt,
 //                then (status == 0) int32 keys[3*table_size], indices[table_size], status[table_size]
+//   6 g2p2g:     zsref_params, int32 n, int32 nb, f32 x[3n], F[9n], logJp[n],
+//                int32 keys[3*nb], f32 v[1536*nb]
+//     reply:     int32 status, f64 seconds, then (status == 0) f32 f[1536*nb]
+//   7 implicit:  zsref_params, int32 op, n, nb, max_iters, f32 tol, rel_tol,
+//                f32 m[n], x[3n], v[3n], C[9n], F[9n], logJp[n], int32 keys[3*nb],
+//                f32 a[1536*nb], b[1536*nb]
+//     reply:     int32 status, int32 iters, f64 seconds, then (status == 0)
+//                f32 out[1536*nb], mass[512*nb]
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -43,6 +51,13 @@ int zsref_activate(int n, const float *x, float dx, int table_expected, int cap,
                    int *out_table_size);
 int zsref_bht(int nkeys, const int *keys, int expected, int cap_slots, int *out_table_size,
               unsigned *out_hash, int *out_keys, int *out_indices, int *out_status, int *out_cnt);
+int zsref_g2p2g(const zsref_params *p, int n, const float *x, const float *F, const float *logJp,
+                int nb_expected, const int *keys, const float *vin, float *fout,
+                double *out_seconds);
+int zsref_implicit(const zsref_params *p, int op, int n, const float *m, const float *x, const float *v,
+                   const float *C, const float *F, const float *logJp, int nb_expected, const int *keys,
+                   const float *a, const float *b, int max_iters, float tol, float rel_tol, float *out,
+                   float *out_mass, int *iters, double *out_seconds);
 }
 
 namespace {
@@ -154,6 +169,50 @@ int main(int argc, char **argv) {
       wrv(tk.data(), 3 * (size_t)ts);
       wrv(ti.data(), (size_t)ts);
       wrv(tst.data(), (size_t)ts);
+    }
+  } else if (cmd == 6) {
+    auto p = rd<zsref_params>();
+    const int n = rd<int32_t>(), nb = rd<int32_t>();
+    std::vector<float> x, F, lj, v;
+    std::vector<int> keys;
+    rdv(x, 3 * (size_t)n);
+    rdv(F, 9 * (size_t)n);
+    rdv(lj, n);
+    rdv(keys, 3 * (size_t)nb);
+    rdv(v, 1536 * (size_t)nb);
+    std::vector<float> f(1536 * (size_t)nb);
+    double secs = 0;
+    int st = zsref_g2p2g(&p, n, x.data(), F.data(), lj.data(), nb, keys.data(), v.data(), f.data(), &secs);
+    wr<int32_t>(st);
+    wr<double>(secs);
+    if (st == 0) wrv(f.data(), f.size());
+  } else if (cmd == 7) {
+    auto p = rd<zsref_params>();
+    const int op = rd<int32_t>(), n = rd<int32_t>(), nb = rd<int32_t>(), max_iters = rd<int32_t>();
+    const float tol = rd<float>(), rel_tol = rd<float>();
+    std::vector<float> m, x, v, C, F, lj, a, b;
+    std::vector<int> keys;
+    rdv(m, n);
+    rdv(x, 3 * (size_t)n);
+    rdv(v, 3 * (size_t)n);
+    rdv(C, 9 * (size_t)n);
+    rdv(F, 9 * (size_t)n);
+    rdv(lj, n);
+    rdv(keys, 3 * (size_t)nb);
+    rdv(a, 1536 * (size_t)nb);
+    rdv(b, 1536 * (size_t)nb);
+    std::vector<float> out(1536 * (size_t)nb), mass(512 * (size_t)nb);
+    int iters = 0;
+    double secs = 0;
+    int st = zsref_implicit(&p, op, n, m.data(), x.data(), v.data(), C.data(), F.data(), lj.data(), nb,
+                            keys.data(), a.data(), b.data(), max_iters, tol, rel_tol, out.data(), mass.data(),
+                            &iters, &secs);
+    wr<int32_t>(st);
+    wr<int32_t>(iters);
+    wr<double>(secs);
+    if (st == 0) {
+      wrv(out.data(), out.size());
+      wrv(mass.data(), mass.size());
     }
   } else if (cmd == 4) {
     const int count = rd<int32_t>();

@@ -19,6 +19,10 @@
 //   5. ApplyBoundaryConditionOnGridBlocks with six analytic planes (GridOp.hpp:113-164,
 //      geometry/Collider.h:80-110, geometry/AnalyticLevelSet.h:11-43)
 //   6. G2PTransfer (simulation/transfer/G2P.hpp:43-84)
+// zsref_g2p2g drives the implicit-force operator G2P2GTransfer
+// (simulation/transfer/G2P2G.hpp:49-142) over a caller-given grid velocity field, and
+// zsref_implicit the implicit system's operators and its conjugate-gradient solve
+// (simulation/mpm/ImplicitMPM.hpp:13-159, math/linear/ConjugateGradient.hpp:69-172).
 // Stress and plasticity are evaluated inside P2G on a local copy of F exactly as the
 // reference does ("ref-verbatim"): the projected F is not written back, logJp is.
 #include <algorithm>
@@ -27,17 +31,22 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <iostream>
 #include <vector>
 
 #include "zensim/omp/execution/ExecutionPolicy.hpp"
 #include "zensim/simulation/sparsity/SparsityOp.hpp"
 #include "zensim/simulation/transfer/P2G.hpp"
 #include "zensim/simulation/transfer/G2P.hpp"
+#include "zensim/simulation/transfer/G2P2G.hpp"
+#include "zensim/simulation/mpm/ImplicitMPM.hpp"
+#include "zensim/math/linear/ConjugateGradient.hpp"
 #include "zensim/geometry/SparseLevelSet.hpp"
 #include "zensim/simulation/grid/GridOp.hpp"
 #include "zensim/geometry/AnalyticLevelSet.h"
 #include "zensim/geometry/Collider.h"
 #include "zensim/container/Bht.hpp"
+#include "zensim/types/View.h"
 
 namespace {
 
@@ -69,6 +78,65 @@ namespace {
   };
 
   using plane_t = AnalyticLevelSet<analytic_geometry_e::Plane, float, 3>;
+
+  // Block activation of zsref_run (ComputeSparsity + EnlargeSparsity, then the canonical key
+  // order and ReinsertHashTable) on the given positions; returns the block count or -1 when the
+  // table is full.
+  template <class Pol, execspace_e space>
+  int activate_canonical(Pol &pol, wrapv<space>, table_t &table, particles_t &pars, float dx) {
+    pol(range(table._tableSize), CleanSparsity{wrapv<space>{}, table});
+    pol(range(pars.size()), ComputeSparsity{wrapv<space>{}, dx, 8, table, pars.attrVector("x")});
+    const int npb = table.size();
+    pol(range((size_t)npb),
+        EnlargeSparsity{wrapv<space>{}, table, vec<int, 3>{0, 0, 0}, vec<int, 3>{2, 2, 2}});
+    const int nb = table.size();
+    if (nb >= table._tableSize - 20) return -1;
+    auto *keys = table._activeKeys.data();
+    std::sort(keys, keys + nb, [](const auto &a, const auto &b) {
+      for (int d = 0; d != 3; ++d)
+        if (a[d] != b[d]) return a[d] < b[d];
+      return false;
+    });
+    pol(range(table._tableSize), ResetHashTable{proxy<space>(table), false});
+    pol(range((size_t)nb), ReinsertHashTable{proxy<space>(table)});
+    return nb;
+  }
+
+
+  // ImplicitMPMSystem's multiply / project / precondition (ImplicitMPM.hpp:34-153) for one
+  // model, one partition, one particle set and the six walls: the same bodies with the
+  // simulator's loops over model groups and boundaries reduced to their single entries, calling
+  // the reference's own functors (DofFill, G2P2GTransfer, ForceDtSqrPlusMass, Projector,
+  // DivPernodeMass).
+  template <class Model> struct RefImplicitSystem {
+    Model model;
+    table_t &table;
+    particles_t &pars;
+    grids_t &grids;
+    std::vector<Collider<plane_t>> &walls;
+    float dt;
+
+    template <class Pol, typename In, typename Out> void multiply(Pol &&policy, In &&in, Out &&out) {
+      constexpr execspace_e space = RM_REF_T(policy)::exec_tag::value;
+      policy(range(out.numEntries()), DofFill{out, 0});
+      policy(range(pars.size()),
+             G2P2GTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{}, dt, model,
+                           proxy<space>(grids.grid()), in, out, table, pars});
+      auto gridm = dof_view<space, 1>(grids.grid(), "m", 0);
+      policy(range(in.numEntries()), ImplicitMPMSystem::ForceDtSqrPlusMass{out, gridm, out, in, dt});
+    }
+    template <class Pol, typename InOut> void project(Pol &&policy, InOut &&inout) {
+      constexpr execspace_e space = RM_REF_T(policy)::exec_tag::value;
+      for (auto &w : walls)
+        policy(range((size_t)inout.numEntries() / 3),
+               ImplicitMPMSystem::Projector{w, proxy<space>(table), proxy<space>(grids.grid()), inout});
+    }
+    template <class Pol, typename In, typename Out> void precondition(Pol &&policy, In &&in, Out &&out) {
+      constexpr execspace_e space = RM_REF_T(policy)::exec_tag::value;
+      auto gridm = dof_view<space, 1>(grids.grid(), "m", 0);
+      policy(range(out.numEntries()), ImplicitMPMSystem::DivPernodeMass{in, gridm, out});
+    }
+  };
 
 }  // namespace
 
@@ -230,6 +298,210 @@ int zsref_run(const zsref_params *p, int n, float *m, float *x, float *v, float 
           out_grid[((size_t)b * 4 + c) * 512 + cell] = block(c, cell);
     }
   }
+  return 0;
+}
+
+// G2P2GTransfer on the given particle state (x: 3n, F: 9n column-major, logJp: n) and grid
+// velocity field vin, node-major over the canonical blocks: vin[(block*512 + cell)*3 + d], the
+// layout of a dof_view<space, 3> over a Vector<float> (types/View.h:77-168).  fout (same
+// layout) is zeroed, then receives the operator's atomic sums.  keys are the canonical block
+// keys the caller built vin for.  Returns 0; 2 when the table is full; 3 when the activation
+// gives other keys than the caller's.
+int zsref_g2p2g(const zsref_params *p, int n, const float *x, const float *F, const float *logJp,
+                int nb_expected, const int *keys, const float *vin, float *fout,
+                double *out_seconds) {
+  constexpr auto host = execspace_e::host;
+  constexpr auto omp = execspace_e::openmp;
+  particles_t pars{(size_t)n, memsrc_e::host, -1};
+  pars.addAttr("m", attrib_e::scalar);
+  pars.addAttr("F", attrib_e::matrix);
+  pars.addAttr("logJp", attrib_e::scalar);
+  std::memcpy((float *)pars.getAttrAddress("x"), x, sizeof(float) * 3 * n);
+  std::memcpy((float *)pars.getAttrAddress("F"), F, sizeof(float) * 9 * n);
+  std::memcpy((float *)pars.getAttrAddress("logJp"), logJp, sizeof(float) * n);
+  table_t table{(size_t)std::max(p->table_expected, 1), memsrc_e::host, -1};
+  grids_t grids{{{"m", 1}, {"v", 3}, {"rhs", 3}}, p->dx, (size_t)1, memsrc_e::host, -1};
+  FixedCorotatedConfig fc{};
+  fc.E = p->E;
+  fc.nu = p->nu;
+  fc.volume = p->volume;
+  DruckerPragerConfig dp{};
+  dp.E = p->E;
+  dp.nu = p->nu;
+  dp.volume = p->volume;
+  dp.fa = p->friction_deg;
+  dp.cohesion = p->cohesion;
+  dp.beta = p->beta;
+  dp.volumeCorrection = p->volume_correction != 0;
+  {
+    float sin_phi = (float)std::sin((double)p->friction_deg / 180.0 * 3.14159265358979323846);
+    dp.yieldSurface = 0.816496580927726f * 2.f * sin_phi / (3.f - sin_phi);
+  }
+  const size_t ndofs = (size_t)std::max(nb_expected, 0) * 512 * 3;
+  Vector<float> vin_vec{ndofs, memsrc_e::host, -1}, f_vec{ndofs, memsrc_e::host, -1};
+  std::memcpy(vin_vec.data(), vin, sizeof(float) * ndofs);
+  std::memset(f_vec.data(), 0, sizeof(float) * ndofs);
+  int status = 0;
+  auto run = [&](auto pol, auto tag) {
+    constexpr auto space = decltype(tag)::value;
+    const int nb = activate_canonical(pol, wrapv<space>{}, table, pars, p->dx);
+    if (nb < 0) {
+      status = 2;
+      return;
+    }
+    if (nb != nb_expected) {
+      status = 3;
+      return;
+    }
+    for (int b = 0; b != nb; ++b)
+      for (int d = 0; d != 3; ++d)
+        if (table._activeKeys[b][d] != keys[3 * b + d]) status = 3;
+    if (status) return;
+    auto vin_view = dof_view<space, 3>(vin_vec);
+    auto f_view = dof_view<space, 3>(f_vec);
+    auto t0 = std::chrono::steady_clock::now();
+    if (p->model == 0)
+      pol(range((size_t)n), G2P2GTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{}, p->dt, fc,
+                                          proxy<space>(grids.grid()), vin_view, f_view, table, pars});
+    else
+      pol(range((size_t)n), G2P2GTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{}, p->dt, dp,
+                                          proxy<space>(grids.grid()), vin_view, f_view, table, pars});
+    auto t1 = std::chrono::steady_clock::now();
+    if (out_seconds) *out_seconds = std::chrono::duration<double>(t1 - t0).count();
+  };
+  if (p->policy == 0)
+    run(seq_exec(), wrapv<host>{});
+  else {
+    auto pol = omp_exec();
+    if (p->threads > 0) pol = OmpExecutionPolicy{}.threads(p->threads);
+    run(pol, wrapv<omp>{});
+  }
+  if (status) return status;
+  std::memcpy(fout, f_vec.data(), sizeof(float) * ndofs);
+  return 0;
+}
+
+// The implicit system on the given particle state (m: n, x/v: 3n, C/F: 9n, logJp: n) after the
+// activation of zsref_run (canonical order; keys must match) and a P2GTransfer that fills the
+// grid mass.  Dof vectors a, b, out hold 1536 floats per block (node-major).  op:
+//   0  multiply(a -> out)
+//   1  project(a in place) -> out
+//   2  precondition(a -> out), out preset to b
+//   3  ConjugateGradient<float, 3>::solve(system, x = a, b) with maxIters / tol / relTol -> out,
+//      *iters = its return value; the solver's q vector is zeroed before the solve (the
+//      reference allocates it uninitialised) and its console output is discarded
+// out_mass (nb * 512) receives the grid mass.  Returns 0, 2 (table full) or 3 (other keys).
+int zsref_implicit(const zsref_params *p, int op, int n, const float *m, const float *x, const float *v,
+                   const float *C, const float *F, const float *logJp, int nb_expected, const int *keys,
+                   const float *a, const float *b, int max_iters, float tol, float rel_tol, float *out,
+                   float *out_mass, int *iters, double *out_seconds) {
+  constexpr auto host = execspace_e::host;
+  particles_t pars{(size_t)n, memsrc_e::host, -1};
+  pars.addAttr("m", attrib_e::scalar);
+  pars.addAttr("v", attrib_e::vector);
+  pars.addAttr("C", attrib_e::matrix);
+  pars.addAttr("F", attrib_e::matrix);
+  pars.addAttr("logJp", attrib_e::scalar);
+  std::memcpy((float *)pars.getAttrAddress("m"), m, sizeof(float) * n);
+  std::memcpy((float *)pars.getAttrAddress("x"), x, sizeof(float) * 3 * n);
+  std::memcpy((float *)pars.getAttrAddress("v"), v, sizeof(float) * 3 * n);
+  std::memcpy((float *)pars.getAttrAddress("C"), C, sizeof(float) * 9 * n);
+  std::memcpy((float *)pars.getAttrAddress("F"), F, sizeof(float) * 9 * n);
+  std::memcpy((float *)pars.getAttrAddress("logJp"), logJp, sizeof(float) * n);
+  table_t table{(size_t)std::max(p->table_expected, 1), memsrc_e::host, -1};
+  auto pol = seq_exec();
+  const int nb = activate_canonical(pol, wrapv<host>{}, table, pars, p->dx);
+  if (nb < 0) return 2;
+  if (nb != nb_expected) return 3;
+  for (int bb = 0; bb != nb; ++bb)
+    for (int d = 0; d != 3; ++d)
+      if (table._activeKeys[bb][d] != keys[3 * bb + d]) return 3;
+  grids_t grids{{{"m", 1}, {"v", 3}, {"rhs", 3}}, p->dx, (size_t)table._tableSize, memsrc_e::host, -1};
+  FixedCorotatedConfig fc{};
+  fc.E = p->E;
+  fc.nu = p->nu;
+  fc.volume = p->volume;
+  DruckerPragerConfig dp{};
+  dp.E = p->E;
+  dp.nu = p->nu;
+  dp.volume = p->volume;
+  dp.fa = p->friction_deg;
+  dp.cohesion = p->cohesion;
+  dp.beta = p->beta;
+  dp.volumeCorrection = p->volume_correction != 0;
+  {
+    float sin_phi = (float)std::sin((double)p->friction_deg / 180.0 * 3.14159265358979323846);
+    dp.yieldSurface = 0.816496580927726f * 2.f * sin_phi / (3.f - sin_phi);
+  }
+  std::vector<Collider<plane_t>> walls;
+  if (p->wall_type != 3) {
+    const float lo = p->wall_cells * p->dx, hi = 1.f - p->wall_cells * p->dx;
+    collider_e ct = p->wall_type == 0 ? collider_e::Sticky
+                    : p->wall_type == 1 ? collider_e::Slip
+                                        : collider_e::Separate;
+    for (int d = 0; d != 3; ++d) {
+      vec<float, 3> o{0.f, 0.f, 0.f}, nrm{0.f, 0.f, 0.f};
+      o[d] = lo;
+      nrm[d] = 1.f;
+      walls.emplace_back(plane_t{o, nrm}, ct);
+      o[d] = hi;
+      nrm[d] = -1.f;
+      walls.emplace_back(plane_t{o, nrm}, ct);
+    }
+  }
+  pol(Collapse{(size_t)nb, (size_t)512}, CleanGridBlocks{wrapv<host>{}, grids});
+  // P2G's stress term reads a copy of F and writes logJp; the implicit operators read the
+  // uploaded logJp, so it is restored
+  if (p->model == 0)
+    pol(range((size_t)n), P2GTransfer{wrapv<host>{}, wrapv<transfer_scheme_e::apic>{}, p->dt, fc, pars, table, grids});
+  else
+    pol(range((size_t)n), P2GTransfer{wrapv<host>{}, wrapv<transfer_scheme_e::apic>{}, p->dt, dp, pars, table, grids});
+  std::memcpy((float *)pars.getAttrAddress("logJp"), logJp, sizeof(float) * n);
+  {
+    auto tv = proxy<host>(grids);
+    for (int bb = 0; bb != nb; ++bb)
+      for (int cell = 0; cell != 512; ++cell) out_mass[(size_t)bb * 512 + cell] = tv[bb](0, cell);
+  }
+  const size_t ndofs = (size_t)nb * 1536;
+  Vector<float> va{ndofs, memsrc_e::host, -1}, vb{ndofs, memsrc_e::host, -1}, vo{ndofs, memsrc_e::host, -1};
+  std::memcpy(va.data(), a, sizeof(float) * ndofs);
+  std::memcpy(vb.data(), b, sizeof(float) * ndofs);
+  std::memset(vo.data(), 0, sizeof(float) * ndofs);
+  auto da = dof_view<host, 3>(va), db = dof_view<host, 3>(vb), dout = dof_view<host, 3>(vo);
+  auto t0 = std::chrono::steady_clock::now();
+  auto go = [&](auto model) {
+    RefImplicitSystem<decltype(model)> sys{model, table, pars, grids, walls, p->dt};
+    if (op == 0) {
+      sys.multiply(pol, da, dout);
+    } else if (op == 1) {
+      sys.project(pol, da);
+      std::memcpy(vo.data(), va.data(), sizeof(float) * ndofs);
+    } else if (op == 2) {
+      std::memcpy(vo.data(), vb.data(), sizeof(float) * ndofs);
+      sys.precondition(pol, da, dout);
+    } else {
+      ConjugateGradient<float, 3> cg{ndofs, memsrc_e::host, -1};
+      cg.maxIters = max_iters;
+      cg.tol = tol;
+      cg.relTol = rel_tol;
+      cg.resize(ndofs);
+      std::memset(cg.q_.data(), 0, sizeof(float) * ndofs);
+      std::FILE *null_in = std::freopen("/dev/null", "r", stdin);
+      (void)null_in;
+      std::streambuf *saved = std::cout.rdbuf(nullptr);
+      *iters = cg.solve(pol, sys, da, db);
+      std::cout.rdbuf(saved);
+      std::cout.clear();
+      std::memcpy(vo.data(), va.data(), sizeof(float) * ndofs);
+    }
+  };
+  if (p->model == 0)
+    go(fc);
+  else
+    go(dp);
+  auto t1 = std::chrono::steady_clock::now();
+  if (out_seconds) *out_seconds = std::chrono::duration<double>(t1 - t0).count();
+  std::memcpy(out, vo.data(), sizeof(float) * ndofs);
   return 0;
 }
 

@@ -152,3 +152,64 @@ def svd(A: np.ndarray, timeout: float = 120.0):
     S = np.frombuffer(rep, "<f4", 3 * cnt, 36 * cnt).reshape(cnt, 3).copy()
     V = np.frombuffer(rep, "<f4", 9 * cnt, 48 * cnt).reshape(cnt, 9).copy()
     return U, S, V
+
+
+def g2p2g(spec, x, F, logJp, keys, vin, dt: float | None = None, policy: int = POLICY_SEQ,
+          threads: int = 0, timeout: float = 600.0):
+    """The reference's G2P2GTransfer (simulation/transfer/G2P2G.hpp) on the given state and
+    velocity field vin ([nb*512*3], node-major over the canonical blocks `keys`): returns
+    (forces, seconds)."""
+    import copy
+    keys = np.ascontiguousarray(keys, dtype="<i4").reshape(-1, 3)
+    nb = len(keys)
+    n = len(x)
+    sp = spec
+    if dt is not None:
+        sp = copy.copy(spec)
+        sp.dt = dt
+    req = struct.pack("<i", 6) + _params_bytes(sp, policy, threads, 1, max(n // 512, 64))
+    req += struct.pack("<2i", n, nb)
+    for a in (x, F, logJp):
+        req += np.ascontiguousarray(a, dtype="<f4").tobytes()
+    req += keys.tobytes() + np.ascontiguousarray(vin, dtype="<f4").reshape(-1).tobytes()
+    rep = _run(req, timeout)
+    st = struct.unpack_from("<i", rep, 0)[0]
+    secs = struct.unpack_from("<d", rep, 4)[0]
+    if st != 0:
+        raise RuntimeError(f"zsref g2p2g failed: {st}")
+    return np.frombuffer(rep, "<f4", 1536 * nb, 12).copy(), secs
+
+
+IMPLICIT_MULTIPLY, IMPLICIT_PROJECT, IMPLICIT_PRECONDITION, IMPLICIT_CG = 0, 1, 2, 3
+
+
+def implicit(spec, particles, keys, a, b=None, op: int = IMPLICIT_MULTIPLY, dt: float | None = None,
+             max_iters: int = 1000, tol: float = 1e-6, rel_tol: float = 0.5, timeout: float = 600.0):
+    """The reference's implicit system (simulation/mpm/ImplicitMPM.hpp) and its
+    ConjugateGradient (math/linear/ConjugateGradient.hpp) on a particle state, after its
+    activation and a P2GTransfer for the grid mass.  Returns (out, mass [nb, 512], iters, seconds)."""
+    import copy
+    keys = np.ascontiguousarray(keys, dtype="<i4").reshape(-1, 3)
+    nb = len(keys)
+    n = particles.n
+    sp = spec
+    if dt is not None:
+        sp = copy.copy(spec)
+        sp.dt = dt
+    if b is None:
+        b = np.zeros(1536 * nb, np.float32)
+    req = struct.pack("<i", 7) + _params_bytes(sp, POLICY_SEQ, 0, 1, max(n // 512, 64))
+    req += struct.pack("<4i2f", op, n, nb, max_iters, tol, rel_tol)
+    for arr in (particles.m, particles.x, particles.v, particles.C, particles.F, particles.plastic):
+        req += np.ascontiguousarray(arr, dtype="<f4").tobytes()
+    req += keys.tobytes()
+    req += np.ascontiguousarray(a, dtype="<f4").reshape(-1).tobytes()
+    req += np.ascontiguousarray(b, dtype="<f4").reshape(-1).tobytes()
+    rep = _run(req, timeout)
+    st, iters = struct.unpack_from("<2i", rep, 0)
+    secs = struct.unpack_from("<d", rep, 8)[0]
+    if st != 0:
+        raise RuntimeError(f"zsref implicit failed: {st}")
+    out = np.frombuffer(rep, "<f4", 1536 * nb, 16).copy()
+    mass = np.frombuffer(rep, "<f4", 512 * nb, 16 + 4 * 1536 * nb).reshape(nb, 512).copy()
+    return out, mass, iters, secs

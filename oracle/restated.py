@@ -52,6 +52,8 @@ def lib() -> C.CDLL:
         _lib.oracle_hash_slot.argtypes = [C.c_int32] * 4
         _lib.oracle_hash_slot.restype = C.c_int32
         _lib.oracle_bin_order.argtypes = [C.c_int, C.c_int, P, P, P, P]
+        _lib.oracle_g2p2g_f32.argtypes = [C.POINTER(OracleParams), C.c_int, P, P, P, C.c_int, P, P, P]
+        _lib.oracle_g2p2g_f64.argtypes = _lib.oracle_g2p2g_f32.argtypes
     return _lib
 
 
@@ -156,3 +158,23 @@ def bin_order(block: np.ndarray, cell: np.ndarray, nblocks: int):
     bstart = np.zeros(nblocks + 1, np.int32)
     lib().oracle_bin_order(len(block), nblocks, _p(block), _p(cell), _p(order), _p(bstart))
     return order, bstart
+
+
+def g2p2g(spec, x, F, plastic, keys, vin, dt: float | None = None, precision: str = "f32"):
+    """G2P2GTransfer restated: forces [nb*512*3] for the velocity field vin (same layout) over
+    the canonical blocks `keys`."""
+    t = np.float32 if precision == "f32" else np.float64
+    prm = params_from_spec(spec, table_expected=max(len(keys), 64))
+    if dt is not None:
+        prm.dt = dt
+    x = np.ascontiguousarray(x, t)
+    F = np.ascontiguousarray(F, t)
+    pl = np.ascontiguousarray(plastic, t)
+    keys = np.ascontiguousarray(keys, np.int32)
+    vin = np.ascontiguousarray(vin, t).reshape(-1)
+    fout = np.zeros_like(vin)
+    fn = lib().oracle_g2p2g_f32 if precision == "f32" else lib().oracle_g2p2g_f64
+    st = fn(C.byref(prm), len(x), _p(x), _p(F), _p(pl), len(keys), _p(keys), _p(vin), _p(fout))
+    if st != 0:
+        raise RuntimeError(f"oracle_g2p2g failed with status {st}")
+    return fout

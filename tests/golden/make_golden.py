@@ -8,6 +8,9 @@ reference itself on seeded synthetic inputs:
   ref_svd.npz                               math::svd_3d on 256 matrices
   ref_stress.npz                            compute_stress_fixedcorotated / _sand on 256 F
   ref_activation.npz                        ComputeSparsity + EnlargeSparsity keys and slots
+  ref_implicit_fc.npz / ref_implicit_dp.npz G2P2GTransfer, ImplicitMPMSystem's multiply /
+                                            project / precondition and ConjugateGradient::solve
+                                            on a small state with a smooth grid velocity field
 Run:  python tests/golden/make_golden.py
 """
 from __future__ import annotations
@@ -66,7 +69,48 @@ def main() -> None:
     keys, slots, npb, ts = reference.activate(p.x, spec.dx, 64)
     np.savez_compressed(HERE / "ref_activation.npz", x=p.x, dx=spec.dx, expected=64, keys=keys,
                         slots=slots, nparblocks=npb, table_size=ts)
+    for model, name in ((0, "fc"), (1, "dp")):
+        make_implicit(model, HERE / f"ref_implicit_{name}.npz")
     print("wrote", sorted(f.name for f in HERE.glob("*.npz")))
+
+
+def velocity_field(keys: np.ndarray, dx: float) -> np.ndarray:
+    """A smooth grid velocity field over the nodes of `keys`, node-major [nb*512*3]."""
+    cell = np.arange(512)
+    loc = np.stack([cell >> 6, (cell >> 3) & 7, cell & 7], 1)
+    pos = (keys[:, None, :].astype(np.int64) * 8 + loc[None]) * dx
+    v = np.stack([np.sin(7 * pos[..., 1]) + 0.3, np.cos(5 * pos[..., 2]) - 0.2,
+                  np.sin(3 * pos[..., 0] + pos[..., 1])], -1)
+    return v.astype(np.float32).reshape(-1)
+
+
+def implicit_state(model: int, seed: int = 5):
+    """A small deformed state for the implicit-system fixtures: random F, and logJp for sand."""
+    spec = scenes.small_scene(model=model, mode=1, n_side=0.04)
+    p = scenes.generate(spec)
+    rng = np.random.default_rng(seed)
+    p.F = random_F(rng, p.n, 0.15)
+    p.plastic = (rng.uniform(-0.05, 0.05, p.n) if model else np.zeros(p.n)).astype(np.float32)
+    return spec, p
+
+
+def make_implicit(model: int, path: Path, dt: float = 1e-3, cg_iters: int = 20) -> None:
+    spec, p = implicit_state(model)
+    keys, _slots, _npb, _ts = reference.activate(p.x, spec.dx, max(p.n // 512, 64))
+    keys = keys[np.lexsort((keys[:, 2], keys[:, 1], keys[:, 0]))]
+    v = velocity_field(keys, spec.dx)
+    f, _ = reference.g2p2g(spec, p.x, p.F, p.plastic, keys, v, dt=dt)
+    mult, mass, _, _ = reference.implicit(spec, p, keys, v, op=reference.IMPLICIT_MULTIPLY, dt=dt)
+    proj, _, _, _ = reference.implicit(spec, p, keys, v, op=reference.IMPLICIT_PROJECT, dt=dt)
+    b = (np.repeat(mass.reshape(-1), 3) * v).astype(np.float32)
+    prec_base = np.full_like(v, 7.0)
+    prec, _, _, _ = reference.implicit(spec, p, keys, v, prec_base, op=reference.IMPLICIT_PRECONDITION, dt=dt)
+    x0 = np.zeros_like(v)
+    cg_x, _, iters, _ = reference.implicit(spec, p, keys, x0, b, op=reference.IMPLICIT_CG, dt=dt,
+                                           max_iters=cg_iters)
+    np.savez_compressed(path, model=model, dt=dt, m=p.m, x=p.x, v=p.v, C=p.C, F=p.F, plastic=p.plastic,
+                        keys=keys, vel=v, f=f, mult=mult, mass=mass, proj=proj, prec_base=prec_base, prec=prec,
+                        b=b, cg_x=cg_x, cg_iters=iters, cg_max_iters=cg_iters)
 
 
 if __name__ == "__main__":

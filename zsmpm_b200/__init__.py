@@ -91,6 +91,7 @@ class Scene:
     def __init__(self, spec: SceneSpec, particles: Particles | None = None, device: int = 0,
                  table_expected: int = 0, max_particles: int = 0):
         self.spec = spec
+        self.device = device
         self._lib = _abi.lib()
         self._h = C.c_void_p()
         desc = scene_desc(spec, max_particles=max_particles, device=device,

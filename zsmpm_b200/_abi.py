@@ -85,6 +85,10 @@ class ClosureAudit(C.Structure):
                 ("fallbacks", C.c_int64)]
 
 
+class CgOptions(C.Structure):
+    _fields_ = [("max_iters", C.c_int32), ("tol", C.c_float), ("rel_tol", C.c_float)]
+
+
 _P = C.c_void_p
 _S = C.c_int  # zsmpm_status
 
@@ -118,6 +122,11 @@ SIGNATURES = {
     "zsmpm_kernels_per_substep": (C.c_int32, [_P]),
     "zsmpm_svd3": (_S, [_P, _P, _P, _P, C.c_int64, _P]),
     "zsmpm_constitutive": (_S, [C.POINTER(Material), _P, _P, _P, C.c_int64, _P]),
+    "zsmpm_g2p2g": (_S, [_P, _P, _P, C.c_int64, C.c_float, _P]),
+    "zsmpm_implicit_multiply": (_S, [_P, _P, _P, C.c_int64, C.c_float, _P]),
+    "zsmpm_implicit_project": (_S, [_P, _P, C.c_int64, _P]),
+    "zsmpm_implicit_precondition": (_S, [_P, _P, _P, C.c_int64, _P]),
+    "zsmpm_implicit_cg": (_S, [_P, _P, _P, C.c_int64, C.c_float, C.POINTER(CgOptions), C.POINTER(C.c_int32), _P]),
     "zsmpm_get_bht_view": (_S, [_P, C.POINTER(BhtView)]),
     "zsmpm_bht_build_host": (_S, [_P, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32, C.POINTER(C.c_int32), _P]),
     "zsmpm_batch_create": (_S, [C.POINTER(SceneDesc), C.POINTER(Material), C.c_int32, C.POINTER(_P)]),

@@ -5,6 +5,8 @@
 // the binning scratch).  Stages enqueue kernels on the caller's stream; zsmpm_run replays
 // a CUDA graph of two substeps (the particle buffers alternate between them).
 #include <algorithm>
+#include <cstdint>
+#include <initializer_list>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -48,6 +50,10 @@ struct zsmpm_scene {
   float *staging = nullptr;
   size_t staging_floats = 0;
   unsigned long long *log_count = nullptr;  // trial-state log counter (device)
+  // implicit solve scratch: four dof vectors and the solver state, grown on demand
+  float *cg_buf = nullptr;
+  int64_t cg_cap = 0;
+  cg_state *cg = nullptr;
 };
 
 namespace {
@@ -996,6 +1002,104 @@ ZSMPM_API zsmpm_status zsmpm_set_tuning(zsmpm_scene *s, const zsmpm_tuning *t) {
   s->dev.prm.p2g_ctas_per_sm = t->p2g_ctas_per_sm;
   invalidate_graphs(s);
   return ZSMPM_OK;
+}
+
+// ---- the implicit system (ImplicitMPM.hpp)
+namespace {
+
+zsmpm_status check_implicit(zsmpm_scene *s, std::initializer_list<const void *> vecs, int64_t ndofs) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (s->nscenes > 0) return fail(ZSMPM_ERR_INVALID_ARG, "the implicit system runs on single scenes");
+  if (!s->binned) return fail(ZSMPM_ERR_NOT_READY, "needs zsmpm_activate_blocks and zsmpm_bin_particles first");
+  if (ndofs < 0) return fail(ZSMPM_ERR_INVALID_ARG, "ndofs < 0");
+  for (const void *v : vecs) {
+    if (!v) return fail(ZSMPM_ERR_INVALID_ARG, "null dof vector");
+    if (reinterpret_cast<uintptr_t>(v) % 16 != 0) return fail(ZSMPM_ERR_INVALID_ARG, "dof vectors must be 16-byte aligned");
+  }
+  bind_buffers(s);
+  return ZSMPM_OK;
+}
+
+}  // namespace
+
+ZSMPM_API zsmpm_status zsmpm_g2p2g(zsmpm_scene *s, const float *v, float *f, int64_t ndofs, float dt, void *stream) {
+  zsmpm_status st = check_implicit(s, {v, f}, ndofs);
+  if (st != ZSMPM_OK) return st;
+  if (!std::isfinite(dt)) return fail(ZSMPM_ERR_INVALID_ARG, "dt must be finite");
+  ZS_TRY(launch_g2p2g(s->dev, v, f, ndofs, dt, nullptr, as_stream(stream)), "g2p2g");
+  s->last_stream = as_stream(stream);
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_implicit_multiply(zsmpm_scene *s, const float *in, float *out, int64_t ndofs, float dt,
+                                               void *stream) {
+  zsmpm_status st = check_implicit(s, {in, out}, ndofs);
+  if (st != ZSMPM_OK) return st;
+  if (!std::isfinite(dt)) return fail(ZSMPM_ERR_INVALID_ARG, "dt must be finite");
+  if (in == out) return fail(ZSMPM_ERR_INVALID_ARG, "multiply needs distinct in and out vectors");
+  cudaStream_t cs = as_stream(stream);
+  ZS_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)ndofs, cs), "multiply: zero");
+  ZS_TRY(launch_g2p2g(s->dev, in, out, ndofs, dt, nullptr, cs), "multiply: g2p2g");
+  ZS_TRY(launch_implicit_mass(s->dev, in, out, dt, ndofs, nullptr, cs), "multiply: mass");
+  s->last_stream = cs;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_implicit_project(zsmpm_scene *s, float *inout, int64_t ndofs, void *stream) {
+  zsmpm_status st = check_implicit(s, {inout}, ndofs);
+  if (st != ZSMPM_OK) return st;
+  ZS_TRY(launch_implicit_project(s->dev, inout, ndofs, nullptr, as_stream(stream)), "project");
+  s->last_stream = as_stream(stream);
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_implicit_precondition(zsmpm_scene *s, const float *in, float *out, int64_t ndofs,
+                                                   void *stream) {
+  zsmpm_status st = check_implicit(s, {in, out}, ndofs);
+  if (st != ZSMPM_OK) return st;
+  ZS_TRY(launch_implicit_precondition(s->dev, in, out, ndofs, nullptr, as_stream(stream)), "precondition");
+  s->last_stream = as_stream(stream);
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_implicit_cg(zsmpm_scene *s, float *x, const float *b, int64_t ndofs, float dt,
+                                         const zsmpm_cg_options *opts, int32_t *iters_out, void *stream) {
+  zsmpm_status st = check_implicit(s, {x, b}, ndofs);
+  if (st != ZSMPM_OK) return st;
+  if (!std::isfinite(dt)) return fail(ZSMPM_ERR_INVALID_ARG, "dt must be finite");
+  zsmpm_cg_options o{1000, 1e-6f, 0.5f};
+  if (opts) o = *opts;
+  if (o.max_iters < 0) return fail(ZSMPM_ERR_INVALID_ARG, "max_iters < 0");
+  cudaStream_t cs = as_stream(stream);
+  if (!s->cg) ZS_ALLOC(s->cg, 1, "cg state");
+  // vectors start on 16-byte boundaries (cudaMalloc returns 256-byte aligned memory)
+  const int64_t stride = (ndofs + 3) / 4 * 4;
+  if (stride > s->cg_cap) {
+    ZS_TRY(cudaStreamSynchronize(cs), "cg scratch");
+    if (s->cg_buf) {
+      s->allocations.erase(std::remove(s->allocations.begin(), s->allocations.end(), (void *)s->cg_buf),
+                           s->allocations.end());
+      cudaFree(s->cg_buf);
+      s->cg_buf = nullptr;
+      s->cg_cap = 0;
+    }
+    ZS_ALLOC(s->cg_buf, 4 * (size_t)stride, "cg scratch");
+    s->cg_cap = stride;
+  }
+  const cg_vectors v{s->cg_buf, s->cg_buf + stride, s->cg_buf + 2 * stride, s->cg_buf + 3 * stride};
+  ZS_TRY(launch_cg_begin(s->dev, x, b, v, ndofs, dt, s->cg, o.tol, o.rel_tol, cs), "cg begin");
+  constexpr int kChunk = 8;
+  cg_state h{};
+  for (int it = 0; it < o.max_iters + 1; it += kChunk) {
+    for (int k = 0; k < kChunk; ++k) ZS_TRY(launch_cg_iteration(s->dev, x, v, ndofs, dt, s->cg, o.max_iters, cs), "cg iteration");
+    ZS_TRY(cudaMemcpyAsync(&h, s->cg, sizeof(cg_state), cudaMemcpyDeviceToHost, cs), "cg state");
+    ZS_TRY(cudaStreamSynchronize(cs), "cg iteration");
+    if (h.done) break;
+  }
+  s->last_stream = cs;
+  if (iters_out) *iters_out = h.iter;
+  return read_status(s);
 }
 
 ZSMPM_API zsmpm_status zsmpm_svd3(const float *A, float *U, float *S, float *V, int64_t count, void *stream) {

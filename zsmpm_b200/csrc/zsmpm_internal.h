@@ -46,7 +46,14 @@ enum counter_slot : int {
   kCtrSubstep = 20,        // substeps begun since the scene was created (audit/log sampling)
   kCtrCount = 24
 };
-enum work_slot : int { kWorkCellStart = 0, kWorkFinalize = 1, kWorkP2G = 2, kWorkG2P = 3, kWorkGrid = 4 };
+enum work_slot : int {
+  kWorkCellStart = 0,
+  kWorkFinalize = 1,
+  kWorkP2G = 2,
+  kWorkG2P = 3,
+  kWorkGrid = 4,
+  kWorkG2P2G = 5  // reset by its own launcher (the operator runs many times per activation)
+};
 
 struct scene_params {
   int n;          // particles
@@ -120,6 +127,30 @@ cudaError_t launch_p2g(scene_device &s, cudaStream_t st);
 cudaError_t launch_grid_update(scene_device &s, cudaStream_t st);
 cudaError_t launch_g2p(scene_device &s, cudaStream_t st);
 int kernels_per_substep();
+// the implicit system (ImplicitMPM.hpp) over node-major dof vectors [nb * 512 * 3]; a kernel
+// returns at once when `skip` (device, may be null) holds a nonzero value
+cudaError_t launch_g2p2g(scene_device &s, const float *v, float *f, long long ndofs, float dt, const int *skip,
+                         cudaStream_t st);
+cudaError_t launch_implicit_mass(scene_device &s, const float *dv, float *out, float dt, long long ndofs,
+                                 const int *skip, cudaStream_t st);
+cudaError_t launch_implicit_project(scene_device &s, float *dof, long long ndofs, const int *skip,
+                                    cudaStream_t st);
+cudaError_t launch_implicit_precondition(scene_device &s, const float *in, float *out, long long ndofs,
+                                         const int *skip, cudaStream_t st);
+
+// ConjugateGradient::solve state on the device
+struct cg_state {
+  double acc;        // dot product accumulator (zeroed by its consumer)
+  float ztrk, norm, local_tol, alpha, beta;
+  int done, iter;
+};
+struct cg_vectors {
+  float *r, *p, *q, *ap;  // residual, search direction, preconditioned residual, A p
+};
+cudaError_t launch_cg_begin(scene_device &s, float *x, const float *b, const cg_vectors &v, long long ndofs, float dt,
+                            cg_state *cs, float tol, float rel_tol, cudaStream_t st);
+cudaError_t launch_cg_iteration(scene_device &s, float *x, const cg_vectors &v, long long ndofs, float dt,
+                                cg_state *cs, int max_iters, cudaStream_t st);
 
 // upload / download helpers: staging is AoS (x: 3n, C/F: 9n), see zsmpm_particle_arrays
 cudaError_t launch_import(scene_device &s, const float *m, const float *x, const float *v,

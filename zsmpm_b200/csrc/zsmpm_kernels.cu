@@ -1125,6 +1125,352 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
   }
 }
 
+// ----------------------------------------------------------------- G2P2G and the implicit system
+// G2P2GTransfer (simulation/transfer/G2P2G.hpp:49-142), the force operator of the implicit
+// solve (simulation/mpm/ImplicitMPM.hpp:34-61).  One CTA per block (persistent): the velocity
+// field is staged in a 12^3 halo; every particle forms C from it and the trial
+// F = (I + dt C) F, evaluates its stress on a copy of its state (nothing is written back) and
+// adds W (4/dx^2) (V0 P F^T)(x_i - x_p) to a 12^3 force halo in shared memory, which is
+// flushed into f with 16-byte reductions.  v and f are node-major over the active blocks in
+// canonical order, v[(block*512 + cell)*3 + d]: the layout of a dof_view<space, 3> over a
+// Vector (types/View.h:77-168).  Within a pass of 256 slots the lanes of a warp take every
+// 8th slot, so that they mostly belong to different cells and their shared-memory atomics
+// to different nodes (the particles of one cell share all 27 nodes).
+constexpr int kG2P2GThreads = 256;
+constexpr size_t kG2P2GSmem = sizeof(float4) * kHaloCells + sizeof(float) * 3 * kHaloCells;
+
+__global__ void __launch_bounds__(kG2P2GThreads, 3)
+    k_g2p2g(scene_device s, const float *__restrict__ vin, float *__restrict__ fout, long long ndofs, float dt,
+            const int *skip) {
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) float gg_smem[];
+  float4 *svf = reinterpret_cast<float4 *>(gg_smem);
+  float *sf = gg_smem + 4 * kHaloCells;  // [3][kHaloCells]
+  __shared__ int s_b;
+  const scene_params &p = s.prm;
+  const int nb = s.ctr[kCtrBlocks];
+  if ((long long)nb * 1536 > ndofs) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_status(s.ctr, kStatusCapacity);
+    return;
+  }
+  const int t = threadIdx.x;
+  const int perm = (t & 31) * 8 + (t >> 5);
+  for (;;) {
+    const int b = grab_block(&s.ctr[kCtrWork + kWorkG2P2G], &s_b);
+    if (b >= nb) break;
+    const int start = s.block_start[b], end = s.block_start[b + 1];
+    if (start == end) continue;
+    for (int q = t; q < 3 * kHaloCells; q += kG2P2GThreads) sf[q] = 0.f;
+    // halo load: items (hx, hy, quad) over 12 x 12 x 3; four consecutive nodes are 12
+    // consecutive floats (three 16-byte loads)
+    for (int it = t; it < kHalo * kHalo * 3; it += kG2P2GThreads) {
+      const int quad = it % 3, hy = (it / 3) % kHalo, hx = it / (3 * kHalo);
+      const int tb = s.nbr[b * 8 + ((hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0))];
+      float4 a = make_float4(0.f, 0.f, 0.f, 0.f), c = a, d = a;
+      if (tb >= 0) {
+        const int cell = ((hx & 7) << 6) | ((hy & 7) << 3) | ((quad * 4) & 7);
+        const float4 *g = reinterpret_cast<const float4 *>(vin + ((size_t)tb * 512 + cell) * 3);
+        a = g[0];
+        c = g[1];
+        d = g[2];
+      }
+      float4 *dst = svf + (hx * kHalo + hy) * kHalo + quad * 4;
+      dst[0] = make_float4(a.x, a.y, a.z, 0.f);
+      dst[1] = make_float4(a.w, c.x, c.y, 0.f);
+      dst[2] = make_float4(c.z, c.w, d.x, 0.f);
+      dst[3] = make_float4(d.y, d.z, d.w, 0.f);
+    }
+    __syncthreads();
+    const int3 bk = unpack_key(s.blk_pk[b]);
+    const int org[3] = {bk.x * 8, bk.y * 8, bk.z * 8};
+    for (int pass = start; pass < end; pass += kG2P2GThreads) {
+      const int slot = pass + perm;
+      // every lane stays (the SVD's early exit is a warp vote); lanes past the block's end
+      // run on a copy of its first particle and add nothing
+      const bool active = slot < end;
+      const int i = s.src[active ? slot : start];
+      const float4 xm = s.cur.xm[i];
+      float F[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) F[k] = s.cur.F[(size_t)k * p.cap + i];
+      float pl = s.cur.plastic ? s.cur.plastic[i] : 0.f;
+      const float X[3] = {__fdiv_rn(xm.x, p.dx), __fdiv_rn(xm.y, p.dx), __fdiv_rn(xm.z, p.dx)};
+      int hb[3];
+      float w[3][3], f[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float bs = floorf(X[d] - 0.5f);
+        f[d] = X[d] - bs;
+        hb[d] = (int)bs - org[d];
+        w[d][0] = 0.5f * (1.5f - f[d]) * (1.5f - f[d]);
+        const float f1 = f[d] - 1.f;
+        w[d][1] = 0.75f - f1 * f1;
+        const float f2 = 0.5f + f1;
+        w[d][2] = 0.5f * f2 * f2;
+      }
+      const bool inside = hb[0] >= 0 && hb[0] <= kHalo - 3 && hb[1] >= 0 && hb[1] <= kHalo - 3 &&
+                          hb[2] >= 0 && hb[2] <= kHalo - 3;
+      if (active && !inside) set_status(s.ctr, kStatusMissingBlock);
+      float B[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // sum W v (node - f)^T
+      if (inside) {
+#pragma unroll
+        for (int ii = 0; ii < 3; ++ii) {
+          const float dxi = (float)ii - f[0];
+#pragma unroll
+          for (int jj = 0; jj < 3; ++jj) {
+            const float dyj = (float)jj - f[1];
+            const float wij = w[0][ii] * w[1][jj];
+            const int hrow = ((hb[0] + ii) * kHalo + (hb[1] + jj)) * kHalo + hb[2];
+            float s0[3] = {0.f, 0.f, 0.f}, s1[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+              const float wz = w[2][kk], wzd = wz * ((float)kk - f[2]);
+              const float4 node = svf[hrow + kk];
+              s0[0] += wz * node.x;
+              s0[1] += wz * node.y;
+              s0[2] += wz * node.z;
+              s1[0] += wzd * node.x;
+              s1[1] += wzd * node.y;
+              s1[2] += wzd * node.z;
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const float a = wij * s0[d];
+              B[d] += a * dxi;
+              B[3 + d] += a * dyj;
+              B[6 + d] += wij * s1[d];
+            }
+          }
+        }
+      }
+      // trial F = (I + dt C) F (G2P2G.hpp:103-105), C = B 4/dx
+      float Fn[9];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+          Fn[3 * c + r] = F[3 * c + r] + dt * p.four_over_dx *
+                                             (B[r] * F[3 * c] + B[3 + r] * F[3 * c + 1] + B[6 + r] * F[3 * c + 2]);
+      float tau[9];
+      constitutive<true>(p.mat, Fn, pl, tau);
+      if (!active || !inside) continue;
+      // f_i += W (4/dx^2) tau (x_i - x_p) = W (4/dx) tau (node - f)
+      float tf[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) tf[k] = tau[k] * p.four_over_dx;
+#pragma unroll
+      for (int ii = 0; ii < 3; ++ii) {
+        const float dxi = (float)ii - f[0];
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+          const float dyj = (float)jj - f[1];
+          const float wij = w[0][ii] * w[1][jj];
+          const int hrow = ((hb[0] + ii) * kHalo + (hb[1] + jj)) * kHalo + hb[2];
+          float base[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) base[d] = tf[d] * dxi + tf[3 + d] * dyj;
+#pragma unroll
+          for (int kk = 0; kk < 3; ++kk) {
+            const float W = wij * w[2][kk], dzk = (float)kk - f[2];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) atomicAdd(&sf[d * kHaloCells + hrow + kk], W * (base[d] + tf[6 + d] * dzk));
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // flush: items (hx, hy, quad); four nodes x three components = three 16-byte reductions
+    for (int it = t; it < kHalo * kHalo * 3; it += kG2P2GThreads) {
+      const int quad = it % 3, hy = (it / 3) % kHalo, hx = it / (3 * kHalo);
+      const int h = (hx * kHalo + hy) * kHalo + quad * 4;
+      float v[12];
+#pragma unroll
+      for (int n = 0; n < 4; ++n)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v[3 * n + d] = sf[d * kHaloCells + h + n];
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < 12; ++k) any = any || v[k] != 0.f;
+      if (!any) continue;
+      const int tb = s.nbr[b * 8 + ((hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0))];
+      if (tb < 0) {
+        set_status(s.ctr, kStatusMissingBlock);
+        continue;
+      }
+      const int cell = ((hx & 7) << 6) | ((hy & 7) << 3) | ((quad * 4) & 7);
+      float *dst = fout + ((size_t)tb * 512 + cell) * 3;
+      red_add_v4(dst, v[0], v[1], v[2], v[3]);
+      red_add_v4(dst + 4, v[4], v[5], v[6], v[7]);
+      red_add_v4(dst + 8, v[8], v[9], v[10], v[11]);
+    }
+  }
+}
+
+// dof entries of the active blocks (nb * 512 * 3), or 0 with the capacity status when the
+// caller's vectors are shorter
+__device__ __forceinline__ long long dof_count(const scene_device &s, long long ndofs) {
+  const long long total = (long long)s.ctr[kCtrBlocks] * 1536;
+  if (total <= ndofs) return total;
+  if (blockIdx.x == 0 && threadIdx.x == 0) set_status(s.ctr, kStatusCapacity);
+  return 0;
+}
+
+// ImplicitMPMSystem::ForceDtSqrPlusMass (ImplicitMPM.hpp:17-33): where the grid mass of the
+// node is positive, out = (f dt^2 + m) dv, with f = out on entry.
+__global__ void __launch_bounds__(kThreads) k_implicit_mass(scene_device s, const float *__restrict__ dv,
+                                                             float *__restrict__ out, float dt, long long ndofs,
+                                                             const int *skip) {
+  if (skip && *skip) return;
+  const long long total = dof_count(s, ndofs);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += grid_threads()) {
+    const long long node = i / 3;
+    const float m = s.grid[(node >> 9) * kGridChannels * 512 + (node & 511)];
+    if (m > 0.f) out[i] = (out[i] * dt * dt + m) * dv[i];
+  }
+}
+
+// ImplicitMPMSystem::Projector (ImplicitMPM.hpp:63-97) with the scene's six walls: nodes with
+// positive mass get the walls' collision response, all others are zeroed.
+__global__ void __launch_bounds__(kThreads) k_implicit_project(scene_device s, float *__restrict__ dof,
+                                                                long long ndofs, const int *skip) {
+  if (skip && *skip) return;
+  const scene_params &p = s.prm;
+  const long long total = dof_count(s, ndofs) / 3;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += grid_threads()) {
+    const int b = (int)(t >> 9), cell = (int)(t & 511);
+    float *v = dof + t * 3;
+    if (s.grid[(size_t)b * kGridChannels * 512 + cell] > 0.f) {
+      const int3 k = unpack_key(s.blk_pk[b]);
+      const float pos[3] = {((float)k.x * 8.f + (float)(cell >> 6)) * p.dx,
+                            ((float)k.y * 8.f + (float)((cell >> 3) & 7)) * p.dx,
+                            ((float)k.z * 8.f + (float)(cell & 7)) * p.dx};
+      float vel[3] = {v[0], v[1], v[2]};
+      apply_walls(p, pos, vel);
+      v[0] = vel[0];
+      v[1] = vel[1];
+      v[2] = vel[2];
+    } else {
+      v[0] = v[1] = v[2] = 0.f;
+    }
+  }
+}
+
+// ImplicitMPMSystem::DivPernodeMass (ImplicitMPM.hpp:126-137): out = in / m where the grid
+// mass is positive; other entries of out are left as they are.
+__global__ void __launch_bounds__(kThreads) k_implicit_precondition(scene_device s, const float *__restrict__ in,
+                                                                     float *__restrict__ out, long long ndofs,
+                                                                     const int *skip) {
+  if (skip && *skip) return;
+  const long long total = dof_count(s, ndofs);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += grid_threads()) {
+    const long long node = i / 3;
+    const float m = s.grid[(node >> 9) * kGridChannels * 512 + (node & 511)];
+    if (m > 0.f) out[i] = in[i] / m;
+  }
+}
+
+// ConjugateGradient::solve (math/linear/ConjugateGradient.hpp:69-172) on the device.  The
+// scalars (r.q, alpha, beta, the stopping test) live in a cg_state in device memory, so no
+// step needs the host: every kernel of an iteration returns at once when the iteration's
+// check found the solve finished.  Dot products sum float products per thread and warp, and
+// the warp sums in double.
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(kThreads) k_cg_fill0(scene_device s, float *__restrict__ v, long long ndofs,
+                                                        const int *skip) {
+  if (skip && *skip) return;
+  const long long total = dof_count(s, ndofs);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += grid_threads()) v[i] = 0.f;
+}
+
+// r = b - Ax (ConjugateGradient.hpp:97-98)
+__global__ void __launch_bounds__(kThreads) k_cg_residual(scene_device s, const float *__restrict__ b,
+                                                           const float *__restrict__ ax, float *__restrict__ r,
+                                                           long long ndofs) {
+  const long long total = dof_count(s, ndofs);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += grid_threads())
+    r[i] = b[i] - ax[i];
+}
+
+__global__ void __launch_bounds__(kThreads) k_cg_copy(scene_device s, const float *__restrict__ src,
+                                                       float *__restrict__ dst, long long ndofs) {
+  const long long total = dof_count(s, ndofs);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += grid_threads()) dst[i] = src[i];
+}
+
+__global__ void __launch_bounds__(kThreads) k_cg_dot(scene_device s, const float *__restrict__ a,
+                                                      const float *__restrict__ b, long long ndofs, cg_state *cs) {
+  if (cs->done) return;
+  const long long total = dof_count(s, ndofs);
+  float acc = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += grid_threads())
+    acc += a[i] * b[i];
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0 && acc != 0.f) atomicAdd(&cs->acc, (double)acc);
+}
+
+// after the first r.q: the norm and the tolerance min(relTol * norm, tol) (:115-117)
+__global__ void k_cg_init(cg_state *cs, float tol, float rel_tol) {
+  const float z = (float)cs->acc;
+  cs->acc = 0.0;
+  cs->ztrk = z;
+  cs->norm = sqrtf(z);
+  cs->local_tol = fminf(rel_tol * cs->norm, tol);
+  cs->iter = 0;
+  cs->done = 0;
+}
+
+// the loop head (:118-122): stop at the tolerance or after max_iters iterations
+__global__ void k_cg_check(cg_state *cs, int max_iters) {
+  if (cs->done) return;
+  if (cs->iter >= max_iters || cs->norm <= cs->local_tol) cs->done = 1;
+}
+
+__global__ void k_cg_alpha(cg_state *cs) {
+  if (cs->done) return;
+  cs->alpha = cs->ztrk / (float)cs->acc;  // alpha = zTrk / (Ap . p)  (:134)
+  cs->acc = 0.0;
+}
+
+// x = alpha p + x, r = -alpha Ap + r (:137-143)
+__global__ void __launch_bounds__(kThreads) k_cg_update_xr(scene_device s, float *__restrict__ x, float *__restrict__ r,
+                                                            const float *__restrict__ p, const float *__restrict__ ap,
+                                                            long long ndofs, const cg_state *cs) {
+  if (cs->done) return;
+  const float alpha = cs->alpha;
+  const long long total = dof_count(s, ndofs);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += grid_threads()) {
+    x[i] = alpha * p[i] + x[i];
+    r[i] = -alpha * ap[i] + r[i];
+  }
+}
+
+// zTrk = q.r, beta = zTrk / zTrkLast, norm = sqrt(zTrk), one iteration done (:156-170)
+__global__ void k_cg_beta(cg_state *cs) {
+  if (cs->done) return;
+  const float last = cs->ztrk;
+  cs->ztrk = (float)cs->acc;
+  cs->acc = 0.0;
+  cs->beta = cs->ztrk / last;
+  cs->norm = sqrtf(cs->ztrk);
+  cs->iter += 1;
+}
+
+// p = beta p + q (:163)
+__global__ void __launch_bounds__(kThreads) k_cg_update_p(scene_device s, float *__restrict__ p,
+                                                           const float *__restrict__ q, long long ndofs,
+                                                           const cg_state *cs) {
+  if (cs->done) return;
+  const float beta = cs->beta;
+  const long long total = dof_count(s, ndofs);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += grid_threads())
+    p[i] = beta * p[i] + q[i];
+}
+
 // ----------------------------------------------------------------- import / export
 // scene of upload index i: the last scene whose start is <= i
 __device__ __forceinline__ int scene_of_index(const scene_params &p, int i) {
@@ -1411,6 +1757,8 @@ cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
 cudaError_t prepare_kernels() {
   cudaError_t e = cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_g2p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kG2P2GSmem);
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_g2p<true, false, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)kG2PSmemLearned);
 }
@@ -1441,7 +1789,73 @@ cudaError_t launch_g2p(scene_device &s, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// k_begin, insert, enlarge, prepare, set, 3 scans, ranks, neighbours; count, 3 scans,
+cudaError_t launch_g2p2g(scene_device &s, const float *v, float *f, long long ndofs, float dt, const int *skip,
+                         cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(&s.ctr[kCtrWork + kWorkG2P2G], 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  k_g2p2g<<<num_sms() * 3, kG2P2GThreads, kG2P2GSmem, st>>>(s, v, f, ndofs, dt, skip);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_implicit_mass(scene_device &s, const float *dv, float *out, float dt, long long ndofs,
+                                 const int *skip, cudaStream_t st) {
+  k_implicit_mass<<<num_sms() * 4, kThreads, 0, st>>>(s, dv, out, dt, ndofs, skip);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_implicit_project(scene_device &s, float *dof, long long ndofs, const int *skip,
+                                    cudaStream_t st) {
+  k_implicit_project<<<num_sms() * 4, kThreads, 0, st>>>(s, dof, ndofs, skip);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_implicit_precondition(scene_device &s, const float *in, float *out, long long ndofs,
+                                         const int *skip, cudaStream_t st) {
+  k_implicit_precondition<<<num_sms() * 4, kThreads, 0, st>>>(s, in, out, ndofs, skip);
+  return cudaGetLastError();
+}
+
+// The solve's start: r = b - A x, project r, q = M r (q zeroed first), p = q, zTrk = r.q.
+cudaError_t launch_cg_begin(scene_device &s, float *x, const float *b, const cg_vectors &v, long long ndofs, float dt,
+                            cg_state *cs, float tol, float rel_tol, cudaStream_t st) {
+  const int grid = num_sms() * 4;
+  cudaError_t e = cudaMemsetAsync(cs, 0, sizeof(cg_state), st);
+  if (e != cudaSuccess) return e;
+  k_cg_fill0<<<grid, kThreads, 0, st>>>(s, v.ap, ndofs, nullptr);
+  if ((e = launch_g2p2g(s, x, v.ap, ndofs, dt, nullptr, st)) != cudaSuccess) return e;
+  if ((e = launch_implicit_mass(s, x, v.ap, dt, ndofs, nullptr, st)) != cudaSuccess) return e;
+  k_cg_residual<<<grid, kThreads, 0, st>>>(s, b, v.ap, v.r, ndofs);
+  if ((e = launch_implicit_project(s, v.r, ndofs, nullptr, st)) != cudaSuccess) return e;
+  k_cg_fill0<<<grid, kThreads, 0, st>>>(s, v.q, ndofs, nullptr);
+  if ((e = launch_implicit_precondition(s, v.r, v.q, ndofs, nullptr, st)) != cudaSuccess) return e;
+  k_cg_copy<<<grid, kThreads, 0, st>>>(s, v.q, v.p, ndofs);
+  k_cg_dot<<<grid, kThreads, 0, st>>>(s, v.r, v.q, ndofs, cs);
+  k_cg_init<<<1, 1, 0, st>>>(cs, tol, rel_tol);
+  return cudaGetLastError();
+}
+
+// One loop iteration (ConjugateGradient.hpp:118-171); does nothing once the solve is done.
+cudaError_t launch_cg_iteration(scene_device &s, float *x, const cg_vectors &v, long long ndofs, float dt,
+                                cg_state *cs, int max_iters, cudaStream_t st) {
+  const int grid = num_sms() * 4;
+  const int *done = &cs->done;
+  k_cg_check<<<1, 1, 0, st>>>(cs, max_iters);
+  k_cg_fill0<<<grid, kThreads, 0, st>>>(s, v.ap, ndofs, done);
+  cudaError_t e = launch_g2p2g(s, v.p, v.ap, ndofs, dt, done, st);
+  if (e != cudaSuccess) return e;
+  if ((e = launch_implicit_mass(s, v.p, v.ap, dt, ndofs, done, st)) != cudaSuccess) return e;
+  if ((e = launch_implicit_project(s, v.ap, ndofs, done, st)) != cudaSuccess) return e;
+  k_cg_dot<<<grid, kThreads, 0, st>>>(s, v.ap, v.p, ndofs, cs);
+  k_cg_alpha<<<1, 1, 0, st>>>(cs);
+  k_cg_update_xr<<<grid, kThreads, 0, st>>>(s, x, v.r, v.p, v.ap, ndofs, cs);
+  if ((e = launch_implicit_precondition(s, v.r, v.q, ndofs, done, st)) != cudaSuccess) return e;
+  k_cg_dot<<<grid, kThreads, 0, st>>>(s, v.q, v.r, ndofs, cs);
+  k_cg_beta<<<1, 1, 0, st>>>(cs);
+  k_cg_update_p<<<grid, kThreads, 0, st>>>(s, v.p, v.q, ndofs, cs);
+  return cudaGetLastError();
+}
+
+// k_begin, insert, enlarge, prepare, set, 3 scans// k_begin, insert, enlarge, prepare, set, 3 scans, ranks, neighbours; count, 3 scans,
 // cell_start, scatter, finalize; p2g; grid update; g2p
 int kernels_per_substep() { return 10 + 7 + 3; }
 
