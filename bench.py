@@ -263,6 +263,97 @@ def mlp_inference_leg(c, n_rows: int, reps: int = 5) -> dict:
     return out
 
 
+def g2p2g_algorithmic_bytes(n: int, nb: int, plastic: bool) -> int:
+    """G2P2G per launch: per particle reads slot index 4, x|m 16, F 36 (+ plastic 4); per
+    active block reads the 3-component velocity of its 512 nodes (12 B each) and adds the
+    3-component force into them (read + write, 24 B each)."""
+    return n * (4 + 16 + 36 + (4 if plastic else 0)) + nb * 512 * 36
+
+
+def implicit_leg(args, zs, sc, spec, upload_pinned, stream, sptr, cpu_sample) -> dict:
+    """The implicit system on the same workload: G2P2GTransfer launches over the grid velocity
+    of a P2G + grid update (timed with CUDA events on the launching stream), and a conjugate-
+    gradient solve of ImplicitMPMSystem for b = m v from x = 0.  cpu_sample: (particles, keys,
+    velocity field) for the reference's own G2P2GTransfer under omp_exec, or None."""
+    import torch
+
+    from zsmpm_b200.implicit import ConjugateGradient, ImplicitMPMSystem
+    upload_pinned()
+    sc.run(2, stream=sptr)
+    sc.activate_blocks(stream=sptr)
+    sc.bin_particles(stream=sptr)
+    sc.p2g(stream=sptr)
+    sc.grid_update(stream=sptr)
+    torch.cuda.synchronize()
+    keys, grid = sc.download_grid()
+    nb = len(keys)
+    n = sc.n
+    plastic = spec.material.model != zs.FIXED_COROTATED
+    system = ImplicitMPMSystem(sc, spec.dt)
+    v = torch.from_numpy(np.ascontiguousarray(grid[:, 1:4, :].transpose(0, 2, 1).reshape(-1))).to("cuda")
+    f = system.zeros()
+    for _ in range(3):
+        system.g2p2g(v, f, stream=stream)
+    reps = 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        system.g2p2g(v, f, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sc.status()
+    ms = e0.elapsed_time(e1) / reps
+    nbytes = g2p2g_algorithmic_bytes(n, nb, plastic)
+    peak, peak_kind = hbm_peak()
+    m = torch.from_numpy(np.repeat(grid[:, 0, :].reshape(-1), 3)).to("cuda")
+    b = m * v
+    x = system.zeros()
+    converged = ConjugateGradient(max_iters=20).solve(system, x, b, stream=stream)  # also sizes the scratch
+    # a fixed iteration count for the per-iteration time (tol 0 never stops early)
+    fixed = ConjugateGradient(max_iters=10, tol=0.0)
+    x.zero_()
+    torch.cuda.synchronize()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    iters = fixed.solve(system, x, b, stream=stream)
+    c1.record(stream)
+    torch.cuda.synchronize()
+    cg_ms = c0.elapsed_time(c1)
+    out = {"particles": n, "active_blocks": nb, "g2p2g_ms": ms, "particles_per_s": n / (ms * 1e-3),
+           "g2p2g_roofline": {"bound": "issue (SVD and return map per particle)", "algorithmic_bytes": nbytes,
+                              "achieved_gbs": nbytes / (ms * 1e-3) / 1e9, "hbm_peak": peak,
+                              "hbm_frac": nbytes / (ms * 1e-3) / 1e9 / peak, "peak_kind": peak_kind},
+           "cg": {"b": "m v of the updated grid", "x0": "0", "iterations_to_converge": converged,
+                  "timed_iterations": iters, "ms": cg_ms, "ms_per_iteration": cg_ms / max(iters, 1),
+                  "what": "CUDA events around zsmpm_implicit_cg with tol 0 and max_iters 10 (the host reads "
+                          "the stopping flag every 8 iterations)"}}
+    if cpu_sample is not None:
+        try:
+            from oracle import reference
+            q, qkeys, qv, desc = cpu_sample
+            threads = os.cpu_count() or 1
+            _, secs = reference.g2p2g(spec, q.x, q.F, q.plastic, qkeys, qv, policy=reference.POLICY_OMP,
+                                      threads=threads, timeout=900)
+            out["cpu_baseline"] = {"value": q.n / secs, "unit": "particles/s", "cores": threads, "kind": "reference",
+                                   "sample": f"{desc}; G2P2GTransfer under zs::omp_exec"}
+        except Exception as exc:
+            out["cpu_baseline"] = {"value": None, "sample": f"failed: {exc}"}
+    return out
+
+
+def implicit_cpu_sample(spec, p, max_particles: int):
+    """A z-slab of the workload, its canonical block keys and a smooth velocity field on them."""
+    from oracle import reference
+    q, desc = cpu_baseline_sample(spec, p, max_particles)
+    keys, _slots, _npb, _ts = reference.activate(q.x, spec.dx, max(q.n // 512, 64), cap=1 << 20)
+    keys = keys[np.lexsort((keys[:, 2], keys[:, 1], keys[:, 0]))]
+    cell = np.arange(512)
+    loc = np.stack([cell >> 6, (cell >> 3) & 7, cell & 7], 1)
+    pos = (keys[:, None, :].astype(np.int64) * 8 + loc[None]) * spec.dx
+    vel = np.stack([np.sin(7 * pos[..., 1]), np.cos(5 * pos[..., 2]), np.sin(3 * pos[..., 0])], -1)
+    return q, keys, vel.astype(np.float32).reshape(-1), desc
+
+
 def cpu_baseline_sample(spec, p, max_particles: int):
     """A spatial slab of the workload (all particles with z below a cut), keeping density."""
     from zsmpm_b200.scenes import Particles
@@ -339,6 +430,7 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-closure leg")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes")
+    ap.add_argument("--no-implicit", action="store_true", help="skip the implicit-system leg")
     ap.add_argument("--train-random", type=int, default=1_500_000)
     ap.add_argument("--train-logged", type=int, default=500_000)
     args = ap.parse_args(argv)
@@ -451,6 +543,19 @@ def main(argv=None):
     if plastic and parts is None and not args.no_learned:
         learned = learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, ms / args.steps)
 
+    # ---------------------------------------------------------------- implicit-system leg
+    implicit = None
+    if parts is None and not args.no_implicit:
+        sample = None
+        if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+            try:
+                from oracle import reference
+                if reference.available():
+                    sample = implicit_cpu_sample(spec, p, args.ref_particles)
+            except Exception:
+                sample = None
+        implicit = implicit_leg(args, zs, sc, spec, upload_pinned, stream, sptr, sample)
+
     # ---------------------------------------------------------------- CPU baseline (rank 0, N=1)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -501,6 +606,7 @@ def main(argv=None):
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "learned": learned,
+            "implicit": implicit,
         }
         print(json.dumps(line))
     sc.close()
