@@ -261,6 +261,46 @@ ZSMPM_API zsmpm_status zsmpm_svd3(const float *A, float *U, float *S, float *V, 
 ZSMPM_API zsmpm_status zsmpm_constitutive(const zsmpm_material *mat, float *F, float *plastic,
                                           float *tau, int64_t count, void *stream);
 
+/* ---- colliders (geometry/Collider.h, geometry/AnalyticLevelSet.h) ------------------------- */
+typedef enum {
+  ZSMPM_SHAPE_PLANE = 0,    /* AnalyticLevelSet<Plane>: a = origin, b = normal (used as given) */
+  ZSMPM_SHAPE_CUBOID = 1,   /* AnalyticLevelSet<Cuboid>: a = min corner, b = max corner */
+  ZSMPM_SHAPE_SPHERE = 2,   /* AnalyticLevelSet<Sphere>: a = center, b[0] = radius */
+  ZSMPM_SHAPE_CYLINDER = 3  /* AnalyticLevelSet<Cylinder>: a = bottom, b[0] = radius,
+                               b[1] = length, axis = 0, 1 or 2 */
+} zsmpm_collider_shape;
+
+/* Collider<AnalyticLevelSet<shape, f32, 3>> (Collider.h:10-200): a rigid analytic level set
+ * placed by scale s, rotation R and translation t, with their rates.  A grid node at x is
+ * inside when the level set's signed distance at X = R^T (x - t) / s is negative; its velocity
+ * then becomes the collider's, omega x (x - t) + (dsdt / s)(x - t) + dt/dt (sticky), or keeps
+ * its tangential part relative to it (slip; separate only when moving into the collider), with
+ * the normal R n(X) (resolveCollision, :80-110). */
+typedef struct {
+  int32_t shape;    /* zsmpm_collider_shape */
+  int32_t type;     /* ZSMPM_WALL_STICKY, ZSMPM_WALL_SLIP or ZSMPM_WALL_SEPARATE */
+  int32_t axis;     /* cylinder axis */
+  int32_t reserved; /* 0 */
+  float a[3], b[3]; /* the shape's parameters, see zsmpm_collider_shape */
+  float s, dsdt;    /* scale (non-zero) and its rate */
+  float R[9];       /* rotation, row-major: R[3*i + j] = R(i, j) */
+  float omega[3];   /* angular velocity */
+  float t[3];       /* translation b */
+  float dtdt[3];    /* its rate db/dt */
+} zsmpm_collider;
+
+#define ZSMPM_MAX_COLLIDERS 16
+
+/* The scene's colliders (at most ZSMPM_MAX_COLLIDERS; count 0 removes them).  The grid update
+ * (and zsmpm_implicit_project) applies the six walls of the scene description first, then the
+ * colliders in list order, each to the nodes with positive mass (ApplyBoundaryConditionOnGridBlocks,
+ * simulation/grid/GridOp.hpp:113-158, one launch per boundary in the reference).  The copy is
+ * ordered on `stream` and the call returns once it is done; the kernels read the colliders when
+ * they run, so moving colliders are updated between substeps without rebuilding the substep
+ * graph.  Single scenes only. */
+ZSMPM_API zsmpm_status zsmpm_scene_set_colliders(zsmpm_scene *scene, const zsmpm_collider *colliders,
+                                                 int32_t count, void *stream);
+
 /* ---- the implicit system (simulation/mpm/ImplicitMPM.hpp) ---------------------------- */
 /* Grid dof vectors are device arrays of `ndofs` floats, node-major over the active blocks in
  * canonical order: entry (block*512 + cell)*3 + d, cell = x*64 + y*8 + z inside the block.

@@ -17,6 +17,10 @@
 #   simulation/transfer/G2P2G.hpp       atomicAdd(&r, v) -> atomic_add(wrapv<space>{}, &r, v),
 #                                       the exec-space atomic that P2G.hpp uses (a plain add
 #                                       under seq_exec)
+#   geometry/AnalyticLevelSet.h         getSignedDistance(..) -> this->getSignedDistance(..)
+#                                       in the finite-difference normals (a member of the
+#                                       CRTP base); the other geometry headers are linked beside
+#                                       it so that their relative includes find the patched copy
 # Logging (plog) and magic_enum are replaced by the small shims in oracle/ref_shims.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -42,6 +46,12 @@ sed -E 's/atomicAdd\(/atomic_add(wrapv<space>{}, /g' \
 # relative includes of the patched copies ("Scheme.hpp", "../transfer/Scheme.hpp", "Property.h")
 ln -sf "$REF/zensim/simulation/transfer/Scheme.hpp" "$OUT/patched/zensim/simulation/transfer/Scheme.hpp"
 ln -sf "$REF/zensim/types/Property.h" "$OUT/patched/zensim/types/Property.h"
+mkdir -p "$OUT/patched/zensim/geometry"
+for f in "$REF"/zensim/geometry/*; do
+  [ "$(basename "$f")" = "AnalyticLevelSet.h" ] || ln -sfn "$f" "$OUT/patched/zensim/geometry/$(basename "$f")"
+done
+sed -E 's/\(getSignedDistance\(/(this->getSignedDistance(/g; s/- getSignedDistance\(/- this->getSignedDistance(/g' \
+  "$REF/zensim/geometry/AnalyticLevelSet.h" > "$OUT/patched/zensim/geometry/AnalyticLevelSet.h"
 
 CXXFLAGS=(-std=c++17 -O2 -fPIC -fopenmp -ffp-contract=off -include cstdint -include utility
   -DZS_ENABLE_OPENMP=1 -DZS_ENABLE_CUDA=0 -DZS_ENABLE_MUSA=0 -DZS_ENABLE_SYCL=0

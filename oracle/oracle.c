@@ -13,6 +13,7 @@
 #define R_LOG logf
 #define R_EXP expf
 #define R_SQRT oracle_ref_sqrtf
+#define R_STDSQRT sqrtf
 #define R_FLOOR floorf
 #define OR_SVD oracle_svd_f32
 #include "oracle_sim.h"
@@ -21,6 +22,7 @@
 #undef R_LOG
 #undef R_EXP
 #undef R_SQRT
+#undef R_STDSQRT
 #undef R_FLOOR
 #undef OR_SVD
 
@@ -29,6 +31,7 @@
 #define R_LOG log
 #define R_EXP exp
 #define R_SQRT sqrt
+#define R_STDSQRT sqrt
 #define R_FLOOR floor
 #define OR_SVD oracle_svd_f64
 #include "oracle_sim.h"

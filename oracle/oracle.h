@@ -20,6 +20,8 @@
  *   snow projection    physics/plasticity_models/SnowPlasticity.hpp:24-32
  *   SVD (FP32)         math/matrix/SVD.hpp:15-1025 (McAdams et al. 2011 quaternion Jacobi)
  *   grid update        simulation/grid/GridOp.hpp:72-164, geometry/Collider.h:80-110
+ *   colliders          geometry/Collider.h:10-200, geometry/AnalyticLevelSet.h (plane, cuboid,
+ *                      sphere, cylinder), math/VecInterface.hpp (vector operation order)
  *   G2P                simulation/transfer/G2P.hpp:43-84, math/matrix/MatrixUtils.h:136-146
  *   G2P2G              simulation/transfer/G2P2G.hpp:49-142 (implicit force operator)
  * Matrices are column-major (M(i,j) = M[3j+i]) as in the reference.
@@ -37,6 +39,18 @@ enum { ORACLE_MODE_COMMITTED = 0, ORACLE_MODE_REFERENCE = 1 };
 enum { ORACLE_WALL_STICKY = 0, ORACLE_WALL_SLIP = 1, ORACLE_WALL_SEPARATE = 2,
        ORACLE_WALL_NONE = 3 };
 
+/* Collider<AnalyticLevelSet<shape, f32, 3>> (geometry/Collider.h:10-200): the layout of
+ * zsmpm_collider.  shape 0 plane (a origin, b normal), 1 cuboid (a min, b max), 2 sphere
+ * (a center, b[0] radius), 3 cylinder (a bottom, b[0] radius, b[1] length, axis); type 0 sticky,
+ * 1 slip, 2 separate; rot is the rotation R, row-major. */
+typedef struct {
+  int shape, type, axis, reserved;
+  float a[3], b[3];
+  float s, dsdt;
+  float rot[9];
+  float omega[3], t[3], dtdt[3];
+} oracle_collider;
+
 typedef struct {
   int model;             /* ORACLE_FC / ORACLE_DP / ORACLE_SNOW */
   int mode;              /* ORACLE_MODE_COMMITTED or ORACLE_MODE_REFERENCE */
@@ -47,6 +61,8 @@ typedef struct {
   double E, nu, volume;
   double friction_deg, cohesion, beta;      /* Drucker-Prager */
   double hardening, theta_c, theta_s;       /* snow */
+  int ncolliders;                           /* applied after the walls, in order */
+  const oracle_collider *colliders;
 } oracle_params;
 
 /* Runs nsteps substeps on SoA/AoS host arrays in place (x, v: 3n; C, F: 9n column-major;

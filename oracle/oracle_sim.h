@@ -172,6 +172,135 @@ void OR_NAME(oracle_stress)(const oracle_params *p, R *F, R *plastic, R *PF) {
   OR_NAME(stress)(&c, F, plastic, PF);
 }
 
+/* ---- colliders: AnalyticLevelSet signed distances and normals (AnalyticLevelSet.h) and
+ * Collider::resolveCollision (Collider.h:80-110), each vector operation in the order of
+ * math/VecInterface.hpp (dot/length accumulate from 0 in index order; a matrix-vector product
+ * accumulates each row from 0); lengths use the C library square root, as zs::sqrt does on
+ * the host (ZpcMathUtils.hpp:760-770) */
+static R OR_NAME(col_len)(const R *v) {
+  R l2 = 0;
+  for (int i = 0; i != 3; ++i) l2 += v[i] * v[i];
+  return R_STDSQRT(l2);
+}
+
+static R OR_NAME(col_sdf)(const oracle_collider *c, const R *X) {
+  if (c->shape == 0) {
+    R r = 0;
+    for (int i = 0; i != 3; ++i) r += (R)c->b[i] * (X[i] - (R)c->a[i]);
+    return r;
+  }
+  if (c->shape == 1) {
+    R p[3], mx;
+    for (int i = 0; i != 3; ++i) {
+      R center = ((R)c->a[i] + (R)c->b[i]) / (R)2;
+      R d = X[i] - center;
+      p[i] = (d > 0 ? d : -d) - ((R)c->b[i] - (R)c->a[i]) / (R)2;
+    }
+    mx = p[0];
+    for (int i = 1; i != 3; ++i)
+      if (p[i] > mx) mx = p[i];
+    for (int i = 0; i != 3; ++i)
+      if (p[i] < 0) p[i] = 0;
+    return (mx < 0 ? mx : (R)0) + OR_NAME(col_len)(p);
+  }
+  if (c->shape == 2) {
+    R d[3];
+    for (int i = 0; i != 3; ++i) d[i] = X[i] - (R)c->a[i];
+    return OR_NAME(col_len)(d) - (R)c->b[0];
+  }
+  {
+    const int ax = c->axis;
+    R dr[2], l2 = 0;
+    for (int k = 0, i = 0; k != 3; ++k)
+      if (k != ax) dr[i++] = X[k] - (R)c->a[k];
+    for (int i = 0; i != 2; ++i) l2 += dr[i] * dr[i];
+    const R dis_r = R_STDSQRT(l2), radius = (R)c->b[0], length = (R)c->b[1], bd = (R)c->a[ax];
+    const int outside = dis_r > radius;
+    if (X[ax] < bd) {
+      R dis_l = bd - X[ax];
+      return outside ? R_STDSQRT((dis_r - radius) * (dis_r - radius) + dis_l * dis_l) : dis_l;
+    } else if (X[ax] > bd + length) {
+      R dis_l = X[ax] - (bd + length);
+      return outside ? R_STDSQRT((dis_r - radius) * (dis_r - radius) + dis_l * dis_l) : dis_l;
+    } else {
+      if (outside) return dis_r - radius;
+      R top = bd + length - X[ax], bot = X[ax] - bd;
+      R dis_l = top < bot ? top : bot;
+      R rr = radius - dis_r;
+      return -(dis_l < rr ? dis_l : rr);
+    }
+  }
+}
+
+static void OR_NAME(col_normal)(const oracle_collider *c, const R *X, R *n) {
+  if (c->shape == 0) {
+    for (int i = 0; i != 3; ++i) n[i] = (R)c->b[i];
+    return;
+  }
+  if (c->shape == 2) {
+    R o[3], l2 = 0;
+    for (int i = 0; i != 3; ++i) o[i] = X[i] - (R)c->a[i];
+    for (int i = 0; i != 3; ++i) l2 += o[i] * o[i];
+    if (l2 < (R)1e-7) {
+      n[0] = n[1] = n[2] = 0;
+      return;
+    }
+    R len = OR_NAME(col_len)(o);
+    for (int i = 0; i != 3; ++i) n[i] = o[i] / len;
+    return;
+  }
+  {
+    const R eps = (R)1e-6;
+    R diff[3];
+    for (int i = 0; i != 3; ++i) {
+      R v1[3] = {X[0], X[1], X[2]}, v2[3] = {X[0], X[1], X[2]};
+      v1[i] = X[i] + eps;
+      v2[i] = X[i] - eps;
+      diff[i] = (OR_NAME(col_sdf)(c, v1) - OR_NAME(col_sdf)(c, v2)) / (eps + eps);
+    }
+    R len = OR_NAME(col_len)(diff);
+    for (int i = 0; i != 3; ++i) n[i] = diff[i] / len;
+  }
+}
+
+static void OR_NAME(col_resolve)(const oracle_collider *c, const R *x, R *v) {
+  R xb[3], X[3];
+  for (int i = 0; i != 3; ++i) xb[i] = x[i] - (R)c->t[i];
+  const R one_over_s = (R)1 / (R)c->s;
+  for (int i = 0; i != 3; ++i) {
+    R r = 0;
+    for (int j = 0; j != 3; ++j) r += (R)c->rot[3 * j + i] * xb[j];
+    X[i] = r * one_over_s;
+  }
+  if (!(OR_NAME(col_sdf)(c, X) < -(R)0)) return;
+  R vo[3], cr[3];
+  cr[0] = (R)c->omega[1] * xb[2] - (R)c->omega[2] * xb[1];
+  cr[1] = (R)c->omega[2] * xb[0] - (R)c->omega[0] * xb[2];
+  cr[2] = (R)c->omega[0] * xb[1] - (R)c->omega[1] * xb[0];
+  const R ds = (R)c->dsdt * one_over_s;
+  for (int i = 0; i != 3; ++i) {
+    R mv = 0;  /* R s times the material velocity of an analytic level set (zero) */
+    for (int j = 0; j != 3; ++j) mv += ((R)c->rot[3 * i + j] * (R)c->s) * (R)0;
+    vo[i] = ((cr[i] + ds * xb[i]) + mv) + (R)c->dtdt[i];
+  }
+  if (c->type == 0) {
+    for (int i = 0; i != 3; ++i) v[i] = vo[i];
+    return;
+  }
+  for (int i = 0; i != 3; ++i) v[i] -= vo[i];
+  R nX[3], n[3], proj = 0;
+  OR_NAME(col_normal)(c, X, nX);
+  for (int i = 0; i != 3; ++i) {
+    R r = 0;
+    for (int j = 0; j != 3; ++j) r += (R)c->rot[3 * i + j] * nX[j];
+    n[i] = r;
+  }
+  for (int i = 0; i != 3; ++i) proj += n[i] * v[i];
+  if ((c->type == 2 && proj < 0) || c->type == 1)
+    for (int i = 0; i != 3; ++i) v[i] -= proj * n[i];
+  for (int i = 0; i != 3; ++i) v[i] += vo[i];
+}
+
 /* quadratic B-spline stencil (Utils.hpp:30-70, InterpolationKernel.hpp:51-57, :93-130) */
 typedef struct {
   int corner[3];
@@ -337,6 +466,23 @@ int OR_NAME(oracle_run)(const oracle_params *p, int n, const R *m, R *x, R *v, R
         }
       }
     }
+    /* the colliders after the walls, each over every node with positive mass */
+    for (int k = 0; k != p->ncolliders; ++k)
+      for (int b = 0; b != nb; ++b) {
+        R *g = &grid[(size_t)b * 7 * 512];
+        const int32_t *key = &t.active[3 * b];
+        for (int cell = 0; cell != 512; ++cell) {
+          if (!(g[cell] > 0)) continue;
+          const int cc[3] = {cell >> 6, (cell >> 3) & 7, cell & 7};
+          R pos[3], vel[3];
+          for (int d = 0; d != 3; ++d) {
+            pos[d] = ((R)key[d] * (R)8 + (R)cc[d]) * dx;
+            vel[d] = g[(1 + d) * 512 + cell];
+          }
+          OR_NAME(col_resolve)(&p->colliders[k], pos, vel);
+          for (int d = 0; d != 3; ++d) g[(1 + d) * 512 + cell] = vel[d];
+        }
+      }
 
     /* 4. G2P (G2P.hpp:43-84), then in committed mode the constitutive update */
     for (int i = 0; i != n; ++i) {

@@ -22,6 +22,8 @@
 //   6 g2p2g:     zsref_params, int32 n, int32 nb, f32 x[3n], F[9n], logJp[n],
 //                int32 keys[3*nb], f32 v[1536*nb]
 //     reply:     int32 status, f64 seconds, then (status == 0) f32 f[1536*nb]
+//   8 run with colliders: as 1, then int32 ncolliders and ncolliders zsmpm_collider records
+//     reply:     as 1
 //   7 implicit:  zsref_params, int32 op, n, nb, max_iters, f32 tol, rel_tol,
 //                f32 m[n], x[3n], v[3n], C[9n], F[9n], logJp[n], int32 keys[3*nb],
 //                f32 a[1536*nb], b[1536*nb]
@@ -42,6 +44,9 @@ struct zsref_params {
 int zsref_run(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
               float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
               float *out_grid, double *out_seconds);
+int zsref_run_colliders(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
+                        float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
+                        float *out_grid, double *out_seconds, int ncolliders, const void *colliders);
 void zsref_stress(int model, float volume, float E, float nu, float friction_deg,
                   float cohesion, float beta, int volume_correction, float *F, float *logJp,
                   float *PF);
@@ -92,7 +97,7 @@ int main(int argc, char **argv) {
   out_f = std::fopen(argv[2], "wb");
   if (!in_f || !out_f) return 2;
   const int cmd = rd<int32_t>();
-  if (cmd == 1) {
+  if (cmd == 1 || cmd == 8) {
     auto p = rd<zsref_params>();
     const int n = rd<int32_t>(), nsteps = rd<int32_t>(), cap = rd<int32_t>();
     std::vector<float> m, x, v, C, F, lj;
@@ -102,13 +107,19 @@ int main(int argc, char **argv) {
     rdv(C, 9 * (size_t)n);
     rdv(F, 9 * (size_t)n);
     rdv(lj, n);
+    int ncol = 0;
+    std::vector<unsigned char> cols;
+    if (cmd == 8) {
+      ncol = rd<int32_t>();
+      rdv(cols, (size_t)ncol * 120);  // 4 int32 + 26 float32 per collider
+    }
     std::vector<int> keys(3 * (size_t)cap);
     std::vector<float> grid((size_t)cap * 4 * 512);
     int nb = 0;
     double secs = 0;
-    int st = zsref_run(&p, n, m.data(), x.data(), v.data(), C.data(), F.data(), lj.data(),
-                       nsteps, cap, &nb, cap ? keys.data() : nullptr,
-                       cap ? grid.data() : nullptr, &secs);
+    int st = zsref_run_colliders(&p, n, m.data(), x.data(), v.data(), C.data(), F.data(), lj.data(),
+                                 nsteps, cap, &nb, cap ? keys.data() : nullptr,
+                                 cap ? grid.data() : nullptr, &secs, ncol, cols.data());
     wr<int32_t>(st);
     wr<int32_t>(nb);
     wr<double>(secs);

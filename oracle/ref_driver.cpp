@@ -79,6 +79,42 @@ namespace {
 
   using plane_t = AnalyticLevelSet<analytic_geometry_e::Plane, float, 3>;
 
+  // zsmpm_collider's layout: shape 0 plane, 1 cuboid, 2 sphere, 3 cylinder; type 0 sticky,
+  // 1 slip, 2 separate; rot row-major
+  struct ref_collider {
+    int shape, type, axis, reserved;
+    float a[3], b[3];
+    float s, dsdt;
+    float rot[9];
+    float omega[3], t[3], dtdt[3];
+  };
+
+  // One ApplyBoundaryConditionOnGridBlocks launch (GridOp.hpp:113-158) with a
+  // Collider<AnalyticLevelSet<shape, f32, 3>> (Collider.h:10-200) placed as described.
+  template <class Pol, execspace_e space, class Table, class Grids>
+  void apply_collider(Pol &pol, wrapv<space>, const ref_collider &c, Table &table, Grids &grids, int nb) {
+    auto go = [&](auto ls) {
+      Collider col{ls, c.type == 0 ? collider_e::Sticky : c.type == 1 ? collider_e::Slip : collider_e::Separate};
+      col.s = c.s;
+      col.dsdt = c.dsdt;
+      for (int i = 0; i != 3; ++i)
+        for (int j = 0; j != 3; ++j) col.R(i, j) = c.rot[3 * i + j];
+      col.omega.omega = vec<float, 3>{c.omega[0], c.omega[1], c.omega[2]};
+      col.b = vec<float, 3>{c.t[0], c.t[1], c.t[2]};
+      col.dbdt = vec<float, 3>{c.dtdt[0], c.dtdt[1], c.dtdt[2]};
+      pol(Collapse{(size_t)nb, (size_t)512}, ApplyBoundaryConditionOnGridBlocks{wrapv<space>{}, col, table, grids});
+    };
+    const vec<float, 3> a{c.a[0], c.a[1], c.a[2]}, b{c.b[0], c.b[1], c.b[2]};
+    if (c.shape == 0)
+      go(AnalyticLevelSet<analytic_geometry_e::Plane, float, 3>{a, b});
+    else if (c.shape == 1)
+      go(AnalyticLevelSet<analytic_geometry_e::Cuboid, float, 3>{a, b});
+    else if (c.shape == 2)
+      go(AnalyticLevelSet<analytic_geometry_e::Sphere, float, 3>{a, c.b[0]});
+    else
+      go(AnalyticLevelSet<analytic_geometry_e::Cylinder, float, 3>{a, c.b[0], c.b[1], c.axis});
+  }
+
   // Block activation of zsref_run (ComputeSparsity + EnlargeSparsity, then the canonical key
   // order and ReinsertHashTable) on the given positions; returns the block count or -1 when the
   // table is full.
@@ -161,9 +197,23 @@ struct zsref_params {
 // index order and per block 512 cells x 4 channels (m, vx, vy, vz) after the boundary
 // conditions of the last substep, channel-major inside a block.
 // Returns 0 on success, 1 if the grid output capacity is too small, 2 if the table is full.
+int zsref_run_colliders(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
+                        float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
+                        float *out_grid, double *out_seconds, int ncolliders, const void *colliders);
+
 int zsref_run(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
               float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
               float *out_grid, double *out_seconds) {
+  return zsref_run_colliders(p, n, m, x, v, C, F, logJp, nsteps, cap_blocks, out_nblocks, out_keys, out_grid,
+                             out_seconds, 0, nullptr);
+}
+
+// zsref_run with `ncolliders` colliders (ref_collider records) applied after the walls, each
+// by its own ApplyBoundaryConditionOnGridBlocks launch.
+int zsref_run_colliders(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
+                        float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
+                        float *out_grid, double *out_seconds, int ncolliders, const void *colliders) {
+  const ref_collider *cols = static_cast<const ref_collider *>(colliders);
   constexpr auto host = execspace_e::host;
   constexpr auto omp = execspace_e::openmp;
   particles_t pars{(size_t)n, memsrc_e::host, -1};
@@ -258,6 +308,7 @@ int zsref_run(const zsref_params *p, int n, float *m, float *x, float *v, float 
       for (auto &w : walls)
         pol(Collapse{(size_t)nb, (size_t)512},
             ApplyBoundaryConditionOnGridBlocks{wrapv<space>{}, w, table, grids});
+      for (int k = 0; k < ncolliders; ++k) apply_collider(pol, wrapv<space>{}, cols[k], table, grids, nb);
       if (p->model == 0)
         pol(range((size_t)n), G2PTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{},
                                           p->dt, fc, grids, table, pars});

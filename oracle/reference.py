@@ -72,14 +72,18 @@ class RefResult:
 
 def run(spec, particles, nsteps: int, policy: int = POLICY_SEQ, threads: int = 0, order: int = 1,
         table_expected: int | None = None, cap_blocks: int = 1 << 15,
-        timeout: float = 600.0) -> RefResult:
+        timeout: float = 600.0, colliders=()) -> RefResult:
+    """`colliders`: zsmpm_collider records (ctypes), applied after the walls by the reference's
+    own Collider<AnalyticLevelSet<...>> launches."""
     n = particles.n
     if table_expected is None:
         table_expected = max(n // 512, 64)
-    req = struct.pack("<i", 1) + _params_bytes(spec, policy, threads, order, table_expected)
+    req = struct.pack("<i", 8 if colliders else 1) + _params_bytes(spec, policy, threads, order, table_expected)
     req += struct.pack("<3i", n, nsteps, cap_blocks)
     for a in (particles.m, particles.x, particles.v, particles.C, particles.F, particles.plastic):
         req += np.ascontiguousarray(a, dtype="<f4").tobytes()
+    if colliders:
+        req += struct.pack("<i", len(colliders)) + b"".join(bytes(c) for c in colliders)
     rep = _run(req, timeout)
     status, nb = struct.unpack_from("<2i", rep, 0)
     secs = struct.unpack_from("<d", rep, 8)[0]

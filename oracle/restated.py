@@ -25,7 +25,8 @@ class OracleParams(C.Structure):
                 ("dx", C.c_double), ("dt", C.c_double), ("gx", C.c_double), ("gy", C.c_double),
                 ("gz", C.c_double), ("E", C.c_double), ("nu", C.c_double), ("volume", C.c_double),
                 ("friction_deg", C.c_double), ("cohesion", C.c_double), ("beta", C.c_double),
-                ("hardening", C.c_double), ("theta_c", C.c_double), ("theta_s", C.c_double)]
+                ("hardening", C.c_double), ("theta_c", C.c_double), ("theta_s", C.c_double),
+                ("ncolliders", C.c_int), ("colliders", C.c_void_p)]
 
 
 _lib = None
@@ -85,13 +86,19 @@ class RunResult:
 
 
 def run(spec, particles, nsteps: int, precision: str = "f32", mode=None, table_expected=None,
-        cap_blocks: int = 1 << 16) -> RunResult:
-    """Runs the restated substep nsteps times on a copy of `particles`."""
+        cap_blocks: int = 1 << 16, colliders=()) -> RunResult:
+    """Runs the restated substep nsteps times on a copy of `particles`; `colliders` are
+    zsmpm_collider records (zsmpm_b200.colliders) applied after the walls."""
     dt = np.float32 if precision == "f32" else np.float64
     n = particles.n
     if table_expected is None:
         table_expected = max(n // 512, 64)
     prm = params_from_spec(spec, mode=mode, table_expected=table_expected)
+    cols = (C.c_char * (120 * max(len(colliders), 1)))()
+    for i, c in enumerate(colliders):
+        C.memmove(C.addressof(cols) + 120 * i, C.addressof(c), 120)
+    prm.ncolliders = len(colliders)
+    prm.colliders = C.addressof(cols)
     m = particles.m.astype(dt)
     x = particles.x.astype(dt).copy()
     v = particles.v.astype(dt).copy()

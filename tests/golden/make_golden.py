@@ -8,6 +8,8 @@ reference itself on seeded synthetic inputs:
   ref_svd.npz                               math::svd_3d on 256 matrices
   ref_stress.npz                            compute_stress_fixedcorotated / _sand on 256 F
   ref_activation.npz                        ComputeSparsity + EnlargeSparsity keys and slots
+  ref_colliders_fc.npz / ref_colliders_dp.npz 5 substeps with four moving analytic colliders
+                                            (Collider<AnalyticLevelSet<...>>) after slip walls
   ref_implicit_fc.npz / ref_implicit_dp.npz G2P2GTransfer, ImplicitMPMSystem's multiply /
                                             project / precondition and ConjugateGradient::solve
                                             on a small state with a smooth grid velocity field
@@ -71,6 +73,7 @@ def main() -> None:
                         slots=slots, nparblocks=npb, table_size=ts)
     for model, name in ((0, "fc"), (1, "dp")):
         make_implicit(model, HERE / f"ref_implicit_{name}.npz")
+        make_colliders(model, HERE / f"ref_colliders_{name}.npz")
     print("wrote", sorted(f.name for f in HERE.glob("*.npz")))
 
 
@@ -115,3 +118,32 @@ def make_implicit(model: int, path: Path, dt: float = 1e-3, cg_iters: int = 20) 
 
 if __name__ == "__main__":
     main()
+
+
+def collider_set():
+    """One moving collider of each shape and every collision type, placed in the small scene's
+    path: a translating sphere (slip), a rotating, growing box (separate), a sticky cylinder
+    and a separating plane."""
+    from zsmpm_b200 import colliders as col
+    R = col.rotation((1, 1, 0), 0.3)
+    return [col.sphere((0.52, 0.46, 0.5), 0.03, "slip", t=(0.0, 0.0, 0.001), dtdt=(0.0, 0.5, 0.0)),
+            col.cuboid((-0.02, -0.01, -0.02), (0.02, 0.01, 0.02), "separate", R=R, t=(0.47, 0.52, 0.5),
+                       omega=(0, 0, 3.0), s=1.2, dsdt=0.1),
+            col.cylinder((0.5, 0.45, 0.53), 0.01, 0.05, 1, "sticky", dtdt=(0.1, 0, 0)),
+            col.plane((0.5, 0.475, 0.5), (0.0, 1.0, 0.0), "separate")]
+
+
+def collider_scene(model: int):
+    return scenes.small_scene(model=model, mode=1, velocity=(0.4, -0.6, 0.2), wall_type=1)
+
+
+def make_colliders(model: int, path: Path, steps: int = 5) -> None:
+    spec = collider_scene(model)
+    p = scenes.generate(spec)
+    cols = collider_set()
+    r = reference.run(spec, p, steps, policy=reference.POLICY_SEQ, colliders=cols)
+    assert r.status == 0
+    raw = np.frombuffer(b"".join(bytes(c) for c in cols), np.uint8)
+    np.savez_compressed(path, m=p.m, x0=p.x, v0=p.v, C0=p.C, F0=p.F, plastic0=p.plastic, colliders=raw,
+                        x=r.x, v=r.v, C=r.C, F=r.F, logJp=r.logJp, keys=r.keys, grid=r.grid, steps=steps,
+                        model=model)

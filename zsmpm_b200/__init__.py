@@ -156,6 +156,14 @@ class Scene:
         _abi.check(self._lib.zsmpm_scene_download(self._h, C.byref(arrs), 1, C.c_void_p(stream)),
                    "scene_download")
 
+    # ---- colliders
+    def set_colliders(self, colliders, stream: int = 0) -> None:
+        """Analytic colliders (zsmpm_b200.colliders) applied after the walls, in list order."""
+        from . import colliders as col
+        arr = col.array(list(colliders))
+        _abi.check(self._lib.zsmpm_scene_set_colliders(self._h, arr, len(colliders), C.c_void_p(stream)),
+                   "scene_set_colliders")
+
     # ---- stages
     def activate_blocks(self, stream: int = 0):
         _abi.check(self._lib.zsmpm_activate_blocks(self._h, C.c_void_p(stream)), "activate_blocks")

@@ -85,6 +85,17 @@ class ClosureAudit(C.Structure):
                 ("fallbacks", C.c_int64)]
 
 
+class Collider(C.Structure):
+    """zsmpm_collider: Collider<AnalyticLevelSet<shape, f32, 3>> (geometry/Collider.h)."""
+    _fields_ = [("shape", C.c_int32), ("type", C.c_int32), ("axis", C.c_int32), ("reserved", C.c_int32),
+                ("a", C.c_float * 3), ("b", C.c_float * 3), ("s", C.c_float), ("dsdt", C.c_float),
+                ("R", C.c_float * 9), ("omega", C.c_float * 3), ("t", C.c_float * 3), ("dtdt", C.c_float * 3)]
+
+
+SHAPE_PLANE, SHAPE_CUBOID, SHAPE_SPHERE, SHAPE_CYLINDER = 0, 1, 2, 3
+MAX_COLLIDERS = 16
+
+
 class CgOptions(C.Structure):
     _fields_ = [("max_iters", C.c_int32), ("tol", C.c_float), ("rel_tol", C.c_float)]
 
@@ -122,6 +133,7 @@ SIGNATURES = {
     "zsmpm_kernels_per_substep": (C.c_int32, [_P]),
     "zsmpm_svd3": (_S, [_P, _P, _P, _P, C.c_int64, _P]),
     "zsmpm_constitutive": (_S, [C.POINTER(Material), _P, _P, _P, C.c_int64, _P]),
+    "zsmpm_scene_set_colliders": (_S, [_P, _P, C.c_int32, _P]),
     "zsmpm_g2p2g": (_S, [_P, _P, _P, C.c_int64, C.c_float, _P]),
     "zsmpm_implicit_multiply": (_S, [_P, _P, _P, C.c_int64, C.c_float, _P]),
     "zsmpm_implicit_project": (_S, [_P, _P, C.c_int64, _P]),

@@ -344,7 +344,51 @@ ZSMPM_API zsmpm_status zsmpm_scene_create(const zsmpm_scene_desc *desc, zsmpm_sc
     delete s;
     return cuda_fail(e, "kernel attributes");
   }
+  {
+    collider_dev *cols = nullptr;
+    int *ncol = nullptr;
+    zsmpm_status st = dev_alloc(s, &cols, kMaxColliders, "colliders");
+    if (st == ZSMPM_OK) st = dev_alloc(s, &ncol, 1, "collider count");
+    if (st == ZSMPM_OK && cudaMemset(ncol, 0, sizeof(int)) != cudaSuccess) st = fail(ZSMPM_ERR_CUDA, "collider count");
+    if (st != ZSMPM_OK) {
+      release(s);
+      delete s;
+      return st;
+    }
+    p.colliders = cols;
+    p.ncolliders = ncol;
+  }
   *out = s;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_set_colliders(zsmpm_scene *s, const zsmpm_collider *colliders, int32_t count,
+                                                 void *stream) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (s->nscenes > 0) return fail(ZSMPM_ERR_INVALID_ARG, "colliders apply to single scenes");
+  if (count < 0 || count > kMaxColliders) return fail(ZSMPM_ERR_INVALID_ARG, "at most ZSMPM_MAX_COLLIDERS colliders");
+  if (count > 0 && !colliders) return fail(ZSMPM_ERR_INVALID_ARG, "null colliders");
+  static_assert(sizeof(collider_dev) == sizeof(zsmpm_collider), "collider layouts differ");
+  std::vector<collider_dev> host(count > 0 ? count : 1);
+  for (int k = 0; k < count; ++k) {
+    const zsmpm_collider &c = colliders[k];
+    if (c.shape < 0 || c.shape > 3) return fail(ZSMPM_ERR_INVALID_ARG, "unknown collider shape");
+    if (c.type < 0 || c.type > 2) return fail(ZSMPM_ERR_INVALID_ARG, "collider type must be sticky, slip or separate");
+    if (c.shape == ZSMPM_SHAPE_CYLINDER && (c.axis < 0 || c.axis > 2))
+      return fail(ZSMPM_ERR_INVALID_ARG, "cylinder axis must be 0, 1 or 2");
+    if (!(c.s != 0.f) || !std::isfinite(c.s)) return fail(ZSMPM_ERR_INVALID_ARG, "collider scale must be finite and non-zero");
+    std::memcpy(&host[k], &c, sizeof(collider_dev));
+  }
+  cudaStream_t cs = as_stream(stream);
+  if (count > 0)
+    ZS_TRY(cudaMemcpyAsync(const_cast<collider_dev *>(s->dev.prm.colliders), host.data(), sizeof(collider_dev) * count,
+                           cudaMemcpyHostToDevice, cs),
+           "colliders");
+  ZS_TRY(cudaMemcpyAsync(const_cast<int *>(s->dev.prm.ncolliders), &count, sizeof(int), cudaMemcpyHostToDevice, cs),
+         "collider count");
+  // the host copies are local: wait for the copies before they go out of scope
+  ZS_TRY(cudaStreamSynchronize(cs), "colliders");
   return ZSMPM_OK;
 }
 

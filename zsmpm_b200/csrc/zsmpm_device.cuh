@@ -271,6 +271,157 @@ struct material_dev {
   float friction_deg;   // Drucker-Prager friction angle (a feature of the learned closure)
 };
 
+// Collider<AnalyticLevelSet<shape, f32, 3>> (geometry/Collider.h:10-200); the same layout as
+// zsmpm_collider
+struct collider_dev {
+  int shape, type, axis, reserved;
+  float a[3], b[3];
+  float s, dsdt;
+  float R[9];  // row-major
+  float omega[3], t[3], dtdt[3];
+};
+constexpr int kMaxColliders = 16;
+
+// signed distance of the analytic level sets (geometry/AnalyticLevelSet.h), in its order of
+// operations
+__device__ __forceinline__ float collider_sdf(const collider_dev &c, const float X[3]) {
+  if (c.shape == 0) {  // Plane: n . (x - origin)
+    float r = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) r += c.b[i] * (X[i] - c.a[i]);
+    return r;
+  }
+  if (c.shape == 1) {  // Cuboid
+    float p[3], mx;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float center = (c.a[i] + c.b[i]) / 2.f;
+      const float d = X[i] - center;
+      p[i] = (d > 0.f ? d : -d) - (c.b[i] - c.a[i]) / 2.f;
+    }
+    mx = p[0];
+    if (p[1] > mx) mx = p[1];
+    if (p[2] > mx) mx = p[2];
+    float l2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (p[i] < 0.f) p[i] = 0.f;
+      l2 += p[i] * p[i];
+    }
+    return (mx < 0.f ? mx : 0.f) + sqrtf(l2);
+  }
+  if (c.shape == 2) {  // Sphere: |x - c| - r
+    float l2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) l2 += (X[i] - c.a[i]) * (X[i] - c.a[i]);
+    return sqrtf(l2) - c.b[0];
+  }
+  // Cylinder along axis d from a, radius b[0], length b[1]
+  const int d = c.axis;
+  float l2 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    if (k != d) l2 += (X[k] - c.a[k]) * (X[k] - c.a[k]);
+  const float dis_r = sqrtf(l2), radius = c.b[0], length = c.b[1];
+  const bool outside = dis_r > radius;
+  const float xd = X[d], bd = c.a[d];
+  if (xd < bd) {
+    const float dis_l = bd - xd;
+    return outside ? sqrtf((dis_r - radius) * (dis_r - radius) + dis_l * dis_l) : dis_l;
+  }
+  if (xd > bd + length) {
+    const float dis_l = xd - (bd + length);
+    return outside ? sqrtf((dis_r - radius) * (dis_r - radius) + dis_l * dis_l) : dis_l;
+  }
+  if (outside) return dis_r - radius;
+  const float dis_l = fminf(bd + length - xd, xd - bd);
+  return -fminf(dis_l, radius - dis_r);
+}
+
+// material-space normal: the plane's normal as given, the sphere's outward direction (zero
+// within 1e-7 of the center), a central difference with eps = 1e-6 for cuboid and cylinder
+__device__ __forceinline__ void collider_normal(const collider_dev &c, const float X[3], float n[3]) {
+  if (c.shape == 0) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) n[i] = c.b[i];
+    return;
+  }
+  if (c.shape == 2) {
+    float l2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      n[i] = X[i] - c.a[i];
+      l2 += n[i] * n[i];
+    }
+    if (l2 < 1e-7f) {
+      n[0] = n[1] = n[2] = 0.f;
+      return;
+    }
+    const float len = sqrtf(l2);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) n[i] = n[i] / len;
+    return;
+  }
+  const float eps = 1e-6f;
+  float l2 = 0.f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float v1[3] = {X[0], X[1], X[2]}, v2[3] = {X[0], X[1], X[2]};
+    v1[i] = X[i] + eps;
+    v2[i] = X[i] - eps;
+    n[i] = (collider_sdf(c, v1) - collider_sdf(c, v2)) / (eps + eps);
+    l2 += n[i] * n[i];
+  }
+  const float len = sqrtf(l2);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) n[i] = n[i] / len;
+}
+
+// Collider::resolveCollision (Collider.h:80-110) with erosion 0
+__device__ __forceinline__ void collider_resolve(const collider_dev &c, const float x[3], float v[3]) {
+  const float xb[3] = {x[0] - c.t[0], x[1] - c.t[1], x[2] - c.t[2]};
+  const float inv_s = 1.f / c.s;
+  float X[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float r = 0.f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r += c.R[3 * j + i] * xb[j];  // R^T (x - b)
+    X[i] = r * inv_s;
+  }
+  if (!(collider_sdf(c, X) < -0.f)) return;
+  const float ds = c.dsdt * inv_s;
+  const float vo[3] = {c.omega[1] * xb[2] - c.omega[2] * xb[1] + ds * xb[0] + c.dtdt[0],
+                       c.omega[2] * xb[0] - c.omega[0] * xb[2] + ds * xb[1] + c.dtdt[1],
+                       c.omega[0] * xb[1] - c.omega[1] * xb[0] + ds * xb[2] + c.dtdt[2]};
+  if (c.type == 0) {
+    v[0] = vo[0];
+    v[1] = vo[1];
+    v[2] = vo[2];
+    return;
+  }
+  float nX[3], n[3];
+  collider_normal(c, X, nX);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float r = 0.f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r += c.R[3 * i + j] * nX[j];
+    n[i] = r;
+  }
+  float rel[3], proj = 0.f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    rel[i] = v[i] - vo[i];
+    proj += n[i] * rel[i];
+  }
+  if ((c.type == 2 && proj < 0.f) || c.type == 1)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) rel[i] -= proj * n[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) v[i] = rel[i] + vo[i];
+}
+
 // out[3c+r] = sum_k M[3k+r] d[k] N[3k+c]
 __device__ __forceinline__ void mul_diag_t(float *out, const float *M, const float *d,
                                            const float *N) {

@@ -70,6 +70,9 @@ struct scene_params {
   int nscenes;
   const material_dev *mats;         // [nscenes] per-scene materials (device)
   const int *scene_start;           // [nscenes + 1] upload-index ranges of the scenes (device)
+  // colliders after the walls (device; the count is read at run time, so updates need no new graph)
+  const collider_dev *colliders;
+  const int *ncolliders;
   // launch shapes (set by the autotuner; 0 = default)
   int g2p_threads;                  // 128 or 256
   int g2p_ctas_per_sm, p2g_ctas_per_sm;
