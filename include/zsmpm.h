@@ -301,6 +301,36 @@ typedef struct {
 ZSMPM_API zsmpm_status zsmpm_scene_set_colliders(zsmpm_scene *scene, const zsmpm_collider *colliders,
                                                  int32_t count, void *stream);
 
+/* LevelSetBoundary<SparseLevelSet<3>> (geometry/Collider.h:204-236 applied by
+ * ApplyBoundaryConditionOnGridBlocks, simulation/grid/GridOp.hpp:32-36, :126-134): a signed
+ * distance sampled on 8^3 blocks, read by trilinear interpolation
+ * (geometry/SparseLevelSet.hpp:660-690, 803-930), with `background` outside the blocks.  A world
+ * position x maps to index space by X = ((x - t) Rinv) Sinv, row vectors times row-major
+ * matrices, the SparseLevelSet's _i2wT, _i2wRinv and _i2wSinv (SparseLevelSet.hpp:366-374); the
+ * node at integer index coordinate c holds sdf[block][(c & 7) as x*64 + y*8 + z] of the block
+ * whose origin (a multiple of 8 per axis) is c - (c & 7).  Nodes with positive grid mass inside
+ * (distance < 0) are made still (sticky), or lose the normal part of their velocity (slip; separate
+ * only when moving into it), with the normal from central differences (eps 1e-6) of the distance. */
+typedef struct {
+  int32_t nblocks;
+  int32_t type;         /* ZSMPM_WALL_STICKY, ZSMPM_WALL_SLIP or ZSMPM_WALL_SEPARATE */
+  const int32_t *keys;  /* host [nblocks][3] block origins, distinct multiples of 8 */
+  const float *sdf;     /* host [nblocks][512] */
+  float background;     /* the distance outside the blocks (SparseLevelSet::_backgroundValue) */
+  float sinv[9], rinv[9], t[3];
+} zsmpm_levelset_desc;
+
+#define ZSMPM_MAX_LEVELSETS 4
+
+/* Adds a sparse level-set boundary, applied after the scene's walls and colliders in the order
+ * added.  The block map spans the keys' bounding box and holds at most 2^22 blocks.  The call
+ * copies the data to the device and synchronises `stream`.  Single scenes only. */
+ZSMPM_API zsmpm_status zsmpm_scene_add_levelset(zsmpm_scene *scene, const zsmpm_levelset_desc *desc,
+                                                void *stream);
+/* Removes every level-set boundary of the scene and frees their device data (synchronises the
+ * device). */
+ZSMPM_API zsmpm_status zsmpm_scene_clear_levelsets(zsmpm_scene *scene);
+
 /* ---- the implicit system (simulation/mpm/ImplicitMPM.hpp) ---------------------------- */
 /* Grid dof vectors are device arrays of `ndofs` floats, node-major over the active blocks in
  * canonical order: entry (block*512 + cell)*3 + d, cell = x*64 + y*8 + z inside the block.

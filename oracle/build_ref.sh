@@ -4,9 +4,10 @@
 # driven by oracle/ref_driver.cpp and oracle/ref_cli.cpp.  The output is the checker and the CPU baseline, never the product.
 #
 # zpc's CMake build needs the zpc_tpls submodule, which is not checked out, so the needed
-# translation units are compiled directly with g++.  Four reference headers do not parse
+# translation units are compiled directly with g++.  Several reference headers do not parse
 # with g++ 13 because a dependent member template is named without the `template`
-# keyword, and G2P2G.hpp calls the CUDA-only two-argument atomicAdd; for those, patched
+# keyword (or call a member of a dependent base without this->), and G2P2G.hpp calls the
+# CUDA-only two-argument atomicAdd; for those, patched
 # copies are written under oracle/_ref/patched (searched before the reference tree).
 # No patch touches arithmetic:
 #   ZpcAsync.hpp                        _storage[i].data<T>()  -> .template data<T>()
@@ -17,10 +18,10 @@
 #   simulation/transfer/G2P2G.hpp       atomicAdd(&r, v) -> atomic_add(wrapv<space>{}, &r, v),
 #                                       the exec-space atomic that P2G.hpp uses (a plain add
 #                                       under seq_exec)
-#   geometry/AnalyticLevelSet.h         getSignedDistance(..) -> this->getSignedDistance(..)
-#                                       in the finite-difference normals (a member of the
+#   geometry/AnalyticLevelSet.h,        getSignedDistance(..) -> this->getSignedDistance(..)
+#   geometry/SparseLevelSet.hpp         in the finite-difference normals (a member of the
 #                                       CRTP base); the other geometry headers are linked beside
-#                                       it so that their relative includes find the patched copy
+#                                       them so that their relative includes find the patched copies
 # Logging (plog) and magic_enum are replaced by the small shims in oracle/ref_shims.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -48,10 +49,14 @@ ln -sf "$REF/zensim/simulation/transfer/Scheme.hpp" "$OUT/patched/zensim/simulat
 ln -sf "$REF/zensim/types/Property.h" "$OUT/patched/zensim/types/Property.h"
 mkdir -p "$OUT/patched/zensim/geometry"
 for f in "$REF"/zensim/geometry/*; do
-  [ "$(basename "$f")" = "AnalyticLevelSet.h" ] || ln -sfn "$f" "$OUT/patched/zensim/geometry/$(basename "$f")"
+  case "$(basename "$f")" in
+    AnalyticLevelSet.h | SparseLevelSet.hpp)
+      rm -f "$OUT/patched/zensim/geometry/$(basename "$f")"
+      sed -E 's/\(getSignedDistance\(/(this->getSignedDistance(/g; s/- getSignedDistance\(/- this->getSignedDistance(/g' \
+        "$f" > "$OUT/patched/zensim/geometry/$(basename "$f")" ;;
+    *) ln -sfn "$f" "$OUT/patched/zensim/geometry/$(basename "$f")" ;;
+  esac
 done
-sed -E 's/\(getSignedDistance\(/(this->getSignedDistance(/g; s/- getSignedDistance\(/- this->getSignedDistance(/g' \
-  "$REF/zensim/geometry/AnalyticLevelSet.h" > "$OUT/patched/zensim/geometry/AnalyticLevelSet.h"
 
 CXXFLAGS=(-std=c++17 -O2 -fPIC -fopenmp -ffp-contract=off -include cstdint -include utility
   -DZS_ENABLE_OPENMP=1 -DZS_ENABLE_CUDA=0 -DZS_ENABLE_MUSA=0 -DZS_ENABLE_SYCL=0

@@ -22,6 +22,9 @@
  *   grid update        simulation/grid/GridOp.hpp:72-164, geometry/Collider.h:80-110
  *   colliders          geometry/Collider.h:10-200, geometry/AnalyticLevelSet.h (plane, cuboid,
  *                      sphere, cylinder), math/VecInterface.hpp (vector operation order)
+ *   level-set boundary geometry/SparseLevelSet.hpp:366-374 (worldToIndex), :477-484 (value_or),
+ *                      :736-752 (distance, normal), :862-875 (linear arena),
+ *                      math/VecInterface.hpp:1043-1049 (xlerp), ZpcMathUtils.hpp:1779-1781
  *   G2P                simulation/transfer/G2P.hpp:43-84, math/matrix/MatrixUtils.h:136-146
  *   G2P2G              simulation/transfer/G2P2G.hpp:49-142 (implicit force operator)
  * Matrices are column-major (M(i,j) = M[3j+i]) as in the reference.
@@ -51,6 +54,16 @@ typedef struct {
   float omega[3], t[3], dtdt[3];
 } oracle_collider;
 
+/* LevelSetBoundary<SparseLevelSet<3>>: block origins (multiples of 8), 512 distances per block
+ * (cell x*64 + y*8 + z), the background value and the world-to-index transform
+ * X = ((x - t) rinv) sinv (row vectors, row-major matrices). */
+typedef struct {
+  int nblocks, type;
+  float background, sinv[9], rinv[9], t[3];
+  const int32_t *keys;
+  const float *sdf;
+} oracle_levelset;
+
 typedef struct {
   int model;             /* ORACLE_FC / ORACLE_DP / ORACLE_SNOW */
   int mode;              /* ORACLE_MODE_COMMITTED or ORACLE_MODE_REFERENCE */
@@ -63,6 +76,8 @@ typedef struct {
   double hardening, theta_c, theta_s;       /* snow */
   int ncolliders;                           /* applied after the walls, in order */
   const oracle_collider *colliders;
+  int nlevelsets;                           /* applied after the colliders, in order */
+  const oracle_levelset *levelsets;
 } oracle_params;
 
 /* Runs nsteps substeps on SoA/AoS host arrays in place (x, v: 3n; C, F: 9n column-major;

@@ -301,6 +301,70 @@ static void OR_NAME(col_resolve)(const oracle_collider *c, const R *x, R *v) {
   for (int i = 0; i != 3; ++i) v[i] += vo[i];
 }
 
+/* ---- sparse level-set boundary: value_or over the blocks (a linear search of the keys; the
+ * reference queries its bht), the linear arena with base_node<0> = floor and xlerp with
+ * linear_interop(a, b, t) = a + (b - a) t */
+static R OR_NAME(ls_node)(const oracle_levelset *L, int32_t cx, int32_t cy, int32_t cz) {
+  const int32_t lx = cx & 7, ly = cy & 7, lz = cz & 7;
+  const int32_t bx = cx - lx, by = cy - ly, bz = cz - lz;
+  for (int b = 0; b != L->nblocks; ++b)
+    if (L->keys[3 * b] == bx && L->keys[3 * b + 1] == by && L->keys[3 * b + 2] == bz)
+      return (R)L->sdf[(size_t)b * 512 + ((lx << 6) | (ly << 3) | lz)];
+  return (R)L->background;
+}
+
+static R OR_NAME(ls_lerp)(R t, R a, R b) { return a + (b - a) * t; }
+
+static R OR_NAME(ls_sdf)(const oracle_levelset *L, const R *x) {
+  R a[3], b[3], X[3], d[3], p[2][2][2];
+  int32_t c[3];
+  for (int i = 0; i != 3; ++i) a[i] = x[i] - (R)L->t[i];
+  for (int j = 0; j != 3; ++j) {
+    R r = 0;
+    for (int i = 0; i != 3; ++i) r += (R)L->rinv[3 * i + j] * a[i];
+    b[j] = r;
+  }
+  for (int j = 0; j != 3; ++j) {
+    R r = 0;
+    for (int i = 0; i != 3; ++i) r += (R)L->sinv[3 * i + j] * b[i];
+    X[j] = r;
+  }
+  for (int k = 0; k != 3; ++k) {
+    c[k] = (int32_t)R_FLOOR(X[k]);
+    d[k] = X[k] - (R)c[k];
+  }
+  for (int i = 0; i != 2; ++i)
+    for (int j = 0; j != 2; ++j)
+      for (int k = 0; k != 2; ++k) p[i][j][k] = OR_NAME(ls_node)(L, c[0] + i, c[1] + j, c[2] + k);
+  return OR_NAME(ls_lerp)(
+      d[0],
+      OR_NAME(ls_lerp)(d[1], OR_NAME(ls_lerp)(d[2], p[0][0][0], p[0][0][1]), OR_NAME(ls_lerp)(d[2], p[0][1][0], p[0][1][1])),
+      OR_NAME(ls_lerp)(d[1], OR_NAME(ls_lerp)(d[2], p[1][0][0], p[1][0][1]), OR_NAME(ls_lerp)(d[2], p[1][1][0], p[1][1][1])));
+}
+
+/* Collider{levelset, type}.resolveCollision with the identity placement: the collider velocity
+ * is zero (the level set has no material-velocity channel) */
+static void OR_NAME(ls_resolve)(const oracle_levelset *L, const R *x, R *v) {
+  if (!(OR_NAME(ls_sdf)(L, x) < -(R)0)) return;
+  if (L->type == 0) {
+    for (int i = 0; i != 3; ++i) v[i] = 0;
+    return;
+  }
+  const R eps = (R)1e-6;
+  R n[3], proj = 0;
+  for (int i = 0; i != 3; ++i) {
+    R v1[3] = {x[0], x[1], x[2]}, v2[3] = {x[0], x[1], x[2]};
+    v1[i] = x[i] + eps;
+    v2[i] = x[i] - eps;
+    n[i] = (OR_NAME(ls_sdf)(L, v1) - OR_NAME(ls_sdf)(L, v2)) / (eps + eps);
+  }
+  const R len = OR_NAME(col_len)(n);
+  for (int i = 0; i != 3; ++i) n[i] = n[i] / len;
+  for (int i = 0; i != 3; ++i) proj += n[i] * v[i];
+  if ((L->type == 2 && proj < 0) || L->type == 1)
+    for (int i = 0; i != 3; ++i) v[i] -= proj * n[i];
+}
+
 /* quadratic B-spline stencil (Utils.hpp:30-70, InterpolationKernel.hpp:51-57, :93-130) */
 typedef struct {
   int corner[3];
@@ -480,6 +544,23 @@ int OR_NAME(oracle_run)(const oracle_params *p, int n, const R *m, R *x, R *v, R
             vel[d] = g[(1 + d) * 512 + cell];
           }
           OR_NAME(col_resolve)(&p->colliders[k], pos, vel);
+          for (int d = 0; d != 3; ++d) g[(1 + d) * 512 + cell] = vel[d];
+        }
+      }
+    /* then the sparse level sets */
+    for (int k = 0; k != p->nlevelsets; ++k)
+      for (int b = 0; b != nb; ++b) {
+        R *g = &grid[(size_t)b * 7 * 512];
+        const int32_t *key = &t.active[3 * b];
+        for (int cell = 0; cell != 512; ++cell) {
+          if (!(g[cell] > 0)) continue;
+          const int cc[3] = {cell >> 6, (cell >> 3) & 7, cell & 7};
+          R pos[3], vel[3];
+          for (int d = 0; d != 3; ++d) {
+            pos[d] = ((R)key[d] * (R)8 + (R)cc[d]) * dx;
+            vel[d] = g[(1 + d) * 512 + cell];
+          }
+          OR_NAME(ls_resolve)(&p->levelsets[k], pos, vel);
           for (int d = 0; d != 3; ++d) g[(1 + d) * 512 + cell] = vel[d];
         }
       }

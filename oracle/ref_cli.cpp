@@ -24,6 +24,10 @@
 //     reply:     int32 status, f64 seconds, then (status == 0) f32 f[1536*nb]
 //   8 run with colliders: as 1, then int32 ncolliders and ncolliders zsmpm_collider records
 //     reply:     as 1
+//   9 run with colliders and sparse level sets: as 8, then int32 nlevelsets and per level set
+//                int32 nblocks, type, f32 background, sinv[9], rinv[9], t[3],
+//                int32 keys[3*nblocks], f32 sdf[512*nblocks]
+//     reply:     as 1
 //   7 implicit:  zsref_params, int32 op, n, nb, max_iters, f32 tol, rel_tol,
 //                f32 m[n], x[3n], v[3n], C[9n], F[9n], logJp[n], int32 keys[3*nb],
 //                f32 a[1536*nb], b[1536*nb]
@@ -46,7 +50,15 @@ int zsref_run(const zsref_params *p, int n, float *m, float *x, float *v, float 
               float *out_grid, double *out_seconds);
 int zsref_run_colliders(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
                         float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
-                        float *out_grid, double *out_seconds, int ncolliders, const void *colliders);
+                        float *out_grid, double *out_seconds, int ncolliders, const void *colliders,
+                        int nlevelsets, const void *levelsets);
+// the driver's ref_levelset record
+struct ref_levelset_rec {
+  int nblocks, type;
+  float background, sinv[9], rinv[9], t[3];
+  const int *keys;
+  const float *sdf;
+};
 void zsref_stress(int model, float volume, float E, float nu, float friction_deg,
                   float cohesion, float beta, int volume_correction, float *F, float *logJp,
                   float *PF);
@@ -97,7 +109,7 @@ int main(int argc, char **argv) {
   out_f = std::fopen(argv[2], "wb");
   if (!in_f || !out_f) return 2;
   const int cmd = rd<int32_t>();
-  if (cmd == 1 || cmd == 8) {
+  if (cmd == 1 || cmd == 8 || cmd == 9) {
     auto p = rd<zsref_params>();
     const int n = rd<int32_t>(), nsteps = rd<int32_t>(), cap = rd<int32_t>();
     std::vector<float> m, x, v, C, F, lj;
@@ -109,9 +121,32 @@ int main(int argc, char **argv) {
     rdv(lj, n);
     int ncol = 0;
     std::vector<unsigned char> cols;
-    if (cmd == 8) {
+    if (cmd == 8 || cmd == 9) {
       ncol = rd<int32_t>();
       rdv(cols, (size_t)ncol * 120);  // 4 int32 + 26 float32 per collider
+    }
+    int nls = 0;
+    std::vector<ref_levelset_rec> lss;
+    std::vector<std::vector<int>> ls_keys;
+    std::vector<std::vector<float>> ls_sdf;
+    if (cmd == 9) {
+      nls = rd<int32_t>();
+      lss.resize(nls);
+      ls_keys.resize(nls);
+      ls_sdf.resize(nls);
+      for (int k = 0; k < nls; ++k) {
+        ref_levelset_rec &L = lss[k];
+        L.nblocks = rd<int32_t>();
+        L.type = rd<int32_t>();
+        L.background = rd<float>();
+        for (float &f : L.sinv) f = rd<float>();
+        for (float &f : L.rinv) f = rd<float>();
+        for (float &f : L.t) f = rd<float>();
+        rdv(ls_keys[k], 3 * (size_t)L.nblocks);
+        rdv(ls_sdf[k], 512 * (size_t)L.nblocks);
+        L.keys = ls_keys[k].data();
+        L.sdf = ls_sdf[k].data();
+      }
     }
     std::vector<int> keys(3 * (size_t)cap);
     std::vector<float> grid((size_t)cap * 4 * 512);
@@ -119,7 +154,7 @@ int main(int argc, char **argv) {
     double secs = 0;
     int st = zsref_run_colliders(&p, n, m.data(), x.data(), v.data(), C.data(), F.data(), lj.data(),
                                  nsteps, cap, &nb, cap ? keys.data() : nullptr,
-                                 cap ? grid.data() : nullptr, &secs, ncol, cols.data());
+                                 cap ? grid.data() : nullptr, &secs, ncol, cols.data(), nls, lss.data());
     wr<int32_t>(st);
     wr<int32_t>(nb);
     wr<double>(secs);

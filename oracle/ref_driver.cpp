@@ -89,6 +89,47 @@ namespace {
     float omega[3], t[3], dtdt[3];
   };
 
+  // A SparseLevelSet<3> boundary: block origins (index space, multiples of 8), 512 "sdf" values
+  // per block in cell order x*64 + y*8 + z, the background value and the world-to-index
+  // transform X = ((x - t) Rinv) Sinv (row-vector products, matrices row-major).
+  struct ref_levelset {
+    int nblocks, type;
+    float background, sinv[9], rinv[9], t[3];
+    const int *keys;
+    const float *sdf;
+  };
+
+  // One ApplyBoundaryConditionOnGridBlocks launch with LevelSetBoundary<SparseLevelSet<3>>
+  // (Collider.h:204-236, GridOp.hpp:32-36, :126-134): the level set is built by the reference's
+  // own bht insert and grid storage, then sampled through its SparseLevelSetView.
+  template <class Pol, execspace_e space, class Table, class Grids>
+  void apply_levelset(Pol &pol, wrapv<space>, const ref_levelset &L, Table &table, Grids &grids, int nb) {
+    SparseLevelSet<3> ls{{{"sdf", 1}}, 1.f, (size_t)std::max(L.nblocks, 1), memsrc_e::host, -1};
+    {
+      auto tv = view<execspace_e::host>(ls._table);
+      for (int b = 0; b != L.nblocks; ++b)
+        tv.insert(vec<int, 3>{L.keys[3 * b], L.keys[3 * b + 1], L.keys[3 * b + 2]});
+      auto gv = proxy<execspace_e::host>({}, ls._grid);
+      for (int b = 0; b != L.nblocks; ++b) {
+        const auto bno = tv.query(vec<int, 3>{L.keys[3 * b], L.keys[3 * b + 1], L.keys[3 * b + 2]});
+        for (int c = 0; c != 512; ++c) gv(0, (size_t)bno, c) = L.sdf[(size_t)b * 512 + c];
+      }
+    }
+    for (int i = 0; i != 3; ++i) {
+      ls._i2wT[i] = L.t[i];
+      for (int j = 0; j != 3; ++j) {
+        ls._i2wSinv(i, j) = L.sinv[3 * i + j];
+        ls._i2wRinv(i, j) = L.rinv[3 * i + j];
+      }
+    }
+    ls._backgroundValue = L.background;
+    LevelSetBoundary<SparseLevelSet<3>> boundary{ls, L.type == 0   ? collider_e::Sticky
+                                                     : L.type == 1 ? collider_e::Slip
+                                                                   : collider_e::Separate};
+    pol(Collapse{(size_t)nb, (size_t)512},
+        ApplyBoundaryConditionOnGridBlocks{wrapv<space>{}, boundary, table, grids});
+  }
+
   // One ApplyBoundaryConditionOnGridBlocks launch (GridOp.hpp:113-158) with a
   // Collider<AnalyticLevelSet<shape, f32, 3>> (Collider.h:10-200) placed as described.
   template <class Pol, execspace_e space, class Table, class Grids>
@@ -199,7 +240,8 @@ struct zsref_params {
 // Returns 0 on success, 1 if the grid output capacity is too small, 2 if the table is full.
 int zsref_run_colliders(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
                         float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
-                        float *out_grid, double *out_seconds, int ncolliders, const void *colliders);
+                        float *out_grid, double *out_seconds, int ncolliders, const void *colliders,
+                        int nlevelsets = 0, const void *levelsets = nullptr);
 
 int zsref_run(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
               float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
@@ -208,12 +250,15 @@ int zsref_run(const zsref_params *p, int n, float *m, float *x, float *v, float 
                              out_seconds, 0, nullptr);
 }
 
-// zsref_run with `ncolliders` colliders (ref_collider records) applied after the walls, each
-// by its own ApplyBoundaryConditionOnGridBlocks launch.
+// zsref_run with `ncolliders` colliders (ref_collider records) and then `nlevelsets` sparse
+// level-set boundaries (ref_levelset records) applied after the walls, each by its own
+// ApplyBoundaryConditionOnGridBlocks launch.
 int zsref_run_colliders(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
                         float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
-                        float *out_grid, double *out_seconds, int ncolliders, const void *colliders) {
+                        float *out_grid, double *out_seconds, int ncolliders, const void *colliders,
+                        int nlevelsets, const void *levelsets) {
   const ref_collider *cols = static_cast<const ref_collider *>(colliders);
+  const ref_levelset *lss = static_cast<const ref_levelset *>(levelsets);
   constexpr auto host = execspace_e::host;
   constexpr auto omp = execspace_e::openmp;
   particles_t pars{(size_t)n, memsrc_e::host, -1};
@@ -309,6 +354,7 @@ int zsref_run_colliders(const zsref_params *p, int n, float *m, float *x, float 
         pol(Collapse{(size_t)nb, (size_t)512},
             ApplyBoundaryConditionOnGridBlocks{wrapv<space>{}, w, table, grids});
       for (int k = 0; k < ncolliders; ++k) apply_collider(pol, wrapv<space>{}, cols[k], table, grids, nb);
+      for (int k = 0; k < nlevelsets; ++k) apply_levelset(pol, wrapv<space>{}, lss[k], table, grids, nb);
       if (p->model == 0)
         pol(range((size_t)n), G2PTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{},
                                           p->dt, fc, grids, table, pars});

@@ -72,18 +72,30 @@ class RefResult:
 
 def run(spec, particles, nsteps: int, policy: int = POLICY_SEQ, threads: int = 0, order: int = 1,
         table_expected: int | None = None, cap_blocks: int = 1 << 15,
-        timeout: float = 600.0, colliders=()) -> RefResult:
+        timeout: float = 600.0, colliders=(), levelsets=()) -> RefResult:
     """`colliders`: zsmpm_collider records (ctypes), applied after the walls by the reference's
-    own Collider<AnalyticLevelSet<...>> launches."""
+    own Collider<AnalyticLevelSet<...>> launches; `levelsets`: LevelSet objects
+    (zsmpm_b200.colliders), applied after them as LevelSetBoundary<SparseLevelSet<3>>."""
     n = particles.n
     if table_expected is None:
         table_expected = max(n // 512, 64)
-    req = struct.pack("<i", 8 if colliders else 1) + _params_bytes(spec, policy, threads, order, table_expected)
+    cmd = 9 if levelsets else (8 if colliders else 1)
+    req = struct.pack("<i", cmd) + _params_bytes(spec, policy, threads, order, table_expected)
     req += struct.pack("<3i", n, nsteps, cap_blocks)
     for a in (particles.m, particles.x, particles.v, particles.C, particles.F, particles.plastic):
         req += np.ascontiguousarray(a, dtype="<f4").tobytes()
-    if colliders:
+    if cmd >= 8:
         req += struct.pack("<i", len(colliders)) + b"".join(bytes(c) for c in colliders)
+    if cmd == 9:
+        from zsmpm_b200.colliders import TYPES
+        req += struct.pack("<i", len(levelsets))
+        for L in levelsets:
+            keys = np.ascontiguousarray(L.keys, dtype="<i4").reshape(-1, 3)
+            kind = TYPES[L.kind] if isinstance(L.kind, str) else int(L.kind)
+            req += struct.pack("<iif", len(keys), kind, float(L.background))
+            for m in (L.sinv, L.rinv, L.t):
+                req += np.ascontiguousarray(m, dtype="<f4").reshape(-1).tobytes()
+            req += keys.tobytes() + np.ascontiguousarray(L.sdf, dtype="<f4").reshape(-1).tobytes()
     rep = _run(req, timeout)
     status, nb = struct.unpack_from("<2i", rep, 0)
     secs = struct.unpack_from("<d", rep, 8)[0]

@@ -26,7 +26,8 @@ class OracleParams(C.Structure):
                 ("gz", C.c_double), ("E", C.c_double), ("nu", C.c_double), ("volume", C.c_double),
                 ("friction_deg", C.c_double), ("cohesion", C.c_double), ("beta", C.c_double),
                 ("hardening", C.c_double), ("theta_c", C.c_double), ("theta_s", C.c_double),
-                ("ncolliders", C.c_int), ("colliders", C.c_void_p)]
+                ("ncolliders", C.c_int), ("colliders", C.c_void_p),
+                ("nlevelsets", C.c_int), ("levelsets", C.c_void_p)]
 
 
 _lib = None
@@ -74,6 +75,22 @@ def params_from_spec(spec, mode=None, table_expected=0) -> OracleParams:
                         hardening=m.hardening, theta_c=m.theta_c, theta_s=m.theta_s)
 
 
+def _abi_levelset_desc():
+    """oracle_levelset has the layout of zsmpm_levelset_desc with the pointers first."""
+    class OracleLevelSet(C.Structure):
+        _fields_ = [("nblocks", C.c_int), ("type", C.c_int), ("background", C.c_float),
+                    ("sinv", C.c_float * 9), ("rinv", C.c_float * 9), ("t", C.c_float * 3),
+                    ("keys", C.c_void_p), ("sdf", C.c_void_p)]
+
+        def __init__(self, d=None):
+            super().__init__()
+            if d is not None:
+                self.nblocks, self.type, self.background = d.nblocks, d.type, d.background
+                self.sinv[:], self.rinv[:], self.t[:] = d.sinv[:], d.rinv[:], d.t[:]
+                self.keys, self.sdf = d.keys, d.sdf
+    return OracleLevelSet
+
+
 @dataclass
 class RunResult:
     x: np.ndarray
@@ -86,9 +103,10 @@ class RunResult:
 
 
 def run(spec, particles, nsteps: int, precision: str = "f32", mode=None, table_expected=None,
-        cap_blocks: int = 1 << 16, colliders=()) -> RunResult:
+        cap_blocks: int = 1 << 16, colliders=(), levelsets=()) -> RunResult:
     """Runs the restated substep nsteps times on a copy of `particles`; `colliders` are
-    zsmpm_collider records (zsmpm_b200.colliders) applied after the walls."""
+    zsmpm_collider records and `levelsets` LevelSet objects (zsmpm_b200.colliders), applied
+    after the walls."""
     dt = np.float32 if precision == "f32" else np.float64
     n = particles.n
     if table_expected is None:
@@ -99,6 +117,12 @@ def run(spec, particles, nsteps: int, precision: str = "f32", mode=None, table_e
         C.memmove(C.addressof(cols) + 120 * i, C.addressof(c), 120)
     prm.ncolliders = len(colliders)
     prm.colliders = C.addressof(cols)
+    ls_cls = _abi_levelset_desc()
+    descs = (ls_cls * max(len(levelsets), 1))()
+    for i, L in enumerate(levelsets):
+        descs[i] = ls_cls(L.desc())
+    prm.nlevelsets = len(levelsets)
+    prm.levelsets = C.addressof(descs)
     m = particles.m.astype(dt)
     x = particles.x.astype(dt).copy()
     v = particles.v.astype(dt).copy()

@@ -10,6 +10,9 @@ reference itself on seeded synthetic inputs:
   ref_activation.npz                        ComputeSparsity + EnlargeSparsity keys and slots
   ref_colliders_fc.npz / ref_colliders_dp.npz 5 substeps with four moving analytic colliders
                                             (Collider<AnalyticLevelSet<...>>) after slip walls
+  ref_levelsets_fc.npz                      5 substeps with two sparse level-set boundaries
+                                            (LevelSetBoundary<SparseLevelSet<3>>), one rotated
+                                            and translated
   ref_implicit_fc.npz / ref_implicit_dp.npz G2P2GTransfer, ImplicitMPMSystem's multiply /
                                             project / precondition and ConjugateGradient::solve
                                             on a small state with a smooth grid velocity field
@@ -74,6 +77,7 @@ def main() -> None:
     for model, name in ((0, "fc"), (1, "dp")):
         make_implicit(model, HERE / f"ref_implicit_{name}.npz")
         make_colliders(model, HERE / f"ref_colliders_{name}.npz")
+    make_levelsets(0, HERE / "ref_levelsets_fc.npz")
     print("wrote", sorted(f.name for f in HERE.glob("*.npz")))
 
 
@@ -147,3 +151,34 @@ def make_colliders(model: int, path: Path, steps: int = 5) -> None:
     np.savez_compressed(path, m=p.m, x0=p.x, v0=p.v, C0=p.C, F0=p.F, plastic0=p.plastic, colliders=raw,
                         x=r.x, v=r.v, C=r.C, F=r.F, logJp=r.logJp, keys=r.keys, grid=r.grid, steps=steps,
                         model=model)
+
+
+def levelset_set(spec):
+    """A sphere of radius 0.025 (slip, voxel size dx) and a thin box rotated 0.4 rad about z and
+    shifted by 0.01 in x (separate), sampled as sparse level sets in the small scene's path."""
+    from zsmpm_b200 import colliders as col
+    ball = col.LevelSet.from_function(lambda x: np.linalg.norm(x - np.array([0.51, 0.465, 0.5]), axis=1) - 0.025,
+                                      (0.48, 0.435, 0.47), (0.54, 0.495, 0.53), spec.dx, "slip")
+
+    def box(x):
+        q = np.abs(x - np.array([0.5, 0.53, 0.5])) - np.array([0.03, 0.006, 0.03])
+        return np.linalg.norm(np.maximum(q, 0), axis=1) + np.minimum(q.max(1), 0)
+
+    slab = col.LevelSet.from_function(box, (0.46, 0.52, 0.46), (0.54, 0.54, 0.54), spec.dx, "separate",
+                                      rinv=col.rotation((0, 0, 1), 0.4), t=(0.01, 0.0, 0.0))
+    return [ball, slab]
+
+
+def make_levelsets(model: int, path: Path, steps: int = 5) -> None:
+    spec = collider_scene(model)
+    p = scenes.generate(spec)
+    ls = levelset_set(spec)
+    r = reference.run(spec, p, steps, policy=reference.POLICY_SEQ, levelsets=ls)
+    assert r.status == 0
+    extra = {}
+    for i, L in enumerate(ls):
+        extra.update({f"ls{i}_keys": L.keys, f"ls{i}_sdf": L.sdf, f"ls{i}_sinv": L.sinv, f"ls{i}_rinv": L.rinv,
+                      f"ls{i}_t": L.t, f"ls{i}_kind": L.kind, f"ls{i}_background": L.background})
+    np.savez_compressed(path, m=p.m, x0=p.x, v0=p.v, C0=p.C, F0=p.F, plastic0=p.plastic, x=r.x, v=r.v, C=r.C,
+                        F=r.F, logJp=r.logJp, keys=r.keys, grid=r.grid, steps=steps, model=model, nls=len(ls),
+                        **extra)

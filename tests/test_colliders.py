@@ -130,3 +130,77 @@ def test_set_colliders_rejects_bad_input(zs, gpu):
         sc.set_colliders([])
         sc.run(2)
         sc.status()
+
+
+# ------------------------------------------------------------------ sparse level sets
+def _levelset_fixture():
+    from zsmpm_b200.colliders import LevelSet
+    from zsmpm_b200.scenes import Particles
+    g = np.load(GOLDEN / "ref_levelsets_fc.npz")
+    ls = [LevelSet(keys=g[f"ls{i}_keys"], sdf=g[f"ls{i}_sdf"], kind=str(g[f"ls{i}_kind"]),
+                   background=float(g[f"ls{i}_background"]), sinv=g[f"ls{i}_sinv"], rinv=g[f"ls{i}_rinv"],
+                   t=g[f"ls{i}_t"]) for i in range(int(g["nls"]))]
+    p = Particles(m=g["m"], x=g["x0"], v=g["v0"], C=g["C0"], F=g["F0"], plastic=g["plastic0"])
+    return g, p, ls
+
+
+def test_restated_levelsets_bit_exact_with_reference():
+    """LevelSetBoundary<SparseLevelSet<3>> through the reference's own bht, grid storage and
+    SparseLevelSetView sampling, against the restated trilinear sampler."""
+    from oracle import restated
+    g, p, ls = _levelset_fixture()
+    spec = _spec(0)
+    o = restated.run(spec, p, int(g["steps"]), mode=1, levelsets=ls)
+    for k in ("x", "v", "C", "F"):
+        assert np.array_equal(getattr(o, k), g[k]), k
+    assert np.array_equal(o.grid, g["grid"])
+    free = restated.run(spec, p, int(g["steps"]), mode=1)
+    assert np.abs(free.v - g["v"]).max() > 0.1
+
+
+@pytest.mark.gpu
+def test_levelsets_match_reference(zs, gpu):
+    g, p, ls = _levelset_fixture()
+    spec = _spec(0)
+    with zs.Scene(spec, p) as sc:
+        for L in ls:
+            sc.add_levelset(L)
+        sc.run(int(g["steps"]))
+        sc.status()
+        out = sc.download()
+        keys, grid = sc.download_grid()
+    ex, ev = rel_l2(out.x, g["x"]), rel_l2(out.v, g["v"])
+    print(f"\nlevel sets: x {ex:.2e} v {ev:.2e}")
+    assert ex < 1e-6
+    assert ev < 1e-4
+    mg, pg = grid_mass_momentum(keys, grid)
+    mb, pb = grid_mass_momentum(g["keys"], g["grid"])
+    assert abs(mg - mb) / mb < 1e-6
+    assert np.linalg.norm(pg - pb) / np.linalg.norm(pb) < 1e-4
+
+
+@pytest.mark.gpu
+def test_levelsets_add_clear_and_reject(zs, gpu):
+    from zsmpm_b200.colliders import LevelSet
+    g, p, ls = _levelset_fixture()
+    spec = _spec(0)
+    with zs.Scene(spec, p) as sc:
+        bad = LevelSet(keys=ls[0].keys + 1, sdf=ls[0].sdf)
+        with pytest.raises(zs._abi.ZsmpmError):
+            sc.add_levelset(bad)  # keys must be block origins
+        dup = LevelSet(keys=np.concatenate([ls[0].keys[:2], ls[0].keys[:1]]), sdf=ls[0].sdf[:3])
+        with pytest.raises(zs._abi.ZsmpmError):
+            sc.add_levelset(dup)
+        for _ in range(4):
+            sc.add_levelset(ls[0])
+        with pytest.raises(zs._abi.ZsmpmError):
+            sc.add_levelset(ls[0])  # at most four
+        sc.clear_levelsets()
+        sc.run(2)
+        sc.status()
+        cleared = sc.download()
+    with zs.Scene(spec, p) as sc:
+        sc.run(2)
+        plain = sc.download()
+    # float atomics make two runs differ in the last bits; a level set left behind would not
+    assert rel_l2(cleared.v, plain.v) < 1e-6

@@ -164,6 +164,15 @@ class Scene:
         _abi.check(self._lib.zsmpm_scene_set_colliders(self._h, arr, len(colliders), C.c_void_p(stream)),
                    "scene_set_colliders")
 
+    def add_levelset(self, levelset, stream: int = 0) -> None:
+        """A sparse level-set boundary (zsmpm_b200.colliders.LevelSet), applied after the colliders."""
+        d = levelset.desc()
+        _abi.check(self._lib.zsmpm_scene_add_levelset(self._h, C.byref(d), C.c_void_p(stream)),
+                   "scene_add_levelset")
+
+    def clear_levelsets(self) -> None:
+        _abi.check(self._lib.zsmpm_scene_clear_levelsets(self._h), "scene_clear_levelsets")
+
     # ---- stages
     def activate_blocks(self, stream: int = 0):
         _abi.check(self._lib.zsmpm_activate_blocks(self._h, C.c_void_p(stream)), "activate_blocks")

@@ -92,6 +92,12 @@ class Collider(C.Structure):
                 ("R", C.c_float * 9), ("omega", C.c_float * 3), ("t", C.c_float * 3), ("dtdt", C.c_float * 3)]
 
 
+class LevelSetDesc(C.Structure):
+    """zsmpm_levelset_desc: LevelSetBoundary<SparseLevelSet<3>> data (host pointers)."""
+    _fields_ = [("nblocks", C.c_int32), ("type", C.c_int32), ("keys", C.c_void_p), ("sdf", C.c_void_p),
+                ("background", C.c_float), ("sinv", C.c_float * 9), ("rinv", C.c_float * 9), ("t", C.c_float * 3)]
+
+
 SHAPE_PLANE, SHAPE_CUBOID, SHAPE_SPHERE, SHAPE_CYLINDER = 0, 1, 2, 3
 MAX_COLLIDERS = 16
 
@@ -134,6 +140,8 @@ SIGNATURES = {
     "zsmpm_svd3": (_S, [_P, _P, _P, _P, C.c_int64, _P]),
     "zsmpm_constitutive": (_S, [C.POINTER(Material), _P, _P, _P, C.c_int64, _P]),
     "zsmpm_scene_set_colliders": (_S, [_P, _P, C.c_int32, _P]),
+    "zsmpm_scene_add_levelset": (_S, [_P, C.POINTER(LevelSetDesc), _P]),
+    "zsmpm_scene_clear_levelsets": (_S, [_P]),
     "zsmpm_g2p2g": (_S, [_P, _P, _P, C.c_int64, C.c_float, _P]),
     "zsmpm_implicit_multiply": (_S, [_P, _P, _P, C.c_int64, C.c_float, _P]),
     "zsmpm_implicit_project": (_S, [_P, _P, C.c_int64, _P]),

@@ -54,6 +54,9 @@ struct zsmpm_scene {
   float *cg_buf = nullptr;
   int64_t cg_cap = 0;
   cg_state *cg = nullptr;
+  // sparse level-set boundaries: their device maps and distances, freed by clear or destroy
+  int nlevelsets = 0;
+  std::vector<void *> levelset_buffers;
 };
 
 namespace {
@@ -246,6 +249,8 @@ void release(zsmpm_scene *s) {
     if (e) cudaEventDestroy(e);
   for (void *p : s->allocations) cudaFree(p);
   s->allocations.clear();
+  for (void *p : s->levelset_buffers) cudaFree(p);
+  s->levelset_buffers.clear();
 }
 
 void invalidate_graphs(zsmpm_scene *s) {
@@ -357,8 +362,94 @@ ZSMPM_API zsmpm_status zsmpm_scene_create(const zsmpm_scene_desc *desc, zsmpm_sc
     }
     p.colliders = cols;
     p.ncolliders = ncol;
+    levelset_dev *lss = nullptr;
+    int *nls = nullptr;
+    st = dev_alloc(s, &lss, kMaxLevelsets, "level sets");
+    if (st == ZSMPM_OK) st = dev_alloc(s, &nls, 1, "level-set count");
+    if (st == ZSMPM_OK && cudaMemset(nls, 0, sizeof(int)) != cudaSuccess) st = fail(ZSMPM_ERR_CUDA, "level-set count");
+    if (st != ZSMPM_OK) {
+      release(s);
+      delete s;
+      return st;
+    }
+    p.levelsets = lss;
+    p.nlevelsets = nls;
   }
   *out = s;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_add_levelset(zsmpm_scene *s, const zsmpm_levelset_desc *d, void *stream) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (s->nscenes > 0) return fail(ZSMPM_ERR_INVALID_ARG, "level sets apply to single scenes");
+  if (!d) return fail(ZSMPM_ERR_INVALID_ARG, "null level set");
+  if (s->nlevelsets >= kMaxLevelsets) return fail(ZSMPM_ERR_CAPACITY, "at most ZSMPM_MAX_LEVELSETS level sets");
+  if (d->type < 0 || d->type > 2) return fail(ZSMPM_ERR_INVALID_ARG, "level-set type must be sticky, slip or separate");
+  if (d->nblocks < 0 || (d->nblocks > 0 && (!d->keys || !d->sdf)))
+    return fail(ZSMPM_ERR_INVALID_ARG, "level-set blocks need keys and distances");
+  levelset_dev L{};
+  L.type = d->type;
+  L.nblocks = d->nblocks;
+  L.background = d->background;
+  std::memcpy(L.sinv, d->sinv, sizeof(L.sinv));
+  std::memcpy(L.rinv, d->rinv, sizeof(L.rinv));
+  std::memcpy(L.t, d->t, sizeof(L.t));
+  int64_t lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+  for (int b = 0; b < d->nblocks; ++b)
+    for (int k = 0; k < 3; ++k) {
+      const int32_t v = d->keys[3 * b + k];
+      if (v % 8 != 0) return fail(ZSMPM_ERR_INVALID_ARG, "level-set block keys are block origins (multiples of 8)");
+      const int64_t bc = v / 8;
+      if (b == 0 || bc < lo[k]) lo[k] = bc;
+      if (b == 0 || bc > hi[k]) hi[k] = bc;
+    }
+  int64_t cells = 1;
+  for (int k = 0; k < 3; ++k) {
+    L.lo[k] = (int)lo[k];
+    L.dim[k] = (int)(hi[k] - lo[k] + 1);
+    cells *= std::max<int64_t>(L.dim[k], 0);
+  }
+  if (cells > ((int64_t)1 << 22)) return fail(ZSMPM_ERR_CAPACITY, "level-set bounding box above 2^22 blocks");
+  std::vector<int> map((size_t)std::max<int64_t>(cells, 1), -1);
+  for (int b = 0; b < d->nblocks; ++b) {
+    const int64_t ix = d->keys[3 * b] / 8 - lo[0], iy = d->keys[3 * b + 1] / 8 - lo[1], iz = d->keys[3 * b + 2] / 8 - lo[2];
+    int &slot = map[(size_t)((ix * L.dim[1] + iy) * L.dim[2] + iz)];
+    if (slot >= 0) return fail(ZSMPM_ERR_INVALID_ARG, "duplicate level-set block key");
+    slot = b;
+  }
+  int *dmap = nullptr;
+  float *dsdf = nullptr;
+  cudaError_t e = cudaMalloc(&dmap, sizeof(int) * map.size());
+  if (e == cudaSuccess) s->levelset_buffers.push_back(dmap);
+  if (e == cudaSuccess) e = cudaMalloc(&dsdf, sizeof(float) * 512 * (size_t)std::max(d->nblocks, 1));
+  if (e == cudaSuccess) s->levelset_buffers.push_back(dsdf);
+  cudaStream_t cs = as_stream(stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dmap, map.data(), sizeof(int) * map.size(), cudaMemcpyHostToDevice, cs);
+  if (e == cudaSuccess && d->nblocks > 0)
+    e = cudaMemcpyAsync(dsdf, d->sdf, sizeof(float) * 512 * (size_t)d->nblocks, cudaMemcpyHostToDevice, cs);
+  L.map = dmap;
+  L.sdf = dsdf;
+  const int count = s->nlevelsets + 1;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(const_cast<levelset_dev *>(s->dev.prm.levelsets) + s->nlevelsets, &L, sizeof(L),
+                        cudaMemcpyHostToDevice, cs);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(const_cast<int *>(s->dev.prm.nlevelsets), &count, sizeof(int), cudaMemcpyHostToDevice, cs);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cs);  // the host sources are local
+  if (e != cudaSuccess) return cuda_fail(e, "add level set");
+  s->nlevelsets = count;
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_scene_clear_levelsets(zsmpm_scene *s) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  ZS_TRY(cudaDeviceSynchronize(), "clear level sets");
+  ZS_TRY(cudaMemset(const_cast<int *>(s->dev.prm.nlevelsets), 0, sizeof(int)), "clear level sets");
+  for (void *ptr : s->levelset_buffers) cudaFree(ptr);
+  s->levelset_buffers.clear();
+  s->nlevelsets = 0;
   return ZSMPM_OK;
 }
 

@@ -282,60 +282,72 @@ struct collider_dev {
 };
 constexpr int kMaxColliders = 16;
 
-// signed distance of the analytic level sets (geometry/AnalyticLevelSet.h), in its order of
-// operations
+// The boundary code below spells every float operation with a round-to-nearest intrinsic, in
+// the reference's order of operations: the finite-difference normals divide differences of
+// nearby distances by 2e-6, which amplifies any change of rounding (such as a contraction to
+// FMA) about a thousandfold, so the device keeps the reference's rounding exactly.
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rn_div(float a, float b) { return __fdiv_rn(a, b); }
+// sum_i a[i] b[i] accumulated from 0 in index order (VecInterface dot / l2NormSqr)
+__device__ __forceinline__ float rn_dot3(float a0, float b0, float a1, float b1, float a2, float b2) {
+  return rn_add(rn_add(rn_add(0.f, rn_mul(a0, b0)), rn_mul(a1, b1)), rn_mul(a2, b2));
+}
+
+// signed distance of the analytic level sets (geometry/AnalyticLevelSet.h)
 __device__ __forceinline__ float collider_sdf(const collider_dev &c, const float X[3]) {
-  if (c.shape == 0) {  // Plane: n . (x - origin)
-    float r = 0.f;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r += c.b[i] * (X[i] - c.a[i]);
-    return r;
-  }
+  if (c.shape == 0)  // Plane: n . (x - origin)
+    return rn_dot3(c.b[0], rn_sub(X[0], c.a[0]), c.b[1], rn_sub(X[1], c.a[1]), c.b[2], rn_sub(X[2], c.a[2]));
   if (c.shape == 1) {  // Cuboid
-    float p[3], mx;
+    float p[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      const float center = (c.a[i] + c.b[i]) / 2.f;
-      const float d = X[i] - center;
-      p[i] = (d > 0.f ? d : -d) - (c.b[i] - c.a[i]) / 2.f;
+      const float center = rn_div(rn_add(c.a[i], c.b[i]), 2.f);
+      const float d = rn_sub(X[i], center);
+      p[i] = rn_sub(d > 0.f ? d : -d, rn_div(rn_sub(c.b[i], c.a[i]), 2.f));
     }
-    mx = p[0];
+    float mx = p[0];
     if (p[1] > mx) mx = p[1];
     if (p[2] > mx) mx = p[2];
-    float l2 = 0.f;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < 3; ++i)
       if (p[i] < 0.f) p[i] = 0.f;
-      l2 += p[i] * p[i];
-    }
-    return (mx < 0.f ? mx : 0.f) + sqrtf(l2);
+    return rn_add(mx < 0.f ? mx : 0.f, __fsqrt_rn(rn_dot3(p[0], p[0], p[1], p[1], p[2], p[2])));
   }
   if (c.shape == 2) {  // Sphere: |x - c| - r
-    float l2 = 0.f;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) l2 += (X[i] - c.a[i]) * (X[i] - c.a[i]);
-    return sqrtf(l2) - c.b[0];
+    const float d0 = rn_sub(X[0], c.a[0]), d1 = rn_sub(X[1], c.a[1]), d2 = rn_sub(X[2], c.a[2]);
+    return rn_sub(__fsqrt_rn(rn_dot3(d0, d0, d1, d1, d2, d2)), c.b[0]);
   }
   // Cylinder along axis d from a, radius b[0], length b[1]
   const int d = c.axis;
-  float l2 = 0.f;
+  float dr[2];
 #pragma unroll
-  for (int k = 0; k < 3; ++k)
-    if (k != d) l2 += (X[k] - c.a[k]) * (X[k] - c.a[k]);
-  const float dis_r = sqrtf(l2), radius = c.b[0], length = c.b[1];
+  for (int k = 0, i = 0; k < 3; ++k)
+    if (k != d) dr[i++] = rn_sub(X[k], c.a[k]);
+  const float dis_r = __fsqrt_rn(rn_add(rn_add(0.f, rn_mul(dr[0], dr[0])), rn_mul(dr[1], dr[1])));
+  const float radius = c.b[0], length = c.b[1];
   const bool outside = dis_r > radius;
   const float xd = X[d], bd = c.a[d];
-  if (xd < bd) {
-    const float dis_l = bd - xd;
-    return outside ? sqrtf((dis_r - radius) * (dis_r - radius) + dis_l * dis_l) : dis_l;
+  const float top = rn_add(bd, length);
+  if (xd < bd || xd > top) {
+    const float dis_l = xd < bd ? rn_sub(bd, xd) : rn_sub(xd, top);
+    if (!outside) return dis_l;
+    const float e = rn_sub(dis_r, radius);
+    return __fsqrt_rn(rn_add(rn_mul(e, e), rn_mul(dis_l, dis_l)));
   }
-  if (xd > bd + length) {
-    const float dis_l = xd - (bd + length);
-    return outside ? sqrtf((dis_r - radius) * (dis_r - radius) + dis_l * dis_l) : dis_l;
-  }
-  if (outside) return dis_r - radius;
-  const float dis_l = fminf(bd + length - xd, xd - bd);
-  return -fminf(dis_l, radius - dis_r);
+  if (outside) return rn_sub(dis_r, radius);
+  const float up = rn_sub(top, xd), down = rn_sub(xd, bd);
+  const float dis_l = up < down ? up : down;
+  const float rr = rn_sub(radius, dis_r);
+  return -(dis_l < rr ? dis_l : rr);
+}
+
+// n / |n| (VecInterface::normalized)
+__device__ __forceinline__ void rn_normalize(float n[3]) {
+  const float len = __fsqrt_rn(rn_dot3(n[0], n[0], n[1], n[1], n[2], n[2]));
+#pragma unroll
+  for (int i = 0; i < 3; ++i) n[i] = rn_div(n[i], len);
 }
 
 // material-space normal: the plane's normal as given, the sphere's outward direction (zero
@@ -347,79 +359,140 @@ __device__ __forceinline__ void collider_normal(const collider_dev &c, const flo
     return;
   }
   if (c.shape == 2) {
-    float l2 = 0.f;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      n[i] = X[i] - c.a[i];
-      l2 += n[i] * n[i];
-    }
-    if (l2 < 1e-7f) {
+    for (int i = 0; i < 3; ++i) n[i] = rn_sub(X[i], c.a[i]);
+    if (rn_dot3(n[0], n[0], n[1], n[1], n[2], n[2]) < 1e-7f) {
       n[0] = n[1] = n[2] = 0.f;
       return;
     }
-    const float len = sqrtf(l2);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) n[i] = n[i] / len;
+    rn_normalize(n);
     return;
   }
   const float eps = 1e-6f;
-  float l2 = 0.f;
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     float v1[3] = {X[0], X[1], X[2]}, v2[3] = {X[0], X[1], X[2]};
-    v1[i] = X[i] + eps;
-    v2[i] = X[i] - eps;
-    n[i] = (collider_sdf(c, v1) - collider_sdf(c, v2)) / (eps + eps);
-    l2 += n[i] * n[i];
+    v1[i] = rn_add(X[i], eps);
+    v2[i] = rn_sub(X[i], eps);
+    n[i] = rn_div(rn_sub(collider_sdf(c, v1), collider_sdf(c, v2)), rn_add(eps, eps));
   }
-  const float len = sqrtf(l2);
+  rn_normalize(n);
+}
+
+// the velocity response shared by the colliders and the level sets (Collider.h:95-108): v_object
+// for sticky, otherwise the relative velocity loses its normal part (slip, or separate when
+// moving into the boundary)
+__device__ __forceinline__ void boundary_respond(int type, const float n[3], const float vo[3], float v[3]) {
+  if (type == 0) {
 #pragma unroll
-  for (int i = 0; i < 3; ++i) n[i] = n[i] / len;
+    for (int i = 0; i < 3; ++i) v[i] = vo[i];
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) v[i] = rn_sub(v[i], vo[i]);
+  const float proj = rn_dot3(n[0], v[0], n[1], v[1], n[2], v[2]);
+  if ((type == 2 && proj < 0.f) || type == 1)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = rn_sub(v[i], rn_mul(proj, n[i]));
+#pragma unroll
+  for (int i = 0; i < 3; ++i) v[i] = rn_add(v[i], vo[i]);
 }
 
 // Collider::resolveCollision (Collider.h:80-110) with erosion 0
 __device__ __forceinline__ void collider_resolve(const collider_dev &c, const float x[3], float v[3]) {
-  const float xb[3] = {x[0] - c.t[0], x[1] - c.t[1], x[2] - c.t[2]};
-  const float inv_s = 1.f / c.s;
+  const float xb[3] = {rn_sub(x[0], c.t[0]), rn_sub(x[1], c.t[1]), rn_sub(x[2], c.t[2])};
+  const float inv_s = rn_div(1.f, c.s);
   float X[3];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    float r = 0.f;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) r += c.R[3 * j + i] * xb[j];  // R^T (x - b)
-    X[i] = r * inv_s;
-  }
+  for (int i = 0; i < 3; ++i)  // R^T (x - b) / s
+    X[i] = rn_mul(rn_dot3(c.R[i], xb[0], c.R[3 + i], xb[1], c.R[6 + i], xb[2]), inv_s);
   if (!(collider_sdf(c, X) < -0.f)) return;
-  const float ds = c.dsdt * inv_s;
-  const float vo[3] = {c.omega[1] * xb[2] - c.omega[2] * xb[1] + ds * xb[0] + c.dtdt[0],
-                       c.omega[2] * xb[0] - c.omega[0] * xb[2] + ds * xb[1] + c.dtdt[1],
-                       c.omega[0] * xb[1] - c.omega[1] * xb[0] + ds * xb[2] + c.dtdt[2]};
-  if (c.type == 0) {
-    v[0] = vo[0];
-    v[1] = vo[1];
-    v[2] = vo[2];
-    return;
+  const float ds = rn_mul(c.dsdt, inv_s);
+  // omega x (x - b) + (dsdt / s)(x - b) + R s V(X) + db/dt, V = 0 for an analytic level set
+  const float cr[3] = {rn_sub(rn_mul(c.omega[1], xb[2]), rn_mul(c.omega[2], xb[1])),
+                       rn_sub(rn_mul(c.omega[2], xb[0]), rn_mul(c.omega[0], xb[2])),
+                       rn_sub(rn_mul(c.omega[0], xb[1]), rn_mul(c.omega[1], xb[0]))};
+  float vo[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) vo[i] = rn_add(rn_add(rn_add(cr[i], rn_mul(ds, xb[i])), 0.f), c.dtdt[i]);
+  float nX[3] = {0.f, 0.f, 0.f}, n[3] = {0.f, 0.f, 0.f};
+  if (c.type != 0) {
+    collider_normal(c, X, nX);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) n[i] = rn_dot3(c.R[3 * i], nX[0], c.R[3 * i + 1], nX[1], c.R[3 * i + 2], nX[2]);
   }
-  float nX[3], n[3];
-  collider_normal(c, X, nX);
+  boundary_respond(c.type, n, vo, v);
+}
+
+// LevelSetBoundary<SparseLevelSet<3>>: 8^3 blocks of signed distance found through a dense map
+// over the keys' bounding box (block coordinates lo .. lo + dim - 1)
+struct levelset_dev {
+  int type, nblocks;
+  int lo[3], dim[3];
+  const int *map;    // dim[0] * dim[1] * dim[2]: block index or -1
+  const float *sdf;  // nblocks * 512
+  float background;
+  float sinv[9], rinv[9], t[3];  // row-major
+};
+constexpr int kMaxLevelsets = 4;
+
+// SparseLevelSetView::value_or (SparseLevelSet.hpp:477-484) at an integer index coordinate
+__device__ __forceinline__ float levelset_node(const levelset_dev &L, int cx, int cy, int cz) {
+  const int lx = cx & 7, ly = cy & 7, lz = cz & 7;
+  const int ix = ((cx - lx) >> 3) - L.lo[0], iy = ((cy - ly) >> 3) - L.lo[1], iz = ((cz - lz) >> 3) - L.lo[2];
+  if (ix < 0 || iy < 0 || iz < 0 || ix >= L.dim[0] || iy >= L.dim[1] || iz >= L.dim[2]) return L.background;
+  const int b = L.map[((size_t)ix * L.dim[1] + iy) * L.dim[2] + iz];
+  return b < 0 ? L.background : L.sdf[(size_t)b * 512 + ((lx << 6) | (ly << 3) | lz)];
+}
+
+// linear_interop(t, a, b) = a + (b - a) t (ZpcMathUtils.hpp:1779-1781)
+__device__ __forceinline__ float lerp_ref(float t, float a, float b) { return rn_add(a, rn_mul(rn_sub(b, a), t)); }
+
+// getSignedDistance: worldToIndex (SparseLevelSet.hpp:366-374), then the linear LevelSetArena
+// (:862-875, base_node<0> = floor) and xlerp (math/VecInterface.hpp:1043-1049)
+__device__ __forceinline__ float levelset_sdf(const levelset_dev &L, const float x[3]) {
+  const float a[3] = {rn_sub(x[0], L.t[0]), rn_sub(x[1], L.t[1]), rn_sub(x[2], L.t[2])};
+  float b[3], X[3];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    float r = 0.f;
+  for (int j = 0; j < 3; ++j) b[j] = rn_dot3(L.rinv[j], a[0], L.rinv[3 + j], a[1], L.rinv[6 + j], a[2]);
 #pragma unroll
-    for (int j = 0; j < 3; ++j) r += c.R[3 * i + j] * nX[j];
-    n[i] = r;
+  for (int j = 0; j < 3; ++j) X[j] = rn_dot3(L.sinv[j], b[0], L.sinv[3 + j], b[1], L.sinv[6 + j], b[2]);
+  int c[3];
+  float d[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    c[k] = (int)floorf(X[k]);
+    d[k] = rn_sub(X[k], (float)c[k]);
   }
-  float rel[3], proj = 0.f;
+  float p[2][2][2];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    rel[i] = v[i] - vo[i];
-    proj += n[i] * rel[i];
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int k = 0; k < 2; ++k) p[i][j][k] = levelset_node(L, c[0] + i, c[1] + j, c[2] + k);
+  return lerp_ref(d[0], lerp_ref(d[1], lerp_ref(d[2], p[0][0][0], p[0][0][1]), lerp_ref(d[2], p[0][1][0], p[0][1][1])),
+                  lerp_ref(d[1], lerp_ref(d[2], p[1][0][0], p[1][0][1]), lerp_ref(d[2], p[1][1][0], p[1][1][1])));
+}
+
+// Collider{levelset view, type}.resolveCollision with the identity placement (Collider.h:80-110):
+// the level set carries no material velocity here, so the collider's velocity is zero
+__device__ __forceinline__ void levelset_resolve(const levelset_dev &L, const float x[3], float v[3]) {
+  if (!(levelset_sdf(L, x) < -0.f)) return;
+  const float vo[3] = {0.f, 0.f, 0.f};
+  float n[3] = {0.f, 0.f, 0.f};
+  if (L.type != 0) {
+    const float eps = 1e-6f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      float v1[3] = {x[0], x[1], x[2]}, v2[3] = {x[0], x[1], x[2]};
+      v1[i] = rn_add(x[i], eps);
+      v2[i] = rn_sub(x[i], eps);
+      n[i] = rn_div(rn_sub(levelset_sdf(L, v1), levelset_sdf(L, v2)), rn_add(eps, eps));
+    }
+    rn_normalize(n);
   }
-  if ((c.type == 2 && proj < 0.f) || c.type == 1)
-#pragma unroll
-    for (int i = 0; i < 3; ++i) rel[i] -= proj * n[i];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) v[i] = rel[i] + vo[i];
+  boundary_respond(L.type, n, vo, v);
 }
 
 // out[3c+r] = sum_k M[3k+r] d[k] N[3k+c]

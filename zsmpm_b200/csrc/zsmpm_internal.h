@@ -73,6 +73,9 @@ struct scene_params {
   // colliders after the walls (device; the count is read at run time, so updates need no new graph)
   const collider_dev *colliders;
   const int *ncolliders;
+  // sparse level-set boundaries after the colliders (device, count read at run time)
+  const levelset_dev *levelsets;
+  const int *nlevelsets;
   // launch shapes (set by the autotuner; 0 = default)
   int g2p_threads;                  // 128 or 256
   int g2p_ctas_per_sm, p2g_ctas_per_sm;

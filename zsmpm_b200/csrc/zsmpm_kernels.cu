@@ -816,15 +816,18 @@ __device__ __forceinline__ void apply_walls(const scene_params &p, const float p
   }
 }
 
-// the scene's colliders after its walls, in list order
-__device__ __forceinline__ void apply_colliders(const scene_params &p, int count, const float pos[3], float v[3]) {
+// the scene's colliders after its walls, then its sparse level sets, each in list order
+__device__ __forceinline__ void apply_colliders(const scene_params &p, int count, int nls, const float pos[3],
+                                                float v[3]) {
   for (int k = 0; k < count; ++k) collider_resolve(p.colliders[k], pos, v);
+  for (int k = 0; k < nls; ++k) levelset_resolve(p.levelsets[k], pos, v);
 }
 
 __global__ void __launch_bounds__(kThreads) k_grid_update(scene_device s) {
   const scene_params &p = s.prm;
   const int nb = s.ctr[kCtrBlocks];
   const int ncol = p.ncolliders ? min(*p.ncolliders, kMaxColliders) : 0;
+  const int nls = p.nlevelsets ? min(*p.nlevelsets, kMaxLevelsets) : 0;
   const long long total = (long long)nb * 512;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += grid_threads()) {
     const int b = (int)(t >> 9), cell = (int)(t & 511);
@@ -840,7 +843,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_update(scene_device s) {
                             ((float)k.y * 8.f + (float)((cell >> 3) & 7)) * p.dx,
                             ((float)k.z * 8.f + (float)(cell & 7)) * p.dx};
       apply_walls(p, pos, v);
-      apply_colliders(p, ncol, pos, v);
+      apply_colliders(p, ncol, nls, pos, v);
     }
     g[512] = v[0];
     g[1024] = v[1];
@@ -1455,6 +1458,7 @@ __global__ void __launch_bounds__(kThreads) k_implicit_project(scene_device s, f
   const scene_params &p = s.prm;
   const long long total = dof_count(s, ndofs) / 3;
   const int ncol = p.ncolliders ? min(*p.ncolliders, kMaxColliders) : 0;
+  const int nls = p.nlevelsets ? min(*p.nlevelsets, kMaxLevelsets) : 0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += grid_threads()) {
     const int b = (int)(t >> 9), cell = (int)(t & 511);
     float *v = dof + t * 3;
@@ -1465,7 +1469,7 @@ __global__ void __launch_bounds__(kThreads) k_implicit_project(scene_device s, f
                             ((float)k.z * 8.f + (float)(cell & 7)) * p.dx};
       float vel[3] = {v[0], v[1], v[2]};
       apply_walls(p, pos, vel);
-      apply_colliders(p, ncol, pos, vel);
+      apply_colliders(p, ncol, nls, pos, vel);
       v[0] = vel[0];
       v[1] = vel[1];
       v[2] = vel[2];
