@@ -818,7 +818,7 @@ __device__ __forceinline__ void apply_walls(const scene_params &p, const float p
 
 // the scene's colliders after its walls, then its sparse level sets, each in list order
 __device__ __forceinline__ void apply_colliders(const scene_params &p, int count, int nls, const float pos[3],
-                                                float v[3]) {
+                                             float v[3]) {
   for (int k = 0; k < count; ++k) collider_resolve(p.colliders[k], pos, v);
   for (int k = 0; k < nls; ++k) levelset_resolve(p.levelsets[k], pos, v);
 }
@@ -826,8 +826,6 @@ __device__ __forceinline__ void apply_colliders(const scene_params &p, int count
 __global__ void __launch_bounds__(kThreads) k_grid_update(scene_device s) {
   const scene_params &p = s.prm;
   const int nb = s.ctr[kCtrBlocks];
-  const int ncol = p.ncolliders ? min(*p.ncolliders, kMaxColliders) : 0;
-  const int nls = p.nlevelsets ? min(*p.nlevelsets, kMaxLevelsets) : 0;
   const long long total = (long long)nb * 512;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += grid_threads()) {
     const int b = (int)(t >> 9), cell = (int)(t & 511);
@@ -843,8 +841,32 @@ __global__ void __launch_bounds__(kThreads) k_grid_update(scene_device s) {
                             ((float)k.y * 8.f + (float)((cell >> 3) & 7)) * p.dx,
                             ((float)k.z * 8.f + (float)(cell & 7)) * p.dx};
       apply_walls(p, pos, v);
-      apply_colliders(p, ncol, nls, pos, v);
     }
+    g[512] = v[0];
+    g[1024] = v[1];
+    g[1536] = v[2];
+  }
+}
+
+// The scene's colliders and level sets, after the walls of k_grid_update, on every node with
+// positive mass (their own launch, so that k_grid_update keeps its registers; without colliders
+// every CTA returns at once).
+__global__ void __launch_bounds__(kThreads) k_grid_boundaries(scene_device s) {
+  const scene_params &p = s.prm;
+  const int ncol = p.ncolliders ? min(*p.ncolliders, kMaxColliders) : 0;
+  const int nls = p.nlevelsets ? min(*p.nlevelsets, kMaxLevelsets) : 0;
+  if (ncol + nls == 0) return;
+  const long long total = (long long)s.ctr[kCtrBlocks] * 512;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += grid_threads()) {
+    const int b = (int)(t >> 9), cell = (int)(t & 511);
+    float *g = s.grid + (size_t)b * kGridChannels * 512 + cell;
+    if (!(g[0] > 0.f)) continue;
+    const int3 k = local_block(p, unpack_key(s.blk_pk[b]));
+    const float pos[3] = {((float)k.x * 8.f + (float)(cell >> 6)) * p.dx,
+                          ((float)k.y * 8.f + (float)((cell >> 3) & 7)) * p.dx,
+                          ((float)k.z * 8.f + (float)(cell & 7)) * p.dx};
+    float v[3] = {g[512], g[1024], g[1536]};
+    apply_colliders(p, ncol, nls, pos, v);
     g[512] = v[0];
     g[1024] = v[1];
     g[1536] = v[2];
@@ -1469,7 +1491,7 @@ __global__ void __launch_bounds__(kThreads) k_implicit_project(scene_device s, f
                             ((float)k.z * 8.f + (float)(cell & 7)) * p.dx};
       float vel[3] = {v[0], v[1], v[2]};
       apply_walls(p, pos, vel);
-      apply_colliders(p, ncol, nls, pos, vel);
+      if (ncol + nls > 0) apply_colliders(p, ncol, nls, pos, vel);
       v[0] = vel[0];
       v[1] = vel[1];
       v[2] = vel[2];
@@ -1895,6 +1917,7 @@ cudaError_t launch_p2g(scene_device &s, cudaStream_t st) {
 
 cudaError_t launch_grid_update(scene_device &s, cudaStream_t st) {
   k_grid_update<<<num_sms() * 8, kThreads, 0, st>>>(s);
+  k_grid_boundaries<<<num_sms() * 4, kThreads, 0, st>>>(s);
   return cudaGetLastError();
 }
 
@@ -1980,8 +2003,8 @@ cudaError_t launch_cg_iteration(scene_device &s, float *x, const cg_vectors &v, 
 }
 
 // k_begin, insert, enlarge, prepare, set, 3 scans// k_begin, insert, enlarge, prepare, set, 3 scans, ranks, neighbours; count, 3 scans,
-// cell_start, scatter, finalize; p2g; grid update; g2p
-int kernels_per_substep() { return 10 + 7 + 3; }
+// cell_start, scatter, finalize; p2g; grid update and boundaries; g2p
+int kernels_per_substep() { return 10 + 7 + 4; }
 
 cudaError_t launch_import(scene_device &s, const float *m, const float *x, const float *v,
                           const float *C, const float *F, const float *plastic, int n,
