@@ -944,7 +944,23 @@ __device__ __forceinline__ void learned_constitutive(const material_dev &mat, co
     const float tr = sum_eps + plastic;
     pl_new = tr >= 0.f ? (mat.volume_correction ? mat.beta * sum_eps + plastic : plastic) : 0.f;
   } else {
+    // snow: the projection is the identity inside the elastic box [1 - theta_c, 1 + theta_s]^3
+    // (an exact test); outside it the network's projected strain is used.  The stress of the
+    // projected state follows from the hardened fixed-corotated formula: its magnitude spans the
+    // gravity-loaded state (1e-3 of the output range) to the yield surface, which the network's
+    // BF16 stress output resolves to only about 1e-3 of that range.
+    bool inside = true;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) inside = inside && S[i] >= 1.f - mat.theta_c && S[i] <= 1.f + mat.theta_s;
+    if (inside)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) Ns[i] = S[i];
     pl_new = plastic * (S[0] * S[1] * S[2] / fmaxf(Ns[0] * Ns[1] * Ns[2], 1e-6f));
+    const float e = expf(mat.hardening * (1.f - pl_new));
+    float Ph[3];
+    fc_principal(mat.mu * e, mat.lambda * e, Ns, Ph);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) tp[i] = Ph[i] * Ns[i];
   }
   const bool audit = active && cd.audit_period > 0 &&
                      ((unsigned)id * 2654435761u + (unsigned)substep * 40503u) % (unsigned)cd.audit_period == 0u;
