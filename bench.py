@@ -231,6 +231,56 @@ def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms
             "mlp_inference": mlp}
 
 
+def batch_learned_leg(args, zs, sc, specs, parts, upload_pinned, stream, sptr, ws, plain_ms):
+    """The batch with one Drucker-Prager closure serving its sand scenes (the fixed-corotated
+    scenes keep the plain path).  The closure is trained on random states plus trial states
+    logged from the first sand scene run alone, then the batch is re-uploaded, warmed up and
+    timed like the plain leg with one particle in 100 audited per substep."""
+    import torch
+
+    from zsmpm_b200 import closure as cl
+    k = next(i for i, sp in enumerate(specs) if sp.material.model == zs.DRUCKER_PRAGER)
+    one = zs.Scene(specs[k], parts[k])
+    buf = torch.empty((args.train_logged, 6), dtype=torch.float32, device="cuda")
+    cl.set_state_log(one, buf, max(1, -(-parts[k].n * 8 // args.train_logged)))
+    one.run(8)
+    n_log = min(cl.state_log_count(one), args.train_logged)
+    cl.set_state_log(one, None, 0)
+    one.close()
+    c = cl.Closure(specs[k].material, specs[k].volume, device=torch.cuda.current_device())
+    t0 = time.perf_counter()
+    c.build_dataset(args.train_random, seed=7, logged=buf[:n_log].contiguous())
+    schedule = ((6, 4096, 2e-3), (6, 4096, 5e-4), (4, 8192, 1e-4))
+    losses = c.fit(schedule)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    upload_pinned()
+    cl.attach(sc, c, audit_period=100)
+    sc.run(args.warmup, stream=sptr)
+    sc.status()
+    cl.audit(sc, reset=True)
+    torch.cuda.synchronize()
+    barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sc.run(args.steps, stream=sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sc.status()
+    lms = max_over_ranks(e0.elapsed_time(e1), ws)
+    a = cl.audit(sc)
+    cl.attach(sc, None)
+    c.close()
+    n = sum(q.n for q in parts)
+    return {"value": n * args.steps * ws / (lms * 1e-3), "unit": UNIT, "ms_per_step": lms / args.steps,
+            "vs_plain": (plain_ms * args.steps) / lms,
+            "scenes_served": sum(1 for sp in specs if sp.material.model == zs.DRUCKER_PRAGER),
+            "audit": {"period": 100, **a},
+            "training": {"random_states": args.train_random, "logged_states": n_log,
+                         "logged_from": f"scene {k} alone", "seconds": train_s,
+                         "first_loss": float(losses[0]), "final_loss": float(losses[-1])}}
+
+
 def mlp_inference_leg(c, n_rows: int, reps: int = 5) -> dict:
     """The closure's network alone over n_rows feature rows, on both tensor-core paths: the
     mma.sync forward that G2P fuses and the tcgen05 forward (tensor-memory accumulators).
@@ -545,6 +595,8 @@ def main(argv=None):
     learned = None
     if plastic and parts is None and not args.no_learned:
         learned = learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, ms / args.steps)
+    elif plastic and not args.no_learned:
+        learned = batch_learned_leg(args, zs, sc, specs, parts, upload_pinned, stream, sptr, ws, ms / args.steps)
 
     # ---------------------------------------------------------------- implicit-system leg
     implicit = None

@@ -479,7 +479,9 @@ ZSMPM_API zsmpm_status zsmpm_closure_set_state(zsmpm_closure *c, const zsmpm_clo
 /* Attach a trained closure to a scene (NULL detaches; the scene keeps the closure's device
  * pointers, so destroy the closure only after detaching it); audit_period N checks one
  * particle in N per substep against the plain map (0 = no audit).  Needs the committed
- * plasticity ordering. */
+ * plasticity ordering.  On a batch the closure serves every scene of its material model and
+ * the others keep the plain return map; the network works in units of each scene's
+ * 3 lambda + 2 mu, so scenes that share the closure material's Poisson ratio share it. */
 ZSMPM_API zsmpm_status zsmpm_scene_set_closure(zsmpm_scene *s, zsmpm_closure *c, int32_t audit_period);
 /* Audit totals since the closure was attached or the last reset (synchronises). */
 ZSMPM_API zsmpm_status zsmpm_scene_closure_audit(zsmpm_scene *s, zsmpm_closure_audit *out, int32_t reset);

@@ -119,3 +119,52 @@ def test_particle_outside_its_slot_is_reported(zs, gpu):
         bt.status()
     assert e.value.status == zs._abi.ERR_OUT_OF_DOMAIN
     bt.close()
+
+
+@pytest.mark.gpu
+def test_learned_closure_on_a_batch(zs, gpu):
+    """One Drucker-Prager closure on a batch of mixed scenes: it serves the sand scenes (their
+    friction angles are a network input) and the fixed-corotated scenes keep the plain path."""
+    import torch
+
+    from zsmpm_b200 import batch
+    from zsmpm_b200 import closure as cl
+    specs = _small_batch()
+    parts = batch.generate_all(specs)
+    steps = 40
+    dp = next(i for i, sp in enumerate(specs) if sp.material.model == zs_dp)
+    sc = zs.Scene(specs[dp], parts[dp])
+    buf = torch.empty((200000, 6), dtype=torch.float32, device=gpu)
+    cl.set_state_log(sc, buf, 3)
+    sc.run(steps)
+    n_log = cl.state_log_count(sc)
+    cl.set_state_log(sc, None, 0)
+    sc.close()
+    c = cl.Closure(specs[dp].material, specs[dp].volume)
+    c.build_dataset(300000, seed=8, logged=buf[:min(n_log, 200000)].contiguous())
+    c.fit()
+    plain = batch.Batch(specs, parts)
+    plain.run(steps)
+    plain.status()
+    ref = plain.download_scenes()
+    plain.close()
+    lb = batch.Batch(specs, parts)
+    cl.attach(lb, c, audit_period=50)
+    lb.run(steps)
+    lb.status()
+    a = cl.audit(lb)
+    got = lb.download_scenes()
+    cl.attach(lb, None)
+    lb.close()
+    c.close()
+    print(f"\nbatched learned closure: audit {a}")
+    # per-particle stress error and the aggregate over the audit (the network was trained on
+    # random states and on the states of one sand scene only; the others differ in friction)
+    assert a["audited"] > 0 and a["mean_rel_error"] < 1e-3 and a["agg_rel_error"] < 0.1
+    for sp, p0, g, r in zip(specs, parts, got, ref):
+        disp = np.linalg.norm(r.x.astype(np.float64) - p0.x)
+        err = np.linalg.norm(g.x.astype(np.float64) - r.x) / max(disp, 1e-12)
+        if sp.material.model == zs_fc:
+            assert np.max(np.abs(g.x - r.x)) <= 1e-6  # the plain path, up to the P2G summation order
+        else:
+            assert err < 0.05, (sp.material.friction_deg, err)

@@ -862,10 +862,10 @@ ZSMPM_API zsmpm_status zsmpm_scene_set_closure(zsmpm_scene *s, zsmpm_closure *c,
     s->dev.aux.learned = 0;
     return ZSMPM_OK;
   }
-  if (s->nscenes > 0) return fail(ZSMPM_ERR_INVALID_ARG, "the learned closure runs on single scenes");
   closure_dev cd{};
   if (!closure_device_view(c, &cd)) return fail(ZSMPM_ERR_NOT_READY, "closure has no dataset or state yet");
-  if (cd.model != s->desc.material.model)
+  // a batch runs the closure on the scenes of its model and the plain return map on the others
+  if (s->nscenes == 0 && cd.model != s->desc.material.model)
     return fail(ZSMPM_ERR_INVALID_ARG, "closure was built for another material model");
   if (s->desc.material.plasticity_mode != ZSMPM_PLASTICITY_COMMITTED && s->desc.material.model != ZSMPM_SNOW)
     return fail(ZSMPM_ERR_INVALID_ARG, "the learned closure runs in the committed plasticity ordering");

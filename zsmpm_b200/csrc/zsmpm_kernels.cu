@@ -920,7 +920,9 @@ __device__ __forceinline__ void learned_constitutive(const material_dev &mat, co
   bool in_hull = true;
   float in[kMlpIn];
   net_scale ns;
-  closure_inputs(cd.model, cd.kappa, cd.hardening, feat, in, ns);
+  // the scale of the stress is the particle material's 3 lambda + 2 mu: the network works in
+  // units of it, so one network serves every scene of a batch that shares the closure's nu
+  closure_inputs(cd.model, 3.f * mat.lambda + 2.f * mat.mu, mat.hardening, feat, in, ns);
 #pragma unroll
   for (int k = 0; k < kMlpIn; ++k) {
     in_hull = in_hull && feat[k] >= cd.in_min[k] && feat[k] <= cd.in_max[k];
@@ -1012,7 +1014,7 @@ constexpr size_t kG2PSmemLearned = kG2PSmemPlain + sizeof(uint2) * kFragTotal + 
 // variant is capped for 2 (128 registers; at 1 CTA per SM it takes 6.2 ms instead of 4.8).
 template <bool kLearned, bool kBatch, int NT>
 __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(scene_device s) {
-  static_assert(!kLearned || (NT == kThreads && !kBatch), "learned G2P runs single scenes at 256 threads");
+  static_assert(!kLearned || NT == kThreads, "learned G2P runs at 256 threads");
   extern __shared__ __align__(16) float g2p_smem[];
   float4 *svf = reinterpret_cast<float4 *>(g2p_smem);
   __shared__ int s_b;
@@ -1149,9 +1151,11 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
           for (int q = 0; q < 6; ++q) s.aux.log_buf[6 * k + q] = feat[q];
       }
       float tau[9];
-      if (kLearned)
-        learned_constitutive(p.mat, s.aux.cd, sfrag, sbias, sxs + warp * 32 * 16, sys + warp * 32 * 8, Fn, pl, tau,
-                             active, id, substep);
+      // in a batch the closure serves the scenes of its material model; the branch is uniform
+      // over the CTA (a block belongs to one scene), as the warp-collective MLP requires
+      if (kLearned && (!kBatch || s_mat.model == s.aux.cd.model))
+        learned_constitutive(kBatch ? s_mat : p.mat, s.aux.cd, sfrag, sbias, sxs + warp * 32 * 16,
+                             sys + warp * 32 * 8, Fn, pl, tau, active, id, substep);
       else if (kBatch)
         constitutive<true>(s_mat, Fn, pl, tau);
       else
@@ -1921,6 +1925,9 @@ cudaError_t prepare_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_g2p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kG2P2GSmem);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_g2p<true, true, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kG2PSmemLearned);
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_g2p<true, false, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)kG2PSmemLearned);
 }
@@ -1941,7 +1948,9 @@ cudaError_t launch_g2p(scene_device &s, cudaStream_t st) {
   const int per_sm = s.prm.g2p_ctas_per_sm > 0 ? s.prm.g2p_ctas_per_sm : (s.aux.learned ? 2 : 3);
   const int grid = num_sms() * per_sm;
   const bool small = s.prm.g2p_threads == 128;
-  if (s.aux.learned)
+  if (s.aux.learned && s.prm.batch)
+    k_g2p<true, true, kThreads><<<grid, kThreads, kG2PSmemLearned, st>>>(s);
+  else if (s.aux.learned)
     k_g2p<true, false, kThreads><<<grid, kThreads, kG2PSmemLearned, st>>>(s);
   else if (s.prm.batch)
     small ? k_g2p<false, true, 128><<<grid, 128, kG2PSmemPlain, st>>>(s)
