@@ -49,7 +49,10 @@ def test_struct_layouts_match_header(zs, tmp_path):
                      "offsetof(zsmpm_closure_state, in_mean), sizeof(zsmpm_closure_audit),"
                      "offsetof(zsmpm_closure_audit, fallbacks));"
                      "printf(\"%zu %zu %zu\\n\", sizeof(zsmpm_bht_view), offsetof(zsmpm_bht_view, table_size),"
-                     "sizeof(zsmpm_tuning));return 0;}\n")
+                     "sizeof(zsmpm_tuning));"
+                     "printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(zsmpm_collider), offsetof(zsmpm_collider, R),"
+                     "sizeof(zsmpm_levelset_desc), offsetof(zsmpm_levelset_desc, background),"
+                     "offsetof(zsmpm_levelset_desc, t), sizeof(zsmpm_cg_options));return 0;}\n")
     exe = tmp_path / "probe"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(probe), "-o", str(exe)], check=True)
     vals = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()))
@@ -59,7 +62,9 @@ def test_struct_layouts_match_header(zs, tmp_path):
                     C.sizeof(a.TileVectorView), C.sizeof(a.TableView),
                     C.sizeof(a.ClosureState), a.ClosureState.in_mean.offset, C.sizeof(a.ClosureAudit),
                     a.ClosureAudit.fallbacks.offset, C.sizeof(a.BhtView), a.BhtView.table_size.offset,
-                    C.sizeof(a.Tuning)]
+                    C.sizeof(a.Tuning),
+                    C.sizeof(a.Collider), a.Collider.R.offset, C.sizeof(a.LevelSetDesc),
+                    a.LevelSetDesc.background.offset, a.LevelSetDesc.t.offset, C.sizeof(a.CgOptions)]
 
 
 def test_host_side_argument_checks_without_gpu(zs):
