@@ -1896,7 +1896,7 @@ int num_sms() {
 cudaError_t launch_activate(scene_device &s, cudaStream_t st) {
   const int sm = num_sms();
   k_begin<<<sm * 4, kThreads, 0, st>>>(s);
-  k_insert_particle_blocks<<<sm * 8, kThreads, 0, st>>>(s);
+  k_insert_particle_blocks<<<sm * 16, kThreads, 0, st>>>(s);
   k_enlarge<<<sm * 2, kThreads, 0, st>>>(s);
   k_bitmap_prepare<<<1, 32, 0, st>>>(s);
   k_bitmap_set<<<sm * 2, kThreads, 0, st>>>(s);
@@ -1909,11 +1909,11 @@ cudaError_t launch_activate(scene_device &s, cudaStream_t st) {
 
 cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
   const int sm = num_sms();
-  k_bin_count<<<sm * 8, kThreads, 0, st>>>(s);
+  k_bin_count<<<sm * 16, kThreads, 0, st>>>(s);
   cudaError_t e = device_scan(load_int{s.block_count}, &s.ctr[kCtrBlocks], s.scan_part, s.block_start, st);
   if (e != cudaSuccess) return e;
   k_cell_start<<<sm * 2, 512, 0, st>>>(s);
-  k_bin_scatter<<<sm * 8, kThreads, 0, st>>>(s);
+  k_bin_scatter<<<sm * 16, kThreads, 0, st>>>(s);
   k_bin_finalize<<<sm * 2, 512, 0, st>>>(s);
   return cudaGetLastError();
 }
