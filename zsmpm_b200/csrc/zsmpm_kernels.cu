@@ -1912,9 +1912,9 @@ cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
   k_bin_count<<<sm * 16, kThreads, 0, st>>>(s);
   cudaError_t e = device_scan(load_int{s.block_count}, &s.ctr[kCtrBlocks], s.scan_part, s.block_start, st);
   if (e != cudaSuccess) return e;
-  k_cell_start<<<sm * 2, 512, 0, st>>>(s);
+  k_cell_start<<<sm * 4, 512, 0, st>>>(s);
   k_bin_scatter<<<sm * 16, kThreads, 0, st>>>(s);
-  k_bin_finalize<<<sm * 2, 512, 0, st>>>(s);
+  k_bin_finalize<<<sm * 4, 512, 0, st>>>(s);
   return cudaGetLastError();
 }
 
