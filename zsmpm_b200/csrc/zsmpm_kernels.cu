@@ -536,9 +536,11 @@ __global__ void __launch_bounds__(512) k_bin_finalize(scene_device s) {
 
 // ----------------------------------------------------------------- P2G
 // One CTA per block (persistent).  The block's 512 cells are processed in chunks of 64:
-//  1. the CTA gathers the chunk's particles and stages, per particle, its 3x3 B-spline
-//     weights, m and the affine terms (q, A dx) in shared memory, laid out [field][rank][cell]
-//     so that lanes reading one rank of consecutive cells hit consecutive banks;
+//  1. the CTA gathers the chunk's particles, two per thread with their loads issued together,
+//     and stages, per particle, its 3x3 B-spline weights, m and the affine terms (q, A dx) in
+//     shared memory as six float4 fields laid out [field][rank][cell], rows padded by one
+//     float4: lanes reading one rank of consecutive cells read 512 contiguous bytes, and the
+//     ranks of one cell, which consecutive lanes write, start 4 banks apart;
 //  2. one thread per (cell, channel) sums the cell's particles into 27 registers -- all
 //     particles of a cell share the same 27 stencil nodes -- and adds them to a 12^3 halo of
 //     the grid in shared memory (cells [8b, 8b+12) per axis: b and its +1 neighbours).
@@ -547,8 +549,7 @@ __global__ void __launch_bounds__(512) k_bin_finalize(scene_device s) {
 // (P2G.hpp:108-125) with A = m C - (4 dt/dx^2) tau precomputed by G2P.
 constexpr int kP2GChunk = 64;     // cells per chunk
 constexpr int kP2GRanks = 12;     // particles per cell staged per chunk (more go direct)
-constexpr int kP2GFields = 22;    // w[9], m, q[3], ax[3], ay[3], az[3]
-constexpr int kP2GRow = kP2GChunk + 1;  // padded row: rank r of cell c in bank (r + c) % 32
+constexpr int kP2GRow = kP2GChunk + 1;  // padded row of float4: rank r of cell c at bank 4 (r + c) % 32
 constexpr int kP2GThreads = 256;  // 4 channels x 64 cells
 constexpr int kP2GMap = 1024;     // slots of a chunk mapped to their cell (more: binary search)
 
@@ -610,16 +611,17 @@ __device__ __forceinline__ void p2g_direct(float *shf, const p2g_particle &pp, i
       }
 }
 
+constexpr int kP2GVec = 6;  // float4 fields: w00 w01 w02 w10 | w11 w12 w20 w21 | w22 m | (q ax ay az) x 3
 constexpr size_t kP2GSmemBytes =
-    sizeof(float) * (kGridChannels * kHaloCells + kP2GFields * kP2GRanks * kP2GRow) +
+    sizeof(float) * kGridChannels * kHaloCells + sizeof(float4) * kP2GVec * kP2GRanks * kP2GRow +
     sizeof(int) * 2 * (kP2GChunk + 1) + sizeof(unsigned char) * 2 * kP2GMap;
 
 __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
-  extern __shared__ float p2g_smem[];
+  extern __shared__ __align__(16) float p2g_smem[];
   float *sh = p2g_smem;
-  auto stg = reinterpret_cast<float(*)[kP2GRanks][kP2GRow]>(p2g_smem + kGridChannels * kHaloCells);
+  auto stg = reinterpret_cast<float4(*)[kP2GRanks][kP2GRow]>(p2g_smem + kGridChannels * kHaloCells);
   int *s_cs = reinterpret_cast<int *>(p2g_smem + kGridChannels * kHaloCells +
-                                      kP2GFields * kP2GRanks * kP2GRow);
+                                      4 * kP2GVec * kP2GRanks * kP2GRow);
   __shared__ int s_b;
   const int nb = s.ctr[kCtrBlocks];
   const int t = threadIdx.x;
@@ -657,7 +659,7 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
       // ---- phase 1: consecutive threads take consecutive slots (coalesced gathers)
       const int c0 = s_cs[0], c1 = s_cs[kP2GChunk];
       const unsigned char *s_map = s_map0 + (chunk & 1) * kP2GMap;
-      for (int slot = c0 + t; slot < c1; slot += blockDim.x) {
+      auto stage_one = [&](int slot, const p2g_particle &pp) {
         int lo = 0;  // the cell of this slot: the last cell whose start is <= slot
         if (slot - c0 < kP2GMap) {
           lo = s_map[slot - c0];
@@ -671,28 +673,30 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
         }
         const int cl = lo, r = slot - s_cs[lo], cell = cell0 + cl;
         const int ex = (cell >> 6) + 1, ey = ((cell >> 3) & 7) + 1, ez = (cell & 7) + 1;
-        p2g_particle pp;
-        p2g_prepare(s, s.src[slot], ox, oy, oz, pp);
         if (r >= kP2GRanks || pp.hb[0] != ex || pp.hb[1] != ey || pp.hb[2] != ez) {
           // beyond the staged ranks, or a stencil origin that rounding moved off the
           // cell: scatter this particle directly and stage a zero-mass stand-in
           p2g_direct(sh, pp, s.ctr);
           if (r < kP2GRanks)
-            for (int f = 0; f < kP2GFields; ++f) stg[f][r][cl] = 0.f;
-          continue;
+            for (int f = 0; f < kP2GVec; ++f) stg[f][r][cl] = make_float4(0.f, 0.f, 0.f, 0.f);
+          return;
         }
+        stg[0][r][cl] = make_float4(pp.w[0][0], pp.w[0][1], pp.w[0][2], pp.w[1][0]);
+        stg[1][r][cl] = make_float4(pp.w[1][1], pp.w[1][2], pp.w[2][0], pp.w[2][1]);
+        stg[2][r][cl] = make_float4(pp.w[2][2], pp.m, 0.f, 0.f);
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) stg[3 * a + c][r][cl] = pp.w[a][c];
-        stg[9][r][cl] = pp.m;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          stg[10 + d][r][cl] = pp.q[d];
-          stg[13 + d][r][cl] = pp.ax[d];
-          stg[16 + d][r][cl] = pp.ay[d];
-          stg[19 + d][r][cl] = pp.az[d];
-        }
+        for (int d = 0; d < 3; ++d) stg[3 + d][r][cl] = make_float4(pp.q[d], pp.ax[d], pp.ay[d], pp.az[d]);
+      };
+      for (int slot = c0 + t; slot < c1; slot += 2 * blockDim.x) {
+        const int slot2 = slot + blockDim.x;
+        const bool two = slot2 < c1;
+        const int i1 = s.src[slot];
+        const int i2 = s.src[two ? slot2 : slot];
+        p2g_particle pa, pb;
+        p2g_prepare(s, i1, ox, oy, oz, pa);
+        p2g_prepare(s, i2, ox, oy, oz, pb);
+        stage_one(slot, pa);
+        if (two) stage_one(slot2, pb);
       }
       __syncthreads();
       if (chunk + 1 < 512 / kP2GChunk) {
@@ -713,12 +717,9 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
           if (my_ch == 0) {
             // mass: W m (the warp is channel-uniform)
             for (int r = 0; r < cnt; ++r) {
-              float w[3][3];
-#pragma unroll
-              for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) w[a][c] = stg[3 * a + c][r][my_cell];
-              const float m = stg[9][r][my_cell];
+              const float4 wa = stg[0][r][my_cell], wb = stg[1][r][my_cell], wc = stg[2][r][my_cell];
+              const float w[3][3] = {{wa.x, wa.y, wa.z}, {wa.w, wb.x, wb.y}, {wb.z, wb.w, wc.x}};
+              const float m = wc.y;
 #pragma unroll
               for (int ii = 0; ii < 3; ++ii) {
                 const float wm = w[0][ii] * m;
@@ -736,15 +737,13 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
           } else {
             // momentum: W (q + ii ax + jj ay + kk az), in cell units of the node offset
             for (int r = 0; r < cnt; ++r) {
-              float w[3][3];
-#pragma unroll
-              for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) w[a][c] = stg[3 * a + c][r][my_cell];
-              const float q = stg[10 + d][r][my_cell];
-              const float ax = stg[13 + d][r][my_cell];
-              const float ay = stg[16 + d][r][my_cell];
-              const float az = stg[19 + d][r][my_cell];
+              const float4 wa = stg[0][r][my_cell], wb = stg[1][r][my_cell], wc = stg[2][r][my_cell];
+              const float w[3][3] = {{wa.x, wa.y, wa.z}, {wa.w, wb.x, wb.y}, {wb.z, wb.w, wc.x}};
+              const float4 qa = stg[3 + d][r][my_cell];
+              const float q = qa.x, ax = qa.y, ay = qa.z, az = qa.w;
+              // wz (qij + kk az) = wz qij + cz[kk], cz = (0, wz1 az, 2 wz2 az): two operations
+              // per node
+              const float cz1 = w[2][1] * az, cz2 = 2.f * w[2][2] * az;
 #pragma unroll
               for (int ii = 0; ii < 3; ++ii) {
                 const float qi = q + (float)ii * ax;
@@ -752,11 +751,10 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
                 for (int jj = 0; jj < 3; ++jj) {
                   const float qij = qi + (float)jj * ay;
                   const float wij = w[0][ii] * w[1][jj];
-#pragma unroll
-                  for (int kk = 0; kk < 3; ++kk) {
-                    const int n = (ii * 3 + jj) * 3 + kk;
-                    acc[n] = fmaf(wij * w[2][kk], qij + (float)kk * az, acc[n]);
-                  }
+                  const int n = (ii * 3 + jj) * 3;
+                  acc[n] = fmaf(wij, w[2][0] * qij, acc[n]);
+                  acc[n + 1] = fmaf(wij, fmaf(w[2][1], qij, cz1), acc[n + 1]);
+                  acc[n + 2] = fmaf(wij, fmaf(w[2][2], qij, cz2), acc[n + 2]);
                 }
               }
             }
@@ -1414,6 +1412,7 @@ __global__ void __launch_bounds__(kG2P2GThreads, 2)
           const float ax = stg[12 + d][r][my_cell];
           const float ay = stg[15 + d][r][my_cell];
           const float az = stg[18 + d][r][my_cell];
+          const float cz1 = w[2][1] * az, cz2 = 2.f * w[2][2] * az;  // as in k_p2g
 #pragma unroll
           for (int ii = 0; ii < 3; ++ii) {
             const float qi = q + (float)ii * ax;
@@ -1421,11 +1420,10 @@ __global__ void __launch_bounds__(kG2P2GThreads, 2)
             for (int jj = 0; jj < 3; ++jj) {
               const float qij = qi + (float)jj * ay;
               const float wij = w[0][ii] * w[1][jj];
-#pragma unroll
-              for (int kk = 0; kk < 3; ++kk) {
-                const int n = (ii * 3 + jj) * 3 + kk;
-                acc[n] = fmaf(wij * w[2][kk], qij + (float)kk * az, acc[n]);
-              }
+              const int n = (ii * 3 + jj) * 3;
+              acc[n] = fmaf(wij, w[2][0] * qij, acc[n]);
+              acc[n + 1] = fmaf(wij, fmaf(w[2][1], qij, cz1), acc[n + 1]);
+              acc[n + 2] = fmaf(wij, fmaf(w[2][2], qij, cz2), acc[n + 2]);
             }
           }
         }
