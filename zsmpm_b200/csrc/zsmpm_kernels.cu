@@ -484,9 +484,11 @@ __global__ void __launch_bounds__(kThreads) k_bin_scatter(scene_device s) {
 
 // Final particle order of a block: cells ascending, the particles of a cell in increasing
 // upload index (a stable sort by (block, cell)).  Also zeroes the block's grid and the
-// counts for the next substep.
-__global__ void __launch_bounds__(512) k_bin_finalize(scene_device s) {
-  constexpr int kMaxList = 24;
+// counts for the next substep.  Lists of up to 12 entries are sorted in registers, which
+// caps the kernel at 3 CTAs of 512 threads per SM (binning 0.71 -> 0.62 ms on the 30 M-particle
+// sand scene against a sort in local memory at 4 CTAs).
+__global__ void __launch_bounds__(512, 3) k_bin_finalize(scene_device s) {
+  constexpr int kMaxList = 12;
   __shared__ int s_b;
   const int nb = s.ctr[kCtrBlocks];
   const int t = threadIdx.x;
@@ -497,23 +499,29 @@ __global__ void __launch_bounds__(512) k_bin_finalize(scene_device s) {
     const int cs = s.cell_start[b * 512 + t];
     s.cell_count[b * 512 + t] = 0;
     if (c <= kMaxList) {
-      // two rounds of independent loads (the cell's particle list, then their upload ids),
-      // then an insertion sort of (id, index) pairs by id
-      int li[kMaxList], lid[kMaxList];
-      for (int r = 0; r < c; ++r) li[r] = s.tmp[cs + r];
-      for (int r = 0; r < c; ++r) lid[r] = s.cur.id[li[r]];
-      for (int r = 1; r < c; ++r) {
-        const int i = li[r], id = lid[r];
-        int q = r;
-        while (q > 0 && lid[q - 1] > id) {
-          lid[q] = lid[q - 1];
-          li[q] = li[q - 1];
-          --q;
+      // in registers (every index known at compile time): two rounds of independent loads
+      // (the cell's particle list, then their upload ids), then an insertion sort of the
+      // (id << 32 | index) entries; ids are unique, so this orders the cell by id
+      unsigned long long e[kMaxList];
+#pragma unroll
+      for (int r = 0; r < kMaxList; ++r) e[r] = r < c ? (unsigned long long)(uint32_t)s.tmp[cs + r] : ~0ull;
+#pragma unroll
+      for (int r = 0; r < kMaxList; ++r)
+        if (r < c) e[r] |= (unsigned long long)(uint32_t)s.cur.id[(int)(uint32_t)e[r]] << 32;
+#pragma unroll
+      for (int r = 1; r < kMaxList; ++r)
+        if (r < c) {
+#pragma unroll
+          for (int q = r; q > 0; --q) {
+            const unsigned long long lo = e[q - 1], hi = e[q];
+            const bool sw = lo > hi;
+            e[q - 1] = sw ? hi : lo;
+            e[q] = sw ? lo : hi;
+          }
         }
-        lid[q] = id;
-        li[q] = i;
-      }
-      for (int r = 0; r < c; ++r) s.src[cs + r] = li[r];
+#pragma unroll
+      for (int r = 0; r < kMaxList; ++r)
+        if (r < c) s.src[cs + r] = (int)(uint32_t)e[r];
     } else {
       // long lists (strongly compressed cells): insertion sort in place in global memory
       for (int r = 1; r < c; ++r) {
@@ -1970,7 +1978,7 @@ cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   k_cell_start<<<sm * 4, 512, 0, st>>>(s);
   k_bin_scatter<<<sm * 16, kThreads, 0, st>>>(s);
-  k_bin_finalize<<<sm * 4, 512, 0, st>>>(s);
+  k_bin_finalize<<<sm * 3, 512, 0, st>>>(s);
   return cudaGetLastError();
 }
 
