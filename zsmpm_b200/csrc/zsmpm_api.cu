@@ -334,6 +334,10 @@ ZSMPM_API zsmpm_status zsmpm_scene_create(const zsmpm_scene_desc *desc, zsmpm_sc
   scene_params &p = s->dev.prm;
   p.dx = desc->dx;
   p.inv_dx = 1.f / desc->dx;
+  {
+    int ex = 0;
+    p.dx_pow2 = std::isfinite(desc->dx) && desc->dx > 0.f && std::frexp(desc->dx, &ex) == 0.5f ? 1 : 0;
+  }
   p.dt = desc->dt;
   p.kappa = desc->dt * (4.f * p.inv_dx * p.inv_dx);  // dt * D_inv (P2G.hpp:52, :104)
   p.four_over_dx = 4.f * p.inv_dx;

@@ -62,6 +62,7 @@ struct scene_params {
   int table_size; // hash table slots (power of two)
   int bitmap_cap; // bitmap words available
   float dx, inv_dx, dt, kappa, four_over_dx;
+  int dx_pow2;    // dx is a power of two: x / dx is exactly x * inv_dx
   float gravity[3];
   int wall_type, wall_cells;
   material_dev mat;
