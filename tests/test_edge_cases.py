@@ -152,3 +152,48 @@ def test_hash_collisions_take_the_probe(zs, gpu):
         # the table index is the key's rank in ascending (bx, by, bz) order
         assert tuple(keys[ih[slot]]) == tuple(kh[slot])
     assert probed > 10
+
+
+def _activation_keys_after(zs, spec, p, steps):
+    """Runs `steps` substeps, then one activation; returns its keys and the particles' positions."""
+    with zs.Scene(spec, p) as sc:
+        sc.run(steps)
+        x = sc.download().x
+        sc.activate_blocks()
+        sc.status()
+        keys, _ = sc.download_grid()
+    return keys, x
+
+
+def _oracle_keys(x, dx):
+    from oracle import restated
+    okeys, _, _, _ = restated.activate(x, dx, max(len(x) // 512, 64))
+    return okeys[np.lexsort((okeys[:, 2], okeys[:, 1], okeys[:, 0]))]
+
+
+def test_activation_from_moved_blocks_matches_oracle(zs, gpu):
+    """After a G2P the activation inserts the blocks recorded per block of the last binning
+    (k_insert_moved_blocks); the keys equal those of the particles' stored positions."""
+    from zsmpm_b200 import scenes
+    spec = scenes.small_scene(model=1, mode=0, n_side=0.2, velocity=(3.0, -2.0, 1.5))
+    p = scenes.generate(spec)
+    for steps in (1, 7):
+        keys, x = _activation_keys_after(zs, spec, p, steps)
+        assert np.array_equal(keys, _oracle_keys(x, spec.dx)), steps
+
+
+def test_activation_after_a_far_move_matches_oracle(zs, gpu):
+    """A particle that crosses more than one block in a substep (|v| dt > 8 dx) sends the next
+    activation back to the particle pass."""
+    from zsmpm_b200 import scenes
+    spec = scenes.small_scene(model=0, mode=0)
+    p = scenes.generate(spec)
+    lone = _random_particles(1, 0.30, 0.30, 5, velocity_scale=0.0)
+    lone.x[:] = (0.2, 0.5, 0.5)
+    lone.v[:] = (1500.0, 0.0, 0.0)  # 0.15 per substep at dt = 1e-4: 19 cells
+    from zsmpm_b200.scenes import Particles
+    both = Particles(*(np.concatenate([a, b]) for a, b in zip(
+        (p.m, p.x, p.v, p.C, p.F, p.plastic), (lone.m, lone.x, lone.v, lone.C, lone.F, lone.plastic))))
+    keys, x = _activation_keys_after(zs, spec, both, 1)
+    assert x[-1, 0] > 0.3  # it crossed blocks
+    assert np.array_equal(keys, _oracle_keys(x, spec.dx))

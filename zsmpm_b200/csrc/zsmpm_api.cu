@@ -211,6 +211,7 @@ zsmpm_status allocate_blocks(zsmpm_scene *s, int64_t n) {
   ZS_ALLOC(d.ins_pk, nbc, "alloc ins_pk");
   ZS_ALLOC(d.ins_slot, nbc, "alloc ins_slot");
   ZS_ALLOC(d.blk_pk, nbc, "alloc blk_pk");
+  ZS_ALLOC(d.bmask, nbc, "alloc block move masks");
   ZS_ALLOC(d.nbr, 8 * nbc, "alloc nbr");
   ZS_ALLOC(d.bitmap, d.prm.bitmap_cap, "alloc bitmap");
   ZS_ALLOC(d.word_prefix, (int64_t)d.prm.bitmap_cap + 1, "alloc word prefix");

@@ -44,6 +44,9 @@ enum counter_slot : int {
   kCtrWords = 10,          // bitmap words in use
   kCtrWork = 11,           // 8 work counters for persistent kernels
   kCtrSubstep = 20,        // substeps begun since the scene was created (audit/log sampling)
+  kCtrMaskFrom = 21,       // blocks whose move masks the last G2P wrote (0: none since the upload)
+  kCtrMaskBad = 22,        // 1: a particle of the last G2P left its block's 3^3 neighbourhood
+  kCtrUseMasks = 23,       // this activation inserts from the move masks of that many blocks
   kCtrCount = 24
 };
 enum work_slot : int {
@@ -106,6 +109,8 @@ struct scene_device {
   uint64_t *ins_pk = nullptr; // [nb_cap] keys by insertion index
   int *ins_slot = nullptr;    // [nb_cap]
   uint64_t *blk_pk = nullptr; // [nb_cap] keys by final block index
+  uint32_t *bmask = nullptr;  // [nb_cap] per block: bit (ox+1)*9+(oy+1)*3+(oz+1) set when one of its
+                              // particles ended G2P in block + (ox, oy, oz)
   int *nbr = nullptr;         // [nb_cap][8]
   uint32_t *bitmap = nullptr; // [bitmap_cap]
   int *word_prefix = nullptr; // [bitmap_cap]

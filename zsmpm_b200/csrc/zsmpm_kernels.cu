@@ -234,7 +234,11 @@ __global__ void __launch_bounds__(kThreads) k_begin(scene_device s) {
   }
   if (blockIdx.x == 0 && threadIdx.x < kCtrCount) {
     const int t = threadIdx.x;
-    if (t == kCtrStatus) return;
+    if (t == kCtrStatus || t == kCtrMaskFrom || t == kCtrMaskBad) return;  // k_bitmap_prepare resets the last two
+    if (t == kCtrUseMasks) {
+      s.ctr[t] = s.ctr[kCtrMaskBad] == 0 ? s.ctr[kCtrMaskFrom] : 0;
+      return;
+    }
     if (t == kCtrSubstep) {
       s.ctr[t] += 1;
       return;
@@ -248,6 +252,7 @@ __global__ void __launch_bounds__(kThreads) k_begin(scene_device s) {
 
 // ComputeSparsity (SparsityOp.hpp:58-86): one insert per distinct block key of a warp.
 __global__ void __launch_bounds__(kThreads) k_insert_particle_blocks(scene_device s) {
+  if (s.ctr[kCtrUseMasks] > 0) return;  // k_insert_moved_blocks inserts this substep's blocks
   const int lane = threadIdx.x & 31;
   const int n = s.prm.n;
   int3 lo = make_int3(0x7fffffff, 0x7fffffff, 0x7fffffff);
@@ -304,6 +309,43 @@ __global__ void __launch_bounds__(kThreads) k_insert_particle_blocks(scene_devic
   }
 }
 
+// ComputeSparsity from the move masks the last G2P wrote: the blocks the particles of each
+// previous block ended in (the same set of keys as the particle pass finds, since G2P computes
+// each particle's block from the position it stores).  Runs instead of the particle pass
+// after a G2P in which no particle left its block's 3^3 neighbourhood.
+__global__ void __launch_bounds__(kThreads) k_insert_moved_blocks(scene_device s) {
+  const int nold = s.ctr[kCtrUseMasks];
+  if (nold == 0) return;
+  int3 lo = make_int3(0x7fffffff, 0x7fffffff, 0x7fffffff);
+  int3 hi = make_int3(-0x7fffffff, -0x7fffffff, -0x7fffffff);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nold * 27; t += grid_threads()) {
+    const int b = t / 27, j = t % 27;
+    if (!((s.bmask[b] >> j) & 1u)) continue;
+    const int3 k = unpack_key(s.blk_pk[b]);
+    const int3 nk = make_int3(k.x + j / 9 - 1, k.y + (j / 3) % 3 - 1, k.z + j % 3 - 1);
+    table_insert(s, pack_key(nk.x, nk.y, nk.z), nk, &s.ctr[kCtrParticleBlocks], 0);
+    lo = make_int3(min(lo.x, nk.x), min(lo.y, nk.y), min(lo.z, nk.z));
+    hi = make_int3(max(hi.x, nk.x), max(hi.y, nk.y), max(hi.z, nk.z));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo.x = min(lo.x, __shfl_xor_sync(kFull, lo.x, o));
+    lo.y = min(lo.y, __shfl_xor_sync(kFull, lo.y, o));
+    lo.z = min(lo.z, __shfl_xor_sync(kFull, lo.z, o));
+    hi.x = max(hi.x, __shfl_xor_sync(kFull, hi.x, o));
+    hi.y = max(hi.y, __shfl_xor_sync(kFull, hi.y, o));
+    hi.z = max(hi.z, __shfl_xor_sync(kFull, hi.z, o));
+  }
+  if ((threadIdx.x & 31) == 0 && lo.x != 0x7fffffff) {
+    atomicMin(&s.ctr[kCtrBoxLo + 0], lo.x);
+    atomicMin(&s.ctr[kCtrBoxLo + 1], lo.y);
+    atomicMin(&s.ctr[kCtrBoxLo + 2], lo.z);
+    atomicMax(&s.ctr[kCtrBoxHi + 0], hi.x);
+    atomicMax(&s.ctr[kCtrBoxHi + 1], hi.y);
+    atomicMax(&s.ctr[kCtrBoxHi + 2], hi.z);
+  }
+}
+
 // EnlargeSparsity{lo=0, hi=2} (SparsityOp.hpp:88-112): the +{0,1}^3 neighbours of every
 // particle block, so that the 3x3x3 stencil of every particle lands in active blocks.
 __global__ void __launch_bounds__(kThreads) k_enlarge(scene_device s) {
@@ -320,6 +362,8 @@ __global__ void __launch_bounds__(kThreads) k_enlarge(scene_device s) {
 // the blocks in ascending (bx, by, bz) order.
 __global__ void k_bitmap_prepare(scene_device s) {
   if (threadIdx.x != 0) return;
+  s.ctr[kCtrMaskFrom] = 0;  // the masks are spent: the ranks below renumber the blocks
+  s.ctr[kCtrMaskBad] = 0;
   int nb = s.ctr[kCtrParticleBlocks] + s.ctr[kCtrEnlarged];
   if (nb >= s.prm.table_size - 20) set_status(s.ctr, kStatusTableFull);  // HashTable.hpp:369
   if (nb > s.prm.nb_cap) {
@@ -1057,9 +1101,11 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
   float4 *svf = reinterpret_cast<float4 *>(g2p_smem);
   __shared__ int s_b;
   __shared__ material_dev s_mat;
+  __shared__ unsigned s_moved;  // the block's move mask
   const scene_params &p = s.prm;
   const int nb = s.ctr[kCtrBlocks];
   const int substep = s.ctr[kCtrSubstep];
+  if (blockIdx.x == 0 && threadIdx.x == 0) s.ctr[kCtrMaskFrom] = nb;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint2 *sfrag = reinterpret_cast<uint2 *>(g2p_smem + 4 * kHaloCells);
   float *sbias = reinterpret_cast<float *>(sfrag + kFragTotal);
@@ -1087,9 +1133,13 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
     const int b = grab_block(&s.ctr[kCtrWork + kWorkG2P], &s_b);
     if (b >= nb) break;
     const int start = s.block_start[b], end = s.block_start[b + 1];
-    if (start == end) continue;
+    if (start == end) {
+      if (threadIdx.x == 0) s.bmask[b] = 0u;
+      continue;
+    }
     const int3 gk = unpack_key(s.blk_pk[b]);
     if (kBatch && threadIdx.x == 0) s_mat = p.mats[scene_of_key(gk)];
+    if (threadIdx.x == 0) s_moved = 0u;
     // halo load: items (hx, hy, quad) over 12 x 12 x 3; each reads four consecutive cells of
     // the three velocity channels (16-byte loads) and writes four float4 nodes
     for (int it = threadIdx.x; it < kHalo * kHalo * 3; it += NT) {
@@ -1205,6 +1255,27 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
       xm.x += vel[0] * p.dt;
       xm.y += vel[1] * p.dt;
       xm.z += vel[2] * p.dt;
+      {
+        // the block of the new position, as the next activation computes it from the stored
+        // x, recorded relative to this block for k_insert_moved_blocks
+        unsigned bit = 0u;
+        bool moved_far = false;
+        if (active) {
+          int3 c2, b2;
+          if (particle_cell(s, kBatch ? s.cur.sid[icur] : 0, xm, c2, b2)) {
+            const int ox = b2.x - gk.x, oy = b2.y - gk.y, oz = b2.z - gk.z;
+            if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1 && oz >= -1 && oz <= 1)
+              bit = 1u << ((ox + 1) * 9 + (oy + 1) * 3 + (oz + 1));
+            else
+              moved_far = true;
+          } else {
+            moved_far = true;  // the particle pass of the next activation reports it
+          }
+        }
+        const unsigned wbits = __reduce_or_sync(kFull, bit);
+        if (lane == 0 && wbits) atomicOr(&s_moved, wbits);
+        if (__any_sync(kFull, moved_far) && lane == 0) s.ctr[kCtrMaskBad] = 1;
+      }
       // F <- (I + dt C) F
       float Fn[9];
 #pragma unroll
@@ -1245,6 +1316,8 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
       s.nxt.id[slot] = id;
       if (kBatch) s.nxt.sid[slot] = s.cur.sid[icur];
     }
+    __syncthreads();
+    if (threadIdx.x == 0) s.bmask[b] = s_moved;
   }
 }
 
@@ -1764,6 +1837,7 @@ __global__ void k_import_tv(scene_device s, const float *base, int nchn, int om,
 
 // stress of the stored state; A = m C - kappa tau (what the previous G2P would have written)
 __global__ void k_prime(scene_device s) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) s.ctr[kCtrMaskFrom] = 0;  // new particles: no move masks
   const size_t cap = (size_t)s.prm.cap;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s.prm.n; i += grid_threads()) {
     float F[9], tau[9];
@@ -1968,6 +2042,7 @@ cudaError_t launch_activate(scene_device &s, cudaStream_t st) {
   const int sm = num_sms();
   k_begin<<<sm * 4, kThreads, 0, st>>>(s);
   k_insert_particle_blocks<<<sm * 16, kThreads, 0, st>>>(s);
+  k_insert_moved_blocks<<<sm * 2, kThreads, 0, st>>>(s);
   k_enlarge<<<sm * 2, kThreads, 0, st>>>(s);
   k_bitmap_prepare<<<1, 32, 0, st>>>(s);
   k_bitmap_set<<<sm * 2, kThreads, 0, st>>>(s);
@@ -2110,9 +2185,10 @@ cudaError_t launch_cg_iteration(scene_device &s, float *x, const cg_vectors &v, 
   return cudaGetLastError();
 }
 
-// k_begin, insert, enlarge, prepare, set, 3 scans// k_begin, insert, enlarge, prepare, set, 3 scans, ranks, neighbours; count, 3 scans,
-// cell_start, scatter, finalize; p2g; grid update and boundaries; g2p
-int kernels_per_substep() { return 10 + 7 + 4; }
+// k_begin, the two particle-block inserts (one returns at once), enlarge, prepare, set, 3 scans,
+// ranks, neighbours; count, 3 scans, cell_start, scatter, finalize; p2g; grid update and
+// boundaries; g2p
+int kernels_per_substep() { return 11 + 7 + 4; }
 
 cudaError_t launch_import(scene_device &s, const float *m, const float *x, const float *v,
                           const float *C, const float *F, const float *plastic, int n,
