@@ -209,6 +209,10 @@ ZSMPM_API int64_t zsmpm_scene_num_particles(const zsmpm_scene *scene);
 ZSMPM_API zsmpm_status zsmpm_scene_status(zsmpm_scene *scene);
 
 /* ---- stages (each enqueues on `stream`, NULL = legacy default stream) --------------- */
+/* The block keys of the particles' current positions.  After a zsmpm_g2p the particle blocks
+ * come from the moves G2P recorded per block of the last binning (a particle that left its
+ * block's 3x3x3 neighbourhood, and every upload, make it read all particles instead); the keys
+ * are the same either way. */
 ZSMPM_API zsmpm_status zsmpm_activate_blocks(zsmpm_scene *scene, void *stream);
 ZSMPM_API zsmpm_status zsmpm_bin_particles(zsmpm_scene *scene, void *stream);
 ZSMPM_API zsmpm_status zsmpm_p2g(zsmpm_scene *scene, void *stream);
