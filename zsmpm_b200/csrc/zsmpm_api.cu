@@ -1091,7 +1091,9 @@ ZSMPM_API zsmpm_status zsmpm_autotune(zsmpm_scene *s, int32_t trials, zsmpm_tuni
   for (int a : g2p_threads)
     for (int b : g2p_per_sm) {
       if (s->dev.aux.learned && (a != 256 || b > 2)) continue;  // learned G2P: 256 threads, <= 2 per SM
-      if (a == 256 && b > 4) continue;                          // beyond what stays resident
+      // beyond what stays resident: 256 threads hold 80 registers and 58 KB of shared memory
+      // (3 CTAs per SM), 128 threads 43 KB (5)
+      if ((a == 256 && b > 3) || (a == 128 && b > 5)) continue;
       p.g2p_threads = a;
       p.g2p_ctas_per_sm = b;
       float ms = 0.f;
