@@ -73,18 +73,58 @@ def generate_workload(spec):
 
 
 class ClockSampler:
-    """nvidia-smi clock and throttle-reason sampling during the timed region."""
+    """SM clock and throttle reasons sampled every few milliseconds during the timed region.
+
+    NVML is read in a thread of this process (read-only queries; nothing is set), and only the
+    samples taken between mark_start() and mark_end() count.  Without NVML it falls back to an
+    nvidia-smi subprocess sampling every 100 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, period_s: float = 0.004):
         self.idx = device_index
+        self.period = period_s
         self.proc = None
         self.file = None
+        self.thread = None
+        self.stop = None
+        self.samples = []  # (time, sm MHz, max sm MHz, reason bits)
+        self.t0 = self.t1 = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.idx)
+        bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
 
     def __enter__(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.stop = threading.Event()
+
+            def run():
+                while not self.stop.is_set():
+                    try:
+                        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((time.perf_counter(), sm, mx, bits))
+                    except Exception:
+                        pass
+                    time.sleep(self.period)
+
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
@@ -94,7 +134,17 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_end(self):
+        self.t1 = time.perf_counter()
+
     def __exit__(self, *exc):
+        if self.thread:
+            time.sleep(2 * self.period)
+            self.stop.set()
+            self.thread.join(1.0)
         if self.proc:
             self.proc.terminate()
             try:
@@ -103,31 +153,36 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self) -> dict:
+        if self.thread is not None:
+            t0 = self.t0 if self.t0 is not None else -1e30
+            t1 = self.t1 if self.t1 is not None else 1e30
+            rows = [r for r in self.samples if t0 <= r[0] <= t1]
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
+            reasons = sorted({name for r in rows for name, bit in self.REASONS if r[3] & bit})
+            return {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": max(r[2] for r in rows),
+                    "reasons": reasons, "samples": len(rows), "source": "nvml, every 4 ms in the timed region"}
         if not self.file:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         self.file.flush()
         rows = []
         for line in Path(self.file.name).read_text().splitlines():
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
+            if len(parts) >= 9:
                 rows.append(parts)
-            except ValueError:
-                pass
         os.unlink(self.file.name)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [n for n, _ in self.REASONS]
         for r in rows:
             for name, val in zip(names, r[5:9]):
                 if val.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+                "reasons": sorted(reasons), "samples": len(rows), "source": "nvidia-smi"}
 
 
 def max_over_ranks(x: float, ws: int) -> float:
@@ -549,10 +604,12 @@ def main(argv=None):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
+        clk.mark_start()
         e0.record(stream)
         sc.run(args.steps, stream=sptr)
         e1.record(stream)
         torch.cuda.synchronize()
+        clk.mark_end()
     sc.status()
     ms = e0.elapsed_time(e1)
     ms = max_over_ranks(ms, ws)
