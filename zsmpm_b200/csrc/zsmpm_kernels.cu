@@ -685,12 +685,14 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
   const int nb = s.ctr[kCtrBlocks];
   const int t = threadIdx.x;
   const int my_cell = t & (kP2GChunk - 1), my_ch = t >> 6;
+  // the halo starts zeroed; each block's flush zeroes the quads it sends, so the next block
+  // finds it zeroed again (the first barrier of grab_block orders both)
+  for (int q = t; q < kGridChannels * kHaloCells; q += blockDim.x) sh[q] = 0.f;
   for (;;) {
     const int b = grab_block(&s.ctr[kCtrWork + kWorkP2G], &s_b);
     if (b >= nb) break;
     const int start = s.block_start[b], end = s.block_start[b + 1];
     if (start == end) continue;
-    for (int q = t; q < kGridChannels * kHaloCells; q += blockDim.x) sh[q] = 0.f;
     const int3 bk = local_block(s.prm, unpack_key(s.blk_pk[b]));
     const int ox = bk.x * 8, oy = bk.y * 8, oz = bk.z * 8;
     // cell starts of chunk k in s_cs0 + (k & 1) * (kP2GChunk + 1); the next chunk's are loaded
@@ -836,9 +838,11 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
     for (int it = t; it < kGridChannels * kHalo * kHalo * 3; it += blockDim.x) {
       const int quad = it % 3, hy = (it / 3) % kHalo, hx = (it / (3 * kHalo)) % kHalo,
                 ch = it / (3 * kHalo * kHalo);
-      const float *src4 = &sh[((ch * kHalo + hx) * kHalo + hy) * kHalo + quad * 4];
-      const float a0 = src4[0], a1 = src4[1], a2 = src4[2], a3 = src4[3];
+      float4 *src4 = reinterpret_cast<float4 *>(&sh[((ch * kHalo + hx) * kHalo + hy) * kHalo + quad * 4]);
+      const float4 q4 = *src4;
+      const float a0 = q4.x, a1 = q4.y, a2 = q4.z, a3 = q4.w;
       if (a0 == 0.f && a1 == 0.f && a2 == 0.f && a3 == 0.f) continue;
+      *src4 = make_float4(0.f, 0.f, 0.f, 0.f);
       const int tt = (hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0);
       const int tb = s.nbr[b * 8 + tt];
       if (tb < 0) {
