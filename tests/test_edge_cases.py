@@ -197,3 +197,19 @@ def test_activation_after_a_far_move_matches_oracle(zs, gpu):
     keys, x = _activation_keys_after(zs, spec, both, 1)
     assert x[-1, 0] > 0.3  # it crossed blocks
     assert np.array_equal(keys, _oracle_keys(x, spec.dx))
+
+
+def test_position_that_becomes_nan_is_reported_after_moved_blocks(zs, gpu):
+    """A NaN velocity turns positions NaN in the first G2P; that G2P cannot record their blocks,
+    so the next activation reads every particle and reports them out of domain."""
+    from zsmpm_b200 import scenes
+    spec = scenes.small_scene(model=0)
+    p = scenes.generate(spec)
+    p.v[7] = np.nan
+    with zs.Scene(spec, p) as sc:
+        sc.substep()
+        sc.status()  # the upload's positions are finite
+        sc.substep()
+        with pytest.raises(zs.ZsmpmError) as e:
+            sc.status()
+        assert e.value.status == zs._abi.ERR_OUT_OF_DOMAIN
