@@ -1371,12 +1371,13 @@ __global__ void __launch_bounds__(kG2P2GThreads, 2)
   }
   const int t = threadIdx.x;
   const int my_cell = t % kG2P2GChunk, my_ch = t / kG2P2GChunk;
+  // the force halo starts zeroed; each block's flush zeroes the quads it sends (as in k_p2g)
+  for (int q = t; q < 3 * kHaloCells; q += kG2P2GThreads) sf[q] = 0.f;
   for (;;) {
     const int b = grab_block(&s.ctr[kCtrWork + kWorkG2P2G], &s_b);
     if (b >= nb) break;
     const int start = s.block_start[b], end = s.block_start[b + 1];
     if (start == end) continue;
-    for (int q = t; q < 3 * kHaloCells; q += kG2P2GThreads) sf[q] = 0.f;
     // velocity halo: items (hx, hy, quad) over 12 x 12 x 3; four consecutive nodes are 12
     // consecutive floats (three 16-byte loads)
     for (int it = t; it < kHalo * kHalo * 3; it += kG2P2GThreads) {
@@ -1603,6 +1604,8 @@ __global__ void __launch_bounds__(kG2P2GThreads, 2)
 #pragma unroll
       for (int k = 0; k < 12; ++k) any = any || v[k] != 0.f;
       if (!any) continue;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) *reinterpret_cast<float4 *>(&sf[d * kHaloCells + h]) = make_float4(0.f, 0.f, 0.f, 0.f);
       const int tb = s.nbr[b * 8 + ((hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0))];
       if (tb < 0) {
         set_status(s.ctr, kStatusMissingBlock);
