@@ -217,6 +217,7 @@ zsmpm_status allocate_blocks(zsmpm_scene *s, int64_t n) {
   ZS_ALLOC(d.word_prefix, (int64_t)d.prm.bitmap_cap + 1, "alloc word prefix");
   ZS_ALLOC(d.ctr, kCtrCount, "alloc counters");
   ZS_ALLOC(d.block_count, nbc, "alloc block count");
+  ZS_ALLOC(d.work_order, nbc, "alloc work order");
   ZS_ALLOC(d.block_start, nbc + 1, "alloc block start");
   ZS_ALLOC(d.cell_count, 512 * nbc, "alloc cell count");
   ZS_ALLOC(d.cell_start, 512 * nbc, "alloc cell start");

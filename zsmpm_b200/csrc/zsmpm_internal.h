@@ -47,7 +47,9 @@ enum counter_slot : int {
   kCtrMaskFrom = 21,       // blocks whose move masks the last G2P wrote (0: none since the upload)
   kCtrMaskBad = 22,        // 1: a particle of the last G2P left its block's 3^3 neighbourhood
   kCtrUseMasks = 23,       // this activation inserts from the move masks of that many blocks
-  kCtrCount = 24
+  kCtrOrderFront = 24,     // blocks of at least kBigBlock particles placed at the front of work_order
+  kCtrOrderBack = 25,      // the others, placed from the back
+  kCtrCount = 28
 };
 enum work_slot : int {
   kWorkCellStart = 0,
@@ -124,11 +126,13 @@ struct scene_device {
   int *rnk = nullptr;         // [cap]
   int *tmp = nullptr;         // [cap]
   int *src = nullptr;         // [cap] slot -> index in cur
+  int *work_order = nullptr;  // [nb_cap] blocks in the order the per-block kernels take them
   int *scan_part = nullptr;   // [2 * kScanCtas + 1]
   float *grid = nullptr;      // [nb_cap][4][512]
 };
 
 constexpr int kScanCtas = 256;
+constexpr int kBigBlock = 2048;  // particles from which a block goes to the front of work_order
 
 // sets per-device kernel attributes (dynamic shared memory sizes); call with the device current
 cudaError_t prepare_kernels();

@@ -439,6 +439,10 @@ __global__ void __launch_bounds__(kThreads) k_neighbors(scene_device s) {
 // Per particle: its block index and stencil-origin cell; counts per cell (rank within the
 // cell from the atomic) and per block (warp-aggregated).
 __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s.ctr[kCtrOrderFront] = 0;  // k_cell_start fills work_order
+    s.ctr[kCtrOrderBack] = 0;
+  }
   const int lane = threadIdx.x & 31;
   const int n = s.prm.n;
   const int nb = s.ctr[kCtrBlocks];
@@ -510,6 +514,13 @@ __global__ void __launch_bounds__(512) k_cell_start(scene_device s) {
     int total;
     const int ex = cta_exclusive_scan<512>(c, total, sm);
     s.cell_start[b * 512 + threadIdx.x] = s.block_start[b] + ex;
+    // the per-block kernels take the big blocks first, so that they end on small ones
+    if (threadIdx.x == 0) {
+      if (total >= kBigBlock)
+        s.work_order[atomicAdd(&s.ctr[kCtrOrderFront], 1)] = b;
+      else
+        s.work_order[nb - 1 - atomicAdd(&s.ctr[kCtrOrderBack], 1)] = b;
+    }
   }
 }
 
@@ -689,8 +700,9 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
   // finds it zeroed again (the first barrier of grab_block orders both)
   for (int q = t; q < kGridChannels * kHaloCells; q += blockDim.x) sh[q] = 0.f;
   for (;;) {
-    const int b = grab_block(&s.ctr[kCtrWork + kWorkP2G], &s_b);
-    if (b >= nb) break;
+    const int w = grab_block(&s.ctr[kCtrWork + kWorkP2G], &s_b);
+    if (w >= nb) break;
+    const int b = s.work_order[w];
     const int start = s.block_start[b], end = s.block_start[b + 1];
     if (start == end) continue;
     const int3 bk = local_block(s.prm, unpack_key(s.blk_pk[b]));
@@ -1134,8 +1146,9 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
     for (int i = threadIdx.x; i < kBiasTotal; i += blockDim.x) sbias[i] = s.aux.cd.bias[i];
   }
   for (;;) {
-    const int b = grab_block(&s.ctr[kCtrWork + kWorkG2P], &s_b);
-    if (b >= nb) break;
+    const int w = grab_block(&s.ctr[kCtrWork + kWorkG2P], &s_b);
+    if (w >= nb) break;
+    const int b = s.work_order[w];
     const int start = s.block_start[b], end = s.block_start[b + 1];
     if (start == end) {
       if (threadIdx.x == 0) s.bmask[b] = 0u;
@@ -1374,8 +1387,9 @@ __global__ void __launch_bounds__(kG2P2GThreads, 2)
   // the force halo starts zeroed; each block's flush zeroes the quads it sends (as in k_p2g)
   for (int q = t; q < 3 * kHaloCells; q += kG2P2GThreads) sf[q] = 0.f;
   for (;;) {
-    const int b = grab_block(&s.ctr[kCtrWork + kWorkG2P2G], &s_b);
-    if (b >= nb) break;
+    const int w = grab_block(&s.ctr[kCtrWork + kWorkG2P2G], &s_b);
+    if (w >= nb) break;
+    const int b = s.work_order[w];
     const int start = s.block_start[b], end = s.block_start[b + 1];
     if (start == end) continue;
     // velocity halo: items (hx, hy, quad) over 12 x 12 x 3; four consecutive nodes are 12
