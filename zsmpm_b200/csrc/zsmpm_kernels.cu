@@ -93,9 +93,10 @@ __device__ __forceinline__ bool cell_of(const scene_params &p, float4 x, int3 &c
   return true;
 }
 
-// x / dx, as G2P computes the particle's position in cells (G2P.hpp:56-58): a multiplication
-// by 1/dx where dx is a power of two (the same number, since both scale by a power of two
-// exactly), else the correctly rounded division.  (In P2G the same branch measured slower.)
+// x / dx, as G2P and G2P2G compute the particle's position in cells (G2P.hpp:56-58,
+// G2P2G.hpp): a multiplication by 1/dx where dx is a power of two (the same number, since both
+// scale by a power of two exactly), else the correctly rounded division.  (In P2G the same
+// branch measured slower.)
 __device__ __forceinline__ float over_dx(const scene_params &p, float x) {
   return p.dx_pow2 ? x * p.inv_dx : __fdiv_rn(x, p.dx);
 }
@@ -1447,7 +1448,7 @@ __global__ void __launch_bounds__(kG2P2GThreads, 2)
 #pragma unroll
         for (int k = 0; k < 9; ++k) F[k] = s.cur.F[(size_t)k * p.cap + i];
         float pl = s.cur.plastic ? s.cur.plastic[i] : 0.f;
-        const float X[3] = {__fdiv_rn(xm.x, p.dx), __fdiv_rn(xm.y, p.dx), __fdiv_rn(xm.z, p.dx)};
+        const float X[3] = {over_dx(p, xm.x), over_dx(p, xm.y), over_dx(p, xm.z)};
         int hb[3];
         float w[3][3], f[3];
 #pragma unroll
