@@ -207,10 +207,17 @@ G2P_TRAFFIC_PER_PARTICLE = {"dp_two_boxes_dx256_8ppc": 745.91e6 / 3703824,
 
 
 def g2p_algorithmic_bytes(n: int, nb: int, plastic: bool) -> int:
-    """G2P per launch: per particle reads slot index 4, x|m 16, F 36, id 4 (+ plastic 4) and
-    writes x|m 16, v 16, C 36, A 36, F 36, id 4 (+ plastic 4); per active block reads the
-    3-channel velocity halo, 12 B per cell of the block (halo reads beyond the block come
-    from neighbours that are counted as their own blocks)."""
+    """G2P per launch, the survey's accounting: per particle reads x 12 and F 36 and writes
+    x 12, v 12, C 36, F 36 and the stress term 36 (180 B; +8 B for the plastic state read and
+    written); per active block reads the 3-channel velocity halo, 12 B per cell of the block
+    (halo reads beyond the block come from neighbours that are counted as their own blocks)."""
+    return n * (180 + (8 if plastic else 0)) + nb * 512 * 12
+
+
+def g2p_implementation_bytes(n: int, nb: int, plastic: bool) -> int:
+    """What this k_g2p actually moves per launch: per particle reads slot index 4, x|m 16,
+    F 36, id 4 (+ plastic 4) and writes x|m 16, v 16 (float4), C 36, A 36, F 36, id 4
+    (+ plastic 4), plus the same 12 B per block cell."""
     per_particle = 4 + 16 + 36 + 4 + 16 + 16 + 36 + 36 + 36 + 4 + (8 if plastic else 0)
     return n * per_particle + nb * 512 * 12
 
@@ -222,7 +229,7 @@ def substep_algorithmic_bytes(n: int, nb: int, plastic: bool) -> int:
     return n * (100 + 180 + (8 if plastic else 0) + 16) + nb * 512 * 72
 
 
-def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms):
+def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms, mlp=True):
     """The same workload with the learned closure in G2P.  The closure is trained on the GPU
     (this library's forward/backward/Adam kernels) on random trial states plus trial states
     logged from a few plain substeps of this scene, then the scene is re-uploaded, warmed up and
@@ -271,7 +278,7 @@ def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms
     sc.set_stage_timing(False)
     sc.status()
     cl.attach(sc, None)
-    mlp = mlp_inference_leg(c, n_rows=min(n, 16_777_216))
+    mlp = mlp_inference_leg(c, n_rows=min(n, 16_777_216)) if mlp else None
     c.close()
     value = n * args.steps * ws / (lms * 1e-3)
     return {"value": value, "unit": UNIT, "ms_per_step": lms / args.steps,
@@ -497,7 +504,7 @@ def reference_cpu_rate(spec, p, parts, steps, warmup, max_particles, threads, ti
         r = reference.run(sp, q, steps, policy=reference.POLICY_OMP, threads=threads, cap_blocks=0, timeout=timeout)
         seconds += r.seconds
         work += q.n * steps
-    return work / seconds, desc
+    return work / seconds, desc, sum(q.n for _, q in jobs)
 
 
 def run_reference_arm(args, spec, workload, n_full):
@@ -511,8 +518,11 @@ def run_reference_arm(args, spec, workload, n_full):
         return 0
     p, parts = generate_workload(spec)
     threads = os.cpu_count() or 1
-    value, desc = reference_cpu_rate(spec, p, parts, args.steps, max(args.warmup, 1), args.ref_particles,
-                                     threads, 3600)
+    # the sample shrinks with the step count so that the run stays within a few minutes
+    # (about 1.5e8 particle-substeps at ~3e6 particle-substeps/s on 16 cores)
+    sample_particles = max(100_000, min(args.ref_particles, int(1.5e8 // max(args.steps, 1))))
+    value, desc, sampled = reference_cpu_rate(spec, p, parts, args.steps, max(args.warmup, 1),
+                                              sample_particles, threads, 3600)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * n_full / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -521,24 +531,196 @@ def run_reference_arm(args, spec, workload, n_full):
                        "policy": "zs::omp_exec"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": desc},
+            "extrapolated_from": sampled,
+            "extrapolation": (f"particle-substeps/s measured on {sampled} of the workload's {n_full} particles; "
+                              "ms_per_step is the whole workload at that rate") if sampled < n_full else None,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
 
+class Workload:
+    """One scene (or batch) resident on the GPU, with pinned host copies of its inputs for the
+    end-to-end leg."""
+
+    def __init__(self, zs, spec, p, parts, local, stream):
+        import torch
+        self.zs, self.spec, self.p, self.parts = zs, spec, p, parts
+        self.n = p.n
+        self.stream, self.sptr = stream, stream.cuda_stream
+        self.specs = spec if isinstance(spec, list) else [spec]
+        self.plastic = any(sp.material.model != zs.FIXED_COROTATED for sp in self.specs)
+        self.pinned = {k: torch.from_numpy(getattr(p, k)).pin_memory() for k in ("m", "x", "v", "C", "F", "plastic")}
+        self.out_x = torch.empty((self.n, 3), dtype=torch.float32).pin_memory()
+        self.out_v = torch.empty((self.n, 3), dtype=torch.float32).pin_memory()
+        self.h2d_bytes = sum(t.numel() * 4 for t in self.pinned.values())
+        self.d2h_bytes = (self.out_x.numel() + self.out_v.numel()) * 4 + 4
+        self.lib = zs._abi.lib()
+        if parts is None:
+            self.sc = zs.Scene(spec, device=local)
+        else:
+            from zsmpm_b200 import batch
+            self.sc = batch.Batch(spec, device=local)
+            self.counts = (C.c_int64 * len(parts))(*[q.n for q in parts])
+
+    def upload_pinned(self):
+        zs = self.zs
+        arrs = zs._abi.ParticleArrays(**{k: C.c_void_p(t.data_ptr()) for k, t in self.pinned.items()})
+        if self.parts is None:
+            zs._abi.check(self.lib.zsmpm_scene_upload(self.sc.handle, C.byref(arrs), self.n, 0,
+                                                      C.c_void_p(self.sptr)), "upload")
+        else:
+            zs._abi.check(self.lib.zsmpm_batch_upload(self.sc.handle, C.byref(arrs), self.counts, 0,
+                                                      C.c_void_p(self.sptr)), "upload")
+        self.sc.n = self.n
+
+    def download_xv(self):
+        zs = self.zs
+        arrs = zs._abi.ParticleArrays(x=C.c_void_p(self.out_x.data_ptr()), v=C.c_void_p(self.out_v.data_ptr()))
+        zs._abi.check(self.lib.zsmpm_scene_download(self.sc.handle, C.byref(arrs), 0, C.c_void_p(self.sptr)),
+                      "download")
+
+    def close(self):
+        self.sc.close()
+
+
+def plain_leg(args, w, ws, local, with_e2e=True):
+    """Device-resident throughput over args.steps substeps (CUDA events on the launching stream,
+    clocks sampled inside the timed region), then a per-stage timing pass, then (optionally)
+    the end-to-end leg: pinned upload, args.steps substeps, download of x and v, status read."""
+    import torch
+    sc, stream, sptr, n = w.sc, w.stream, w.sptr, w.n
+    tuning = None
+    if not args.no_autotune:
+        w.upload_pinned()
+        tuning = sc.autotune(trials=2, stream=sptr)
+    w.upload_pinned()
+    torch.cuda.synchronize()
+    sc.run(args.warmup, stream=sptr)
+    sc.status()
+    torch.cuda.synchronize()
+    barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        clk.mark_start()
+        e0.record(stream)
+        sc.run(args.steps, stream=sptr)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk.mark_end()
+    sc.status()
+    ms = max_over_ranks(e0.elapsed_time(e1), ws)
+    barrier(ws)
+    nb = sc.num_blocks()
+    # per-stage timing pass (events between the stages of single substeps)
+    sc.set_stage_timing(True)
+    stage = np.zeros(5)
+    reps = min(args.steps, 8)
+    for _ in range(reps):
+        sc.substep(stream=sptr)
+        stage += np.array(sc.stage_times())
+    sc.set_stage_timing(False)
+    stage /= reps
+    sc.status()
+    peak, peak_kind = hbm_peak()
+    g2p_bytes = g2p_algorithmic_bytes(n, nb, w.plastic)
+    g2p_gbs = g2p_bytes / (stage[4] * 1e-3) / 1e9
+    total_bytes = substep_algorithmic_bytes(n, nb, w.plastic)
+    out = {
+        "value": n * args.steps * ws / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps,
+        "particles": n, "active_blocks": nb, "launch_shapes": tuning, "clocks": clk.summary(),
+        "stage_ms": {"activate": stage[0], "bin": stage[1], "p2g": stage[2], "grid_update": stage[3],
+                     "g2p": stage[4]},
+        "g2p_roofline": {"bound": "hbm", "kernel": "k_g2p", "achieved": g2p_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": g2p_gbs / peak, "peak_kind": f"{peak_kind} copy bandwidth",
+                         "algorithmic_bytes_per_launch": g2p_bytes,
+                         "implementation_bytes_per_launch": g2p_implementation_bytes(n, nb, w.plastic),
+                         "launch_ms": stage[4]},
+        "substep_roofline": {"algorithmic_bytes_per_substep": total_bytes,
+                             "achieved_gbs": total_bytes / (ms / args.steps * 1e-3) / 1e9,
+                             "frac": total_bytes / (ms / args.steps * 1e-3) / 1e9 / peak,
+                             "peak": peak, "peak_kind": f"{peak_kind} copy bandwidth"},
+        "gpu_launches": sc.kernels_per_substep() * args.steps,
+    }
+    if with_e2e:
+        torch.cuda.synchronize()
+        barrier(ws)
+        t0 = time.perf_counter()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        w.upload_pinned()
+        sc.run(args.steps, stream=sptr)
+        w.download_xv()
+        f1.record(stream)
+        sc.status()  # device -> host status word
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(f0.elapsed_time(f1), ws)
+        out["e2e"] = {"value": n * args.steps * ws / (e2e_ms * 1e-3), "unit": UNIT,
+                      "h2d_bytes_per_step": w.h2d_bytes / args.steps, "d2h_bytes_per_step": w.d2h_bytes / args.steps,
+                      "wall_s": time.perf_counter() - t0,
+                      "what": "upload from pinned host, K substeps, download x and v, status read"}
+    return out
+
+
+def cpu_baselines(args, spec, p, parts):
+    """The compiled reference's zs::omp_exec path on a bounded sample, on all host cores and at
+    zpc's default thread count (hardware_concurrency - 1, omp/execution/ExecutionPolicy.hpp:1242)."""
+    from oracle import reference
+    if not reference.available():
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/zsref_cli not built"}
+    try:
+        threads = os.cpu_count() or 1
+        rate, desc, sampled = reference_cpu_rate(spec, p, parts, args.ref_steps, 0, args.ref_particles, threads, 900)
+        out = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+               "sample": f"{desc}, {args.ref_steps} substeps, zs::omp_exec", "extrapolated_from": sampled}
+        # zpc's own default: omp_exec() with hardware_concurrency - 1 threads (threads <= 0 in the driver)
+        rate_d, _, _ = reference_cpu_rate(spec, p, parts, args.ref_steps, 0, args.ref_particles, 0, 900)
+        out["zpc_default_threads"] = {"value": rate_d, "unit": UNIT, "cores": max(threads - 1, 1),
+                                      "what": "zs::omp_exec() default, hardware_concurrency - 1 threads"}
+        return out
+    except Exception as exc:  # report, never fail the GPU line
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
+
+
+def extra_leg(args, name, ws, local, stream, learned: bool):
+    """Another workload of the survey's configurations, measured the same way as the main one
+    (plain device-resident throughput, stage times and rooflines; learned closure if asked)."""
+    import zsmpm_b200 as zs
+    spec, workload = scene_for(name)
+    p, parts = generate_workload(spec)
+    w = Workload(zs, spec, p, parts, local, stream)
+    try:
+        out = {"workload": workload, **plain_leg(args, w, ws, local, with_e2e=False)}
+        if learned:
+            if parts is None:
+                out["learned"] = learned_leg(args, zs, w.sc, spec, w.n, w.upload_pinned, stream, w.sptr, ws,
+                                             out["ms_per_step"], mlp=False)
+            else:
+                out["learned"] = batch_learned_leg(args, zs, w.sc, spec, parts, w.upload_pinned, stream, w.sptr,
+                                                   ws, out["ms_per_step"])
+    finally:
+        w.close()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scene", default="dp", choices=["dp", "dp128", "fc", "snow16m", "batch256"])
     ap.add_argument("--ref-particles", type=int, default=1_500_000)
     ap.add_argument("--ref-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-learned", action="store_true", help="skip the learned-closure leg")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-closure legs")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes")
     ap.add_argument("--no-implicit", action="store_true", help="skip the implicit-system leg")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="measure only --scene (by default the sand scene run also measures the 16 M snow "
+                         "scene, plain and learned, and the 256-scene batch)")
     ap.add_argument("--train-random", type=int, default=1_500_000)
     ap.add_argument("--train-logged", type=int, default=500_000)
     args = ap.parse_args(argv)
@@ -556,104 +738,21 @@ def main(argv=None):
 
     import zsmpm_b200 as zs
     torch.cuda.set_device(local)
-    p, parts = generate_workload(spec)
-    n = p.n
     stream = torch.cuda.Stream()
-    sptr = stream.cuda_stream
-    specs = spec if isinstance(spec, list) else [spec]
-    plastic = any(sp.material.model != zs.FIXED_COROTATED for sp in specs)
-
-    # pinned host copies of the inputs for the end-to-end leg
-    pinned = {k: torch.from_numpy(getattr(p, k)).pin_memory() for k in ("m", "x", "v", "C", "F", "plastic")}
-    out_x = torch.empty((n, 3), dtype=torch.float32).pin_memory()
-    out_v = torch.empty((n, 3), dtype=torch.float32).pin_memory()
-    h2d_bytes = sum(t.numel() * 4 for t in pinned.values())
-    d2h_bytes = (out_x.numel() + out_v.numel()) * 4 + 4
-
-    lib = zs._abi.lib()
-    if parts is None:
-        sc = zs.Scene(spec, device=local)
-    else:
-        from zsmpm_b200 import batch
-        sc = batch.Batch(spec, device=local)
-        counts = (C.c_int64 * len(parts))(*[q.n for q in parts])
-
-    def upload_pinned():
-        arrs = zs._abi.ParticleArrays(**{k: C.c_void_p(t.data_ptr()) for k, t in pinned.items()})
-        if parts is None:
-            zs._abi.check(lib.zsmpm_scene_upload(sc.handle, C.byref(arrs), n, 0, C.c_void_p(sptr)), "upload")
-        else:
-            zs._abi.check(lib.zsmpm_batch_upload(sc.handle, C.byref(arrs), counts, 0, C.c_void_p(sptr)), "upload")
-        sc.n = n
-
-    def download_xv():
-        arrs = zs._abi.ParticleArrays(x=C.c_void_p(out_x.data_ptr()), v=C.c_void_p(out_v.data_ptr()))
-        zs._abi.check(lib.zsmpm_scene_download(sc.handle, C.byref(arrs), 0, C.c_void_p(sptr)), "download")
-
-    # ---------------------------------------------------------------- launch shapes
-    upload_pinned()
-    tuning = sc.autotune(trials=2, stream=sptr) if not args.no_autotune else None
-
-    # ---------------------------------------------------------------- device-resident leg
-    upload_pinned()
-    torch.cuda.synchronize()
-    sc.run(args.warmup, stream=sptr)
-    sc.status()
-    torch.cuda.synchronize()
-    barrier(ws)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        torch.cuda.synchronize()
-        clk.mark_start()
-        e0.record(stream)
-        sc.run(args.steps, stream=sptr)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        clk.mark_end()
-    sc.status()
-    ms = e0.elapsed_time(e1)
-    ms = max_over_ranks(ms, ws)
-    barrier(ws)
-    value = n * args.steps * ws / (ms * 1e-3)
-    nb = sc.num_blocks()
-
-    # ---------------------------------------------------------------- per-stage timing pass
-    sc.set_stage_timing(True)
-    stage = np.zeros(5)
-    reps = min(args.steps, 8)
-    for _ in range(reps):
-        sc.substep(stream=sptr)
-        stage += np.array(sc.stage_times())
-    sc.set_stage_timing(False)
-    stage /= reps
-    sc.status()
-    peak, peak_kind = hbm_peak()
-    g2p_bytes = g2p_algorithmic_bytes(n, nb, plastic)
-    g2p_gbs = g2p_bytes / (stage[4] * 1e-3) / 1e9
-
-    # ---------------------------------------------------------------- end-to-end leg
-    torch.cuda.synchronize()
-    barrier(ws)
-    t0 = time.perf_counter()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    upload_pinned()
-    sc.run(args.steps, stream=sptr)
-    download_xv()
-    f1.record(stream)
-    sc.status()  # device -> host status word
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(f0.elapsed_time(f1), ws)
-    wall = time.perf_counter() - t0
-    e2e = n * args.steps * ws / (e2e_ms * 1e-3)
+    p, parts = generate_workload(spec)
+    w = Workload(zs, spec, p, parts, local, stream)
+    n = w.n
+    specs = w.specs
+    main_leg = plain_leg(args, w, ws, local, with_e2e=True)
+    ms = main_leg["ms_per_step"] * args.steps
 
     # ---------------------------------------------------------------- learned-closure leg
     learned = None
-    if plastic and parts is None and not args.no_learned:
-        learned = learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, ms / args.steps)
-    elif plastic and not args.no_learned:
-        learned = batch_learned_leg(args, zs, sc, specs, parts, upload_pinned, stream, sptr, ws, ms / args.steps)
+    if w.plastic and parts is None and not args.no_learned:
+        learned = learned_leg(args, zs, w.sc, spec, n, w.upload_pinned, stream, w.sptr, ws, ms / args.steps)
+    elif w.plastic and not args.no_learned:
+        learned = batch_learned_leg(args, zs, w.sc, specs, parts, w.upload_pinned, stream, w.sptr, ws,
+                                    ms / args.steps)
 
     # ---------------------------------------------------------------- implicit-system leg
     implicit = None
@@ -666,62 +765,52 @@ def main(argv=None):
                     sample = implicit_cpu_sample(spec, p, args.ref_particles)
             except Exception:
                 sample = None
-        implicit = implicit_leg(args, zs, sc, spec, upload_pinned, stream, sptr, sample)
+        implicit = implicit_leg(args, zs, w.sc, spec, w.upload_pinned, stream, w.sptr, sample)
+    w.close()
+    del w
+
+    # ---------------------------------------------------------------- the other stated workloads
+    legs = {}
+    if args.scene == "dp" and not args.no_extra:
+        legs["snow16m"] = extra_leg(args, "snow16m", ws, local, stream, learned=not args.no_learned)
+        legs["batch256"] = extra_leg(args, "batch256", ws, local, stream, learned=False)
 
     # ---------------------------------------------------------------- CPU baseline (rank 0, N=1)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        try:
-            from oracle import reference
-            if reference.available():
-                threads = os.cpu_count() or 1
-                rate, desc = reference_cpu_rate(spec, p, parts, args.ref_steps, 0, args.ref_particles, threads, 900)
-                cpu = {"value": rate, "unit": UNIT, "cores": threads,
-                       "kind": "reference", "sample": f"{desc}, {args.ref_steps} substeps, zs::omp_exec"}
-            else:
-                cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                       "sample": "unavailable: oracle/_ref/zsref_cli not built"}
-        except Exception as exc:  # report, never fail the GPU line
-            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
+        cpu = cpu_baselines(args, spec, p, parts)
 
-    total_bytes = substep_algorithmic_bytes(n, nb, plastic)
     if rank == 0:
+        g2p = main_leg["g2p_roofline"]
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "metric": METRIC, "value": main_leg["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": main_leg["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload, "particles": n, "active_blocks": nb, "scenes": len(specs),
-                       "dx": specs[0].dx, "ppc": specs[0].ppc, "dt": specs[0].dt,
+            "config": {"workload": workload, "particles": n, "active_blocks": main_leg["active_blocks"],
+                       "scenes": len(specs), "dx": specs[0].dx, "ppc": specs[0].ppc, "dt": specs[0].dt,
                        "material": "mixed fixed_corotated / drucker_prager" if len(specs) > 1 else
                        ("drucker_prager" if specs[0].material.model == zs.DRUCKER_PRAGER else
                         ("snow" if specs[0].material.model == zs.SNOW else "fixed_corotated")),
-                       "closure": "plain", "parallelism": f"replicas{ws}", "launch_shapes": tuning,
-                       "l2": "inputs larger than L2 (particle state 4+ GB)",
+                       "closure": "plain", "parallelism": f"replicas{ws}",
+                       "launch_shapes": main_leg["launch_shapes"],
+                       "l2": "inputs larger than L2 (particle state 2+ GB per workload)",
                        "substep_graph": "CUDA graph of 2 substeps"},
-            "roofline": {"bound": "hbm", "kernel": "k_g2p", "achieved": g2p_gbs, "peak": peak,
-                         "unit": "GB/s", "frac": g2p_gbs / peak,
+            "roofline": {**g2p,
                          "traffic": (G2P_TRAFFIC_PER_PARTICLE[workload] * n if workload in G2P_TRAFFIC_PER_PARTICLE
                                      else None),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per particle of a "
-                                           "k_g2p launch (profiles/), times this launch's particles",
-                         "peak_kind": f"{peak_kind} copy bandwidth",
-                         "algorithmic_bytes_per_launch": g2p_bytes, "launch_ms": stage[4]},
-            "stage_ms": {"activate": stage[0], "bin": stage[1], "p2g": stage[2], "grid_update": stage[3],
-                         "g2p": stage[4]},
-            "substep_roofline": {"algorithmic_bytes_per_substep": total_bytes,
-                                 "achieved_gbs": total_bytes / (ms / args.steps * 1e-3) / 1e9,
-                                 "frac": total_bytes / (ms / args.steps * 1e-3) / 1e9 / peak},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes / args.steps,
-                    "d2h_bytes_per_step": d2h_bytes / args.steps, "wall_s": wall,
-                    "what": "upload from pinned host, K substeps, download x and v, status read"},
-            "gpu_launches": sc.kernels_per_substep() * args.steps,
-            "clocks": clk.summary(),
+                                           "k_g2p launch (profiles/), times this launch's particles"},
+            "stage_ms": main_leg["stage_ms"],
+            "substep_roofline": main_leg["substep_roofline"],
+            "e2e": main_leg["e2e"],
+            "gpu_launches": main_leg["gpu_launches"],
+            "clocks": main_leg["clocks"],
             "cpu_baseline": cpu,
             "learned": learned,
             "implicit": implicit,
+            "legs": legs,
         }
         print(json.dumps(line))
-    sc.close()
     replicas.finish()
     return 0
 

@@ -507,9 +507,11 @@ ZSMPM_API zsmpm_status zsmpm_scene_state_log_count(zsmpm_scene *s, int64_t *coun
  * reached, -2 more than cap_blocks blocks, -3 a position is NaN/Inf or out of range.
  * Its scratch is one fixed array of about 3 MB in device memory, held on every GPU that
  * loads the library until the process exits; it limits a call to 1,048,576 particles
- * (larger n is rejected with ZSMPM_ERR_CAPACITY), 32,748 active blocks and an active-block
- * bounding box of 2^21 positions.  The first call on a device looks up the array's device
- * address with that device current, so make that first call before any stream capture.
+ * (larger n, or n < 1, is rejected with ZSMPM_ERR_CAPACITY), 32,748 active blocks (a
+ * 32,768-slot table on every call, whatever n) and an active-block bounding box of 2^21
+ * positions.  The array's device address is looked up once per CUDA context, on the first
+ * call made with that context current, so make that first call before any stream capture;
+ * a context recreated after cudaDeviceReset gets its own lookup.
  * All calls share the array and each overwrites the last one's contents; calls whose work
  * overlaps on the GPU race and give undefined results. */
 ZSMPM_API zsmpm_status zsmpm_activate_blocks_noalloc(const float *x, int64_t n, float dx,

@@ -30,3 +30,14 @@ def gpu(zs):
     import torch
     torch.cuda.init()
     return torch.device("cuda:0")
+
+
+@pytest.fixture(scope="session")
+def reference_cli():
+    """The compiled reference (oracle/_ref/zsref_cli).  GPU parity tests compare against it and
+    fail when it is missing, rather than compare against the restatement in its place."""
+    from oracle import reference
+    if not reference.available():
+        pytest.fail("oracle/_ref/zsref_cli (the reference compiled by oracle/build_ref.sh) is missing; "
+                    "the parity tests that name the reference never fall back to the restatement")
+    return reference

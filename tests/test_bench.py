@@ -34,6 +34,18 @@ def test_reference_arm_prints_the_contract_line():
     assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["value"] == line["value"]
     assert line["e2e"]["value"] == line["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    # a sample of the 30 M-particle workload: the line says how many particles it ran
+    assert 0 < line["extrapolated_from"] < line["config"]["particles"]
+    assert line["extrapolation"]
+
+
+def test_g2p_bytes_follow_the_survey_accounting():
+    bench = _bench_module()
+    # 188 B per plastic particle (180 + logJp read and write) and 12 B per active cell
+    assert bench.g2p_algorithmic_bytes(30_089_900, 10_450, True) == 30_089_900 * 188 + 10_450 * 512 * 12
+    assert bench.g2p_algorithmic_bytes(1, 0, False) == 180
+    assert bench.g2p_implementation_bytes(1, 0, True) == 212
+    assert bench.substep_algorithmic_bytes(1, 0, True) == 304
 
 
 def test_clock_sampler_keeps_the_timed_region():

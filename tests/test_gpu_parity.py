@@ -89,8 +89,9 @@ def test_constitutive_matches_oracle(zs, gpu, model, mode):
     assert np.max(np.abs(dpl.cpu().numpy() - pl_o)) < 1e-4
 
 
-def test_block_keys_bit_exact_vs_reference(zs, gpu):
-    from oracle import reference, restated
+def test_block_keys_bit_exact_vs_reference(zs, gpu, reference_cli):
+    from oracle import restated
+    reference = reference_cli
     from zsmpm_b200 import scenes
     spec = scenes.small_scene(model=0, n_side=0.2, velocity=(0, 0, 0))
     p = scenes.generate(spec)
@@ -108,11 +109,10 @@ def test_block_keys_bit_exact_vs_reference(zs, gpu):
     # canonical order: ascending (bx, by, bz)
     srt = okeys[np.lexsort((okeys[:, 2], okeys[:, 1], okeys[:, 0]))]
     assert np.array_equal(keys, srt)
-    if reference.available():
-        rkeys, rslots, _, rts = reference.activate(p.x, spec.dx, expected)
-        assert rts == T
-        assert np.array_equal(np.sort(rkeys.view("i4,i4,i4"), axis=0), np.sort(okeys.view("i4,i4,i4"), axis=0))
-        assert np.array_equal(rslots, oslots)
+    rkeys, rslots, _, rts = reference.activate(p.x, spec.dx, expected)
+    assert rts == T
+    assert np.array_equal(np.sort(rkeys.view("i4,i4,i4"), axis=0), np.sort(okeys.view("i4,i4,i4"), axis=0))
+    assert np.array_equal(rslots, oslots)
 
 
 def _d2h(ptr: int, shape, dtype) -> np.ndarray:
@@ -200,20 +200,21 @@ def _run_gpu(zs, spec, p, steps, graph=False):
 
 
 @pytest.mark.parametrize("model", [0, 1])
-def test_substep_matches_reference_cpu_path(zs, gpu, model):
+def test_substep_matches_reference_cpu_path(zs, gpu, reference_cli, model):
     """Reference ordering (stress and return map in P2G, F not projected) against the
     reference's own sequential CPU path.  Relative L2 errors: x below 1e-6, v below 1e-5,
     F - I and C below 1e-4, grid mass 1e-6 and momentum 1e-5."""
-    from oracle import reference, restated
+    from oracle import restated
     from zsmpm_b200 import scenes
+    reference = reference_cli
     spec = scenes.small_scene(model=model, mode=1, velocity=(0.4, -0.3, 0.2))
     p = deforming(scenes.generate(spec))
     steps = 10
     g, gk, gg = _run_gpu(zs, spec, p, steps)
-    ref = reference.run(spec, p, steps, policy=0) if reference.available() else None
-    o32 = restated.run(spec, p, steps, "f32", mode=1)
+    ref = reference.run(spec, p, steps, policy=0)
+    assert ref.status == 0
     o64 = restated.run(spec, p, steps, "f64", mode=1)
-    base = ref if ref is not None else o32
+    base = ref
     assert rel_l2(g.x, base.x) < 1e-6
     assert rel_l2(g.v, base.v) < 1e-5
     assert rel_l2(g.F, base.F) < 1e-6
@@ -240,7 +241,7 @@ def test_substep_matches_reference_cpu_path(zs, gpu, model):
           f"momentum {np.linalg.norm(pb - p64) / np.linalg.norm(p64):.2e}")
     if model == 1:
         # the GPU keeps logJp one projection ahead (see zsmpm.h); advance the reference's
-        _, _, lj = restated.stress(spec, base.F, base.plastic if ref is None else ref.logJp, mode=1)
+        _, _, lj = restated.stress(spec, base.F, ref.logJp, mode=1)
         assert np.max(np.abs(g.plastic - lj)) < 1e-4
 
 

@@ -8,6 +8,7 @@
 //   transfer    k_p2g, k_grid_update, k_g2p
 // Reference operators replaced: SparsityOp.hpp:41-112 (activation), SparsityOp.hpp:115-196
 // (binning), P2G.hpp:45-127, GridOp.hpp:54-164, G2P.hpp:43-84 (paths inside include/zensim).
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -366,7 +367,8 @@ __global__ void k_bitmap_prepare(scene_device s) {
   s.ctr[kCtrMaskFrom] = 0;  // the masks are spent: the ranks below renumber the blocks
   s.ctr[kCtrMaskBad] = 0;
   int nb = s.ctr[kCtrParticleBlocks] + s.ctr[kCtrEnlarged];
-  if (nb >= s.prm.table_size - 20) set_status(s.ctr, kStatusTableFull);  // HashTable.hpp:369
+  // HashTable.hpp:369 flags an insertion index >= T - 20, i.e. more than T - 20 blocks
+  if (nb > s.prm.table_size - 20) set_status(s.ctr, kStatusTableFull);
   if (nb > s.prm.nb_cap) {
     set_status(s.ctr, kStatusCapacity);
     nb = s.prm.nb_cap;
@@ -2046,15 +2048,21 @@ __global__ void __launch_bounds__(kThreads) k_export_keys(scene_device s, int *k
     keys_out[t] = s.active_keys[t];
 }
 
-int g_num_sms = 0;
+// SM count of the current device, looked up once per device ordinal.  Two host threads that
+// look up the same device at once store the same value, so the atomics need no lock.
+constexpr int kMaxDevices = 64;
+std::atomic<int> g_num_sms[kMaxDevices];
 int num_sms() {
-  if (g_num_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) dev = -1;
+  int n = dev >= 0 ? g_num_sms[dev].load(std::memory_order_relaxed) : 0;
+  if (n <= 0) {
+    if (dev < 0 || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+    else
+      g_num_sms[dev].store(n, std::memory_order_relaxed);
   }
-  return g_num_sms;
+  return n;
 }
 
 }  // namespace

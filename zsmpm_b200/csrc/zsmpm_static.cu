@@ -7,11 +7,12 @@
 // bitmap, scan partials, counters) lives in a fixed file-scope device array instead of
 // scene-owned buffers; the caller passes the inputs and the outputs.
 //
-// Limits: at most kNoAllocMaxParticles particles (the table is sized by the reference's
-// rule next_2pow(max(n/512, 64)) * 16 slots, at most kNoAllocTableSlots), at most
-// kNoAllocTableSlots - 20 active blocks, and an active-block bounding box of at most
-// kNoAllocBitmapWords * 32 positions.  The array occupies kNoAllocScratchBytes (about 3 MB)
-// on every GPU that loads the library, until the process exits.
+// Limits: at most kNoAllocMaxParticles particles, at most kNoAllocTableSlots - 20 active
+// blocks (every call uses the whole kNoAllocTableSlots-slot table: the sorted keys do not
+// depend on the table size, so a sparse input of few particles may still activate up to that
+// many blocks), and an active-block bounding box of at most kNoAllocBitmapWords * 32
+// positions.  The array occupies kNoAllocScratchBytes (about 3 MB) on every GPU that loads the
+// library, until the process exits.
 //
 // Every call shares the one array and overwrites what the previous call left there; each
 // call clears the parts that must start at zero (table, counters, bitmap, status) itself.
@@ -21,6 +22,7 @@
 #include <mutex>
 #include <string>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "zsmpm.h"
@@ -55,27 +57,79 @@ constexpr size_t kNoAllocScratchBytes = kOffScan + align256(4 * kNoAllocScanPart
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 // Host code must not pass &g_noalloc_scratch to a kernel: on the host that name is a
-// stand-in, not a device address.  The device address is looked up once per device with
-// that device current and cached here.
-constexpr int kMaxDevices = 64;
+// stand-in, not a device address.  The device address belongs to a CUDA context (the module
+// holding the array is loaded per context), so it is looked up with cudaGetSymbolAddress once
+// per context, with that context's device current, and cached under the context's
+// process-unique id (cuCtxGetId).  A context that the caller destroys and recreates (for
+// example after cudaDeviceReset), or a context the host made itself, has a new id and gets a
+// fresh lookup, so a cached address is never used outside the context it came from.  The two
+// driver calls are reached through cudaGetDriverEntryPoint, so the library needs no libcuda
+// link.
+using ctx_get_current_fn = CUresult (*)(CUcontext *);
+using ctx_get_id_fn = CUresult (*)(CUcontext, unsigned long long *);
+constexpr int kMaxContexts = 64;
 std::mutex g_mutex;
-unsigned char *g_address[kMaxDevices] = {};
+ctx_get_current_fn g_ctx_get_current = nullptr;
+ctx_get_id_fn g_ctx_get_id = nullptr;
+struct cached_address {
+  unsigned long long ctx_id;
+  unsigned char *ptr;
+};
+cached_address g_cache[kMaxContexts] = {};
+int g_cached = 0;  // entries in use
+int g_oldest = 0;  // entry replaced next once all are in use
 
-int scratch_address(int device, unsigned char **out) {
-  if (device < 0 || device >= kMaxDevices)
-    return record_error(ZSMPM_ERR_INVALID_ARG, "device ordinal out of range");
+int driver_calls() {
+  if (g_ctx_get_current && g_ctx_get_id) return ZSMPM_OK;
+  void *f0 = nullptr, *f1 = nullptr;
+  cudaDriverEntryPointQueryResult q0{}, q1{};
+  cudaError_t e0 = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0);
+  cudaError_t e1 = cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1);
+  if (e0 != cudaSuccess || e1 != cudaSuccess || !f0 || !f1 || q0 != cudaDriverEntryPointSuccess ||
+      q1 != cudaDriverEntryPointSuccess)
+    return record_error(ZSMPM_ERR_CUDA, "cuCtxGetCurrent / cuCtxGetId not available from the CUDA driver");
+  g_ctx_get_current = reinterpret_cast<ctx_get_current_fn>(f0);
+  g_ctx_get_id = reinterpret_cast<ctx_get_id_fn>(f1);
+  return ZSMPM_OK;
+}
+
+int current_context_id(unsigned long long *id) {
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return 1;
+  return g_ctx_get_id(ctx, id) == CUDA_SUCCESS ? 0 : 1;
+}
+
+int scratch_address(unsigned char **out) {
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_address[device]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      std::string msg = std::string("cudaGetSymbolAddress of the no-alloc scratch: ") +
-                        cudaGetErrorString(e);
-      return record_error(ZSMPM_ERR_CUDA, msg.c_str());
-    }
-    g_address[device] = static_cast<unsigned char *>(p);
+  int st = driver_calls();
+  if (st != ZSMPM_OK) return st;
+  unsigned long long id = 0;
+  const bool have_ctx = current_context_id(&id) == 0;
+  if (have_ctx)
+    for (int k = 0; k < g_cached; ++k)
+      if (g_cache[k].ctx_id == id) {
+        *out = g_cache[k].ptr;
+        return ZSMPM_OK;
+      }
+  // the lookup also makes the device's primary context current when none is
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    std::string msg = std::string("cudaGetSymbolAddress of the no-alloc scratch: ") + cudaGetErrorString(e);
+    return record_error(ZSMPM_ERR_CUDA, msg.c_str());
   }
-  *out = g_address[device];
+  if (current_context_id(&id) == 0) {
+    // once every entry is in use (a process that recreates contexts often), the oldest goes
+    int k = g_cached;
+    if (g_cached < kMaxContexts) {
+      ++g_cached;
+    } else {
+      k = g_oldest;
+      g_oldest = (g_oldest + 1) % kMaxContexts;
+    }
+    g_cache[k] = cached_address{id, static_cast<unsigned char *>(p)};
+  }
+  *out = static_cast<unsigned char *>(p);
   return ZSMPM_OK;
 }
 
@@ -96,21 +150,12 @@ extern "C" ZSMPM_API zsmpm_status zsmpm_activate_blocks_noalloc(const float *x, 
         ZSMPM_ERR_CAPACITY,
         "zsmpm_activate_blocks_noalloc takes 1 to 1048576 particles (its fixed scratch holds a "
         "32768-slot table); use a scene (zsmpm_scene_create) for more");
-  int device = 0;
-  cudaError_t e = cudaGetDevice(&device);
-  if (e != cudaSuccess) {
-    std::string msg = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
-    return (zsmpm_status)record_error(ZSMPM_ERR_CUDA, msg.c_str());
-  }
   unsigned char *base = nullptr;
-  int st = scratch_address(device, &base);
+  int st = scratch_address(&base);
   if (st != ZSMPM_OK) return (zsmpm_status)st;
 
-  // the table follows the reference's sizing rule, as a scene of n particles would
-  int64_t expected = n / 512 < 64 ? 64 : n / 512;
-  int64_t T = 1;
-  while (T < expected) T <<= 1;
-  T *= 16;
+  // the whole table on every call: the sorted keys are the same for any table that holds them
+  const int64_t T = kNoAllocTableSlots;
   scene_device s{};
   s.prm.n = (int)n;
   s.prm.dx = dx;
@@ -131,7 +176,7 @@ extern "C" ZSMPM_API zsmpm_status zsmpm_activate_blocks_noalloc(const float *x, 
   s.ctr = reinterpret_cast<int *>(base + kOffCtr);
   s.view_cnt = reinterpret_cast<int *>(base + kOffCnt);
   s.scan_part = reinterpret_cast<int *>(base + kOffScan);
-  e = launch_activate_static(s, x, keys_out, cap_blocks, count_out, static_cast<cudaStream_t>(stream));
+  cudaError_t e = launch_activate_static(s, x, keys_out, cap_blocks, count_out, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) {
     std::string msg = std::string("zsmpm_activate_blocks_noalloc launch: ") + cudaGetErrorString(e);
     return (zsmpm_status)record_error(ZSMPM_ERR_CUDA, msg.c_str());
