@@ -250,6 +250,13 @@ ZSMPM_API zsmpm_status zsmpm_download_grid(zsmpm_scene *scene, int32_t *keys, fl
  * index of the particle in slot, block_start[nb+1]. */
 ZSMPM_API zsmpm_status zsmpm_download_binning(zsmpm_scene *scene, int32_t *order,
                                               int32_t *block_start, int32_t cap_blocks);
+/* How the last binning ordered the particles (synchronises): *movers_merged = -1 when it
+ * counted every particle (SpatiallyCount + exclusive_scan + SpatiallyDistribute,
+ * simulation/sparsity/SparsityOp.hpp:115-196), else the number of particles it moved into
+ * other cells while keeping the rest of the previous binning's order (the incremental path,
+ * taken after a G2P whose particles all stayed within their block's 3x3x3 neighbourhood).
+ * Both give the same order.  Valid until the next activation. */
+ZSMPM_API zsmpm_status zsmpm_binning_info(zsmpm_scene *scene, int32_t *movers_merged);
 /* Per-stage device times (ms) of the last zsmpm_substep when timing is enabled. */
 ZSMPM_API zsmpm_status zsmpm_set_stage_timing(zsmpm_scene *scene, int32_t enabled);
 ZSMPM_API zsmpm_status zsmpm_stage_times(zsmpm_scene *scene, float *ms, int32_t count);
@@ -407,7 +414,7 @@ ZSMPM_API zsmpm_status zsmpm_batch_num_scenes(const zsmpm_scene *s, int32_t *out
 typedef struct {
   int32_t g2p_threads;      /* G2P CTA size: 128 or 256 (0 = default 256) */
   int32_t g2p_ctas_per_sm;  /* persistent G2P CTAs per SM, 1-6 (0 = default: 3, learned 2) */
-  int32_t p2g_ctas_per_sm;  /* persistent P2G CTAs per SM, 1-2 (0 = default 2) */
+  int32_t p2g_ctas_per_sm;  /* persistent P2G CTAs per SM, 1-4 (0 = default 3) */
   float g2p_ms, p2g_ms;     /* stage times of the chosen shapes (autotune output) */
 } zsmpm_tuning;
 

@@ -87,6 +87,17 @@ def test_run_stays_finite_and_inside_at_full_size(zs, gpu, sand):
         sc.run(20)
         sc.status()
         out = sc.download()
+        # the graph's binnings merge the movers of each G2P; a full binning of the same
+        # activation gives the same order
+        sc.activate_blocks()
+        sc.bin_particles()
+        merged = sc.binning_info()
+        order_inc, bstart_inc = sc.download_binning()
+        sc.bin_particles()
+        order_full, bstart_full = sc.download_binning()
+    assert 0 < merged < p.n // 10
+    assert np.array_equal(bstart_inc, bstart_full)
+    assert np.array_equal(order_inc, order_full)
     assert np.all(np.isfinite(out.x)) and np.all(np.isfinite(out.v)) and np.all(np.isfinite(out.F))
     lo, hi = 2 * spec.dx, 1 - 2 * spec.dx  # slip walls 3 cells in
     assert out.x.min() > lo and out.x.max() < hi

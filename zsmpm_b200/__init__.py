@@ -204,6 +204,13 @@ class Scene:
         _abi.check(self._lib.zsmpm_num_blocks(self._h, C.byref(nb)), "num_blocks")
         return nb.value
 
+    def binning_info(self) -> int:
+        """-1 when the last binning counted every particle, else the number of particles that
+        the incremental binning moved into other cells (see zsmpm_binning_info)."""
+        m = C.c_int32()
+        _abi.check(self._lib.zsmpm_binning_info(self._h, C.byref(m)), "binning_info")
+        return m.value
+
     def download_grid(self):
         nb = self.num_blocks()
         keys = np.empty((max(nb, 1), 3), np.int32)

@@ -132,6 +132,7 @@ SIGNATURES = {
     "zsmpm_get_table_view": (_S, [_P, C.POINTER(TableView)]),
     "zsmpm_get_grid_view": (_S, [_P, C.POINTER(GridView)]),
     "zsmpm_num_blocks": (_S, [_P, C.POINTER(C.c_int32)]),
+    "zsmpm_binning_info": (_S, [_P, C.POINTER(C.c_int32)]),
     "zsmpm_download_grid": (_S, [_P, _P, _P, C.c_int32, C.POINTER(C.c_int32)]),
     "zsmpm_download_binning": (_S, [_P, _P, _P, C.c_int32]),
     "zsmpm_set_stage_timing": (_S, [_P, C.c_int32]),

@@ -28,6 +28,10 @@ struct zsmpm_scene {
   int cur = 0;
   bool uploaded = false;
   bool binned = false;  // src[] valid for the current particle order
+  int bins_since_activation = 0;  // a second binning after one activation recounts every particle
+  // the two sets of cell and block starts the binnings alternate between (by particle buffer parity)
+  int *cell_start_buf[2] = {nullptr, nullptr};
+  int *block_start_buf[2] = {nullptr, nullptr};
   cudaStream_t last_stream = nullptr;
   // graphs of two consecutive substeps, one per starting buffer parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -133,6 +137,12 @@ zsmpm_status check_scene(zsmpm_scene *s, bool need_particles) {
 void bind_buffers(zsmpm_scene *s) {
   s->dev.cur = s->bufs[s->cur];
   s->dev.nxt = s->bufs[s->cur ^ 1];
+  // a binning writes the set of its particle buffer parity; the last binning (before the G2P
+  // that flipped the parity) wrote the other one
+  s->dev.cell_start = s->cell_start_buf[s->cur];
+  s->dev.block_start = s->block_start_buf[s->cur];
+  s->dev.cell_start_prev = s->cell_start_buf[s->cur ^ 1];
+  s->dev.block_start_prev = s->block_start_buf[s->cur ^ 1];
 }
 
 zsmpm_status status_from_word(int w) {
@@ -190,6 +200,13 @@ zsmpm_status allocate_particles(zsmpm_scene *s, int64_t cap) {
   ZS_ALLOC(d.rnk, cap, "alloc rnk");
   ZS_ALLOC(d.tmp, cap, "alloc tmp");
   ZS_ALLOC(d.src, cap, "alloc src");
+  // incremental binning: a flag per slot and a list of the particles that left their cell (a
+  // G2P whose movers overflow the list makes the next binning a full one)
+  d.prm.mover_cap = (int)std::min<int64_t>(cap / 4 + 1024, 0x7fffffff);
+  ZS_ALLOC(d.moved, cap, "alloc moved flags");
+  ZS_ALLOC(d.movers, d.prm.mover_cap, "alloc movers");
+  ZS_ALLOC(d.mover_pos, d.prm.mover_cap, "alloc mover positions");
+  ZS_ALLOC(d.dirty, d.prm.mover_cap, "alloc dirty cells");
   return ZSMPM_OK;
 }
 
@@ -218,9 +235,13 @@ zsmpm_status allocate_blocks(zsmpm_scene *s, int64_t n) {
   ZS_ALLOC(d.ctr, kCtrCount, "alloc counters");
   ZS_ALLOC(d.block_count, nbc, "alloc block count");
   ZS_ALLOC(d.work_order, nbc, "alloc work order");
-  ZS_ALLOC(d.block_start, nbc + 1, "alloc block start");
+  ZS_ALLOC(s->block_start_buf[0], nbc + 1, "alloc block start");
+  ZS_ALLOC(s->block_start_buf[1], nbc + 1, "alloc block start");
   ZS_ALLOC(d.cell_count, 512 * nbc, "alloc cell count");
-  ZS_ALLOC(d.cell_start, 512 * nbc, "alloc cell start");
+  ZS_ALLOC(s->cell_start_buf[0], 512 * nbc, "alloc cell start");
+  ZS_ALLOC(s->cell_start_buf[1], 512 * nbc, "alloc cell start");
+  ZS_ALLOC(d.old_pk, nbc, "alloc previous block keys");
+  ZS_ALLOC(d.new_of_old, nbc, "alloc previous block map");
   ZS_ALLOC(d.scan_part, 2 * kScanCtas + 1, "alloc scan partials");
   ZS_ALLOC(d.grid, (size_t)kGridChannels * 512 * nbc, "alloc grid");
   ZS_TRY(cudaMemset(d.bitmap, 0, sizeof(uint32_t) * d.prm.bitmap_cap), "memset bitmap");
@@ -278,6 +299,7 @@ zsmpm_status substep_enqueue(zsmpm_scene *s, cudaStream_t st) {
   if (s->timing) cudaEventRecord(s->ev[0], st);
   ZS_TRY(launch_activate(s->dev, st), "activate");
   if (s->timing) cudaEventRecord(s->ev[1], st);
+  s->dev.prm.bin_full = 0;
   ZS_TRY(launch_bin(s->dev, st), "bin");
   if (s->timing) cudaEventRecord(s->ev[2], st);
   ZS_TRY(launch_p2g(s->dev, st), "p2g");
@@ -651,6 +673,7 @@ ZSMPM_API zsmpm_status zsmpm_activate_blocks(zsmpm_scene *s, void *stream) {
   bind_buffers(s);
   ZS_TRY(launch_activate(s->dev, as_stream(stream)), "activate");
   s->binned = false;
+  s->bins_since_activation = 0;
   s->last_stream = as_stream(stream);
   return ZSMPM_OK;
 }
@@ -659,7 +682,12 @@ ZSMPM_API zsmpm_status zsmpm_bin_particles(zsmpm_scene *s, void *stream) {
   zsmpm_status st = check_scene(s, true);
   if (st != ZSMPM_OK) return st;
   bind_buffers(s);
-  ZS_TRY(launch_bin(s->dev, as_stream(stream)), "bin");
+  // only the first binning after an activation may merge the movers of the last G2P
+  s->dev.prm.bin_full = s->bins_since_activation > 0 ? 1 : 0;
+  cudaError_t e = launch_bin(s->dev, as_stream(stream));
+  s->dev.prm.bin_full = 0;
+  ZS_TRY(e, "bin");
+  s->bins_since_activation += 1;
   s->binned = true;
   s->last_stream = as_stream(stream);
   return ZSMPM_OK;
@@ -788,6 +816,16 @@ ZSMPM_API zsmpm_status zsmpm_num_blocks(zsmpm_scene *s, int32_t *out) {
   if (!out) return fail(ZSMPM_ERR_INVALID_ARG, "null output");
   ZS_TRY(cudaStreamSynchronize(s->last_stream), "synchronize");
   ZS_TRY(cudaMemcpy(out, s->dev.view_cnt, sizeof(int), cudaMemcpyDeviceToHost), "read block count");
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_binning_info(zsmpm_scene *s, int32_t *movers_merged) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!movers_merged) return fail(ZSMPM_ERR_INVALID_ARG, "null output");
+  ZS_TRY(cudaStreamSynchronize(s->last_stream), "synchronize");
+  ZS_TRY(cudaMemcpy(movers_merged, &s->dev.ctr[kCtrBinInfo], sizeof(int), cudaMemcpyDeviceToHost),
+         "read binning info");
   return ZSMPM_OK;
 }
 
@@ -1108,7 +1146,7 @@ ZSMPM_API zsmpm_status zsmpm_autotune(zsmpm_scene *s, int32_t trials, zsmpm_tuni
     }
   float best_p2g = 3.4e38f;
   if (st == ZSMPM_OK)
-    for (int b : {1, 2}) {
+    for (int b : {2, 3, 4}) {
       p.p2g_ctas_per_sm = b;
       float ms = 0.f;
       st = time_stage(2, &ms);
@@ -1136,7 +1174,7 @@ ZSMPM_API zsmpm_status zsmpm_set_tuning(zsmpm_scene *s, const zsmpm_tuning *t) {
   if (st != ZSMPM_OK) return st;
   if (!t) return fail(ZSMPM_ERR_INVALID_ARG, "null tuning");
   if ((t->g2p_threads != 0 && t->g2p_threads != 128 && t->g2p_threads != 256) || t->g2p_ctas_per_sm < 0 ||
-      t->g2p_ctas_per_sm > 6 || t->p2g_ctas_per_sm < 0 || t->p2g_ctas_per_sm > 2)
+      t->g2p_ctas_per_sm > 6 || t->p2g_ctas_per_sm < 0 || t->p2g_ctas_per_sm > 4)
     return fail(ZSMPM_ERR_INVALID_ARG, "tuning out of range");
   if (s->dev.aux.learned && t->g2p_threads == 128)
     return fail(ZSMPM_ERR_INVALID_ARG, "the learned G2P runs 256-thread CTAs");

@@ -49,7 +49,11 @@ enum counter_slot : int {
   kCtrUseMasks = 23,       // this activation inserts from the move masks of that many blocks
   kCtrOrderFront = 24,     // blocks of at least kBigBlock particles placed at the front of work_order
   kCtrOrderBack = 25,      // the others, placed from the back
-  kCtrCount = 28
+  kCtrMovers = 26,         // particles the last G2P listed as having left their cell (cleared by the binning)
+  kCtrIncBin = 27,         // 1: this substep's binning merges the movers into the last binning's order
+  kCtrBinInfo = 28,        // the last binning: -1 full, else the number of movers it merged
+  kCtrDirty = 29,          // cells the incremental binning's movers arrived in (to be sorted by id)
+  kCtrCount = 32
 };
 enum work_slot : int {
   kWorkCellStart = 0,
@@ -85,6 +89,9 @@ struct scene_params {
   // launch shapes (set by the autotuner; 0 = default)
   int g2p_threads;                  // 128 or 256
   int g2p_ctas_per_sm, p2g_ctas_per_sm;
+  // incremental binning
+  int mover_cap;                    // entries of the mover list
+  int bin_full;                     // 1: this binning launch recounts every particle
 };
 
 // G2P options beside the plain path: the learned closure and the trial-state log.
@@ -126,6 +133,17 @@ struct scene_device {
   int *rnk = nullptr;         // [cap]
   int *tmp = nullptr;         // [cap]
   int *src = nullptr;         // [cap] slot -> index in cur
+  // the previous binning's cell and block starts (the binning alternates between two sets, so
+  // that an incremental binning reads the last one while it writes its own)
+  int *cell_start_prev = nullptr;  // [nb_cap * 512]
+  int *block_start_prev = nullptr; // [nb_cap + 1]
+  uint64_t *old_pk = nullptr;      // [nb_cap] keys of the previous binning's blocks, by their index then
+  int *new_of_old = nullptr;       // [nb_cap] their indices in the current activation (-1: gone)
+  uint8_t *moved = nullptr;        // [cap] per slot of the last binning: 1 when G2P moved the particle out
+                                   // of its cell (or out of reach of the move masks)
+  int *movers = nullptr;           // [mover_cap] slots of the particles that left their cell
+  int2 *mover_pos = nullptr;       // [mover_cap] (new cell index b * 512 + cell, arrival rank in it)
+  int *dirty = nullptr;            // [mover_cap] new cells that received movers
   int *work_order = nullptr;  // [nb_cap] blocks in the order the per-block kernels take them
   int *scan_part = nullptr;   // [2 * kScanCtas + 1]
   float *grid = nullptr;      // [nb_cap][4][512]

@@ -236,9 +236,16 @@ __global__ void __launch_bounds__(kThreads) k_begin(scene_device s) {
   }
   if (blockIdx.x == 0 && threadIdx.x < kCtrCount) {
     const int t = threadIdx.x;
-    if (t == kCtrStatus || t == kCtrMaskFrom || t == kCtrMaskBad) return;  // k_bitmap_prepare resets the last two
+    // k_bitmap_prepare resets the two mask counters; the binning clears the mover count
+    if (t == kCtrStatus || t == kCtrMaskFrom || t == kCtrMaskBad || t == kCtrMovers) return;
     if (t == kCtrUseMasks) {
       s.ctr[t] = s.ctr[kCtrMaskBad] == 0 ? s.ctr[kCtrMaskFrom] : 0;
+      return;
+    }
+    if (t == kCtrIncBin) {
+      // the move masks are valid exactly when the last G2P listed every particle that left
+      // its cell, so the binning can merge those into the last binning's order
+      s.ctr[t] = (s.ctr[kCtrMaskBad] == 0 && s.ctr[kCtrMaskFrom] > 0) ? 1 : 0;
       return;
     }
     if (t == kCtrSubstep) {
@@ -318,6 +325,8 @@ __global__ void __launch_bounds__(kThreads) k_insert_particle_blocks(scene_devic
 __global__ void __launch_bounds__(kThreads) k_insert_moved_blocks(scene_device s) {
   const int nold = s.ctr[kCtrUseMasks];
   if (nold == 0) return;
+  // the previous binning's block keys by their index then (k_assign_ranks renumbers blk_pk)
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nold; b += grid_threads()) s.old_pk[b] = s.blk_pk[b];
   int3 lo = make_int3(0x7fffffff, 0x7fffffff, 0x7fffffff);
   int3 hi = make_int3(-0x7fffffff, -0x7fffffff, -0x7fffffff);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nold * 27; t += grid_threads()) {
@@ -441,11 +450,23 @@ __global__ void __launch_bounds__(kThreads) k_neighbors(scene_device s) {
 // ----------------------------------------------------------------- binning
 // Per particle: its block index and stencil-origin cell; counts per cell (rank within the
 // cell from the atomic) and per block (warp-aggregated).
+__device__ __forceinline__ bool incremental_binning(const scene_device &s) {
+  return s.ctr[kCtrIncBin] != 0 && !s.prm.bin_full;
+}
+
 __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     s.ctr[kCtrOrderFront] = 0;  // k_cell_start fills work_order
     s.ctr[kCtrOrderBack] = 0;
+    // the persistent kernels of this binning and of the transfers after it start from their
+    // first block (a second binning after one activation must not find them spent)
+    s.ctr[kCtrWork + kWorkCellStart] = 0;
+    s.ctr[kCtrWork + kWorkFinalize] = 0;
+    s.ctr[kCtrWork + kWorkP2G] = 0;
+    s.ctr[kCtrWork + kWorkG2P] = 0;
+    s.ctr[kCtrDirty] = 0;
   }
+  if (incremental_binning(s)) return;  // k_inc_stayers and k_inc_movers count this substep
   const int lane = threadIdx.x & 31;
   const int n = s.prm.n;
   const int nb = s.ctr[kCtrBlocks];
@@ -487,7 +508,11 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
     const unsigned cpeers = __match_any_sync(kFull, k32);
     const int cleader = __ffs(cpeers) - 1;
     int cbase = 0;
-    if (ok && lane == cleader) cbase = atomicAdd(&s.cell_count[k32], __popc(cpeers));
+    if (ok && lane == cleader) {
+      cbase = atomicAdd(&s.cell_count[k32], __popc(cpeers));
+      // cell counts share their word with the incremental binning's arrival count (high 16 bits)
+      if (cbase + __popc(cpeers) > 0xffff) set_status(s.ctr, kStatusCapacity);
+    }
     cbase = __shfl_sync(kFull, cbase, cleader);
     if (i < n) {
       s.key32[i] = ok ? k32 : 0xffffffffu;
@@ -513,7 +538,10 @@ __global__ void __launch_bounds__(512) k_cell_start(scene_device s) {
   for (;;) {
     const int b = grab_block(&s.ctr[kCtrWork + kWorkCellStart], &s_b);
     if (b >= nb) break;
-    const int c = s.cell_count[b * 512 + threadIdx.x];
+    // low 16 bits: particles counted in place (every particle of a full binning, the stayers of
+    // an incremental one); high 16 bits: the incremental binning's arrivals
+    const int craw = s.cell_count[b * 512 + threadIdx.x];
+    const int c = (craw & 0xffff) + (craw >> 16);
     int total;
     const int ex = cta_exclusive_scan<512>(c, total, sm);
     s.cell_start[b * 512 + threadIdx.x] = s.block_start[b] + ex;
@@ -528,6 +556,7 @@ __global__ void __launch_bounds__(512) k_cell_start(scene_device s) {
 }
 
 __global__ void __launch_bounds__(kThreads) k_bin_scatter(scene_device s) {
+  if (incremental_binning(s)) return;
   const int n = s.prm.n;
   const int stride = grid_threads();
   for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += kPass * stride) {
@@ -547,63 +576,227 @@ __global__ void __launch_bounds__(kThreads) k_bin_scatter(scene_device s) {
   }
 }
 
-// Final particle order of a block: cells ascending, the particles of a cell in increasing
-// upload index (a stable sort by (block, cell)).  Also zeroes the block's grid and the
-// counts for the next substep.  Lists of up to 12 entries are sorted in registers, which
-// caps the kernel at 3 CTAs of 512 threads per SM (binning 0.71 -> 0.62 ms on the 30 M-particle
-// sand scene against a sort in local memory at 4 CTAs).
-__global__ void __launch_bounds__(512, 3) k_bin_finalize(scene_device s) {
+// Orders the list of one cell (indices into cur) by upload id, from `in` into `out` (which may
+// be the same array).  Lists of up to 12 entries are sorted in registers (every index known at
+// compile time): two rounds of independent loads (the list, then the ids), then an insertion
+// sort of (id << 32 | index) entries; ids are unique, so this orders the cell by id.  Longer
+// lists (strongly compressed cells) take an insertion sort in place in global memory.
+__device__ __forceinline__ void sort_cell_by_id(const scene_device &s, const int *in, int *out, int cs, int c) {
   constexpr int kMaxList = 12;
+  if (c <= kMaxList) {
+    unsigned long long e[kMaxList];
+#pragma unroll
+    for (int r = 0; r < kMaxList; ++r) e[r] = r < c ? (unsigned long long)(uint32_t)in[cs + r] : ~0ull;
+#pragma unroll
+    for (int r = 0; r < kMaxList; ++r)
+      if (r < c) e[r] |= (unsigned long long)(uint32_t)s.cur.id[(int)(uint32_t)e[r]] << 32;
+#pragma unroll
+    for (int r = 1; r < kMaxList; ++r)
+      if (r < c) {
+#pragma unroll
+        for (int q = r; q > 0; --q) {
+          const unsigned long long lo = e[q - 1], hi = e[q];
+          const bool sw = lo > hi;
+          e[q - 1] = sw ? hi : lo;
+          e[q] = sw ? lo : hi;
+        }
+      }
+#pragma unroll
+    for (int r = 0; r < kMaxList; ++r)
+      if (r < c) out[cs + r] = (int)(uint32_t)e[r];
+  } else {
+    int *w = const_cast<int *>(in);
+    for (int r = 1; r < c; ++r) {
+      const int i = w[cs + r];
+      const int id = s.cur.id[i];
+      int q = r;
+      while (q > 0 && s.cur.id[w[cs + q - 1]] > id) {
+        w[cs + q] = w[cs + q - 1];
+        --q;
+      }
+      w[cs + q] = i;
+    }
+    if (out != in)
+      for (int r = 0; r < c; ++r) out[cs + r] = w[cs + r];
+  }
+}
+
+// Final particle order of a block (full binning): cells ascending, the particles of a cell in
+// increasing upload index (a stable sort by (block, cell)).  Also zeroes the block's grid and
+// the counts for the next substep.  The register sort caps the kernel at 3 CTAs of 512
+// threads per SM (binning 0.71 -> 0.62 ms on the 30 M-particle sand scene against a sort in
+// local memory at 4 CTAs).
+__global__ void __launch_bounds__(512, 3) k_bin_finalize(scene_device s) {
+  if (incremental_binning(s)) return;
   __shared__ int s_b;
   const int nb = s.ctr[kCtrBlocks];
   const int t = threadIdx.x;
+  if (blockIdx.x == 0 && t == 0) {
+    s.ctr[kCtrMovers] = 0;  // the next G2P lists its movers afresh
+    s.ctr[kCtrBinInfo] = -1;
+  }
   for (;;) {
     const int b = grab_block(&s.ctr[kCtrWork + kWorkFinalize], &s_b);
     if (b >= nb) break;
     const int c = s.cell_count[b * 512 + t];
     const int cs = s.cell_start[b * 512 + t];
     s.cell_count[b * 512 + t] = 0;
-    if (c <= kMaxList) {
-      // in registers (every index known at compile time): two rounds of independent loads
-      // (the cell's particle list, then their upload ids), then an insertion sort of the
-      // (id << 32 | index) entries; ids are unique, so this orders the cell by id
-      unsigned long long e[kMaxList];
-#pragma unroll
-      for (int r = 0; r < kMaxList; ++r) e[r] = r < c ? (unsigned long long)(uint32_t)s.tmp[cs + r] : ~0ull;
-#pragma unroll
-      for (int r = 0; r < kMaxList; ++r)
-        if (r < c) e[r] |= (unsigned long long)(uint32_t)s.cur.id[(int)(uint32_t)e[r]] << 32;
-#pragma unroll
-      for (int r = 1; r < kMaxList; ++r)
-        if (r < c) {
-#pragma unroll
-          for (int q = r; q > 0; --q) {
-            const unsigned long long lo = e[q - 1], hi = e[q];
-            const bool sw = lo > hi;
-            e[q - 1] = sw ? hi : lo;
-            e[q] = sw ? lo : hi;
-          }
-        }
-#pragma unroll
-      for (int r = 0; r < kMaxList; ++r)
-        if (r < c) s.src[cs + r] = (int)(uint32_t)e[r];
-    } else {
-      // long lists (strongly compressed cells): insertion sort in place in global memory
-      for (int r = 1; r < c; ++r) {
-        const int i = s.tmp[cs + r];
-        const int id = s.cur.id[i];
-        int q = r;
-        while (q > 0 && s.cur.id[s.tmp[cs + q - 1]] > id) {
-          s.tmp[cs + q] = s.tmp[cs + q - 1];
-          --q;
-        }
-        s.tmp[cs + q] = i;
-      }
-      for (int r = 0; r < c; ++r) s.src[cs + r] = s.tmp[cs + r];
-    }
+    sort_cell_by_id(s, s.tmp, s.src, cs, c);
     float4 *g = reinterpret_cast<float4 *>(s.grid + (size_t)b * kGridChannels * 512);
     g[t] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (t == 0) s.block_count[b] = 0;
+  }
+}
+
+// ----------------------------------------------------------------- incremental binning
+// After a G2P whose particles all stayed within their block's 3^3 neighbourhood, the particles
+// are stored in the last binning's slot order, and G2P has flagged each slot whose particle
+// left its cell (moved[]) and listed those slots (movers[]).  The particles that stayed
+// (typically 98-99%) keep their relative order: it is already (cell, upload id) within their
+// cell, and the block order is ascending keys both times.  So the new order is the stayers of
+// every old cell, placed in order at the start of the same cell's new range, with the movers
+// appended behind them and only the cells that received movers sorted again by id.  The result
+// equals the full binning's order bit for bit.
+//   k_inc_map            per old block: its index in the new activation
+//   k_inc_stayers        per old cell: its stayers -> cell_count (low 16 bits) of the cell in
+//                        the block's new index, and the block's total
+//   k_inc_movers         per mover: its new cell, arrival rank (high 16 bits of cell_count)
+//   (scan, k_cell_start) as in the full binning
+//   k_inc_place_stayers  per old cell: src of its stayers
+//   k_inc_place_movers   per mover: src behind the stayers of its cell
+//   k_inc_sort           per cell that received movers: sorted by id
+//   k_inc_finalize       per new cell: counts and grid zeroed
+
+// the new index of every old block (one query per block, before the per-block passes)
+__global__ void __launch_bounds__(kThreads) k_inc_map(scene_device s) {
+  if (!incremental_binning(s)) return;
+  const int nold = s.ctr[kCtrUseMasks];
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nold; b += grid_threads()) {
+    const uint64_t key = s.old_pk[b];
+    s.new_of_old[b] = table_query(s, key, unpack_key(key));
+  }
+}
+
+// The stayers of one old cell j = b * 512 + c: its slot range in the previous binning and the
+// number of its particles that did not move out (the flags of a cell are a few adjacent bytes)
+__device__ __forceinline__ int2 prev_cell_range(const scene_device &s, int j) {
+  const int b = j >> 9, c = j & 511;
+  const int cs = s.cell_start_prev[j];
+  const int ce = c < 511 ? s.cell_start_prev[j + 1] : s.block_start_prev[b + 1];
+  return make_int2(cs, ce);
+}
+
+__global__ void __launch_bounds__(kThreads) k_inc_stayers(scene_device s) {
+  if (!incremental_binning(s)) return;
+  const int nold = s.ctr[kCtrUseMasks], nb = s.ctr[kCtrBlocks];
+  const long long cells = (long long)nold * 512;  // a warp covers 32 cells of one block
+  const int lane = threadIdx.x & 31;
+  for (long long j0 = blockIdx.x * (long long)blockDim.x; j0 < cells; j0 += grid_threads()) {
+    const long long j = j0 + threadIdx.x;
+    const bool in = j < cells;
+    int stay = 0, nbi = -1;
+    if (in) {
+      const int2 r = prev_cell_range(s, (int)j);
+      int slot = r.x;
+      for (; slot + 4 <= r.y; slot += 4) {
+        const uint8_t a = s.moved[slot], b1 = s.moved[slot + 1], c = s.moved[slot + 2], d = s.moved[slot + 3];
+        stay += (a == 0) + (b1 == 0) + (c == 0) + (d == 0);
+      }
+      for (; slot < r.y; ++slot) stay += s.moved[slot] == 0;
+      nbi = s.new_of_old[(int)(j >> 9)];
+      if (stay > 0xffff) set_status(s.ctr, kStatusCapacity);  // shares its word with the arrivals
+      if (nbi >= 0 && nbi < nb)
+        s.cell_count[nbi * 512 + (int)(j & 511)] = stay;
+      else if (stay > 0)
+        set_status(s.ctr, kStatusMissingBlock);
+    }
+    const int wsum = __reduce_add_sync(kFull, stay);
+    if (lane == 0 && wsum > 0 && nbi >= 0 && nbi < nb) atomicAdd(&s.block_count[nbi], wsum);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_inc_movers(scene_device s) {
+  if (!incremental_binning(s)) return;
+  const int nmov = min(s.ctr[kCtrMovers], s.prm.mover_cap);
+  const int nb = s.ctr[kCtrBlocks];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nmov; k += grid_threads()) {
+    const int slot = s.movers[k];
+    int3 c, b;
+    int2 pos = make_int2(-1, 0);
+    if (particle_cell(s, s.prm.batch ? s.cur.sid[slot] : 0, s.cur.xm[slot], c, b)) {
+      const int blk = table_query(s, pack_key(b.x, b.y, b.z), b);
+      if (blk >= 0 && blk < nb) {
+        const int k32 = blk * 512 + (((c.x - 8 * b.x) << 6) | ((c.y - 8 * b.y) << 3) | (c.z - 8 * b.z));
+        const int old = atomicAdd(&s.cell_count[k32], 1 << 16);
+        atomicAdd(&s.block_count[blk], 1);
+        pos = make_int2(k32, old >> 16);
+        if ((old >> 16) >= 0x7fff) set_status(s.ctr, kStatusCapacity);
+        // the first arrival lists the cell for k_inc_sort (at most one entry per mover)
+        if ((old >> 16) == 0) s.dirty[atomicAdd(&s.ctr[kCtrDirty], 1)] = k32;
+      }
+    }
+    if (pos.x < 0) set_status(s.ctr, kStatusMissingBlock);
+    s.mover_pos[k] = pos;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_inc_place_stayers(scene_device s) {
+  if (!incremental_binning(s)) return;
+  const int nold = s.ctr[kCtrUseMasks], nb = s.ctr[kCtrBlocks];
+  const long long cells = (long long)nold * 512;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < cells; j += grid_threads()) {
+    const int nbi = s.new_of_old[(int)(j >> 9)];
+    if (nbi < 0 || nbi >= nb) continue;
+    const int2 r = prev_cell_range(s, (int)j);
+    int dst = s.cell_start[nbi * 512 + (int)(j & 511)];
+    // four flags loaded together per round (a cell holds a few adjacent slots)
+    for (int slot = r.x; slot < r.y; slot += 4) {
+      uint8_t f[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) f[u] = slot + u < r.y ? s.moved[slot + u] : (uint8_t)1;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (f[u] == 0) s.src[dst++] = slot + u;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_inc_place_movers(scene_device s) {
+  if (!incremental_binning(s)) return;
+  const int nmov = min(s.ctr[kCtrMovers], s.prm.mover_cap);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nmov; k += grid_threads()) {
+    const int2 pos = s.mover_pos[k];
+    if (pos.x < 0) continue;
+    s.src[s.cell_start[pos.x] + (s.cell_count[pos.x] & 0xffff) + pos.y] = s.movers[k];
+  }
+}
+
+// the cells that received movers, in upload-id order (stayers and arrivals merged)
+__global__ void __launch_bounds__(kThreads) k_inc_sort(scene_device s) {
+  if (!incremental_binning(s)) return;
+  const int nd = min(s.ctr[kCtrDirty], s.prm.mover_cap);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nd; k += grid_threads()) {
+    const int j = s.dirty[k];
+    const int craw = s.cell_count[j];
+    const int c = (craw & 0xffff) + (craw >> 16);
+    if (c > 1) sort_cell_by_id(s, s.src, s.src, s.cell_start[j], c);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_inc_finalize(scene_device s) {
+  if (!incremental_binning(s)) return;
+  const int nb = s.ctr[kCtrBlocks];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s.ctr[kCtrBinInfo] = min(s.ctr[kCtrMovers], s.prm.mover_cap);
+    s.ctr[kCtrMovers] = 0;  // the next G2P lists its movers afresh (k_inc_place_movers has read them)
+  }
+  const long long cells = (long long)nb * 512;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < cells; j += grid_threads()) {
+    s.cell_count[j] = 0;
+    const int b = (int)(j >> 9), cell = (int)(j & 511);
+#pragma unroll
+    for (int ch = 0; ch < kGridChannels; ++ch) s.grid[((size_t)b * kGridChannels + ch) * 512 + cell] = 0.f;
+    if (cell == 0) s.block_count[b] = 0;
   }
 }
 
@@ -615,93 +808,177 @@ __global__ void __launch_bounds__(512, 3) k_bin_finalize(scene_device s) {
 //     float4: lanes reading one rank of consecutive cells read 512 contiguous bytes, and the
 //     ranks of one cell, which consecutive lanes write, start 4 banks apart;
 //  2. one thread per (cell, channel) sums the cell's particles into 27 registers -- all
-//     particles of a cell share the same 27 stencil nodes -- and adds them to a 12^3 halo of
-//     the grid in shared memory (cells [8b, 8b+12) per axis: b and its +1 neighbours).
-// The halo is flushed with 16-byte vector reductions into the 8 neighbour blocks.  Grid
-// channels: m and p = sum W (m v + A (x_i - x_p)), the reference's mv + rhs
+//     particles of a cell share the same 27 stencil nodes -- and adds them to a halo of the
+//     grid in shared memory.
+// Ranks are staged kP2GRanks at a time: a chunk with a cell of more particles runs phases 1-2
+// again for the next ranks (a round), so that no particle needs the slow per-node path for
+// lack of staging room and the staging stays small enough for three CTAs per SM.
+// The halo holds the nodes the block's particles reach: a particle binned in cell c of the
+// block has its stencil origin at c + 1 (SparsityOp.hpp:72-77 against P2G.hpp:62-66), so its
+// nodes lie in [8b + 1, 8b + 11) per axis; the halo spans exactly that in x and y and
+// [8b, 8b + 12) in z, so that the flush moves whole 16-byte quads of the neighbour blocks.
+// Grid channels: m and p = sum W (m v + A (x_i - x_p)), the reference's mv + rhs
 // (P2G.hpp:108-125) with A = m C - (4 dt/dx^2) tau precomputed by G2P.
+// Staging variants (compile-time): ZSMPM_P2G_RANKS particles per cell per round,
+// ZSMPM_P2G_STAGE_F = 1 stages the particle's fractional position in the cell instead of its
+// nine weights (phase 2 recomputes them: more arithmetic, a third less shared memory), and
+// ZSMPM_P2G_MIN_CTAS resident CTAs per SM that the register budget is cut for.
+#ifndef ZSMPM_P2G_RANKS
+#define ZSMPM_P2G_RANKS 12
+#endif
+#ifndef ZSMPM_P2G_STAGE_F
+#define ZSMPM_P2G_STAGE_F 1
+#endif
+#ifndef ZSMPM_P2G_MIN_CTAS
+#define ZSMPM_P2G_MIN_CTAS 3
+#endif
 constexpr int kP2GChunk = 64;     // cells per chunk
-constexpr int kP2GRanks = 12;     // particles per cell staged per chunk (more go direct)
+constexpr int kP2GRanks = ZSMPM_P2G_RANKS;  // particles per cell staged per round
+constexpr int kP2GMinCtas = ZSMPM_P2G_MIN_CTAS;
+constexpr bool kP2GStageF = ZSMPM_P2G_STAGE_F != 0;
 constexpr int kP2GRow = kP2GChunk + 1;  // padded row of float4: rank r of cell c at bank 4 (r + c) % 32
 constexpr int kP2GThreads = 256;  // 4 channels x 64 cells
 constexpr int kP2GMap = 1024;     // slots of a chunk mapped to their cell (more: binary search)
+constexpr int kP2GHx = 10, kP2GHy = 10, kP2GHz = 12;  // halo extents (x, y from 8b + 1; z from 8b)
+constexpr int kP2GHaloNodes = kP2GHx * kP2GHy * kP2GHz;
 
 struct p2g_particle {
-  float m, w[3][3], q[3], ax[3], ay[3], az[3];
-  int hb[3];
+  float m, w[3][3], f[3], q[3], ax[3], ay[3], az[3];
+  int hb[3];  // stencil origin relative to the block's first cell 8b (1..8 when binned in it)
 };
 
-__device__ __forceinline__ void p2g_prepare(const scene_device &s, int i, int ox, int oy, int oz,
-                                            p2g_particle &pp) {
-  const scene_params &p = s.prm;
-  const float4 xm = s.cur.xm[i];
-  const float4 vv = s.cur.v[i];
+// quadratic B-spline weights of the nodes 0, 1, 2 of a stencil at fractional position f
+// (InterpolationKernel.hpp:93-130)
+__device__ __forceinline__ void bspline_weights(float f, float *w) {
+  w[0] = 0.5f * (1.5f - f) * (1.5f - f);
+  const float f1 = f - 1.f;
+  w[1] = 0.75f - f1 * f1;
+  const float f2 = 0.5f + f1;
+  w[2] = 0.5f * f2 * f2;
+}
+
+struct p2g_raw {
+  float4 xm, v;
   float A[9];
+};
+
+__device__ __forceinline__ void p2g_load(const scene_device &s, int i, p2g_raw &r) {
+  r.xm = s.cur.xm[i];
+  r.v = s.cur.v[i];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) A[k] = s.cur.A[(size_t)k * p.cap + i];
-  const float X[3] = {__fdiv_rn(xm.x, p.dx), __fdiv_rn(xm.y, p.dx), __fdiv_rn(xm.z, p.dx)};
+  for (int k = 0; k < 9; ++k) r.A[k] = s.cur.A[(size_t)k * s.prm.cap + i];
+}
+
+__device__ __forceinline__ void p2g_prepare(const scene_params &p, const p2g_raw &r, int ox, int oy, int oz,
+                                            p2g_particle &pp) {
+  // x / dx as P2G.hpp:62 divides; a multiplication when dx is a power of two (the same number)
+  const float X[3] = {over_dx(p, r.xm.x), over_dx(p, r.xm.y), over_dx(p, r.xm.z)};
   float lp[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const float base = floorf(X[d] - 0.5f);
     const float f = X[d] - base;
     pp.hb[d] = (int)base - (d == 0 ? ox : d == 1 ? oy : oz);
-    pp.w[d][0] = 0.5f * (1.5f - f) * (1.5f - f);
-    const float f1 = f - 1.f;
-    pp.w[d][1] = 0.75f - f1 * f1;
-    const float f2 = 0.5f + f1;
-    pp.w[d][2] = 0.5f * f2 * f2;
+    pp.f[d] = f;
+    bspline_weights(f, pp.w[d]);
     lp[d] = f * p.dx;
   }
-  pp.m = xm.w;
-  const float vel[3] = {vv.x, vv.y, vv.z};
+  pp.m = r.xm.w;
+  const float vel[3] = {r.v.x, r.v.y, r.v.z};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    pp.q[d] = pp.m * vel[d] - (A[d] * lp[0] + A[3 + d] * lp[1] + A[6 + d] * lp[2]);
-    pp.ax[d] = A[d] * p.dx;
-    pp.ay[d] = A[3 + d] * p.dx;
-    pp.az[d] = A[6 + d] * p.dx;
+    pp.q[d] = pp.m * vel[d] - (r.A[d] * lp[0] + r.A[3 + d] * lp[1] + r.A[6 + d] * lp[2]);
+    pp.ax[d] = r.A[d] * p.dx;
+    pp.ay[d] = r.A[3 + d] * p.dx;
+    pp.az[d] = r.A[6 + d] * p.dx;
   }
 }
 
-// all 27 nodes x 4 channels of one particle straight into the shared halo
-__device__ __forceinline__ void p2g_direct(float *shf, const p2g_particle &pp, int *ctr) {
-  if (pp.hb[0] < 0 || pp.hb[0] > kHalo - 3 || pp.hb[1] < 0 || pp.hb[1] > kHalo - 3 || pp.hb[2] < 0 ||
-      pp.hb[2] > kHalo - 3) {
-    set_status(ctr, kStatusMissingBlock);
+// Every node of one particle by itself: shared atomics into the halo when its stencil lies in
+// it, else global atomics into the grid blocks b + {0,1}^3 (a stencil origin that rounding
+// put one cell off the binned cell, possible when dx is not a power of two).
+__device__ __forceinline__ void p2g_direct(const scene_device &s, float *sh, const p2g_particle &pp, int b) {
+  const int hx = pp.hb[0] - 1, hy = pp.hb[1] - 1, hz = pp.hb[2];
+  const bool in_halo = hx >= 0 && hx <= kP2GHx - 3 && hy >= 0 && hy <= kP2GHy - 3 && hz >= 0 && hz <= kP2GHz - 3;
+  const bool in_reach = pp.hb[0] >= 0 && pp.hb[0] <= 13 && pp.hb[1] >= 0 && pp.hb[1] <= 13 && pp.hb[2] >= 0 &&
+                        pp.hb[2] <= 13;
+  if (!in_halo && !in_reach) {
+    set_status(s.ctr, kStatusMissingBlock);
     return;
   }
   for (int ii = 0; ii < 3; ++ii)
     for (int jj = 0; jj < 3; ++jj)
       for (int kk = 0; kk < 3; ++kk) {
         const float W = pp.w[0][ii] * pp.w[1][jj] * pp.w[2][kk];
-        const int h = ((pp.hb[0] + ii) * kHalo + (pp.hb[1] + jj)) * kHalo + pp.hb[2] + kk;
-        atomicAdd(&shf[h], W * pp.m);
+        float v[4];
+        v[0] = W * pp.m;
 #pragma unroll
         for (int d = 0; d < 3; ++d)
-          atomicAdd(&shf[(1 + d) * kHaloCells + h],
-                    W * (pp.q[d] + (float)ii * pp.ax[d] + (float)jj * pp.ay[d] + (float)kk * pp.az[d]));
+          v[1 + d] = W * (pp.q[d] + (float)ii * pp.ax[d] + (float)jj * pp.ay[d] + (float)kk * pp.az[d]);
+        if (in_halo) {
+          const int h = ((hx + ii) * kP2GHy + (hy + jj)) * kP2GHz + hz + kk;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) atomicAdd(&sh[c * kP2GHaloNodes + h], v[c]);
+        } else {
+          const int X = pp.hb[0] + ii, Y = pp.hb[1] + jj, Z = pp.hb[2] + kk;  // cells from 8b
+          if (X >= 16 || Y >= 16 || Z >= 16) {
+            set_status(s.ctr, kStatusMissingBlock);
+            continue;
+          }
+          const int tb = s.nbr[b * 8 + ((X >> 3) << 2) + ((Y >> 3) << 1) + (Z >> 3)];
+          if (tb < 0) {
+            set_status(s.ctr, kStatusMissingBlock);
+            continue;
+          }
+          const int cell = ((X & 7) << 6) | ((Y & 7) << 3) | (Z & 7);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) atomicAdd(&s.grid[((size_t)tb * kGridChannels + c) * 512 + cell], v[c]);
+        }
       }
 }
 
-constexpr int kP2GVec = 6;  // float4 fields: w00 w01 w02 w10 | w11 w12 w20 w21 | w22 m | (q ax ay az) x 3
-constexpr size_t kP2GSmemBytes =
-    sizeof(float) * kGridChannels * kHaloCells + sizeof(float4) * kP2GVec * kP2GRanks * kP2GRow +
-    sizeof(int) * 2 * (kP2GChunk + 1) + sizeof(unsigned char) * 2 * kP2GMap;
+// float4 fields: w00 w01 w02 w10 | w11 w12 w20 w21 | w22 m | (q ax ay az) x 3, or with the
+// fractional position: fx fy fz m | (q ax ay az) x 3
+constexpr int kP2GVec = kP2GStageF ? 4 : 6;
+constexpr int kP2GQ = kP2GVec - 3;  // first momentum field
+constexpr size_t kP2GSmemBytes = sizeof(float) * kGridChannels * kP2GHaloNodes +
+                                 sizeof(float4) * kP2GVec * kP2GRanks * kP2GRow +
+                                 sizeof(int) * 2 * (kP2GChunk + 1) + sizeof(int) * 4 +
+                                 sizeof(unsigned char) * 2 * kP2GMap;
 
-__global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
+// the weights and the mass of staged rank r of cell cl
+__device__ __forceinline__ void staged_weights(const float4 (*stg)[kP2GRanks][kP2GRow], int r, int cl, float (&w)[3][3],
+                                               float &m) {
+  if (kP2GStageF) {
+    const float4 fm = stg[0][r][cl];
+    bspline_weights(fm.x, w[0]);
+    bspline_weights(fm.y, w[1]);
+    bspline_weights(fm.z, w[2]);
+    m = fm.w;
+  } else {
+    const float4 wa = stg[0][r][cl], wb = stg[1][r][cl], wc = stg[2][r][cl];
+    w[0][0] = wa.x, w[0][1] = wa.y, w[0][2] = wa.z;
+    w[1][0] = wa.w, w[1][1] = wb.x, w[1][2] = wb.y;
+    w[2][0] = wb.z, w[2][1] = wb.w, w[2][2] = wc.x;
+    m = wc.y;
+  }
+}
+
+__global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s) {
   extern __shared__ __align__(16) float p2g_smem[];
   float *sh = p2g_smem;
-  auto stg = reinterpret_cast<float4(*)[kP2GRanks][kP2GRow]>(p2g_smem + kGridChannels * kHaloCells);
-  int *s_cs = reinterpret_cast<int *>(p2g_smem + kGridChannels * kHaloCells +
+  auto stg = reinterpret_cast<float4(*)[kP2GRanks][kP2GRow]>(p2g_smem + kGridChannels * kP2GHaloNodes);
+  int *s_cs = reinterpret_cast<int *>(p2g_smem + kGridChannels * kP2GHaloNodes +
                                       4 * kP2GVec * kP2GRanks * kP2GRow);
+  int *const s_wmax = s_cs + 2 * (kP2GChunk + 1);  // per chunk parity: the largest cell count of each half
+  unsigned char *const s_map0 = reinterpret_cast<unsigned char *>(s_wmax + 4);
   __shared__ int s_b;
   const int nb = s.ctr[kCtrBlocks];
   const int t = threadIdx.x;
   const int my_cell = t & (kP2GChunk - 1), my_ch = t >> 6;
   // the halo starts zeroed; each block's flush zeroes the quads it sends, so the next block
   // finds it zeroed again (the first barrier of grab_block orders both)
-  for (int q = t; q < kGridChannels * kHaloCells; q += blockDim.x) sh[q] = 0.f;
+  for (int q = t; q < kGridChannels * kP2GHaloNodes; q += blockDim.x) sh[q] = 0.f;
   for (;;) {
     const int w = grab_block(&s.ctr[kCtrWork + kWorkP2G], &s_b);
     if (w >= nb) break;
@@ -710,13 +987,15 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
     if (start == end) continue;
     const int3 bk = local_block(s.prm, unpack_key(s.blk_pk[b]));
     const int ox = bk.x * 8, oy = bk.y * 8, oz = bk.z * 8;
-    // cell starts of chunk k in s_cs0 + (k & 1) * (kP2GChunk + 1); the next chunk's are loaded
-    // during this chunk's phase 2, so a chunk needs two barriers
     int *const s_cs0 = s_cs;
-    unsigned char *const s_map0 = reinterpret_cast<unsigned char *>(s_cs0 + 2 * (kP2GChunk + 1));
-    // slot -> cell map of chunk k in s_map0 + (k & 1) * kP2GMap, written by the chunk's cell
-    // threads from the global cell starts
-    auto fill_map = [&](int chunk_to_fill) {
+    // cell starts of chunk k in s_cs0 + (k & 1) * (kP2GChunk + 1), its slot -> cell map in
+    // s_map0 + (k & 1) * kP2GMap and its largest cell count in s_wmax[2 (k & 1) ..]; the next
+    // chunk's are filled during this chunk's last phase 2, so a round needs two barriers
+    auto fill = [&](int chunk_to_fill) {
+      if (t <= kP2GChunk) {
+        const int c = chunk_to_fill * kP2GChunk + t;
+        s_cs0[(chunk_to_fill & 1) * (kP2GChunk + 1) + t] = c < 512 ? s.cell_start[b * 512 + c] : end;
+      }
       if (t < kP2GChunk) {
         const int c = chunk_to_fill * kP2GChunk + t;
         const int cs = s.cell_start[b * 512 + c];
@@ -724,67 +1003,87 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
         const int base = s.cell_start[b * 512 + chunk_to_fill * kP2GChunk];
         unsigned char *m = s_map0 + (chunk_to_fill & 1) * kP2GMap;
         for (int q = cs - base; q < ce - base && q < kP2GMap; ++q) m[q] = (unsigned char)t;
+        const int wmax = __reduce_max_sync(kFull, ce - cs);
+        if ((t & 31) == 0) s_wmax[2 * (chunk_to_fill & 1) + (t >> 5)] = wmax;
       }
     };
-    if (t <= kP2GChunk) s_cs0[t] = t < 512 ? s.cell_start[b * 512 + t] : end;
-    fill_map(0);
+    fill(0);
     for (int chunk = 0; chunk < 512 / kP2GChunk; ++chunk) {
       const int cell0 = chunk * kP2GChunk;
-      __syncthreads();  // previous chunk's staging consumed, this chunk's starts loaded, halo zeroed
-      int *s_cs = s_cs0 + (chunk & 1) * (kP2GChunk + 1);
-      // ---- phase 1: consecutive threads take consecutive slots (coalesced gathers)
-      const int c0 = s_cs[0], c1 = s_cs[kP2GChunk];
-      const unsigned char *s_map = s_map0 + (chunk & 1) * kP2GMap;
-      auto stage_one = [&](int slot, const p2g_particle &pp) {
-        int lo = 0;  // the cell of this slot: the last cell whose start is <= slot
-        if (slot - c0 < kP2GMap) {
-          lo = s_map[slot - c0];
-        } else {
-          int hi = kP2GChunk;
-          while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (s_cs[mid] <= slot) lo = mid;
-            else hi = mid;
+      const int par = chunk & 1;
+      int *s_cs = s_cs0 + par * (kP2GChunk + 1);
+      const unsigned char *s_map = s_map0 + par * kP2GMap;
+      for (int round = 0;; ++round) {
+        __syncthreads();  // previous staging consumed, this chunk's starts loaded, halo zeroed
+        const int maxc = max(s_wmax[2 * par], s_wmax[2 * par + 1]);
+        const int rlo = round * kP2GRanks;
+        const bool last = rlo + kP2GRanks >= maxc;
+        // ---- phase 1: consecutive threads take consecutive slots (coalesced gathers); the
+        // slots whose rank falls in this round's window are staged
+        const int c0 = s_cs[0], c1 = s_cs[kP2GChunk];
+        auto cell_of_slot = [&](int slot) {
+          int lo = 0;  // the cell of this slot: the last cell whose start is <= slot
+          if (slot - c0 < kP2GMap) {
+            lo = s_map[slot - c0];
+          } else {
+            int hi = kP2GChunk;
+            while (hi - lo > 1) {
+              const int mid = (lo + hi) >> 1;
+              if (s_cs[mid] <= slot) lo = mid;
+              else hi = mid;
+            }
+          }
+          return lo;
+        };
+        auto stage_one = [&](int cl, int r, const p2g_particle &pp) {
+          const int cell = cell0 + cl;
+          const int ex = (cell >> 6) + 1, ey = ((cell >> 3) & 7) + 1, ez = (cell & 7) + 1;
+          if (pp.hb[0] != ex || pp.hb[1] != ey || pp.hb[2] != ez) {
+            // a stencil origin that rounding moved off the cell: this particle by itself, and a
+            // zero-mass stand-in in its staging place
+            p2g_direct(s, sh, pp, b);
+            for (int f = 0; f < kP2GVec; ++f) stg[f][r][cl] = make_float4(0.f, 0.f, 0.f, 0.f);
+            return;
+          }
+          if (kP2GStageF) {
+            stg[0][r][cl] = make_float4(pp.f[0], pp.f[1], pp.f[2], pp.m);
+          } else {
+            stg[0][r][cl] = make_float4(pp.w[0][0], pp.w[0][1], pp.w[0][2], pp.w[1][0]);
+            stg[1][r][cl] = make_float4(pp.w[1][1], pp.w[1][2], pp.w[2][0], pp.w[2][1]);
+            stg[2][r][cl] = make_float4(pp.w[2][2], pp.m, 0.f, 0.f);
+          }
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            stg[kP2GQ + d][r][cl] = make_float4(pp.q[d], pp.ax[d], pp.ay[d], pp.az[d]);
+        };
+        for (int slot = c0 + t; slot < c1; slot += 2 * blockDim.x) {
+          const int slot2 = slot + blockDim.x;
+          const int cl1 = cell_of_slot(slot), r1 = slot - s_cs[cl1] - rlo;
+          const bool in1 = r1 >= 0 && r1 < kP2GRanks;
+          int cl2 = 0, r2 = -1;
+          if (slot2 < c1) {
+            cl2 = cell_of_slot(slot2);
+            r2 = slot2 - s_cs[cl2] - rlo;
+          }
+          const bool in2 = r2 >= 0 && r2 < kP2GRanks;
+          if (!in1 && !in2) continue;
+          p2g_raw ra, rb;
+          p2g_load(s, s.src[in1 ? slot : slot2], ra);
+          p2g_load(s, s.src[in2 ? slot2 : slot], rb);
+          p2g_particle pp;
+          if (in1) {
+            p2g_prepare(s.prm, ra, ox, oy, oz, pp);
+            stage_one(cl1, r1, pp);
+          }
+          if (in2) {
+            p2g_prepare(s.prm, rb, ox, oy, oz, pp);
+            stage_one(cl2, r2, pp);
           }
         }
-        const int cl = lo, r = slot - s_cs[lo], cell = cell0 + cl;
-        const int ex = (cell >> 6) + 1, ey = ((cell >> 3) & 7) + 1, ez = (cell & 7) + 1;
-        if (r >= kP2GRanks || pp.hb[0] != ex || pp.hb[1] != ey || pp.hb[2] != ez) {
-          // beyond the staged ranks, or a stencil origin that rounding moved off the
-          // cell: scatter this particle directly and stage a zero-mass stand-in
-          p2g_direct(sh, pp, s.ctr);
-          if (r < kP2GRanks)
-            for (int f = 0; f < kP2GVec; ++f) stg[f][r][cl] = make_float4(0.f, 0.f, 0.f, 0.f);
-          return;
-        }
-        stg[0][r][cl] = make_float4(pp.w[0][0], pp.w[0][1], pp.w[0][2], pp.w[1][0]);
-        stg[1][r][cl] = make_float4(pp.w[1][1], pp.w[1][2], pp.w[2][0], pp.w[2][1]);
-        stg[2][r][cl] = make_float4(pp.w[2][2], pp.m, 0.f, 0.f);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) stg[3 + d][r][cl] = make_float4(pp.q[d], pp.ax[d], pp.ay[d], pp.az[d]);
-      };
-      for (int slot = c0 + t; slot < c1; slot += 2 * blockDim.x) {
-        const int slot2 = slot + blockDim.x;
-        const bool two = slot2 < c1;
-        const int i1 = s.src[slot];
-        const int i2 = s.src[two ? slot2 : slot];
-        p2g_particle pa, pb;
-        p2g_prepare(s, i1, ox, oy, oz, pa);
-        p2g_prepare(s, i2, ox, oy, oz, pb);
-        stage_one(slot, pa);
-        if (two) stage_one(slot2, pb);
-      }
-      __syncthreads();
-      if (chunk + 1 < 512 / kP2GChunk) {
-        if (t <= kP2GChunk) {
-          const int nc = cell0 + kP2GChunk + t;
-          s_cs0[((chunk + 1) & 1) * (kP2GChunk + 1) + t] = nc < 512 ? s.cell_start[b * 512 + nc] : end;
-        }
-        fill_map(chunk + 1);
-      }
-      // ---- phase 2: thread (cell, channel) sums the staged particles of its cell
-      {
-        const int cnt = min(s_cs[my_cell + 1] - s_cs[my_cell], kP2GRanks);
+        __syncthreads();
+        if (last && chunk + 1 < 512 / kP2GChunk) fill(chunk + 1);
+        // ---- phase 2: thread (cell, channel) sums the staged particles of its cell
+        const int cnt = min(s_cs[my_cell + 1] - s_cs[my_cell] - rlo, kP2GRanks);
         if (cnt > 0) {
           float acc[27];
 #pragma unroll
@@ -793,9 +1092,8 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
           if (my_ch == 0) {
             // mass: W m (the warp is channel-uniform)
             for (int r = 0; r < cnt; ++r) {
-              const float4 wa = stg[0][r][my_cell], wb = stg[1][r][my_cell], wc = stg[2][r][my_cell];
-              const float w[3][3] = {{wa.x, wa.y, wa.z}, {wa.w, wb.x, wb.y}, {wb.z, wb.w, wc.x}};
-              const float m = wc.y;
+              float w[3][3], m;
+              staged_weights(stg, r, my_cell, w, m);
 #pragma unroll
               for (int ii = 0; ii < 3; ++ii) {
                 const float wm = w[0][ii] * m;
@@ -813,9 +1111,9 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
           } else {
             // momentum: W (q + ii ax + jj ay + kk az), in cell units of the node offset
             for (int r = 0; r < cnt; ++r) {
-              const float4 wa = stg[0][r][my_cell], wb = stg[1][r][my_cell], wc = stg[2][r][my_cell];
-              const float w[3][3] = {{wa.x, wa.y, wa.z}, {wa.w, wb.x, wb.y}, {wb.z, wb.w, wc.x}};
-              const float4 qa = stg[3 + d][r][my_cell];
+              float w[3][3], m_unused;
+              staged_weights(stg, r, my_cell, w, m_unused);
+              const float4 qa = stg[kP2GQ + d][r][my_cell];
               const float q = qa.x, ax = qa.y, ay = qa.z, az = qa.w;
               // wz (qij + kk az) = wz qij + cz[kk], cz = (0, wz1 az, 2 wz2 az): two operations
               // per node
@@ -835,37 +1133,41 @@ __global__ void __launch_bounds__(kP2GThreads, 2) k_p2g(scene_device s) {
               }
             }
           }
+          // cell (lx, ly, lz): stencil origin (lx + 1, ly + 1, lz + 1) from 8b, halo node
+          // (lx, ly, lz + 1)
           const int cell = cell0 + my_cell;
-          const int ex = (cell >> 6) + 1, ey = ((cell >> 3) & 7) + 1, ez = (cell & 7) + 1;
-          float *dst = sh + my_ch * kHaloCells;
+          const int hx = cell >> 6, hy = (cell >> 3) & 7, hz = (cell & 7) + 1;
+          float *dst = sh + my_ch * kP2GHaloNodes;
 #pragma unroll
           for (int ii = 0; ii < 3; ++ii)
 #pragma unroll
             for (int jj = 0; jj < 3; ++jj)
 #pragma unroll
               for (int kk = 0; kk < 3; ++kk)
-                atomicAdd(&dst[((ex + ii) * kHalo + (ey + jj)) * kHalo + ez + kk], acc[(ii * 3 + jj) * 3 + kk]);
+                atomicAdd(&dst[((hx + ii) * kP2GHy + (hy + jj)) * kP2GHz + hz + kk], acc[(ii * 3 + jj) * 3 + kk]);
         }
+        if (last) break;
       }
     }
     __syncthreads();
-    // flush: items (ch, hx, hy, quad) over 4 x 12 x 12 x 3
-    for (int it = t; it < kGridChannels * kHalo * kHalo * 3; it += blockDim.x) {
-      const int quad = it % 3, hy = (it / 3) % kHalo, hx = (it / (3 * kHalo)) % kHalo,
-                ch = it / (3 * kHalo * kHalo);
-      float4 *src4 = reinterpret_cast<float4 *>(&sh[((ch * kHalo + hx) * kHalo + hy) * kHalo + quad * 4]);
+    // flush: items (ch, hx, hy, quad) over 4 x 10 x 10 x 3; halo node (hx, hy, 4 quad + j) is
+    // the grid cell (8b + 1 + hx, 8b + 1 + hy, 8b + 4 quad + j)
+    for (int it = t; it < kGridChannels * kP2GHx * kP2GHy * 3; it += blockDim.x) {
+      const int quad = it % 3, hy = (it / 3) % kP2GHy, hx = (it / (3 * kP2GHy)) % kP2GHx,
+                ch = it / (3 * kP2GHy * kP2GHx);
+      float4 *src4 = reinterpret_cast<float4 *>(&sh[((ch * kP2GHx + hx) * kP2GHy + hy) * kP2GHz + quad * 4]);
       const float4 q4 = *src4;
-      const float a0 = q4.x, a1 = q4.y, a2 = q4.z, a3 = q4.w;
-      if (a0 == 0.f && a1 == 0.f && a2 == 0.f && a3 == 0.f) continue;
+      if (q4.x == 0.f && q4.y == 0.f && q4.z == 0.f && q4.w == 0.f) continue;
       *src4 = make_float4(0.f, 0.f, 0.f, 0.f);
-      const int tt = (hx >= 8 ? 4 : 0) | (hy >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0);
+      const int X = hx + 1, Y = hy + 1;
+      const int tt = (X >= 8 ? 4 : 0) | (Y >= 8 ? 2 : 0) | (quad == 2 ? 1 : 0);
       const int tb = s.nbr[b * 8 + tt];
       if (tb < 0) {
         set_status(s.ctr, kStatusMissingBlock);
         continue;
       }
-      const int cell = ((hx & 7) << 6) | ((hy & 7) << 3) | ((quad * 4) & 7);
-      red_add_v4(s.grid + ((size_t)tb * kGridChannels + ch) * 512 + cell, a0, a1, a2, a3);
+      const int cell = ((X & 7) << 6) | ((Y & 7) << 3) | ((quad * 4) & 7);
+      red_add_v4(s.grid + ((size_t)tb * kGridChannels + ch) * 512 + cell, q4.x, q4.y, q4.z, q4.w);
     }
   }
 }
@@ -1232,6 +1534,10 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
       const bool inside = hb[0] >= 0 && hb[0] <= kHalo - 3 && hb[1] >= 0 && hb[1] <= kHalo - 3 &&
                           hb[2] >= 0 && hb[2] <= kHalo - 3;
       if (active && !inside) set_status(s.ctr, kStatusMissingBlock);
+      // the cell this slot was binned in, as the binning computed it from the same position
+      const int sid = kBatch ? s.cur.sid[icur] : 0;
+      int3 cell_old = make_int3(0x7fffffff, 0, 0), blk_old;
+      if (active && !particle_cell(s, sid, xm, cell_old, blk_old)) cell_old.x = 0x7fffffff;
       float vel[3] = {0.f, 0.f, 0.f};
       float B[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // sum W v (node - f)^T
       if (inside) {
@@ -1277,24 +1583,41 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
       xm.z += vel[2] * p.dt;
       {
         // the block of the new position, as the next activation computes it from the stored
-        // x, recorded relative to this block for k_insert_moved_blocks
+        // x, recorded relative to this block for k_insert_moved_blocks; and whether the
+        // particle left the cell it was binned in, for the next (incremental) binning
         unsigned bit = 0u;
-        bool moved_far = false;
+        bool moved_far = false, left_cell = false;
         if (active) {
           int3 c2, b2;
-          if (particle_cell(s, kBatch ? s.cur.sid[icur] : 0, xm, c2, b2)) {
+          if (particle_cell(s, sid, xm, c2, b2)) {
             const int ox = b2.x - gk.x, oy = b2.y - gk.y, oz = b2.z - gk.z;
             if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1 && oz >= -1 && oz <= 1)
               bit = 1u << ((ox + 1) * 9 + (oy + 1) * 3 + (oz + 1));
             else
               moved_far = true;
+            left_cell = c2.x != cell_old.x || c2.y != cell_old.y || c2.z != cell_old.z;
           } else {
             moved_far = true;  // the particle pass of the next activation reports it
           }
+          s.moved[slot] = (uint8_t)(left_cell || moved_far);
         }
         const unsigned wbits = __reduce_or_sync(kFull, bit);
         if (lane == 0 && wbits) atomicOr(&s_moved, wbits);
-        if (__any_sync(kFull, moved_far) && lane == 0) s.ctr[kCtrMaskBad] = 1;
+        bool bad = moved_far;
+        const unsigned leavers = __ballot_sync(kFull, left_cell && !moved_far);
+        if (leavers) {
+          int base = 0;
+          if (lane == 0) base = atomicAdd(&s.ctr[kCtrMovers], __popc(leavers));
+          base = __shfl_sync(kFull, base, 0);
+          if ((leavers >> lane) & 1u) {
+            const int k = base + __popc(leavers & lanemask_lt());
+            if (k < p.mover_cap)
+              s.movers[k] = slot;
+            else
+              bad = true;  // list full: the next substep bins every particle
+          }
+        }
+        if (__any_sync(kFull, bad) && lane == 0) s.ctr[kCtrMaskBad] = 1;
       }
       // F <- (I + dt C) F
       float Fn[9];
@@ -1334,7 +1657,7 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
       }
       if (s.nxt.plastic) s.nxt.plastic[slot] = pl;
       s.nxt.id[slot] = id;
-      if (kBatch) s.nxt.sid[slot] = s.cur.sid[icur];
+      if (kBatch) s.nxt.sid[slot] = sid;
     }
     __syncthreads();
     if (threadIdx.x == 0) s.bmask[b] = s_moved;
@@ -2083,14 +2406,23 @@ cudaError_t launch_activate(scene_device &s, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Both binnings are enqueued; each kernel returns at once unless the device counter
+// kCtrIncBin (set by the activation) selects its path, so one CUDA graph serves both.
 cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
   const int sm = num_sms();
   k_bin_count<<<sm * 16, kThreads, 0, st>>>(s);
+  k_inc_map<<<sm, kThreads, 0, st>>>(s);
+  k_inc_stayers<<<sm * 8, kThreads, 0, st>>>(s);
+  k_inc_movers<<<sm * 4, kThreads, 0, st>>>(s);
   cudaError_t e = device_scan(load_int{s.block_count}, &s.ctr[kCtrBlocks], s.scan_part, s.block_start, st);
   if (e != cudaSuccess) return e;
   k_cell_start<<<sm * 4, 512, 0, st>>>(s);
   k_bin_scatter<<<sm * 16, kThreads, 0, st>>>(s);
+  k_inc_place_stayers<<<sm * 8, kThreads, 0, st>>>(s);
+  k_inc_place_movers<<<sm * 4, kThreads, 0, st>>>(s);
   k_bin_finalize<<<sm * 3, 512, 0, st>>>(s);
+  k_inc_sort<<<sm * 2, kThreads, 0, st>>>(s);
+  k_inc_finalize<<<sm * 8, kThreads, 0, st>>>(s);
   return cudaGetLastError();
 }
 
@@ -2098,6 +2430,8 @@ cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
 // capture of its launches
 cudaError_t prepare_kernels() {
   cudaError_t e = cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_p2g, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_g2p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kG2P2GSmem);
   if (e != cudaSuccess) return e;
@@ -2121,7 +2455,7 @@ cudaError_t prepare_kernels() {
 }
 
 cudaError_t launch_p2g(scene_device &s, cudaStream_t st) {
-  const int per_sm = s.prm.p2g_ctas_per_sm > 0 ? s.prm.p2g_ctas_per_sm : 2;
+  const int per_sm = s.prm.p2g_ctas_per_sm > 0 ? s.prm.p2g_ctas_per_sm : kP2GMinCtas;
   k_p2g<<<num_sms() * per_sm, kP2GThreads, kP2GSmemBytes, st>>>(s);
   return cudaGetLastError();
 }
@@ -2216,9 +2550,9 @@ cudaError_t launch_cg_iteration(scene_device &s, float *x, const cg_vectors &v, 
 }
 
 // k_begin, the two particle-block inserts (one returns at once), enlarge, prepare, set, 3 scans,
-// ranks, neighbours; count, 3 scans, cell_start, scatter, finalize; p2g; grid update and
-// boundaries; g2p
-int kernels_per_substep() { return 11 + 7 + 4; }
+// ranks, neighbours; the binning's 14 launches (the full and the incremental path, one of
+// which returns at once); p2g; grid update and boundaries; g2p
+int kernels_per_substep() { return 11 + 14 + 4; }
 
 cudaError_t launch_import(scene_device &s, const float *m, const float *x, const float *v,
                           const float *C, const float *F, const float *plastic, int n,
