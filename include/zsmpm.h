@@ -502,6 +502,25 @@ ZSMPM_API zsmpm_status zsmpm_scene_set_state_log(zsmpm_scene *s, float *buffer, 
 /* Rows logged so far (at most cap; synchronises). */
 ZSMPM_API zsmpm_status zsmpm_scene_state_log_count(zsmpm_scene *s, int64_t *count_out);
 
+/* ---- particle output (io/ParticleIO.hpp:11-22) ---------------------------------- */
+/* Houdini classic binary geometry (.bgeo), the format zs::write_partio writes through partio:
+ * big-endian "Bgeo" V5, one point per particle with its position as P (and w = 1), one
+ * particle-system primitive over all points.  Host arrays; the path must end in ".bgeo"
+ * (the gzip-compressed ".bgeo.gz" that partio also writes is not built).
+ * zsmpm_write_partio replaces write_partio<float,3>(filename, data, tag): with tag
+ * "position" (or null) data[n][3] are the positions; with another tag they are stored as a
+ * vector point attribute of that name and P is zero.  _with_stress and _with_grid replace
+ * write_partio_with_stress (a float attribute "stress") and write_partio_with_grid (a vector
+ * attribute "force").  No device needed. */
+ZSMPM_API zsmpm_status zsmpm_write_partio(const char *path, const float *data, int64_t n, const char *tag);
+ZSMPM_API zsmpm_status zsmpm_write_partio_with_stress(const char *path, const float *pos, const float *stress,
+                                                      int64_t n);
+ZSMPM_API zsmpm_status zsmpm_write_partio_with_grid(const char *path, const float *pos, const float *force,
+                                                    int64_t n);
+/* The scene's particle positions, in upload order, written as with zsmpm_write_partio
+ * (synchronises). */
+ZSMPM_API zsmpm_status zsmpm_scene_write_partio(zsmpm_scene *scene, const char *path);
+
 /* ---- allocation-free variant --------------------------------------------------- */
 /* Block activation without any device allocation.  No counterpart in the reference: it is
  * for callers that cannot call cudaMalloc at this point -- hosts whose own memory pool has

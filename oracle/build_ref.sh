@@ -1,6 +1,7 @@
 #!/usr/bin/env bash
 # Test infrastructure: builds the reference's own OpenMP/sequential MPM path
-# (littlemine/zpc, read from /root/reference) into the executable oracle/_ref/zsref_cli,
+# (littlemine/zpc, its include/ tree at $ZSMPM_REFERENCE_ROOT, by default the directory
+# "reference" beside this repository) into the executable oracle/_ref/zsref_cli,
 # driven by oracle/ref_driver.cpp and oracle/ref_cli.cpp.  The output is the checker and the CPU baseline, never the product.
 #
 # zpc's CMake build needs the zpc_tpls submodule, which is not checked out, so the needed
@@ -25,7 +26,7 @@
 # Logging (plog) and magic_enum are replaced by the small shims in oracle/ref_shims.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${ZSMPM_REFERENCE_ROOT:-/root/reference}/include"
+REF="${ZSMPM_REFERENCE_ROOT:-$(cd "$HERE/../.." && pwd)/reference}/include"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/zensim" ]; then
   echo "build_ref: reference sources not found at $REF; keeping any prebuilt $OUT" >&2

@@ -169,6 +169,10 @@ SIGNATURES = {
     "zsmpm_scene_closure_audit": (_S, [_P, C.POINTER(ClosureAudit), C.c_int32]),
     "zsmpm_scene_set_state_log": (_S, [_P, _P, C.c_int64, C.c_int32]),
     "zsmpm_scene_state_log_count": (_S, [_P, C.POINTER(C.c_int64)]),
+    "zsmpm_write_partio": (_S, [C.c_char_p, _P, C.c_int64, C.c_char_p]),
+    "zsmpm_write_partio_with_stress": (_S, [C.c_char_p, _P, _P, C.c_int64]),
+    "zsmpm_write_partio_with_grid": (_S, [C.c_char_p, _P, _P, C.c_int64]),
+    "zsmpm_scene_write_partio": (_S, [_P, C.c_char_p]),
     "zsmpm_activate_blocks_noalloc": (_S, [_P, C.c_int64, C.c_float, _P, C.c_int32, _P, _P]),
 }
 

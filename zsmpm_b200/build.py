@@ -17,7 +17,7 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 OBJ_DIR = PKG / "_build"
 LIB = LIB_DIR / "libzsmpm.so"
-SOURCES = ["zsmpm_kernels.cu", "zsmpm_closure.cu", "zsmpm_bht.cu", "zsmpm_api.cu", "zsmpm_static.cu"]
+SOURCES = ["zsmpm_kernels.cu", "zsmpm_closure.cu", "zsmpm_bht.cu", "zsmpm_api.cu", "zsmpm_static.cu", "zsmpm_io.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

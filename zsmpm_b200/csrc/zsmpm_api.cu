@@ -645,6 +645,17 @@ ZSMPM_API zsmpm_status zsmpm_scene_download(zsmpm_scene *s, zsmpm_particle_array
   return ZSMPM_OK;
 }
 
+ZSMPM_API zsmpm_status zsmpm_scene_write_partio(zsmpm_scene *s, const char *path) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  std::vector<float> x(3 * (size_t)s->dev.prm.n);
+  zsmpm_particle_arrays arrs{};
+  arrs.x = x.data();
+  st = zsmpm_scene_download(s, &arrs, 0, s->last_stream);
+  if (st != ZSMPM_OK) return st;
+  return zsmpm_write_partio(path, x.data(), s->dev.prm.n, "position");
+}
+
 ZSMPM_API zsmpm_status zsmpm_scene_download_tilevector(zsmpm_scene *s, const zsmpm_tilevector_view *tv,
                                                        void *stream) {
   zsmpm_status st = check_scene(s, true);
