@@ -229,10 +229,10 @@ ZSMPM_API zsmpm_status zsmpm_run(zsmpm_scene *scene, int32_t nsteps, void *strea
 ZSMPM_API zsmpm_status zsmpm_get_table_view(zsmpm_scene *scene, zsmpm_table_view *out);
 ZSMPM_API zsmpm_status zsmpm_get_grid_view(zsmpm_scene *scene, zsmpm_grid_view *out);
 /* The active blocks of the last activation as a bht<i32,3,int,16> (synchronises; rebuilt on
- * every call, on the host): the table that the reference's host BHTView::insert
- * (container/Bht.hpp:612-665) builds when the keys are inserted in ascending block order into
- * a bht sized for max(blocks, 16) entries, so index == block index.  The view stays valid until the next call or
- * the scene's destruction. */
+ * every call, on the device from the device's active keys): the table that the reference's
+ * host BHTView::insert (container/Bht.hpp:612-665) builds when the keys are inserted in
+ * ascending block order into a bht sized for max(blocks, 16) entries, so index == block index.
+ * The view stays valid until the next call or the scene's destruction. */
 ZSMPM_API zsmpm_status zsmpm_get_bht_view(zsmpm_scene *scene, zsmpm_bht_view *out);
 /* The same table built on the host from keys[nkeys][3] in order, sized for `expected` entries
  * (0: nkeys): table_keys [cap_slots][4], indices and status [cap_slots]; *table_size and the
@@ -241,6 +241,15 @@ ZSMPM_API zsmpm_status zsmpm_get_bht_view(zsmpm_scene *scene, zsmpm_bht_view *ou
 ZSMPM_API zsmpm_status zsmpm_bht_build_host(const int32_t *keys, int32_t nkeys, int32_t expected,
                                             int32_t *table_keys, int32_t *indices, int32_t *status,
                                             int32_t cap_slots, int32_t *table_size, uint32_t *hashers);
+/* The same table built on the device (the bht's device insert, container/Bht.hpp:490-610,
+ * with the layout of the in-order host insert): keys, table_keys [cap_slots][4], indices and
+ * status [cap_slots] are device pointers; *table_size and hashers[6] are host outputs.  All
+ * keys are placed at once by an iteration over their bucket choices that settles on the
+ * in-order layout (synchronises on `stream`). */
+ZSMPM_API zsmpm_status zsmpm_bht_build_device(const int32_t *keys, int32_t nkeys, int32_t expected,
+                                              int32_t *table_keys, int32_t *indices, int32_t *status,
+                                              int32_t cap_slots, int32_t *table_size, uint32_t *hashers,
+                                              void *stream);
 /* Number of active blocks of the last activation (synchronises). */
 ZSMPM_API zsmpm_status zsmpm_num_blocks(zsmpm_scene *scene, int32_t *out);
 /* Copies the active keys [nb][3] and the grid [nb][4][512] to host memory. */

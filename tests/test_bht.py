@@ -1,6 +1,7 @@
 """The bht<i32,3,int,16> layout (container/Bht.hpp) of block keys: the library's host builder
-against the reference's own host insert (oracle/_ref/zsref_cli), slot for slot, and on the GPU
-the scene's bht view against the library's block indices."""
+against the reference's own host insert (oracle/_ref/zsref_cli), slot for slot; on the GPU the
+device builder against both (including tables dense enough that keys move to their second and
+third buckets), and the scene's bht view against the library's block indices."""
 import numpy as np
 import pytest
 
@@ -97,3 +98,40 @@ def test_scene_bht_view_indexes_blocks(zs, gpu):
     occupied = tk[:, 0] != SENT
     found = {tuple(k): i for k, i in zip(tk[occupied, :3].tolist(), ti[occupied].tolist())}
     assert [found[tuple(k)] for k in keys.tolist()] == list(range(len(keys)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("expected_factor", [1.0, 0.7, 0.55])
+def test_device_build_bit_exact_with_reference(zs, gpu, reference_cli, expected_factor):
+    from zsmpm_b200 import scenes
+    keys = _scene_keys(scenes.small_scene(model=1, n_side=0.3))
+    expected = max(int(len(keys) * expected_factor), 16)
+    theirs = reference_cli.bht(keys, expected)
+    ours = zs.bht_build_device(keys, expected)
+    _compare(ours, theirs, len(keys))
+    host = zs.bht_build_host(keys, expected)
+    for k in ("keys", "indices", "status"):
+        assert np.array_equal(ours[k], host[k])
+
+
+@pytest.mark.gpu
+def test_device_build_edge_cases(zs, gpu, reference_cli):
+    for keys in (np.zeros((0, 3), np.int32), np.array([[0, 0, 0]], np.int32),
+                 np.array([[-1, -2, -3], [1048575, -1048576, 7]], np.int32)):
+        theirs = reference_cli.bht(keys, 16)
+        ours = zs.bht_build_device(keys, 16)
+        _compare(ours, theirs, len(keys))
+
+
+@pytest.mark.gpu
+def test_device_build_many_keys(zs, gpu):
+    """A large random key set at the densest table the sizing rule allows (n just below a power
+    of two, about 7.9 keys per 16-slot bucket): the device table equals the in-order host one."""
+    rng = np.random.default_rng(5)
+    n = 60000
+    keys = np.unique(rng.integers(-5000, 5000, size=(2 * n, 3)).astype(np.int32), axis=0)[:n]
+    keys = keys[rng.permutation(len(keys))]
+    ours = zs.bht_build_device(keys, len(keys))
+    host = zs.bht_build_host(keys, len(keys))
+    for k in ("keys", "indices", "status"):
+        assert np.array_equal(ours[k], host[k])

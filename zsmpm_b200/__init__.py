@@ -48,6 +48,26 @@ def bht_build_host(keys: np.ndarray, expected: int = 0) -> dict:
             "status": ts}
 
 
+def bht_build_device(keys: np.ndarray, expected: int = 0) -> dict:
+    """The same layout built on the device (zsmpm_bht_build_device); returns host copies."""
+    import torch
+    keys = np.ascontiguousarray(keys, dtype=np.int32).reshape(-1, 3)
+    lib = _abi.lib()
+    size = C.c_int32()
+    hashers = (C.c_uint32 * 6)()
+    lib.zsmpm_bht_build_host(_ptr(keys), len(keys), expected, None, None, None, 0, C.byref(size), hashers)
+    n = size.value
+    dk = torch.from_numpy(keys.copy()).cuda() if len(keys) else torch.zeros((1, 3), dtype=torch.int32).cuda()
+    tk = torch.empty((max(n, 1), 4), dtype=torch.int32, device="cuda")
+    ti = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    ts = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    _abi.check(lib.zsmpm_bht_build_device(C.c_void_p(dk.data_ptr()), len(keys), expected, C.c_void_p(tk.data_ptr()),
+                                          C.c_void_p(ti.data_ptr()), C.c_void_p(ts.data_ptr()), n, C.byref(size),
+                                          hashers, None), "bht_build_device")
+    return {"table_size": n, "hash": np.array(list(hashers), np.uint32), "keys": tk[:n].cpu().numpy(),
+            "indices": ti[:n].cpu().numpy(), "status": ts[:n].cpu().numpy()}
+
+
 def device_count() -> int:
     return int(_abi.lib().zsmpm_device_count())
 

@@ -150,6 +150,7 @@ SIGNATURES = {
     "zsmpm_implicit_cg": (_S, [_P, _P, _P, C.c_int64, C.c_float, C.POINTER(CgOptions), C.POINTER(C.c_int32), _P]),
     "zsmpm_get_bht_view": (_S, [_P, C.POINTER(BhtView)]),
     "zsmpm_bht_build_host": (_S, [_P, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32, C.POINTER(C.c_int32), _P]),
+    "zsmpm_bht_build_device": (_S, [_P, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32, C.POINTER(C.c_int32), _P, _P]),
     "zsmpm_batch_create": (_S, [C.POINTER(SceneDesc), C.POINTER(Material), C.c_int32, C.POINTER(_P)]),
     "zsmpm_batch_upload": (_S, [_P, C.POINTER(ParticleArrays), _P, C.c_int32, _P]),
     "zsmpm_batch_num_scenes": (_S, [_P, C.POINTER(C.c_int32)]),

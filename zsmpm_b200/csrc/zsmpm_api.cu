@@ -1004,15 +1004,10 @@ ZSMPM_API zsmpm_status zsmpm_get_bht_view(zsmpm_scene *s, zsmpm_bht_view *out) {
   if (nb > 0)
     ZS_TRY(cudaMemcpy(keys.data(), s->dev.active_keys, sizeof(int32_t) * 3 * nb, cudaMemcpyDeviceToHost),
            "read active keys");
-  int32_t size = 0;
-  uint32_t hash[6] = {};
   // sized for max(nb, 16) entries: below that the reference's proximity rule (an index at or
   // above size - 20 fails) rejects even a single key
-  const int32_t expected = std::max(nb, 16);
-  zsmpm_bht_build_host(keys.data(), nb, expected, nullptr, nullptr, nullptr, 0, &size, hash);
-  std::vector<int32_t> tk(4 * (size_t)size), ti(size), ts(size);
-  st = zsmpm_bht_build_host(keys.data(), nb, expected, tk.data(), ti.data(), ts.data(), size, &size, hash);
-  if (st != ZSMPM_OK) return st;
+  const int64_t size = bht_table_size(std::max(nb, 16));
+  if (nb > 0 && (int64_t)nb - 1 >= size - 20) return fail(ZSMPM_ERR_TABLE_FULL, "bht table too small for the keys");
   if (size > s->bht_cap) {
     release_bht(s);
     ZS_TRY(cudaMalloc(&s->bht_keys, sizeof(int32_t) * 4 * (size_t)size), "alloc bht keys");
@@ -1022,20 +1017,18 @@ ZSMPM_API zsmpm_status zsmpm_get_bht_view(zsmpm_scene *s, zsmpm_bht_view *out) {
     ZS_TRY(cudaMalloc(&s->bht_cnt, sizeof(int32_t) * 2), "alloc bht count");
     s->bht_cap = size;
   }
-  const int32_t cs[2] = {nb, 1};  // cnt, build success
-  ZS_TRY(cudaMemcpy(s->bht_keys, tk.data(), sizeof(int32_t) * tk.size(), cudaMemcpyHostToDevice), "bht keys");
-  ZS_TRY(cudaMemcpy(s->bht_indices, ti.data(), sizeof(int32_t) * ti.size(), cudaMemcpyHostToDevice), "bht indices");
-  ZS_TRY(cudaMemcpy(s->bht_status, ts.data(), sizeof(int32_t) * ts.size(), cudaMemcpyHostToDevice), "bht status");
-  if (nb > 0)
-    ZS_TRY(cudaMemcpy(s->bht_active, keys.data(), sizeof(int32_t) * 3 * nb, cudaMemcpyHostToDevice), "bht active");
-  ZS_TRY(cudaMemcpy(s->bht_cnt, cs, sizeof(cs), cudaMemcpyHostToDevice), "bht count");
+  // built on the device from the active keys in canonical order (zsmpm_bht.cu)
+  uint32_t hash[6] = {};
+  const int built = bht_build_device(s->dev.active_keys, nb, size, s->bht_keys, s->bht_indices, s->bht_status,
+                                     s->bht_active, s->bht_cnt, hash, s->last_stream);
+  if (built != ZSMPM_OK) return (zsmpm_status)built;
   out->keys = s->bht_keys;
   out->indices = s->bht_indices;
   out->status = s->bht_status;
   out->active_keys = s->bht_active;
   out->cnt = s->bht_cnt;
   out->success = s->bht_cnt + 1;
-  out->table_size = size;
+  out->table_size = (int32_t)size;
   for (int k = 0; k < 6; ++k) out->hashers[k] = hash[k];
   return ZSMPM_OK;
 }

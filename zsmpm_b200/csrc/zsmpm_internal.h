@@ -210,6 +210,13 @@ bool closure_device_view(const zsmpm_closure *c, closure_dev *out);
 int record_error(int status, const char *message);
 cudaError_t launch_svd_batch(const float *A, float *U, float *S, float *V, long long count,
                              cudaStream_t st);
+// the bht<i32,3,int,16> of keys[n][3] built on the device (zsmpm_bht.cu); returns a zsmpm_status
+int bht_build_device(const int32_t *keys, int n, int64_t size, int32_t *tkeys, int32_t *indices, int32_t *status,
+                     int32_t *active, int32_t *cnt_success, uint32_t *hashers_out, cudaStream_t st);
+int64_t bht_table_size(int64_t n);
+// exclusive scan of in[0, *n_ptr) into out[0, *n_ptr] (out[n] = total); part holds
+// 2 * kScanCtas + 1 partial sums
+cudaError_t launch_exclusive_scan(const int *in, const int *n_ptr, int *part, int *out, cudaStream_t st);
 cudaError_t launch_constitutive_batch(const material_dev &mat, float *F, float *plastic,
                                       float *tau, long long count, cudaStream_t st);
 

@@ -2609,6 +2609,10 @@ cudaError_t launch_activate_static(scene_device &s, const float *x, int *keys_ou
   return cudaGetLastError();
 }
 
+cudaError_t launch_exclusive_scan(const int *in, const int *n_ptr, int *part, int *out, cudaStream_t st) {
+  return device_scan(load_int{in}, n_ptr, part, out, st);
+}
+
 cudaError_t launch_svd_batch(const float *A, float *U, float *S, float *V, long long count,
                              cudaStream_t st) {
   k_svd_batch<<<num_sms() * 4, kThreads, 0, st>>>(A, U, S, V, count);
