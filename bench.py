@@ -279,6 +279,7 @@ def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms
     sc.status()
     cl.attach(sc, None)
     mlp = mlp_inference_leg(c, n_rows=min(n, 16_777_216)) if mlp else None
+    kept = c.dataset_size()[1]
     c.close()
     value = n * args.steps * ws / (lms * 1e-3)
     return {"value": value, "unit": UNIT, "ms_per_step": lms / args.steps,
@@ -287,6 +288,8 @@ def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms
                       "what": "principal Kirchhoff stress of audited particles vs the plain return map; "
                               "rel = |dtau| / (|tau| + 1e-4 (3 lambda + 2 mu)); agg = sqrt(sum|dtau|^2/sum|tau|^2)"},
             "training": {"random_states": args.train_random, "logged_states": n_log,
+                         "projected_states_kept": kept,
+                         "cohesion": "Pa mapped to the log-strain shift c / (3 lambda + 2 mu)",
                          "epochs": sum(e for e, _, _ in schedule), "seconds": train_s,
                          "first_loss": float(losses[0]), "final_loss": float(losses[-1])},
             "inference": "BF16 mma.sync m16n8k16, FP32 accumulation, fused in G2P",
@@ -332,6 +335,7 @@ def batch_learned_leg(args, zs, sc, specs, parts, upload_pinned, stream, sptr, w
     lms = max_over_ranks(e0.elapsed_time(e1), ws)
     a = cl.audit(sc)
     cl.attach(sc, None)
+    kept = c.dataset_size()[1]
     c.close()
     n = sum(q.n for q in parts)
     return {"value": n * args.steps * ws / (lms * 1e-3), "unit": UNIT, "ms_per_step": lms / args.steps,
@@ -339,6 +343,7 @@ def batch_learned_leg(args, zs, sc, specs, parts, upload_pinned, stream, sptr, w
             "scenes_served": sum(1 for sp in specs if sp.material.model == zs.DRUCKER_PRAGER),
             "audit": {"period": 100, **a},
             "training": {"random_states": args.train_random, "logged_states": n_log,
+                         "projected_states_kept": kept,
                          "logged_from": f"scene {k} alone", "seconds": train_s,
                          "first_loss": float(losses[0]), "final_loss": float(losses[-1])}}
 
@@ -721,8 +726,10 @@ def main(argv=None):
     ap.add_argument("--no-extra", action="store_true",
                     help="measure only --scene (by default the sand scene run also measures the 16 M snow "
                          "scene, plain and learned, and the 256-scene batch)")
-    ap.add_argument("--train-random", type=int, default=1_500_000)
-    ap.add_argument("--train-logged", type=int, default=500_000)
+    # 20 M training states in all, as the learned-closure configuration states: random trial
+    # states plus states logged from the plain path
+    ap.add_argument("--train-random", type=int, default=16_000_000)
+    ap.add_argument("--train-logged", type=int, default=4_000_000)
     args = ap.parse_args(argv)
 
     spec, workload = scene_for(args.scene)

@@ -456,13 +456,19 @@ typedef struct {
 } zsmpm_closure_state;
 
 typedef struct {
-  int64_t audited;          /* particles checked against the plain return map */
+  int64_t audited;          /* network-projected particle updates checked against the plain return map */
   double mean_rel_error;    /* mean of |tau_mlp - tau_plain| / (|tau_plain| + 1e-4 (3 lambda + 2 mu)) */
   double max_rel_error;
   double agg_rel_error;     /* sqrt(sum |dtau|^2 / sum |tau_plain|^2) over the audited particles */
-  int64_t fallbacks;        /* particle updates outside the hull that used the plain map */
+  int64_t fallbacks;        /* projections outside the training hull that used the plain map */
+  int64_t network_updates;  /* particle updates whose projection the network gave */
+  int64_t updates;          /* all particle updates of G2P with the closure attached */
 } zsmpm_closure_audit;
 
+/* Rows of the last dataset: generated (random plus logged) and kept (those the plain return
+ * map projects, the training set; G2P decides the branch exactly and runs the network only for
+ * projections). */
+ZSMPM_API zsmpm_status zsmpm_closure_dataset_size(const zsmpm_closure *c, int64_t *generated, int64_t *kept);
 ZSMPM_API zsmpm_status zsmpm_closure_create(const zsmpm_material *mat, int32_t device, zsmpm_closure **out);
 ZSMPM_API zsmpm_status zsmpm_closure_destroy(zsmpm_closure *c);
 /* Training set: n_random random trial states (log singular values uniform in

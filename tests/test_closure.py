@@ -48,6 +48,24 @@ def random_rows(model, n, seed, E, nu):
     return np.ascontiguousarray(np.concatenate([l, f], 1), dtype=np.float32)
 
 
+def projected(model, rows, E, nu):
+    """Rows whose trial state the plain return map projects: Drucker-Prager onto the cone
+    (tr < 0 and dgamma > 0, compute_stress_sand), snow when a singular value leaves
+    [1 - theta_c, 1 + theta_s].  The closure's network replaces that branch only."""
+    r = rows.astype(np.float64)
+    mu, lam = E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+    if model == DP:
+        eps = r[:, :3] - r[:, 4:5]
+        tr = eps.sum(1) + r[:, 5]
+        eh = eps - tr[:, None] / 3
+        s = np.sin(np.radians(r[:, 3]))
+        ys = np.sqrt(2 / 3) * 2 * s / (3 - s)
+        dg = np.linalg.norm(eh, axis=1) + (3 * lam + 2 * mu) / (2 * mu) * tr * ys
+        return (tr < 0) & (dg > 0)
+    S = np.exp(r[:, :3])
+    return np.any((S < 1 - r[:, 3:4]) | (S > 1 + r[:, 4:5]), axis=1)
+
+
 def oracle_targets(spec, rows):
     """(D, tau) of the restated return map (float64) on F = diag(exp(l))."""
     from oracle import restated
@@ -203,15 +221,17 @@ def stress_errors(y, ref, mat):
 @pytest.mark.gpu
 @pytest.mark.parametrize("model", [DP, SNOW])
 def test_training_reduces_loss_and_beats_no_return_map(zs, gpu, model):
-    """What the trained network gains over the method without it: on held-out trial states,
-    its stress error against the plain return map is compared with the error of dropping the
-    return map (the elastic trial stress)."""
+    """What the trained network gains over the method without it: on held-out trial states that
+    the return map projects (the branch the network replaces), its stress error against the
+    plain return map is compared with the error of dropping the return map (the elastic trial
+    stress)."""
     import torch
     spec, c = _closure(zs, model, n_random=400000)
     losses = c.fit()
     assert np.all(np.isfinite(losses))
     assert losses[-1] < 0.02 * losses[0]
-    rows = random_rows(model, 50000, 99, spec.material.E, spec.material.nu)
+    rows = random_rows(model, 100000, 99, spec.material.E, spec.material.nu)
+    rows = rows[projected(model, rows, spec.material.E, spec.material.nu)][:50000]
     x = torch.from_numpy(rows).to(gpu)
     ref = c.targets(x).cpu().numpy().astype(np.float64)
     y16 = c.infer(x, bf16=True).cpu().numpy().astype(np.float64)
@@ -287,28 +307,33 @@ def test_learned_scene_follows_plain_and_audits(zs, gpu):
     err_learned = np.linalg.norm(learned.x.astype(np.float64) - plain.x) / disp
     err_elastic = np.linalg.norm(elastic.x.astype(np.float64) - plain.x) / disp
     print(f"audit {a}; displacement error learned {err_learned:.3e} elastic {err_elastic:.3e}")
-    # one in 100 particles per substep is audited
-    expect = parts.n * steps / 100
-    assert 0.7 * expect < a["audited"] < 1.3 * expect
+    # every particle update is counted; one in 100 of those the network projected is audited
+    assert a["updates"] == parts.n * steps
+    assert a["network_updates"] > 0
+    expect = a["network_updates"] / 100
+    assert 0.7 * expect < a["audited"] < 1.3 * expect + 5
     assert np.isfinite(a["mean_rel_error"]) and a["max_rel_error"] >= a["mean_rel_error"]
-    assert a["agg_rel_error"] < 0.05
+    assert a["mean_rel_error"] < 1e-2 and a["agg_rel_error"] < 2e-2
     assert err_learned < 0.2 * err_elastic
     c.close()
 
 
 @pytest.mark.gpu
 def test_outside_hull_falls_back_to_plain(zs, gpu):
-    """A hull that excludes every state: each particle takes the plain return map."""
+    """A hull that excludes every state: each projection takes the plain return map."""
     spec = _sand_scene()
-    steps = 10
+    steps = 60  # the box lands after ~35 substeps, and its particles start to project
     _, c = _closure(zs, DP, n_random=5000)
     st = c.get_state()
     st.in_max[0] = -10.0  # no trial state has a largest log singular value below -10
     c.set_state(st)
     learned, a = _run_scene(zs, spec, steps, closure=c, audit_period=0)
     plain, _ = _run_scene(zs, spec, steps)
-    assert a["fallbacks"] == learned.n * steps
+    # the box lands: projections happen, each by the plain map, none by the network
+    assert a["fallbacks"] > 0 and a["network_updates"] == 0
     assert a["audited"] == 0
+    # the same arithmetic as the plain path; two runs differ by the order of P2G's float sums,
+    # which the landing's plastic flow amplifies in F over 60 substeps
     assert np.max(np.abs(learned.x - plain.x)) <= 1e-6
-    assert np.max(np.abs(learned.F - plain.F)) <= 1e-5
+    assert np.max(np.abs(learned.F - plain.F)) <= 1e-4
     c.close()

@@ -56,11 +56,13 @@ def test_snow_subset_plain_and_learned_against_fp64(zs, gpu):
            "learned_x": rel_l2(lrn.x - q.x, o64.x - q.x), "learned_v": rel_l2(lrn.v, o64.v)}
     print(f"\nsnow subset {q.n} of {n_full} particles, {STEPS} substeps, relative L2 against FP64: "
           + ", ".join(f"{k} {v:.2e}" for k, v in err.items())
-          + f"; learned audit mean {a['mean_rel_error']:.2e} agg {a['agg_rel_error']:.2e} fallbacks {a['fallbacks']}")
+          + f"; learned audit {a}")
     # the plain GPU path is as close to FP64 as the FP32 CPU restatement (within 2x)
     assert err["gpu_v"] <= max(2 * err["cpu32_v"], 1e-6)
     assert err["gpu_x"] <= max(2 * err["cpu32_x"], 1e-6)
     assert rel_l2(g.v, o32.v) < 5e-5
-    # the learned closure stays within its audited stress error of the plain path
-    assert err["learned_v"] < 1e-3
-    assert a["audited"] > 0 and a["mean_rel_error"] < 1e-2
+    # In these 10 substeps the sphere has not reached the slab: every trial state stays inside
+    # the clamp box, the exact branch test keeps the strain, and the network never runs (the
+    # snow column started in contact, tests/test_config_parity.py, exercises it).
+    assert a["network_updates"] == 0 and a["updates"] == q.n * STEPS
+    assert err["learned_v"] <= max(2 * err["cpu32_v"], 1e-6)

@@ -82,7 +82,7 @@ class ClosureState(C.Structure):
 class ClosureAudit(C.Structure):
     _fields_ = [("audited", C.c_int64), ("mean_rel_error", C.c_double),
                 ("max_rel_error", C.c_double), ("agg_rel_error", C.c_double),
-                ("fallbacks", C.c_int64)]
+                ("fallbacks", C.c_int64), ("network_updates", C.c_int64), ("updates", C.c_int64)]
 
 
 class Collider(C.Structure):
@@ -167,6 +167,7 @@ SIGNATURES = {
     "zsmpm_closure_get_state": (_S, [_P, C.POINTER(ClosureState)]),
     "zsmpm_closure_set_state": (_S, [_P, C.POINTER(ClosureState)]),
     "zsmpm_scene_set_closure": (_S, [_P, _P, C.c_int32]),
+    "zsmpm_closure_dataset_size": (_S, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "zsmpm_scene_closure_audit": (_S, [_P, C.POINTER(ClosureAudit), C.c_int32]),
     "zsmpm_scene_set_state_log": (_S, [_P, _P, C.c_int64, C.c_int32]),
     "zsmpm_scene_state_log_count": (_S, [_P, C.POINTER(C.c_int64)]),

@@ -72,6 +72,12 @@ class Closure:
         _abi.check(self._lib.zsmpm_closure_build_dataset(self._h, int(n_random), C.c_uint64(seed), ptr,
                                                          n_logged, _stream(stream)), "closure_build_dataset")
 
+    def dataset_size(self) -> tuple:
+        """(rows generated or logged, rows kept: those the plain return map projects)."""
+        g, k = C.c_int64(), C.c_int64()
+        _abi.check(self._lib.zsmpm_closure_dataset_size(self._h, C.byref(g), C.byref(k)), "closure_dataset_size")
+        return int(g.value), int(k.value)
+
     def train(self, epochs: int, batch: int = 4096, lr: float = 1e-3, seed: int = 0,
               stream=None) -> np.ndarray:
         """Adam epochs over the training set; returns the mean loss of each epoch."""
@@ -147,7 +153,8 @@ def audit(scene, reset: bool = False) -> dict:
                "scene_closure_audit")
     return {"audited": int(a.audited), "mean_rel_error": a.mean_rel_error,
             "max_rel_error": a.max_rel_error, "agg_rel_error": a.agg_rel_error,
-            "fallbacks": int(a.fallbacks)}
+            "fallbacks": int(a.fallbacks), "network_updates": int(a.network_updates), "updates": int(a.updates),
+            "network_share": (a.network_updates / a.updates) if a.updates else 0.0}
 
 
 def set_state_log(scene, buffer, period: int) -> None:

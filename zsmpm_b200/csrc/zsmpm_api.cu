@@ -954,6 +954,8 @@ ZSMPM_API zsmpm_status zsmpm_scene_closure_audit(zsmpm_scene *s, zsmpm_closure_a
   out->max_rel_error = h[2];
   out->agg_rel_error = h[4] > 0 ? std::sqrt(h[3] / h[4]) : 0.0;
   out->fallbacks = (int64_t)h[5];
+  out->network_updates = (int64_t)h[6];
+  out->updates = (int64_t)h[7];
   if (reset) ZS_TRY(cudaMemset(s->audit, 0, sizeof(h)), "reset audit");
   return ZSMPM_OK;
 }

@@ -35,6 +35,7 @@ struct zsmpm_closure {
   float *data_xt = nullptr;   // network inputs [n][6] (closure_inputs of data_x)
   float *data_yt = nullptr;   // network targets [n][6] (closure_net_targets of data_y)
   int64_t data_n = 0, data_cap = 0;
+  int64_t data_generated = 0;  // rows generated or logged; data_n of them are projected by the plain map
   float *stats = nullptr;     // reduction scratch
   float *loss = nullptr;
   int adam_t = 0;
@@ -80,6 +81,46 @@ __device__ __forceinline__ void closure_target(const material_dev &md, int model
   for (int i = 0; i < 3; ++i) {
     y[i] = r.H[i] - l[i];
     y[3 + i] = r.tau[i];
+  }
+}
+
+// whether the plain map projects a raw row (the branch the network replaces): Drucker-Prager
+// onto the cone (tr < 0 and dgamma > 0, compute_stress_sand), snow when a singular value
+// leaves [1 - theta_c, 1 + theta_s]; elastic states and the Drucker-Prager tip are computed
+// exactly in G2P and need no network
+__device__ __forceinline__ bool closure_projects(const material_dev &md, int model, const float *x) {
+  if (model == 1) {
+    float eps[3], eh[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) eps[i] = x[i] - x[4];
+    const float tr = eps[0] + eps[1] + eps[2] + x[5];
+    if (tr >= 0.f) return false;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) eh[i] = eps[i] - tr / 3.f;
+    const float ehn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2]);
+    const float smu = 2.f * md.mu;
+    return ehn + (3.f * md.lambda + smu) / smu * tr * yield_surface_of(x[3]) > 0.f;
+  }
+  bool out = false;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float S = expf(x[i]);
+    out = out || S < 1.f - x[3] || S > 1.f + x[4];
+  }
+  return out;
+}
+
+// the rows the plain map projects, compacted (in any order) into (xo, yo); *count their number
+__global__ void k_closure_keep_projected(material_dev md, int model, const float *x, const float *y, int64_t n,
+                                         float *xo, float *yo, unsigned long long *count) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (!closure_projects(md, model, x + 6 * i)) continue;
+    const unsigned long long j = atomicAdd(count, 1ull);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      xo[6 * j + k] = x[6 * i + k];
+      yo[6 * j + k] = y[6 * i + k];
+    }
   }
 }
 
@@ -841,7 +882,23 @@ ZSMPM_API zsmpm_status zsmpm_closure_build_dataset(zsmpm_closure *c, int64_t n_r
     k_closure_targets<<<sms() * 8, kThreads, 0, st>>>(c->md, c->cd.model, c->data_x + 6 * n_random,
                                                       c->data_y + 6 * n_random, n_logged);
   }
-  k_closure_transform<<<sms() * 8, kThreads, 0, st>>>(c->cd, c->data_x, c->data_y, c->data_xt, c->data_yt, n);
+  // only states that the plain map projects: G2P evaluates the network on those alone
+  {
+    unsigned long long *kept = reinterpret_cast<unsigned long long *>(c->stats + 30);  // 8-byte aligned slot
+    CZ_TRY(cudaMemsetAsync(kept, 0, sizeof(unsigned long long), st), "dataset count");
+    k_closure_keep_projected<<<sms() * 8, kThreads, 0, st>>>(c->md, c->cd.model, c->data_x, c->data_y, n,
+                                                             c->data_xt, c->data_yt, kept);
+    unsigned long long h_kept = 0;
+    CZ_TRY(cudaMemcpyAsync(&h_kept, kept, sizeof(h_kept), cudaMemcpyDeviceToHost, st), "dataset count");
+    CZ_TRY(cudaStreamSynchronize(st), "dataset count");
+    if (h_kept < 1) return cerr(ZSMPM_ERR_INVALID_ARG, "no state of the dataset is projected by the return map");
+    std::swap(c->data_x, c->data_xt);
+    std::swap(c->data_y, c->data_yt);
+    c->data_generated = n;
+    c->data_n = (int64_t)h_kept;
+  }
+  const int64_t m = c->data_n;
+  k_closure_transform<<<sms() * 8, kThreads, 0, st>>>(c->cd, c->data_x, c->data_y, c->data_xt, c->data_yt, m);
   CZ_TRY(cudaGetLastError(), "dataset kernels");
   // normalisation of the network's inputs and targets; hull of the raw training rows
   float init[32];
@@ -852,7 +909,7 @@ ZSMPM_API zsmpm_status zsmpm_closure_build_dataset(zsmpm_closure *c, int64_t n_r
     std::memcpy(&init[18 + k], &hi, 4);
   }
   CZ_TRY(cudaMemcpyAsync(c->stats, init, sizeof(init), cudaMemcpyHostToDevice, st), "stats init");
-  k_closure_stats<<<sms() * 4, kThreads, 0, st>>>(c->data_xt, c->data_x, c->data_yt, n, c->stats);
+  k_closure_stats<<<sms() * 4, kThreads, 0, st>>>(c->data_xt, c->data_x, c->data_yt, m, c->stats);
   float h[32];
   CZ_TRY(cudaMemcpyAsync(h, c->stats, sizeof(h), cudaMemcpyDeviceToHost, st), "stats read");
   CZ_TRY(cudaStreamSynchronize(st), "stats sync");
@@ -865,17 +922,24 @@ ZSMPM_API zsmpm_status zsmpm_closure_build_dataset(zsmpm_closure *c, int64_t n_r
     return r;
   };
   for (int k = 0; k < 6; ++k) {
-    const double mean = h[k] / (double)n;
-    const double var = std::max(h[6 + k] / (double)n - mean * mean, 1e-20);
+    const double mean = h[k] / (double)m;
+    const double var = std::max(h[6 + k] / (double)m - mean * mean, 1e-20);
     c->cd.in_mean[k] = (float)mean;
     c->cd.in_inv_std[k] = (float)(1.0 / std::sqrt(var));
     c->cd.in_min[k] = unorder(h[12 + k]);
     c->cd.in_max[k] = unorder(h[18 + k]);
-    const double rms = std::sqrt(h[24 + k] / (double)n);
+    const double rms = std::sqrt(h[24 + k] / (double)m);
     c->cd.out_scale[k] = (float)std::max(rms, 1e-12);
   }
   c->normalized = true;
   return pack(c, st);
+}
+
+ZSMPM_API zsmpm_status zsmpm_closure_dataset_size(const zsmpm_closure *c, int64_t *generated, int64_t *kept) {
+  if (!c || !generated || !kept) return cerr(ZSMPM_ERR_INVALID_ARG, "null argument");
+  *generated = c->data_generated;
+  *kept = c->data_n;
+  return ZSMPM_OK;
 }
 
 ZSMPM_API zsmpm_status zsmpm_closure_train(zsmpm_closure *c, int32_t epochs, int32_t batch, float lr, uint64_t seed,

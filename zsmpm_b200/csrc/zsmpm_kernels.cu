@@ -1291,14 +1291,60 @@ __device__ __forceinline__ principal_result plain_principal(const material_dev &
 
 // The learned constitutive update (committed ordering).  Warp-collective: every lane of the
 // warp calls it.  Inactive lanes compute on their copy and record nothing.
+//
+// The network replaces the return-mapping branch, i.e. the projection of a trial state that
+// lies outside the yield surface.  Which branch a trial state takes is decided exactly, by the
+// tests of the plain map: Drucker-Prager (compute_stress_sand) projects to the tip when
+// tr >= 0 and onto the cone when tr < 0 and dgamma > 0, and is elastic otherwise; snow clamps
+// the singular values that leave [1 - theta_c, 1 + theta_s].  Elastic states keep their strain
+// and the tip takes its closed form; the network gives the projected log strain of the cone
+// (snow: of the clamp), and the principal Kirchhoff stress follows from the projected state by
+// the model's own formula (Hencky for Drucker-Prager, hardened fixed corotated for snow), so the
+// stress is consistent with the strain the particle keeps.  The network runs for a warp only
+// when one of its lanes needs a projection.  One network-projected particle in
+// audit_period per substep is audited against the plain map (double accumulators); the
+// counters also record how many updates ran the network.
 __device__ __forceinline__ void learned_constitutive(const material_dev &mat, const closure_dev &cd,
                                                      const uint2 *frag, const float *bias, __nv_bfloat16 *xs,
                                                      float *ys, float *F, float &plastic, float *tau, bool active,
-                                                     int id, int substep) {
+                                                     int id, int substep, unsigned &net_updates,
+                                                     unsigned &all_updates) {
   float U[9], S[3], V[9];
   svd3<true>(F, U, S, V);
   float feat[6];
   closure_features(mat, S, plastic, feat);
+  // ---- the exact branch test
+  bool project = false;  // the network's branch
+  float H[3], pl_new = plastic;
+  if (mat.model == 1) {
+    float eps[3], eh[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) eps[i] = feat[i] - mat.cohesion;
+    const float sum_eps = eps[0] + eps[1] + eps[2];
+    const float tr = sum_eps + plastic;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) eh[i] = eps[i] - tr / 3.f;
+    const float ehn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2]);
+    const float smu = 2.f * mat.mu;
+    if (tr >= 0.f) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) H[i] = mat.cohesion;
+      if (mat.volume_correction) pl_new = mat.beta * sum_eps + plastic;
+    } else {
+      pl_new = 0.f;
+      const float dg = ehn + (3.f * mat.lambda + smu) / smu * tr * mat.yield_surface;
+      project = dg > 0.f;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) H[i] = feat[i];
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      project = project || S[i] < 1.f - mat.theta_c || S[i] > 1.f + mat.theta_s;
+      H[i] = feat[i];
+    }
+  }
+  // ---- the network, for the warps where a lane projects
   bool in_hull = true;
   float in[kMlpIn];
   net_scale ns;
@@ -1310,35 +1356,26 @@ __device__ __forceinline__ void learned_constitutive(const material_dev &mat, co
     in_hull = in_hull && feat[k] >= cd.in_min[k] && feat[k] <= cd.in_max[k];
     in[k] = (in[k] - cd.in_mean[k]) * cd.in_inv_std[k];
   }
-  float out[kMlpOut];
-  mlp_forward_warp(in, out, frag, bias, xs, ys);
+  const bool use_net = active && project && in_hull;
+  if (__any_sync(0xffffffffu, use_net)) {
+    float out[kMlpOut];
+    mlp_forward_warp(in, out, frag, bias, xs, ys);
 #pragma unroll
-  for (int k = 0; k < kMlpOut; ++k) out[k] *= cd.out_scale[k];
-  float y[6];
-  closure_from_net(ns, out, y);
-  float tp[3], Ns[3], pl_new;
+    for (int k = 0; k < kMlpOut; ++k) out[k] *= cd.out_scale[k];
+    float y[6];
+    closure_from_net(ns, out, y);
+    if (use_net)
 #pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    tp[i] = y[3 + i];
-    Ns[i] = expf(feat[i] + y[i]);
+      for (int i = 0; i < 3; ++i) H[i] = feat[i] + y[i];
   }
-  // the plastic state follows the branch the projection took, which the projected strain shows
+  float Ns[3], tp[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) Ns[i] = (mat.model == 1 || use_net) ? expf(H[i]) : S[i];
   if (mat.model == 1) {
-    const float sum_eps = feat[0] + feat[1] + feat[2] - 3.f * mat.cohesion;
-    const float tr = sum_eps + plastic;
-    pl_new = tr >= 0.f ? (mat.volume_correction ? mat.beta * sum_eps + plastic : plastic) : 0.f;
+    const float trl = H[0] + H[1] + H[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) tp[i] = 2.f * mat.mu * H[i] + mat.lambda * trl;
   } else {
-    // snow: the projection is the identity inside the elastic box [1 - theta_c, 1 + theta_s]^3
-    // (an exact test); outside it the network's projected strain is used.  The stress of the
-    // projected state follows from the hardened fixed-corotated formula: its magnitude spans the
-    // gravity-loaded state (1e-3 of the output range) to the yield surface, which the network's
-    // BF16 stress output resolves to only about 1e-3 of that range.
-    bool inside = true;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) inside = inside && S[i] >= 1.f - mat.theta_c && S[i] <= 1.f + mat.theta_s;
-    if (inside)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) Ns[i] = S[i];
     pl_new = plastic * (S[0] * S[1] * S[2] / fmaxf(Ns[0] * Ns[1] * Ns[2], 1e-6f));
     const float e = expf(mat.hardening * (1.f - pl_new));
     float Ph[3];
@@ -1346,9 +1383,11 @@ __device__ __forceinline__ void learned_constitutive(const material_dev &mat, co
 #pragma unroll
     for (int i = 0; i < 3; ++i) tp[i] = Ph[i] * Ns[i];
   }
-  const bool audit = active && cd.audit_period > 0 &&
+  // ---- audit of network projections, and the plain map outside the training hull
+  const bool audit = use_net && cd.audit_period > 0 &&
                      ((unsigned)id * 2654435761u + (unsigned)substep * 40503u) % (unsigned)cd.audit_period == 0u;
-  if (!in_hull || audit) {
+  const bool fallback = active && project && !in_hull;
+  if (audit || fallback) {
     const principal_result r = plain_principal(mat, S, feat, plastic);
     if (audit) {
       float d2 = 0.f, t2 = 0.f;
@@ -1367,16 +1406,19 @@ __device__ __forceinline__ void learned_constitutive(const material_dev &mat, co
       atomicAdd(&cd.audit[3], (double)d2);
       atomicAdd(&cd.audit[4], (double)t2);
     }
-    if (!in_hull) {
+    if (fallback) {
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         tp[i] = r.tau[i];
         Ns[i] = r.Ns[i];
       }
       pl_new = r.plastic;
-      if (active) atomicAdd(&cd.audit[5], 1.0);
+      atomicAdd(&cd.audit[5], 1.0);
     }
   }
+  // how many updates ran the network, of how many (counted per warp; k_g2p adds them up once)
+  net_updates += __popc(__ballot_sync(0xffffffffu, use_net));
+  all_updates += __popc(__ballot_sync(0xffffffffu, active));
   plastic = pl_new;
   const float d[3] = {tp[0] * mat.volume, tp[1] * mat.volume, tp[2] * mat.volume};
   mul_diag_t(tau, U, d, U);
@@ -1435,6 +1477,7 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
   float *const pf = g2p_smem + 4 * kHaloCells + (kLearned ? kG2PLearnedExtra / sizeof(float) : 0) +
                     warp * 2 * kG2PPrefetch;
   const size_t cap = (size_t)p.cap;
+  unsigned net_updates = 0, all_updates = 0;  // learned closure: updates that ran the network, all updates
   // the lane's particle of a batch into prefetch buffer `buf` (lanes past the block's end copy
   // the block's first particle)
   auto prefetch = [&](int buf, int i) {
@@ -1641,7 +1684,7 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
       // over the CTA (a block belongs to one scene), as the warp-collective MLP requires
       if (kLearned && (!kBatch || s_mat.model == s.aux.cd.model))
         learned_constitutive(kBatch ? s_mat : p.mat, s.aux.cd, sfrag, sbias, sxs + warp * 32 * 16,
-                             sys + warp * 32 * 8, Fn, pl, tau, active, id, substep);
+                             sys + warp * 32 * 8, Fn, pl, tau, active, id, substep, net_updates, all_updates);
       else if (kBatch)
         constitutive<true>(s_mat, Fn, pl, tau);
       else
@@ -1661,6 +1704,10 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
     }
     __syncthreads();
     if (threadIdx.x == 0) s.bmask[b] = s_moved;
+  }
+  if (kLearned && lane == 0 && all_updates) {
+    atomicAdd(&s.aux.cd.audit[6], (double)net_updates);
+    atomicAdd(&s.aux.cd.audit[7], (double)all_updates);
   }
 }
 
