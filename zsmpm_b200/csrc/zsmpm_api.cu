@@ -931,6 +931,25 @@ ZSMPM_API zsmpm_status zsmpm_scene_set_closure(zsmpm_scene *s, zsmpm_closure *c,
     s->audit = a;
     ZS_TRY(cudaMemset(s->audit, 0, sizeof(double) * 8), "memset audit");
   }
+  // the queue of projections for the network: one entry per particle of the capacity
+  if (s->uploaded && s->dev.aux.qcap < s->dev.prm.cap) {
+    const long long q = s->dev.prm.cap;
+    float *feat = nullptr, *outr = nullptr, *uvs = nullptr;
+    int2 *slots = nullptr;
+    int *ids = nullptr;
+    ZS_ALLOC(feat, 6 * q, "alloc closure queue");
+    ZS_ALLOC(outr, 6 * q, "alloc closure queue");
+    ZS_ALLOC(uvs, (size_t)kQueueFloats * q, "alloc closure queue");
+    ZS_ALLOC(slots, q, "alloc closure queue");
+    ZS_ALLOC(ids, q, "alloc closure queue");
+    s->dev.aux.q_feat = feat;
+    s->dev.aux.q_out = outr;
+    s->dev.aux.q_uvs = uvs;
+    s->dev.aux.q_slot = slots;
+    s->dev.aux.q_id = ids;
+    s->dev.aux.qcap = q;
+  }
+  if (s->dev.aux.qcap < 1) return fail(ZSMPM_ERR_NOT_READY, "attach the closure after the particles are uploaded");
   invalidate_graphs(s);
   cd.audit = s->audit;
   cd.audit_period = audit_period;
@@ -1135,7 +1154,7 @@ ZSMPM_API zsmpm_status zsmpm_autotune(zsmpm_scene *s, int32_t trials, zsmpm_tuni
   const int g2p_per_sm[6] = {1, 2, 3, 4, 5, 6};
   for (int a : g2p_threads)
     for (int b : g2p_per_sm) {
-      if (s->dev.aux.learned && (a != 256 || b > 2)) continue;  // learned G2P: 256 threads, <= 2 per SM
+      if (s->dev.aux.learned && a != 256) continue;  // the learned G2P runs 256-thread CTAs
       // beyond what stays resident: 256 threads hold 80 registers and 58 KB of shared memory
       // (3 CTAs per SM), 128 threads 43 KB (5)
       if ((a == 256 && b > 3) || (a == 128 && b > 5)) continue;

@@ -598,8 +598,11 @@ __device__ __forceinline__ void tc_hidden_epilogue(uint32_t tmem_row, const floa
   }
 }
 
+// n_dev (optional): the row count in device memory, at most n (the G2P queue of a substep)
 __global__ void __launch_bounds__(kTcRows) k_closure_infer_tc(closure_dev cd, const uint4 *wpack, const float *x,
-                                                              float *y, int64_t n, int *status) {
+                                                              float *y, int64_t n, const int *n_dev, int *status) {
+  if (n_dev) n = min(n, (int64_t)*n_dev);
+  if ((int64_t)blockIdx.x * kTcRows >= n) return;  // no tile for this CTA (before any allocation)
   extern __shared__ __align__(1024) unsigned char tsm[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t taddr_s;
@@ -767,7 +770,15 @@ namespace zsmpm {
 bool closure_device_view(const zsmpm_closure *c, closure_dev *out) {
   if (!c || !c->normalized) return false;
   *out = c->cd;
+  out->umma_w = c->umma_w;
+  out->tc_status = c->tc_status;
   return true;
+}
+
+cudaError_t launch_closure_rows(const closure_dev &cd, const float *x, float *y, const int *n_dev, long long cap,
+                                cudaStream_t st) {
+  k_closure_infer_tc<<<sms() * 6, kTcRows, kTcSmem, st>>>(cd, cd.umma_w, x, y, cap, n_dev, cd.tc_status);
+  return cudaGetLastError();
 }
 }  // namespace zsmpm
 
@@ -1025,7 +1036,7 @@ ZSMPM_API zsmpm_status zsmpm_closure_infer(zsmpm_closure *c, const float *x, flo
     // six resident CTAs per SM (37.7 KB of shared memory and 64 tensor-memory columns each), so
     // that six tiles' layer chains overlap on the SM's tensor core
     const int grid = (int)std::min<int64_t>(tiles, (int64_t)sms() * 6);
-    k_closure_infer_tc<<<grid, kTcRows, kTcSmem, st>>>(c->cd, c->umma_w, x, y, n, c->tc_status);
+    k_closure_infer_tc<<<grid, kTcRows, kTcSmem, st>>>(c->cd, c->umma_w, x, y, n, nullptr, c->tc_status);
   } else if (bf16) {
     const zsmpm_status ps = pack(c, st);
     if (ps != ZSMPM_OK) return ps;

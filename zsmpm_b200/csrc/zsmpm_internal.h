@@ -53,6 +53,7 @@ enum counter_slot : int {
   kCtrIncBin = 27,         // 1: this substep's binning merges the movers into the last binning's order
   kCtrBinInfo = 28,        // the last binning: -1 full, else the number of movers it merged
   kCtrDirty = 29,          // cells the incremental binning's movers arrived in (to be sorted by id)
+  kCtrQueue = 30,          // projections the last G2P queued for the closure's network
   kCtrCount = 32
 };
 enum work_slot : int {
@@ -94,10 +95,20 @@ struct scene_params {
   int bin_full;                     // 1: this binning launch recounts every particle
 };
 
+// floats of a queue entry: U 9, V 9, S 3, plastic state, m, C 9
+constexpr int kQueueFloats = 32;
+
 // G2P options beside the plain path: the learned closure and the trial-state log.
 struct g2p_aux {
-  int learned = 0;            // 1: G2P runs the closure's MLP in place of the return map
+  int learned = 0;            // 1: the closure's MLP replaces the return map's projection
   closure_dev cd{};           // its weights, normalisation, hull and audit accumulators
+  // the projections G2P hands to the network: raw features [qcap][6], network outputs
+  // [qcap][6], [qcap][kQueueFloats] U V S, the plastic state, m and C, (binned slot, scene)
+  // [qcap] and the upload index [qcap]
+  float *q_feat = nullptr, *q_out = nullptr, *q_uvs = nullptr;
+  int2 *q_slot = nullptr;
+  int *q_id = nullptr;
+  long long qcap = 0;
   float *log_buf = nullptr;   // [log_cap][6] raw closure features of sampled particles
   long long log_cap = 0;
   int log_period = 0;         // one particle in log_period per substep (0 = off)
@@ -206,6 +217,10 @@ cudaError_t launch_activate_static(scene_device &s, const float *x, int *keys_ou
                                    int *count_out, cudaStream_t st);
 // the device view of a closure that has a dataset or a loaded state (false otherwise)
 bool closure_device_view(const zsmpm_closure *c, closure_dev *out);
+// the network (tcgen05) over rows x[0, min(*n_dev, cap)) of raw features into y; fixed launch
+// shape, so that it can be captured in a CUDA graph
+cudaError_t launch_closure_rows(const closure_dev &cd, const float *x, float *y, const int *n_dev, long long cap,
+                                cudaStream_t st);
 // records the calling thread's error message (read back by zsmpm_last_error_string)
 int record_error(int status, const char *message);
 cudaError_t launch_svd_batch(const float *A, float *U, float *S, float *V, long long count,

@@ -465,6 +465,7 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
     s.ctr[kCtrWork + kWorkP2G] = 0;
     s.ctr[kCtrWork + kWorkG2P] = 0;
     s.ctr[kCtrDirty] = 0;
+    s.ctr[kCtrQueue] = 0;  // the next G2P queues its projections afresh
   }
   if (incremental_binning(s)) return;  // k_inc_stayers and k_inc_movers count this substep
   const int lane = threadIdx.x & 31;
@@ -1289,32 +1290,29 @@ __device__ __forceinline__ principal_result plain_principal(const material_dev &
   return snow_principal(mat.mu, mat.lambda, mat.hardening, mat.theta_c, mat.theta_s, S, plastic);
 }
 
-// The learned constitutive update (committed ordering).  Warp-collective: every lane of the
-// warp calls it.  Inactive lanes compute on their copy and record nothing.
+// The learned constitutive update (committed ordering), G2P's part.
 //
 // The network replaces the return-mapping branch, i.e. the projection of a trial state that
-// lies outside the yield surface.  Which branch a trial state takes is decided exactly, by the
-// tests of the plain map: Drucker-Prager (compute_stress_sand) projects to the tip when
+// lies outside the yield surface.  Which branch a trial state takes is decided here exactly,
+// by the tests of the plain map: Drucker-Prager (compute_stress_sand) projects to the tip when
 // tr >= 0 and onto the cone when tr < 0 and dgamma > 0, and is elastic otherwise; snow clamps
 // the singular values that leave [1 - theta_c, 1 + theta_s].  Elastic states keep their strain
-// and the tip takes its closed form; the network gives the projected log strain of the cone
-// (snow: of the clamp), and the principal Kirchhoff stress follows from the projected state by
-// the model's own formula (Hencky for Drucker-Prager, hardened fixed corotated for snow), so the
-// stress is consistent with the strain the particle keeps.  The network runs for a warp only
-// when one of its lanes needs a projection.  One network-projected particle in
-// audit_period per substep is audited against the plain map (double accumulators); the
-// counters also record how many updates ran the network.
-__device__ __forceinline__ void learned_constitutive(const material_dev &mat, const closure_dev &cd,
-                                                     const uint2 *frag, const float *bias, __nv_bfloat16 *xs,
-                                                     float *ys, float *F, float &plastic, float *tau, bool active,
-                                                     int id, int substep, unsigned &net_updates,
-                                                     unsigned &all_updates) {
+// and the tip takes its closed form, here.  A projection inside the network's training hull is
+// queued (raw features, U, V, S, the plastic state and the binned slot): after G2P the
+// tcgen05 kernel runs the network over the queue in 128-row tiles, and k_closure_finish forms
+// the projected state, its stress by the model's own formula (Hencky for Drucker-Prager,
+// hardened fixed corotated for snow) and writes F, the affine momentum and the plastic state.
+// Projections outside the hull, or beyond the queue's capacity, take the plain map here.
+// Returns true when the particle was queued (its F, A and plastic state are then not written
+// by G2P).
+__device__ __forceinline__ bool learned_update(const scene_device &s, const material_dev &mat, const closure_dev &cd,
+                                               float *F, float &plastic, float *tau, bool active, int slot, int sid,
+                                               int id, float m, const float *Cm, unsigned &all_updates) {
   float U[9], S[3], V[9];
   svd3<true>(F, U, S, V);
   float feat[6];
   closure_features(mat, S, plastic, feat);
-  // ---- the exact branch test
-  bool project = false;  // the network's branch
+  bool project = false;
   float H[3], pl_new = plastic;
   if (mat.model == 1) {
     float eps[3], eh[3];
@@ -1344,52 +1342,136 @@ __device__ __forceinline__ void learned_constitutive(const material_dev &mat, co
       H[i] = feat[i];
     }
   }
-  // ---- the network, for the warps where a lane projects
   bool in_hull = true;
-  float in[kMlpIn];
-  net_scale ns;
-  // the scale of the stress is the particle material's 3 lambda + 2 mu: the network works in
-  // units of it, so one network serves every scene of a batch that shares the closure's nu
-  closure_inputs(cd.model, 3.f * mat.lambda + 2.f * mat.mu, mat.hardening, feat, in, ns);
 #pragma unroll
-  for (int k = 0; k < kMlpIn; ++k) {
-    in_hull = in_hull && feat[k] >= cd.in_min[k] && feat[k] <= cd.in_max[k];
-    in[k] = (in[k] - cd.in_mean[k]) * cd.in_inv_std[k];
+  for (int k = 0; k < kMlpIn; ++k) in_hull = in_hull && feat[k] >= cd.in_min[k] && feat[k] <= cd.in_max[k];
+  bool queued = false;
+  const bool want = active && project && in_hull;
+  const unsigned wq = __ballot_sync(0xffffffffu, want);
+  all_updates += __popc(__ballot_sync(0xffffffffu, active));
+  if (wq) {
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == __ffs(wq) - 1) base = atomicAdd(&s.ctr[kCtrQueue], __popc(wq));
+    base = __shfl_sync(0xffffffffu, base, __ffs(wq) - 1);
+    if (want) {
+      const long long k = base + __popc(wq & lanemask_lt());
+      if (k < s.aux.qcap) {
+        float *fr = s.aux.q_feat + 6 * k;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) fr[i] = feat[i];
+        float *u = s.aux.q_uvs + kQueueFloats * k;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+          u[i] = U[i];
+          u[9 + i] = V[i];
+        }
+        u[18] = S[0];
+        u[19] = S[1];
+        u[20] = S[2];
+        u[21] = plastic;
+        // the particle's mass and C, for the affine momentum (so that the finish reads only the
+        // queue)
+        u[22] = m;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) u[23 + i] = Cm[i];
+        s.aux.q_slot[k] = make_int2(slot, sid);
+        s.aux.q_id[k] = id;
+        queued = true;
+      }
+    }
   }
-  const bool use_net = active && project && in_hull;
-  if (__any_sync(0xffffffffu, use_net)) {
-    float out[kMlpOut];
-    mlp_forward_warp(in, out, frag, bias, xs, ys);
-#pragma unroll
-    for (int k = 0; k < kMlpOut; ++k) out[k] *= cd.out_scale[k];
-    float y[6];
-    closure_from_net(ns, out, y);
-    if (use_net)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) H[i] = feat[i] + y[i];
-  }
+  if (queued) return true;
   float Ns[3], tp[3];
+  if (active && project) {
+    // outside the hull (or a full queue): the plain map
+    const principal_result r = plain_principal(mat, S, feat, plastic);
 #pragma unroll
-  for (int i = 0; i < 3; ++i) Ns[i] = (mat.model == 1 || use_net) ? expf(H[i]) : S[i];
-  if (mat.model == 1) {
+    for (int i = 0; i < 3; ++i) {
+      tp[i] = r.tau[i];
+      Ns[i] = r.Ns[i];
+    }
+    pl_new = r.plastic;
+    atomicAdd(&cd.audit[5], 1.0);
+  } else if (mat.model == 1) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) Ns[i] = expf(H[i]);
     const float trl = H[0] + H[1] + H[2];
 #pragma unroll
     for (int i = 0; i < 3; ++i) tp[i] = 2.f * mat.mu * H[i] + mat.lambda * trl;
   } else {
-    pl_new = plastic * (S[0] * S[1] * S[2] / fmaxf(Ns[0] * Ns[1] * Ns[2], 1e-6f));
-    const float e = expf(mat.hardening * (1.f - pl_new));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) Ns[i] = S[i];  // inside the clamp box: no projection, Jp unchanged
+    const float e = expf(mat.hardening * (1.f - plastic));
     float Ph[3];
     fc_principal(mat.mu * e, mat.lambda * e, Ns, Ph);
 #pragma unroll
     for (int i = 0; i < 3; ++i) tp[i] = Ph[i] * Ns[i];
   }
-  // ---- audit of network projections, and the plain map outside the training hull
-  const bool audit = use_net && cd.audit_period > 0 &&
-                     ((unsigned)id * 2654435761u + (unsigned)substep * 40503u) % (unsigned)cd.audit_period == 0u;
-  const bool fallback = active && project && !in_hull;
-  if (audit || fallback) {
-    const principal_result r = plain_principal(mat, S, feat, plastic);
-    if (audit) {
+  plastic = pl_new;
+  const float d[3] = {tp[0] * mat.volume, tp[1] * mat.volume, tp[2] * mat.volume};
+  mul_diag_t(tau, U, d, U);
+  mul_diag_t(F, U, Ns, V);
+  return false;
+}
+
+// The learned update's second part, for the projections the network has given (after the
+// tcgen05 pass over the queue): projected state, its stress, F, the affine momentum and the
+// plastic state written to the particle's binned slot; one projection in audit_period is
+// checked against the plain map (double accumulators).
+__global__ void __launch_bounds__(kThreads) k_closure_finish(scene_device s) {
+  const closure_dev &cd = s.aux.cd;
+  const int nq = (int)min((long long)s.ctr[kCtrQueue], s.aux.qcap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (nq > 0) atomicAdd(&cd.audit[6], (double)nq);
+    // a bounded tensor-core wait of the network pass that gave up is the scene's error too
+    if (cd.tc_status && *cd.tc_status) set_status(s.ctr, kStatusTimeout);
+  }
+  const int substep = s.ctr[kCtrSubstep];
+  const size_t cap = (size_t)s.prm.cap;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nq; k += grid_threads()) {
+    const int2 sl = s.aux.q_slot[k];
+    const int slot = sl.x;
+    const material_dev mat = s.prm.batch ? s.prm.mats[sl.y] : s.prm.mat;
+    const float *u = s.aux.q_uvs + kQueueFloats * (size_t)k;
+    float U[9], V[9], S[3], feat[6], y[6];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      U[i] = u[i];
+      V[i] = u[9 + i];
+    }
+    S[0] = u[18];
+    S[1] = u[19];
+    S[2] = u[20];
+    const float plastic = u[21];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      feat[i] = s.aux.q_feat[6 * (size_t)k + i];
+      y[i] = s.aux.q_out[6 * (size_t)k + i];
+    }
+    float H[3], Ns[3], tp[3], pl_new;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      H[i] = feat[i] + y[i];
+      Ns[i] = expf(H[i]);
+    }
+    if (mat.model == 1) {
+      pl_new = 0.f;  // the cone branch (tr < 0) resets logJp, as compute_stress_sand does
+      const float trl = H[0] + H[1] + H[2];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) tp[i] = 2.f * mat.mu * H[i] + mat.lambda * trl;
+    } else {
+      pl_new = plastic * (S[0] * S[1] * S[2] / fmaxf(Ns[0] * Ns[1] * Ns[2], 1e-6f));
+      const float e = expf(mat.hardening * (1.f - pl_new));
+      float Ph[3];
+      fc_principal(mat.mu * e, mat.lambda * e, Ns, Ph);
+#pragma unroll
+      for (int i = 0; i < 3; ++i) tp[i] = Ph[i] * Ns[i];
+    }
+    const int id = s.aux.q_id[k];
+    if (cd.audit_period > 0 &&
+        ((unsigned)id * 2654435761u + (unsigned)substep * 40503u) % (unsigned)cd.audit_period == 0u) {
+      const principal_result r = plain_principal(mat, S, feat, plastic);
       float d2 = 0.f, t2 = 0.f;
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
@@ -1406,38 +1488,27 @@ __device__ __forceinline__ void learned_constitutive(const material_dev &mat, co
       atomicAdd(&cd.audit[3], (double)d2);
       atomicAdd(&cd.audit[4], (double)t2);
     }
-    if (fallback) {
+    const float dd[3] = {tp[0] * mat.volume, tp[1] * mat.volume, tp[2] * mat.volume};
+    float tau[9], Fn[9];
+    mul_diag_t(tau, U, dd, U);
+    mul_diag_t(Fn, U, Ns, V);
+    const float m = u[22];
 #pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        tp[i] = r.tau[i];
-        Ns[i] = r.Ns[i];
-      }
-      pl_new = r.plastic;
-      atomicAdd(&cd.audit[5], 1.0);
+    for (int c = 0; c < 9; ++c) {
+      s.nxt.F[c * cap + slot] = Fn[c];
+      s.nxt.A[c * cap + slot] = m * u[23 + c] - s.prm.kappa * tau[c];
     }
+    if (s.nxt.plastic) s.nxt.plastic[slot] = pl_new;
   }
-  // how many updates ran the network, of how many (counted per warp; k_g2p adds them up once)
-  net_updates += __popc(__ballot_sync(0xffffffffu, use_net));
-  all_updates += __popc(__ballot_sync(0xffffffffu, active));
-  plastic = pl_new;
-  const float d[3] = {tp[0] * mat.volume, tp[1] * mat.volume, tp[2] * mat.volume};
-  mul_diag_t(tau, U, d, U);
-  mul_diag_t(F, U, Ns, V);
 }
 
 // Shared memory of k_g2p: the velocity halo, one float4 (vx, vy, vz, 0) per node so that a
-// node is one 16-byte load; for the learned variant the MLP's fragments, biases and per-warp
-// tiles; then per warp two prefetch buffers of 32 particles, each laid out as x|m float4[32],
-// F[9][32], plastic[32], id[32] (kG2PPrefetch floats).
+// node is one 16-byte load; then per warp two prefetch buffers of 32 particles, each laid out
+// as x|m float4[32], F[9][32], plastic[32], id[32] (kG2PPrefetch floats).
 constexpr int kG2PPrefetch = 4 * 32 + 9 * 32 + 32 + 32;
-constexpr size_t kG2PLearnedExtra = sizeof(uint2) * kFragTotal + sizeof(float) * kBiasTotal +
-                                    (kThreads / 32) * (32 * 16 * sizeof(__nv_bfloat16) + 32 * 8 * sizeof(float));
-static_assert(kG2PLearnedExtra % 16 == 0, "prefetch buffers start 16-byte aligned");
-constexpr size_t g2p_smem_bytes(bool learned, int nt) {
-  return sizeof(float4) * kHaloCells + (learned ? kG2PLearnedExtra : 0) +
-         sizeof(float) * 2 * kG2PPrefetch * (size_t)(nt / 32);
+constexpr size_t g2p_smem_bytes(int nt) {
+  return sizeof(float4) * kHaloCells + sizeof(float) * 2 * kG2PPrefetch * (size_t)(nt / 32);
 }
-constexpr size_t kG2PSmemLearned = g2p_smem_bytes(true, kThreads);
 
 // cp.async (sm_80 and later): copies that land in shared memory while the warp computes
 __device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
@@ -1451,14 +1522,14 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// kLearned: the closure's MLP replaces the return map (256 threads only); kBatch: batched
-// scenes (per-block scene material, scene-local block origin); NT threads per CTA.
-// The plain variants are register-capped for 3 (256 threads) or 5 (128 threads) resident CTAs
-// per SM: the kernel is issue- and latency-bound, and the extra warps hide more latency than
-// the cap costs (2.41 -> 2.09 ms on the 30 M-particle sand scene, no spills).  The learned
-// variant is capped for 2 (128 registers; at 1 CTA per SM it takes 6.2 ms instead of 4.8).
+// kLearned: the closure's network gives the return map's projections (queued for the tcgen05
+// pass, 256 threads only); kBatch: batched scenes (per-block scene material, scene-local block
+// origin); NT threads per CTA.  The variants are register-capped for 3 (256 threads) or 5 (128
+// threads) resident CTAs per SM: the kernel is issue- and latency-bound, and the extra warps
+// hide more latency than the cap costs (2.41 -> 2.09 ms on the 30 M-particle sand scene, no
+// spills).
 template <bool kLearned, bool kBatch, int NT>
-__global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(scene_device s) {
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
   static_assert(!kLearned || NT == kThreads, "learned G2P runs at 256 threads");
   extern __shared__ __align__(16) float g2p_smem[];
   float4 *svf = reinterpret_cast<float4 *>(g2p_smem);
@@ -1470,14 +1541,9 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
   const int substep = s.ctr[kCtrSubstep];
   if (blockIdx.x == 0 && threadIdx.x == 0) s.ctr[kCtrMaskFrom] = nb;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint2 *sfrag = reinterpret_cast<uint2 *>(g2p_smem + 4 * kHaloCells);
-  float *sbias = reinterpret_cast<float *>(sfrag + kFragTotal);
-  __nv_bfloat16 *sxs = reinterpret_cast<__nv_bfloat16 *>(sbias + kBiasTotal);
-  float *sys = reinterpret_cast<float *>(sxs + (kThreads / 32) * 32 * 16);
-  float *const pf = g2p_smem + 4 * kHaloCells + (kLearned ? kG2PLearnedExtra / sizeof(float) : 0) +
-                    warp * 2 * kG2PPrefetch;
+  float *const pf = g2p_smem + 4 * kHaloCells + warp * 2 * kG2PPrefetch;
   const size_t cap = (size_t)p.cap;
-  unsigned net_updates = 0, all_updates = 0;  // learned closure: updates that ran the network, all updates
+  unsigned all_updates = 0;  // learned closure: particle updates of this warp
   // the lane's particle of a batch into prefetch buffer `buf` (lanes past the block's end copy
   // the block's first particle)
   auto prefetch = [&](int buf, int i) {
@@ -1489,10 +1555,6 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
     cp_async4(b + 448 + lane, &s.cur.id[i]);
     cp_async_commit();
   };
-  if (kLearned) {
-    for (int i = threadIdx.x; i < kFragTotal; i += blockDim.x) sfrag[i] = s.aux.cd.frag[i];
-    for (int i = threadIdx.x; i < kBiasTotal; i += blockDim.x) sbias[i] = s.aux.cd.bias[i];
-  }
   for (;;) {
     const int w = grab_block(&s.ctr[kCtrWork + kWorkG2P], &s_b);
     if (w >= nb) break;
@@ -1680,11 +1742,13 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
           for (int q = 0; q < 6; ++q) s.aux.log_buf[6 * k + q] = feat[q];
       }
       float tau[9];
-      // in a batch the closure serves the scenes of its material model; the branch is uniform
-      // over the CTA (a block belongs to one scene), as the warp-collective MLP requires
+      // in a batch the closure serves the scenes of its material model (uniform over a CTA: a
+      // block belongs to one scene); a queued projection's F, A and plastic state are written
+      // by k_closure_finish
+      bool queued = false;
       if (kLearned && (!kBatch || s_mat.model == s.aux.cd.model))
-        learned_constitutive(kBatch ? s_mat : p.mat, s.aux.cd, sfrag, sbias, sxs + warp * 32 * 16,
-                             sys + warp * 32 * 8, Fn, pl, tau, active, id, substep, net_updates, all_updates);
+        queued = learned_update(s, kBatch ? s_mat : p.mat, s.aux.cd, Fn, pl, tau, active, slot, sid, id, xm.w, C,
+                                all_updates);
       else if (kBatch)
         constitutive<true>(s_mat, Fn, pl, tau);
       else
@@ -1693,22 +1757,22 @@ __global__ void __launch_bounds__(NT, kLearned ? 2 : (NT == 256 ? 3 : 5)) k_g2p(
       s.nxt.xm[slot] = xm;
       s.nxt.v[slot] = make_float4(vel[0], vel[1], vel[2], 0.f);
 #pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        s.nxt.C[k * cap + slot] = C[k];
-        s.nxt.A[k * cap + slot] = xm.w * C[k] - p.kappa * tau[k];
-        s.nxt.F[k * cap + slot] = Fn[k];
+      for (int k = 0; k < 9; ++k) s.nxt.C[k * cap + slot] = C[k];
+      if (!queued) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          s.nxt.A[k * cap + slot] = xm.w * C[k] - p.kappa * tau[k];
+          s.nxt.F[k * cap + slot] = Fn[k];
+        }
+        if (s.nxt.plastic) s.nxt.plastic[slot] = pl;
       }
-      if (s.nxt.plastic) s.nxt.plastic[slot] = pl;
       s.nxt.id[slot] = id;
       if (kBatch) s.nxt.sid[slot] = sid;
     }
     __syncthreads();
     if (threadIdx.x == 0) s.bmask[b] = s_moved;
   }
-  if (kLearned && lane == 0 && all_updates) {
-    atomicAdd(&s.aux.cd.audit[6], (double)net_updates);
-    atomicAdd(&s.aux.cd.audit[7], (double)all_updates);
-  }
+  if (kLearned && lane == 0 && all_updates) atomicAdd(&s.aux.cd.audit[7], (double)all_updates);
 }
 
 // ----------------------------------------------------------------- G2P2G and the implicit system
@@ -2483,22 +2547,22 @@ cudaError_t prepare_kernels() {
   e = cudaFuncSetAttribute(k_g2p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kG2P2GSmem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_g2p<true, true, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)kG2PSmemLearned);
+                           (int)g2p_smem_bytes(kThreads));
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_g2p<true, false, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)kG2PSmemLearned);
+                           (int)g2p_smem_bytes(kThreads));
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_g2p<false, true, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)g2p_smem_bytes(false, kThreads));
+                           (int)g2p_smem_bytes(kThreads));
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_g2p<false, false, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)g2p_smem_bytes(false, kThreads));
+                           (int)g2p_smem_bytes(kThreads));
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_g2p<false, true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)g2p_smem_bytes(false, 128));
+                           (int)g2p_smem_bytes(128));
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_g2p<false, false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)g2p_smem_bytes(false, 128));
+                              (int)g2p_smem_bytes(128));
 }
 
 cudaError_t launch_p2g(scene_device &s, cudaStream_t st) {
@@ -2514,19 +2578,27 @@ cudaError_t launch_grid_update(scene_device &s, cudaStream_t st) {
 }
 
 cudaError_t launch_g2p(scene_device &s, cudaStream_t st) {
-  const int per_sm = s.prm.g2p_ctas_per_sm > 0 ? s.prm.g2p_ctas_per_sm : (s.aux.learned ? 2 : 3);
+  const int per_sm = s.prm.g2p_ctas_per_sm > 0 ? s.prm.g2p_ctas_per_sm : 3;
   const int grid = num_sms() * per_sm;
   const bool small = s.prm.g2p_threads == 128;
-  if (s.aux.learned && s.prm.batch)
-    k_g2p<true, true, kThreads><<<grid, kThreads, kG2PSmemLearned, st>>>(s);
-  else if (s.aux.learned)
-    k_g2p<true, false, kThreads><<<grid, kThreads, kG2PSmemLearned, st>>>(s);
-  else if (s.prm.batch)
-    small ? k_g2p<false, true, 128><<<grid, 128, g2p_smem_bytes(false, 128), st>>>(s)
-          : k_g2p<false, true, kThreads><<<grid, kThreads, g2p_smem_bytes(false, kThreads), st>>>(s);
+  if (s.aux.learned) {
+    // G2P queues the projections, the network runs over the queue on the tensor cores, and
+    // k_closure_finish completes the queued particles
+    if (s.prm.batch)
+      k_g2p<true, true, kThreads><<<grid, kThreads, g2p_smem_bytes(kThreads), st>>>(s);
+    else
+      k_g2p<true, false, kThreads><<<grid, kThreads, g2p_smem_bytes(kThreads), st>>>(s);
+    cudaError_t e = launch_closure_rows(s.aux.cd, s.aux.q_feat, s.aux.q_out, &s.ctr[kCtrQueue], s.aux.qcap, st);
+    if (e != cudaSuccess) return e;
+    k_closure_finish<<<num_sms() * 4, kThreads, 0, st>>>(s);
+    return cudaGetLastError();
+  }
+  if (s.prm.batch)
+    small ? k_g2p<false, true, 128><<<grid, 128, g2p_smem_bytes(128), st>>>(s)
+          : k_g2p<false, true, kThreads><<<grid, kThreads, g2p_smem_bytes(kThreads), st>>>(s);
   else
-    small ? k_g2p<false, false, 128><<<grid, 128, g2p_smem_bytes(false, 128), st>>>(s)
-          : k_g2p<false, false, kThreads><<<grid, kThreads, g2p_smem_bytes(false, kThreads), st>>>(s);
+    small ? k_g2p<false, false, 128><<<grid, 128, g2p_smem_bytes(128), st>>>(s)
+          : k_g2p<false, false, kThreads><<<grid, kThreads, g2p_smem_bytes(kThreads), st>>>(s);
   return cudaGetLastError();
 }
 

@@ -43,7 +43,10 @@ struct closure_dev {
   float out_scale[kMlpOut];  // of the network targets (closure_net_targets)
   const uint2 *frag;         // kFragTotal BF16 weight fragments
   const float *bias;         // kBiasTotal
-  double *audit;             // [count, sum rel err, max rel err, sum |dtau|^2, sum |tau|^2, fallbacks]
+  const uint4 *umma_w;       // the weights in the tcgen05 shared-memory layout
+  int *tc_status;            // bounded-wait failures of the tcgen05 inference
+  double *audit;             // [audited, sum rel err, max rel err, sum |dtau|^2, sum |tau|^2, fallbacks,
+                             //  network updates, all updates]
 };
 
 // ---------------------------------------------------------------- principal return maps
