@@ -292,7 +292,9 @@ def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms
                          "cohesion": "Pa mapped to the log-strain shift c / (3 lambda + 2 mu)",
                          "epochs": sum(e for e, _, _ in schedule), "seconds": train_s,
                          "first_loss": float(losses[0]), "final_loss": float(losses[-1])},
-            "inference": "BF16 mma.sync m16n8k16, FP32 accumulation, fused in G2P",
+            "inference": ("exact branch test in G2P; projections inside the training hull queued and run "
+                          "through the network by tcgen05.mma (BF16 operands, FP32 accumulators in tensor "
+                          "memory, 128-row tiles), completed by a finish kernel"),
             "mlp_inference": mlp}
 
 
