@@ -13,6 +13,7 @@
 # No patch touches arithmetic:
 #   ZpcAsync.hpp                        _storage[i].data<T>()  -> .template data<T>()
 #   simulation/transfer/G2P.hpp         grid_block.pack<N>()   -> .template pack<N>()
+#   simulation/transfer/G2C2P.hpp       block.pack<N>()        -> .template pack<N>()
 #   simulation/grid/GridOp.hpp          block.pack<N>()        -> .template pack<N>()
 #   types/View.h                        dof_detail::T_t        -> dof_detail::template T_t;
 #                                       typename integral_constant<..> -> integral_constant<..>
@@ -39,6 +40,8 @@ sed -E 's/(grid_block|block)\.pack</\1.template pack</g' \
   "$REF/zensim/simulation/transfer/G2P.hpp" > "$OUT/patched/zensim/simulation/transfer/G2P.hpp"
 sed -E 's/(grid_block|block)\.pack</\1.template pack</g' \
   "$REF/zensim/simulation/grid/GridOp.hpp" > "$OUT/patched/zensim/simulation/grid/GridOp.hpp"
+sed -E 's/(grid_block|block)\.pack</\1.template pack</g' \
+  "$REF/zensim/simulation/transfer/G2C2P.hpp" > "$OUT/patched/zensim/simulation/transfer/G2C2P.hpp"
 mkdir -p "$OUT/patched/zensim/types"
 sed -E -e 's/= typename integral_constant</= integral_constant</' \
   -e 's/dof_detail::(value_t|T_t|size_t|index_t|counter_t|dim_t|extent_t)/dof_detail::template \1/g' \

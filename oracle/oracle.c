@@ -15,6 +15,7 @@
 #define R_SQRT oracle_ref_sqrtf
 #define R_STDSQRT sqrtf
 #define R_FLOOR floorf
+#define R_ABS fabsf
 #define OR_SVD oracle_svd_f32
 #include "oracle_sim.h"
 #undef R
@@ -24,6 +25,7 @@
 #undef R_SQRT
 #undef R_STDSQRT
 #undef R_FLOOR
+#undef R_ABS
 #undef OR_SVD
 
 #define R double
@@ -33,5 +35,6 @@
 #define R_SQRT sqrt
 #define R_STDSQRT sqrt
 #define R_FLOOR floor
+#define R_ABS fabs
 #define OR_SVD oracle_svd_f64
 #include "oracle_sim.h"

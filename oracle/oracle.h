@@ -27,6 +27,8 @@
  *                      math/VecInterface.hpp:1043-1049 (xlerp), ZpcMathUtils.hpp:1779-1781
  *   G2P                simulation/transfer/G2P.hpp:43-84, math/matrix/MatrixUtils.h:136-146
  *   G2P2G              simulation/transfer/G2P2G.hpp:49-142 (implicit force operator)
+ *   P2C2G / G2C2P      simulation/transfer/P2C2G.hpp:27-189, G2C2P.hpp:36-278 (cell-centric
+ *                      transfers), simulation/particle/Query.tpp:8-58 (index buckets)
  * Matrices are column-major (M(i,j) = M[3j+i]) as in the reference.
  */
 #ifndef ZSMPM_ORACLE_H
@@ -91,6 +93,18 @@ int oracle_run_f32(const oracle_params *p, int n, const float *m, float *x, floa
 int oracle_run_f64(const oracle_params *p, int n, const double *m, double *x, double *v,
                    double *C, double *F, double *plastic, int nsteps, int cap_blocks,
                    int *out_nblocks, int *out_keys, double *out_grid);
+
+/* oracle_run with the cell-centric transfer pair in place of P2G / G2P: P2C2GTransfer
+ * (simulation/transfer/P2C2G.hpp:27-189) over every active (block, cell), then after the grid
+ * update PreG2C2PTransfer, G2C2PTransfer and PostG2C2PTransfer (G2C2P.hpp:36-278), on the
+ * index buckets of simulation/particle/Query.tpp:8-58 with displacement 0.5.  Fixed corotated
+ * only (returns 6 for another model); C carries the pair's B attribute. */
+int oracle_run_cell_f32(const oracle_params *p, int n, const float *m, float *x, float *v, float *C,
+                        float *F, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
+                        float *out_grid);
+int oracle_run_cell_f64(const oracle_params *p, int n, const double *m, double *x, double *v, double *C,
+                        double *F, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
+                        double *out_grid);
 
 /* G2P2GTransfer, the implicit force operator (simulation/transfer/G2P2G.hpp:49-142): fout
  * (zeroed first) receives sum_p W (4/dx^2) (V0 P(F*) F*^T)(x_i - x_p), F* = (I + dt C(vin)) F,

@@ -3,8 +3,8 @@
  * reference's operand order (the FP32 instance is pinned bit-exactly against the compiled
  * reference under a sequential schedule); see oracle.h for the file:line list.
  *
- * Required macros: R (float or double), SFX, R_LOG/R_EXP/R_SQRT/R_FLOOR (logf/expf/sqrtf/
- * floorf or their double forms), OR_SVD (oracle_svd_f32 / oracle_svd_f64).
+ * Required macros: R (float or double), SFX, R_LOG/R_EXP/R_SQRT/R_FLOOR/R_ABS (logf/expf/
+ * sqrtf/floorf/fabsf or their double forms), OR_SVD (oracle_svd_f32 / oracle_svd_f64).
  */
 #define OR_CAT2(a, b) a##b
 #define OR_CAT(a, b) OR_CAT2(a, b)
@@ -697,6 +697,302 @@ int OR_NAME(oracle_g2p2g)(const oracle_params *p, int n, const R *x, const R *F,
             fi[d] += W * (contrib[d] * xixp[0] + contrib[3 + d] * xixp[1] + contrib[6 + d] * xixp[2]);
         }
   }
+  oracle_table_free(&t);
+  return status;
+}
+
+
+/* ---- the cell-centric transfer pair: P2C2GTransfer (simulation/transfer/P2C2G.hpp:27-189)
+ * and G2C2PTransfer with PreG2C2PTransfer / PostG2C2PTransfer (G2C2P.hpp:36-278), the
+ * fixed-corotated branch, on the index buckets of simulation/particle/Query.tpp:8-58 (one
+ * bucket per cell coordinate floor(x / dx + 0.5), particles in index order within a bucket,
+ * as a sequential SpatiallyDistribute leaves them).  Cells run in block-index then cell order
+ * and particles within a bucket in index order, the sequential schedule of the compiled
+ * reference; the atomics of the reference are plain additions in that order. */
+typedef struct {
+  uint64_t key;
+  int32_t idx;
+} OR_NAME(bucket_entry);
+
+static int OR_NAME(bucket_cmp)(const void *a, const void *b) {
+  const OR_NAME(bucket_entry) *x = (const OR_NAME(bucket_entry) *)a, *y = (const OR_NAME(bucket_entry) *)b;
+  if (x->key != y->key) return x->key < y->key ? -1 : 1;
+  return x->idx < y->idx ? -1 : (x->idx > y->idx);
+}
+
+static uint64_t OR_NAME(bucket_key)(int32_t bx, int32_t by, int32_t bz) {
+  const uint64_t bias = (uint64_t)1 << 20;
+  return (((uint64_t)(bx + (int64_t)bias)) << 42) | (((uint64_t)(by + (int64_t)bias)) << 21) |
+         (uint64_t)(bz + (int64_t)bias);
+}
+
+/* [*first, *last) of the entries of bucket (bx, by, bz) */
+static void OR_NAME(bucket_range)(const OR_NAME(bucket_entry) * e, int n, int32_t bx, int32_t by, int32_t bz,
+                                  int *first, int *last) {
+  const uint64_t k = OR_NAME(bucket_key)(bx, by, bz);
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) / 2;
+    if (e[mid].key < k) lo = mid + 1;
+    else hi = mid;
+  }
+  *first = lo;
+  while (lo < n && e[lo].key == k) ++lo;
+  *last = lo;
+}
+
+/* Dinv of a position component (P2C2G.hpp:87-91, G2C2P.hpp PostG2C2PTransfer): the offset from
+ * the nearest node, then 2 / (dx^2 - 2 offset^2) */
+static R OR_NAME(cell_dinv)(R pos, R dx, R dx_inv) {
+  R X = pos - (R)(int32_t)R_FLOOR(pos * dx_inv + (R)0.5) * dx;
+  return (R)2 / (dx * dx - (R)2 * X * X);
+}
+
+int OR_NAME(oracle_run_cell)(const oracle_params *p, int n, const R *m, R *x, R *v, R *C, R *F, int nsteps,
+                             int cap_blocks, int *out_nblocks, int *out_keys, R *out_grid) {
+  OR_NAME(cfg) cfg;
+  OR_NAME(make_cfg)(p, &cfg);
+  if (cfg.model != ORACLE_FC) return 6;
+  const R dx = cfg.dx, dt = cfg.dt;
+  const R dx_inv = (R)1 / dx;
+  oracle_table t;
+  if (oracle_table_init(&t, p->table_expected)) return 3;
+  R *grid = NULL;
+  size_t grid_blocks = 0;
+  int status = 0;
+  OR_NAME(bucket_entry) *bk = (OR_NAME(bucket_entry) *)malloc(sizeof(*bk) * (size_t)(n > 0 ? n : 1));
+  R *contrib = (R *)malloc(sizeof(R) * 9 * (size_t)(n > 0 ? n : 1));
+  for (int step = 0; step != nsteps && !status; ++step) {
+    /* activation (SparsityOp.hpp:58-112) and canonical order, as in oracle_run */
+    oracle_table_clear(&t);
+    for (int i = 0; i != n && !status; ++i) {
+      int32_t b[3];
+      if (OR_NAME(block_of)(&x[3 * i], dx_inv, b)) status = 4;
+      else if (oracle_table_insert(&t, b, -1) < 0) status = 2;
+    }
+    const int npb = t.count;
+    for (int i = 0; i != npb && !status; ++i) {
+      int32_t k[3] = {t.active[3 * i], t.active[3 * i + 1], t.active[3 * i + 2]};
+      for (int a = 0; a != 2; ++a)
+        for (int b = 0; b != 2; ++b)
+          for (int c = 0; c != 2; ++c) {
+            int32_t nk[3] = {k[0] + a, k[1] + b, k[2] + c};
+            if (oracle_table_insert(&t, nk, -1) < 0) status = 2;
+          }
+    }
+    if (status) break;
+    if (t.count >= t.size - 20) {
+      status = 2;
+      break;
+    }
+    oracle_table_canonicalize(&t);
+    const int nb = t.count;
+    if ((size_t)nb > grid_blocks) {
+      free(grid);
+      grid_blocks = (size_t)nb;
+      grid = (R *)malloc(sizeof(R) * 4 * 512 * grid_blocks);
+    }
+    memset(grid, 0, sizeof(R) * 4 * 512 * (size_t)nb);
+
+    /* index buckets (Query.tpp:20-56, ComputeSparsity with blockLen 1, displacement 0.5) */
+    for (int i = 0; i != n; ++i) {
+      int32_t c[3];
+      for (int d = 0; d != 3; ++d) c[d] = (int32_t)R_FLOOR(x[3 * i + d] * dx_inv + (R)0.5);
+      bk[i].key = OR_NAME(bucket_key)(c[0], c[1], c[2]);
+      bk[i].idx = i;
+    }
+    qsort(bk, (size_t)n, sizeof(*bk), OR_NAME(bucket_cmp));
+
+    /* the per-particle part of P2C2G (P2C2G.hpp:87-146): contrib = (m B - dt V0 P F^T) Dinv,
+     * columns scaled; a function of the particle alone, evaluated once per particle */
+    for (int i = 0; i != n; ++i) {
+      R Dinv[3], Cs[9], PF[9];
+      for (int d = 0; d != 3; ++d) Dinv[d] = OR_NAME(cell_dinv)(x[3 * i + d], dx, dx_inv);
+      for (int d = 0; d != 9; ++d) Cs[d] = C[9 * i + d] * Dinv[d / 3];
+      OR_NAME(stress_fc)(cfg.volume, cfg.mu, cfg.lam, &F[9 * i], PF);
+      for (int d = 0; d != 9; ++d) PF[d] = PF[d] * (Dinv[d / 3] * -dt);
+      for (int d = 0; d != 9; ++d) contrib[9 * i + d] = PF[d] + Cs[d] * m[i];
+    }
+
+    /* P2C2G over every (block, cell): stage 1 gathers the particles within dx of the cell's
+     * center (tent weights), stage 2 adds the cell's sums to its 8 corner nodes (1/8 each) */
+    for (int b = 0; b != nb; ++b) {
+      const int32_t *key = &t.active[3 * b];
+      for (int cell = 0; cell != 512; ++cell) {
+        const int32_t coord[3] = {key[0] * 8 + (cell >> 6), key[1] * 8 + ((cell >> 3) & 7), key[2] * 8 + (cell & 7)};
+        R posc[3];
+        for (int d = 0; d != 3; ++d) posc[d] = ((R)coord[d] + (R)0.5) * dx;
+        R m_c = 0, mv_c[3] = {0, 0, 0}, QD[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, QDX[3] = {0, 0, 0};
+        for (int a = 0; a != 3; ++a)
+          for (int bb = 0; bb != 3; ++bb)
+            for (int c = 0; c != 3; ++c) {
+              int first, last;
+              OR_NAME(bucket_range)(bk, n, coord[0] - 1 + a, coord[1] - 1 + bb, coord[2] - 1 + c, &first, &last);
+              for (int e = first; e != last; ++e) {
+                const int i = bk[e].idx;
+                const R *posp = &x[3 * i];
+                int in = 1;
+                for (int d = 0; d != 3; ++d)
+                  if (R_ABS(posp[d] - posc[d]) > dx) in = 0;
+                if (!in) continue;
+                const R *q = &contrib[9 * i];
+                R Wpc = 1;
+                for (int d = 0; d != 3; ++d) Wpc *= ((R)1 - R_ABS((posc[d] - posp[d]) * dx_inv));
+                m_c += m[i] * Wpc;
+                for (int d = 0; d != 3; ++d) {
+                  mv_c[d] += m[i] * v[3 * i + d] * Wpc;
+                  QDX[d] += (q[d] * posp[0] + q[3 + d] * posp[1] + q[6 + d] * posp[2]) * Wpc;
+                }
+                for (int d = 0; d != 9; ++d) QD[d] += q[d] * Wpc;
+              }
+            }
+        for (int a = 0; a != 2; ++a)
+          for (int bb = 0; bb != 2; ++bb)
+            for (int c = 0; c != 2; ++c) {
+              const int32_t ci[3] = {coord[0] + a, coord[1] + bb, coord[2] + c};
+              int32_t loc[3], bkey[3];
+              R posi[3];
+              for (int d = 0; d != 3; ++d) {
+                loc[d] = ci[d] & 7;
+                bkey[d] = (ci[d] - loc[d]) / 8;
+                posi[d] = (R)ci[d] * dx;
+              }
+              const int32_t blk = oracle_table_query(&t, bkey);
+              if (blk < 0) continue;
+              const R Wci = (R)0.125;
+              const int nc = (loc[0] << 6) | (loc[1] << 3) | loc[2];
+              R *g = &grid[(size_t)blk * 4 * 512];
+              g[nc] += m_c * Wci;
+              for (int d = 0; d != 3; ++d)
+                g[(1 + d) * 512 + nc] +=
+                    (mv_c[d] + ((QD[d] * posi[0] + QD[3 + d] * posi[1] + QD[6 + d] * posi[2]) - QDX[d])) * Wci;
+            }
+      }
+    }
+
+    /* grid velocity and walls, as in oracle_run (the restated rhs channel is zero here) */
+    const R lo = (R)cfg.wall_cells * dx, hi = (R)1 - (R)cfg.wall_cells * dx;
+    for (int b = 0; b != nb; ++b) {
+      R *g = &grid[(size_t)b * 4 * 512];
+      const int32_t *key = &t.active[3 * b];
+      for (int cell = 0; cell != 512; ++cell) {
+        R mass = g[cell];
+        if (mass != 0) {
+          mass = (R)1 / mass;
+          R vel[3];
+          for (int d = 0; d != 3; ++d) vel[d] = (g[(1 + d) * 512 + cell] + (R)0) * mass + cfg.g[d] * dt;
+          for (int d = 0; d != 3; ++d) g[(1 + d) * 512 + cell] = vel[d];
+        }
+      }
+      if (cfg.wall_type == ORACLE_WALL_NONE) continue;
+      for (int w = 0; w != 6; ++w) {
+        const int axis = w / 2;
+        const R sgn = (w & 1) ? (R)-1 : (R)1;
+        const R origin = (w & 1) ? hi : lo;
+        for (int cell = 0; cell != 512; ++cell) {
+          if (!(g[cell] > 0)) continue;
+          const int cc[3] = {cell >> 6, (cell >> 3) & 7, cell & 7};
+          R pos = ((R)key[axis] * (R)8 + (R)cc[axis]) * dx;
+          R sd = sgn * (pos - origin);
+          if (!(sd < 0)) continue;
+          if (cfg.wall_type == ORACLE_WALL_STICKY) {
+            for (int d = 0; d != 3; ++d) g[(1 + d) * 512 + cell] = 0;
+          } else {
+            R proj = sgn * g[(1 + axis) * 512 + cell];
+            if (cfg.wall_type == ORACLE_WALL_SLIP || proj < 0)
+              g[(1 + axis) * 512 + cell] = g[(1 + axis) * 512 + cell] - proj * sgn;
+          }
+        }
+      }
+    }
+
+    /* PreG2C2PTransfer, then G2C2PTransfer over every (block, cell): the cell's mean corner
+     * velocity and its moment, added to the particles within dx of the center */
+    R *B = C;
+    for (int i = 0; i != n; ++i) {
+      for (int d = 0; d != 3; ++d) v[3 * i + d] = 0;
+      for (int d = 0; d != 9; ++d) B[9 * i + d] = 0;
+    }
+    for (int b = 0; b != nb; ++b) {
+      const int32_t *key = &t.active[3 * b];
+      for (int cell = 0; cell != 512; ++cell) {
+        const int32_t coord[3] = {key[0] * 8 + (cell >> 6), key[1] * 8 + ((cell >> 3) & 7), key[2] * 8 + (cell & 7)};
+        R v_c[3] = {0, 0, 0}, vx_c[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int a = 0; a != 2; ++a)
+          for (int bb = 0; bb != 2; ++bb)
+            for (int c = 0; c != 2; ++c) {
+              const int32_t ci[3] = {coord[0] + a, coord[1] + bb, coord[2] + c};
+              int32_t loc[3], bkey[3];
+              R posi[3];
+              for (int d = 0; d != 3; ++d) {
+                loc[d] = ci[d] & 7;
+                bkey[d] = (ci[d] - loc[d]) / 8;
+                posi[d] = (R)ci[d] * dx;
+              }
+              const int32_t blk = oracle_table_query(&t, bkey);
+              if (blk < 0) continue;
+              const R W = (R)0.125;
+              const int nc = (loc[0] << 6) | (loc[1] << 3) | loc[2];
+              const R *g = &grid[(size_t)blk * 4 * 512];
+              const R vi[3] = {g[1 * 512 + nc], g[2 * 512 + nc], g[3 * 512 + nc]};
+              for (int d = 0; d != 3; ++d) v_c[d] += vi[d] * W;
+              for (int d = 0; d != 9; ++d) vx_c[d] += W * vi[d % 3] * posi[d / 3];
+            }
+        R posc[3];
+        for (int d = 0; d != 3; ++d) posc[d] = ((R)coord[d] + (R)0.5) * dx;
+        for (int a = 0; a != 3; ++a)
+          for (int bb = 0; bb != 3; ++bb)
+            for (int c = 0; c != 3; ++c) {
+              int first, last;
+              OR_NAME(bucket_range)(bk, n, coord[0] - 1 + a, coord[1] - 1 + bb, coord[2] - 1 + c, &first, &last);
+              for (int e = first; e != last; ++e) {
+                const int i = bk[e].idx;
+                const R *posp = &x[3 * i];
+                int in = 1;
+                for (int d = 0; d != 3; ++d)
+                  if (R_ABS(posp[d] - posc[d]) > dx) in = 0;
+                if (!in) continue;
+                R W = 1;
+                for (int d = 0; d != 3; ++d) {
+                  const R xabs = R_ABS((posc[d] - posp[d]) * dx_inv);
+                  if (xabs <= (R)1) W *= ((R)1 - xabs);
+                  else W *= (R)0;
+                }
+                for (int d = 0; d != 3; ++d) v[3 * i + d] += v_c[d] * W;
+                for (int d = 0; d != 9; ++d) B[9 * i + d] += W * (vx_c[d] - v_c[d % 3] * posp[d / 3]);
+              }
+            }
+      }
+    }
+    /* PostG2C2PTransfer: F <- (I + dt B Dinv) F, x += v dt; B stays in C */
+    for (int i = 0; i != n; ++i) {
+      R *xp = &x[3 * i], *Fp = &F[9 * i];
+      R Dinv[3], Cs[9], tmp[9], Fn[9];
+      for (int d = 0; d != 3; ++d) Dinv[d] = OR_NAME(cell_dinv)(xp[d], dx, dx_inv);
+      for (int d = 0; d != 9; ++d) Cs[d] = B[9 * i + d] * Dinv[d / 3];
+      for (int d = 0; d != 9; ++d) tmp[d] = Cs[d] * dt + ((d & 0x3) ? (R)0 : (R)1);
+      for (int c = 0; c != 3; ++c)
+        for (int r = 0; r != 3; ++r)
+          Fn[3 * c + r] = tmp[r] * Fp[3 * c] + tmp[3 + r] * Fp[3 * c + 1] + tmp[6 + r] * Fp[3 * c + 2];
+      for (int d = 0; d != 9; ++d) Fp[d] = Fn[d];
+      for (int d = 0; d != 3; ++d) xp[d] += v[3 * i + d] * dt;
+    }
+  }
+  if (!status) {
+    const int nb = t.count;
+    if (out_nblocks) *out_nblocks = nb;
+    if (out_keys) {
+      if (nb > cap_blocks) status = 1;
+      else
+        for (int b = 0; b != nb; ++b) {
+          for (int d = 0; d != 3; ++d) out_keys[3 * b + d] = t.active[3 * b + d];
+          memcpy(&out_grid[(size_t)b * 4 * 512], &grid[(size_t)b * 4 * 512], sizeof(R) * 4 * 512);
+        }
+    }
+  }
+  free(grid);
+  free(bk);
+  free(contrib);
   oracle_table_free(&t);
   return status;
 }

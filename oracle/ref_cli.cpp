@@ -28,6 +28,8 @@
 //                int32 nblocks, type, f32 background, sinv[9], rinv[9], t[3],
 //                int32 keys[3*nblocks], f32 sdf[512*nblocks]
 //     reply:     as 1
+//  10 run with the cell-centric transfers (P2C2G / G2C2P): as 1
+//     reply:     as 1 (logJp unchanged)
 //   7 implicit:  zsref_params, int32 op, n, nb, max_iters, f32 tol, rel_tol,
 //                f32 m[n], x[3n], v[3n], C[9n], F[9n], logJp[n], int32 keys[3*nb],
 //                f32 a[1536*nb], b[1536*nb]
@@ -52,6 +54,9 @@ int zsref_run_colliders(const zsref_params *p, int n, float *m, float *x, float 
                         float *logJp, int nsteps, int cap_blocks, int *out_nblocks, int *out_keys,
                         float *out_grid, double *out_seconds, int ncolliders, const void *colliders,
                         int nlevelsets, const void *levelsets);
+int zsref_run_cell(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
+                   int nsteps, int cap_blocks, int *out_nblocks, int *out_keys, float *out_grid,
+                   double *out_seconds);
 // the driver's ref_levelset record
 struct ref_levelset_rec {
   int nblocks, type;
@@ -109,7 +114,7 @@ int main(int argc, char **argv) {
   out_f = std::fopen(argv[2], "wb");
   if (!in_f || !out_f) return 2;
   const int cmd = rd<int32_t>();
-  if (cmd == 1 || cmd == 8 || cmd == 9) {
+  if (cmd == 1 || cmd == 8 || cmd == 9 || cmd == 10) {
     auto p = rd<zsref_params>();
     const int n = rd<int32_t>(), nsteps = rd<int32_t>(), cap = rd<int32_t>();
     std::vector<float> m, x, v, C, F, lj;
@@ -152,9 +157,11 @@ int main(int argc, char **argv) {
     std::vector<float> grid((size_t)cap * 4 * 512);
     int nb = 0;
     double secs = 0;
-    int st = zsref_run_colliders(&p, n, m.data(), x.data(), v.data(), C.data(), F.data(), lj.data(),
-                                 nsteps, cap, &nb, cap ? keys.data() : nullptr,
-                                 cap ? grid.data() : nullptr, &secs, ncol, cols.data(), nls, lss.data());
+    int st = cmd == 10 ? zsref_run_cell(&p, n, m.data(), x.data(), v.data(), C.data(), F.data(), nsteps, cap,
+                                        &nb, cap ? keys.data() : nullptr, cap ? grid.data() : nullptr, &secs)
+                       : zsref_run_colliders(&p, n, m.data(), x.data(), v.data(), C.data(), F.data(), lj.data(),
+                                             nsteps, cap, &nb, cap ? keys.data() : nullptr,
+                                             cap ? grid.data() : nullptr, &secs, ncol, cols.data(), nls, lss.data());
     wr<int32_t>(st);
     wr<int32_t>(nb);
     wr<double>(secs);

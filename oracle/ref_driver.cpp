@@ -19,6 +19,7 @@
 //   5. ApplyBoundaryConditionOnGridBlocks with six analytic planes (GridOp.hpp:113-164,
 //      geometry/Collider.h:80-110, geometry/AnalyticLevelSet.h:11-43)
 //   6. G2PTransfer (simulation/transfer/G2P.hpp:43-84)
+// zsref_run_cell composes the cell-centric transfer pair instead of P2G / G2P (below).
 // zsref_g2p2g drives the implicit-force operator G2P2GTransfer
 // (simulation/transfer/G2P2G.hpp:49-142) over a caller-given grid velocity field, and
 // zsref_implicit the implicit system's operators and its conjugate-gradient solve
@@ -39,6 +40,9 @@
 #include "zensim/simulation/transfer/P2G.hpp"
 #include "zensim/simulation/transfer/G2P.hpp"
 #include "zensim/simulation/transfer/G2P2G.hpp"
+#include "zensim/simulation/transfer/P2C2G.hpp"
+#include "zensim/simulation/transfer/G2C2P.hpp"
+#include "zensim/container/IndexBuckets.hpp"
 #include "zensim/simulation/mpm/ImplicitMPM.hpp"
 #include "zensim/math/linear/ConjugateGradient.hpp"
 #include "zensim/geometry/SparseLevelSet.hpp"
@@ -381,6 +385,139 @@ int zsref_run_colliders(const zsref_params *p, int n, float *m, float *x, float 
   std::memcpy(F, (float *)pars.getAttrAddress("F"), sizeof(float) * 9 * n);
   std::memcpy(logJp, (float *)pars.getAttrAddress("logJp"), sizeof(float) * n);
 
+  const int nb = table.size();
+  if (out_nblocks) *out_nblocks = nb;
+  if (out_keys) {
+    if (nb > cap_blocks) return 1;
+    auto tv = proxy<host>(grids);
+    for (int b = 0; b != nb; ++b) {
+      auto key = table._activeKeys[b];
+      for (int d = 0; d != 3; ++d) out_keys[b * 3 + d] = key[d];
+      auto block = tv[b];
+      for (int c = 0; c != 4; ++c)
+        for (int cell = 0; cell != 512; ++cell)
+          out_grid[((size_t)b * 4 + c) * 512 + cell] = block(c, cell);
+    }
+  }
+  return 0;
+}
+
+// The cell-centric transfer pair the reference ships without a caller, P2C2GTransfer
+// (simulation/transfer/P2C2G.hpp:27-189) and G2C2PTransfer with PreG2C2PTransfer and
+// PostG2C2PTransfer (simulation/transfer/G2C2P.hpp:36-278), composed into nsteps substeps:
+//   1. the activation of zsref_run, in canonical order;
+//   2. the particles' index buckets, built as index_buckets_for_particles does
+//      (simulation/particle/Query.tpp:8-58): one bucket per cell coordinate
+//      floor(x / dx + 0.5), the collocated offset of IndexBucketsView::bucketCoord;
+//   3. CleanGridBlocks, then P2C2GTransfer over every active (block, cell);
+//   4. the grid velocity and the walls of zsref_run;
+//   5. PreG2C2PTransfer over the particles, G2C2PTransfer over every (block, cell), then
+//      PostG2C2PTransfer over the particles.
+// Fixed corotated only (p->model == 0; returns 4 otherwise): P2C2G's Drucker-Prager branch
+// writes logJp once per visiting cell.  C carries the pair's B attribute between substeps.
+// Returns as zsref_run.
+int zsref_run_cell(const zsref_params *p, int n, float *m, float *x, float *v, float *C, float *F,
+                   int nsteps, int cap_blocks, int *out_nblocks, int *out_keys, float *out_grid,
+                   double *out_seconds) {
+  if (p->model != 0 || p->order != 1) return 4;
+  constexpr auto host = execspace_e::host;
+  constexpr auto omp = execspace_e::openmp;
+  particles_t pars{(size_t)n, memsrc_e::host, -1};
+  pars.addAttr("m", attrib_e::scalar);
+  pars.addAttr("v", attrib_e::vector);
+  pars.addAttr("C", attrib_e::matrix);
+  pars.addAttr("F", attrib_e::matrix);
+  pars.addAttr("logJp", attrib_e::scalar);
+  std::memcpy((float *)pars.getAttrAddress("m"), m, sizeof(float) * n);
+  std::memcpy((float *)pars.getAttrAddress("x"), x, sizeof(float) * 3 * n);
+  std::memcpy((float *)pars.getAttrAddress("v"), v, sizeof(float) * 3 * n);
+  std::memcpy((float *)pars.getAttrAddress("C"), C, sizeof(float) * 9 * n);
+  std::memcpy((float *)pars.getAttrAddress("F"), F, sizeof(float) * 9 * n);
+  std::memset((float *)pars.getAttrAddress("logJp"), 0, sizeof(float) * n);
+
+  table_t table{(size_t)std::max(p->table_expected, 1), memsrc_e::host, -1};
+  grids_t grids{{{"m", 1}, {"v", 3}, {"rhs", 3}}, p->dx, (size_t)table._tableSize,
+                memsrc_e::host, -1};
+  FixedCorotatedConfig fc{};
+  fc.E = p->E;
+  fc.nu = p->nu;
+  fc.volume = p->volume;
+  std::vector<Collider<plane_t>> walls;
+  {
+    const float lo = p->wall_cells * p->dx, hi = 1.f - p->wall_cells * p->dx;
+    collider_e ct = p->wall_type == 0 ? collider_e::Sticky
+                    : p->wall_type == 1 ? collider_e::Slip
+                                        : collider_e::Separate;
+    for (int d = 0; d != 3; ++d) {
+      vec<float, 3> o{0.f, 0.f, 0.f}, nrm{0.f, 0.f, 0.f};
+      o[d] = lo;
+      nrm[d] = 1.f;
+      walls.emplace_back(plane_t{o, nrm}, ct);
+      o[d] = hi;
+      nrm[d] = -1.f;
+      walls.emplace_back(plane_t{o, nrm}, ct);
+    }
+  }
+  const vec<float, 3> grav{p->gx, p->gy, p->gz};
+  using buckets_t = IndexBuckets<3, i32, i32>;
+  using bvec_t = typename buckets_t::vector_t;
+  int status = 0;
+
+  auto run = [&](auto pol, auto tag) {
+    constexpr auto space = decltype(tag)::value;
+    auto t0 = std::chrono::steady_clock::now();
+    for (int step = 0; step != nsteps; ++step) {
+      const int nb = activate_canonical(pol, wrapv<space>{}, table, pars, p->dx);
+      if (nb < 0) {
+        status = 2;
+        return;
+      }
+      // index buckets (Query.tpp:20-56, displacement 0.5)
+      buckets_t ib{};
+      ib._dx = p->dx;
+      ib._table = typename buckets_t::table_t{pars.get_allocator(), pars.size()};
+      auto &bt = ib._table;
+      pol(range(bt._tableSize), CleanSparsity{wrapv<space>{}, bt});
+      pol(range(pars.size()), ComputeSparsity{wrapv<space>{}, p->dx, 1, bt, pars.attrVector("x"), 0, 0.5f});
+      const size_t ncells = (size_t)bt.size() + 1;
+      ib._counts = bvec_t{pars.get_allocator(), ncells};
+      std::memset(ib._counts.data(), 0, sizeof(i32) * ncells);
+      auto tmp = ib._counts;
+      pol(range(pars.size()),
+          SpatiallyCount{wrapv<space>{}, p->dx, bt, pars.attrVector("x"), ib._counts, 1, 0, 0.5f});
+      ib._offsets = bvec_t{pars.get_allocator(), ncells};
+      exclusive_scan(pol, ib._counts.begin(), ib._counts.end(), ib._offsets.begin());
+      ib._indices = bvec_t{pars.get_allocator(), pars.size()};
+      pol(range(pars.size()), SpatiallyDistribute{wrapv<space>{}, p->dx, bt, pars.attrVector("x"), tmp,
+                                                  ib._offsets, ib._indices, 1, 0, 0.5f});
+      pol(Collapse{(size_t)nb, (size_t)512}, CleanGridBlocks{wrapv<space>{}, grids});
+      pol(Collapse{(size_t)nb, (size_t)512},
+          P2C2GTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{}, p->dt, fc, ib, pars, table, grids});
+      pol(Collapse{(size_t)nb, (size_t)512}, GridVelocityWithRhs<space>{wrapv<space>{}, grids, p->dt, grav});
+      for (auto &w : walls)
+        pol(Collapse{(size_t)nb, (size_t)512},
+            ApplyBoundaryConditionOnGridBlocks{wrapv<space>{}, w, table, grids});
+      pol(range(pars.size()), PreG2C2PTransfer{wrapv<space>{}, pars});
+      pol(Collapse{(size_t)nb, (size_t)512},
+          G2C2PTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{}, p->dt, fc, ib, grids, table, pars});
+      pol(range(pars.size()),
+          PostG2C2PTransfer{wrapv<space>{}, wrapv<transfer_scheme_e::apic>{}, p->dt, p->dx, fc, pars});
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (out_seconds) *out_seconds = std::chrono::duration<double>(t1 - t0).count();
+  };
+  if (p->policy == 0)
+    run(seq_exec(), wrapv<host>{});
+  else {
+    auto pol = omp_exec();
+    if (p->threads > 0) pol = OmpExecutionPolicy{}.threads(p->threads);
+    run(pol, wrapv<omp>{});
+  }
+  if (status) return status;
+  std::memcpy(x, (float *)pars.getAttrAddress("x"), sizeof(float) * 3 * n);
+  std::memcpy(v, (float *)pars.getAttrAddress("v"), sizeof(float) * 3 * n);
+  std::memcpy(C, (float *)pars.getAttrAddress("C"), sizeof(float) * 9 * n);
+  std::memcpy(F, (float *)pars.getAttrAddress("F"), sizeof(float) * 9 * n);
   const int nb = table.size();
   if (out_nblocks) *out_nblocks = nb;
   if (out_keys) {

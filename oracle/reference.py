@@ -72,19 +72,23 @@ class RefResult:
 
 def run(spec, particles, nsteps: int, policy: int = POLICY_SEQ, threads: int = 0, order: int = 1,
         table_expected: int | None = None, cap_blocks: int = 1 << 15,
-        timeout: float = 600.0, colliders=(), levelsets=()) -> RefResult:
+        timeout: float = 600.0, colliders=(), levelsets=(), cell: bool = False) -> RefResult:
     """`colliders`: zsmpm_collider records (ctypes), applied after the walls by the reference's
     own Collider<AnalyticLevelSet<...>> launches; `levelsets`: LevelSet objects
-    (zsmpm_b200.colliders), applied after them as LevelSetBoundary<SparseLevelSet<3>>."""
+    (zsmpm_b200.colliders), applied after them as LevelSetBoundary<SparseLevelSet<3>>.
+    `cell`: the substep transfers with P2C2GTransfer / G2C2PTransfer instead of P2G / G2P
+    (fixed corotated; C carries the pair's B attribute)."""
     n = particles.n
     if table_expected is None:
         table_expected = max(n // 512, 64)
-    cmd = 9 if levelsets else (8 if colliders else 1)
+    if cell and (colliders or levelsets):
+        raise ValueError("the cell-centric run takes the walls only")
+    cmd = 10 if cell else (9 if levelsets else (8 if colliders else 1))
     req = struct.pack("<i", cmd) + _params_bytes(spec, policy, threads, order, table_expected)
     req += struct.pack("<3i", n, nsteps, cap_blocks)
     for a in (particles.m, particles.x, particles.v, particles.C, particles.F, particles.plastic):
         req += np.ascontiguousarray(a, dtype="<f4").tobytes()
-    if cmd >= 8:
+    if cmd in (8, 9):
         req += struct.pack("<i", len(colliders)) + b"".join(bytes(c) for c in colliders)
     if cmd == 9:
         from zsmpm_b200.colliders import TYPES

@@ -56,6 +56,8 @@ def lib() -> C.CDLL:
         _lib.oracle_bin_order.argtypes = [C.c_int, C.c_int, P, P, P, P]
         _lib.oracle_g2p2g_f32.argtypes = [C.POINTER(OracleParams), C.c_int, P, P, P, C.c_int, P, P, P]
         _lib.oracle_g2p2g_f64.argtypes = _lib.oracle_g2p2g_f32.argtypes
+        _lib.oracle_run_cell_f32.argtypes = [C.POINTER(OracleParams), C.c_int] + [P] * 5 + [C.c_int, C.c_int, P, P, P]
+        _lib.oracle_run_cell_f64.argtypes = _lib.oracle_run_cell_f32.argtypes
     return _lib
 
 
@@ -139,6 +141,32 @@ def run(spec, particles, nsteps: int, precision: str = "f32", mode=None, table_e
         raise RuntimeError(f"oracle_run failed with status {st}")
     return RunResult(x=x, v=v, C=Cm, F=F, plastic=pl, keys=keys[:nb.value].copy(),
                      grid=grid[:nb.value].copy())
+
+
+def run_cell(spec, particles, nsteps: int, precision: str = "f32", table_expected=None,
+             cap_blocks: int = 1 << 16) -> RunResult:
+    """The substep with the cell-centric transfers (P2C2GTransfer / G2C2PTransfer, fixed
+    corotated), restated, nsteps times on a copy of `particles`; C carries the B attribute."""
+    dt = np.float32 if precision == "f32" else np.float64
+    n = particles.n
+    if table_expected is None:
+        table_expected = max(n // 512, 64)
+    prm = params_from_spec(spec, table_expected=table_expected)
+    m = particles.m.astype(dt)
+    x = particles.x.astype(dt).copy()
+    v = particles.v.astype(dt).copy()
+    Cm = particles.C.astype(dt).copy()
+    F = particles.F.astype(dt).copy()
+    nb = C.c_int()
+    keys = np.zeros((cap_blocks, 3), np.int32)
+    grid = np.zeros((cap_blocks, 4, 512), dt)
+    fn = lib().oracle_run_cell_f32 if precision == "f32" else lib().oracle_run_cell_f64
+    st = fn(C.byref(prm), n, _p(m), _p(x), _p(v), _p(Cm), _p(F), nsteps, cap_blocks, C.byref(nb), _p(keys),
+            _p(grid))
+    if st != 0:
+        raise RuntimeError(f"oracle_run_cell failed with status {st}")
+    return RunResult(x=x, v=v, C=Cm, F=F, plastic=particles.plastic.astype(dt).copy(),
+                     keys=keys[:nb.value].copy(), grid=grid[:nb.value].copy())
 
 
 def svd(A: np.ndarray, precision: str = "f32"):

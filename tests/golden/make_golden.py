@@ -16,7 +16,11 @@ reference itself on seeded synthetic inputs:
   ref_implicit_fc.npz / ref_implicit_dp.npz G2P2GTransfer, ImplicitMPMSystem's multiply /
                                             project / precondition and ConjugateGradient::solve
                                             on a small state with a smooth grid velocity field
-Run:  python tests/golden/make_golden.py
+  ref_cell_fc.npz                           5 substeps with the cell-centric transfers
+                                            (P2C2GTransfer / G2C2PTransfer, fixed corotated)
+                                            from a state with random B and F
+Run:  python tests/golden/make_golden.py [name ...]   (no names: every fixture; a name such as
+      "cell" makes only the fixtures whose file name contains it)
 """
 from __future__ import annotations
 
@@ -46,9 +50,13 @@ def random_F(rng, n, spread):
     return np.ascontiguousarray(A.transpose(0, 2, 1).reshape(n, 9)).astype(np.float32)
 
 
-def main() -> None:
+def main(only=()) -> None:
     if not reference.available():
         raise SystemExit("oracle/_ref/zsref_cli is missing: run oracle/build_ref.sh first")
+    if only:
+        if any("cell" in o for o in only):
+            make_cell(HERE / "ref_cell_fc.npz")
+        return
     for model, name in ((0, "fc"), (1, "dp")):
         spec = scenes.small_scene(model=model, mode=1, velocity=(0.4, -0.3, 0.2))
         p = scenes.generate(spec)
@@ -78,6 +86,7 @@ def main() -> None:
         make_implicit(model, HERE / f"ref_implicit_{name}.npz")
         make_colliders(model, HERE / f"ref_colliders_{name}.npz")
     make_levelsets(0, HERE / "ref_levelsets_fc.npz")
+    make_cell(HERE / "ref_cell_fc.npz")
     print("wrote", sorted(f.name for f in HERE.glob("*.npz")))
 
 
@@ -120,8 +129,6 @@ def make_implicit(model: int, path: Path, dt: float = 1e-3, cg_iters: int = 20) 
                         b=b, cg_x=cg_x, cg_iters=iters, cg_max_iters=cg_iters)
 
 
-if __name__ == "__main__":
-    main()
 
 
 def collider_set():
@@ -182,3 +189,26 @@ def make_levelsets(model: int, path: Path, steps: int = 5) -> None:
     np.savez_compressed(path, m=p.m, x0=p.x, v0=p.v, C0=p.C, F0=p.F, plastic0=p.plastic, x=r.x, v=r.v, C=r.C,
                         F=r.F, logJp=r.logJp, keys=r.keys, grid=r.grid, steps=steps, model=model, nls=len(ls),
                         **extra)
+
+
+def cell_state(seed: int = 9):
+    """The small fixed-corotated scene moving at (0.4, -0.3, 0.2) with a random B (the
+    cell-centric pair's affine attribute) of size 1e-3 dx and a random F near the identity."""
+    spec = scenes.small_scene(model=0, mode=0, velocity=(0.4, -0.3, 0.2))
+    p = scenes.generate(spec)
+    rng = np.random.default_rng(seed)
+    p.C = (rng.normal(size=(p.n, 9)) * 1e-3 * spec.dx).astype(np.float32)
+    p.F = random_F(rng, p.n, 0.02)
+    return spec, p
+
+
+def make_cell(path: Path, steps: int = 5) -> None:
+    spec, p = cell_state()
+    r = reference.run(spec, p, steps, policy=reference.POLICY_SEQ, cell=True)
+    assert r.status == 0
+    np.savez_compressed(path, m=p.m, x0=p.x, v0=p.v, C0=p.C, F0=p.F, x=r.x, v=r.v, C=r.C, F=r.F, keys=r.keys,
+                        grid=r.grid, steps=steps)
+
+
+if __name__ == "__main__":
+    main(tuple(sys.argv[1:]))

@@ -131,3 +131,43 @@ def test_restatement_matches_reference_live_omp():
     o = restated.run(spec, p, 5, "f32", mode=1)
     assert rel_l2(o.v, r.v) < 1e-5
     assert rel_l2(o.x, r.x) < 1e-6
+
+
+def _cell_particles(z):
+    from zsmpm_b200.scenes import Particles
+    n = len(z["m"])
+    return Particles(m=z["m"], x=z["x0"], v=z["v0"], C=z["C0"], F=z["F0"], plastic=np.zeros(n, np.float32))
+
+
+def test_cell_transfer_restatement_bit_exact_with_reference():
+    """P2C2GTransfer / G2C2PTransfer (fixed corotated) restated: 5 substeps equal the compiled
+    reference's sequential run bit for bit (particles, keys and grid)."""
+    from oracle import restated
+    from zsmpm_b200 import scenes
+    z = np.load(GOLDEN / "ref_cell_fc.npz")
+    spec = scenes.small_scene(model=0, mode=0, velocity=(0.4, -0.3, 0.2))
+    p = _cell_particles(z)
+    assert np.array_equal(p.x, scenes.generate(spec).x), "scene generator changed"
+    o = restated.run_cell(spec, p, int(z["steps"]), "f32")
+    for f in ("x", "v", "C", "F"):
+        assert np.array_equal(getattr(o, f), z[f]), f
+    assert np.array_equal(o.keys, z["keys"])
+    assert np.array_equal(o.grid, z["grid"])
+
+
+def test_cell_transfer_fp64_against_reference():
+    """The FP64 restatement against the FP32 reference: x and v differ by rounding.  B (the C
+    attribute) and F - I differ by about 1%: G2C2P forms B as W (sum_i v_i x_i / 8 - v_c x_p)
+    from absolute positions (x ~ 0.5) for a term of size v dx, so FP32 keeps only about
+    eps * 0.5 / dx of it."""
+    from oracle import restated
+    from zsmpm_b200 import scenes
+    z = np.load(GOLDEN / "ref_cell_fc.npz")
+    spec = scenes.small_scene(model=0, mode=0, velocity=(0.4, -0.3, 0.2))
+    o = restated.run_cell(spec, _cell_particles(z), int(z["steps"]), "f64")
+    assert rel_l2(o.v, z["v"]) < 1e-5
+    assert rel_l2(o.x - z["x0"], z["x"] - z["x0"]) < 2e-3
+    assert rel_l2(o.C, z["C"]) < 5e-2
+    assert rel_l2(o.F - z["F0"], z["F"] - z["F0"]) < 5e-2
+    # mass: the pair's node weights sum to one per particle
+    assert abs(float(o.grid[:, 0].sum()) / float(z["m"].sum()) - 1) < 1e-12
