@@ -91,6 +91,26 @@ typedef enum {
                                      inserts them (first particle, then enlargement) */
 } zsmpm_block_order;
 
+/* Particle-grid transfers of a scene's substep (zsmpm_scene_set_transfer). */
+typedef enum {
+  /* P2GTransfer / G2PTransfer (simulation/transfer/P2G.hpp, G2P.hpp): APIC with the quadratic
+   * B-spline; the C attribute is the APIC C */
+  ZSMPM_TRANSFER_APIC = 0,
+  /* P2C2GTransfer / G2C2PTransfer with PreG2C2PTransfer and PostG2C2PTransfer
+   * (simulation/transfer/P2C2G.hpp:27-189, G2C2P.hpp:36-278): through the grid cells, tent
+   * weights to the cell centers and 1/8 to the corners; fixed corotated only; the C attribute
+   * holds the pair's B matrix (as the reference's "C" attribute does for it) */
+  ZSMPM_TRANSFER_CELL = 1
+} zsmpm_transfer;
+
+/* Parts of P2C2G (zsmpm_p2c2g). */
+typedef enum {
+  ZSMPM_P2C2G_ALL = 0,      /* P2C2GTransfer: mass, momentum and the stress term */
+  ZSMPM_P2C2G_MOMENTUM = 1, /* P2C2GTransferMomentum: mass and momentum m (v + B Dinv (x_i - x_p)) */
+  ZSMPM_P2C2G_FORCE = 2     /* P2C2GTransferForce: the stress term alone, into the momentum
+                               channels (the mass channel untouched) */
+} zsmpm_p2c2g_part;
+
 typedef enum {
   ZSMPM_CLOSURE_PLAIN = 0,   /* analytic return map */
   ZSMPM_CLOSURE_LEARNED = 1  /* MLP closure (zsmpm_closure_*), falls back per particle */
@@ -218,6 +238,21 @@ ZSMPM_API zsmpm_status zsmpm_bin_particles(zsmpm_scene *scene, void *stream);
 ZSMPM_API zsmpm_status zsmpm_p2g(zsmpm_scene *scene, void *stream);
 ZSMPM_API zsmpm_status zsmpm_grid_update(zsmpm_scene *scene, void *stream);
 ZSMPM_API zsmpm_status zsmpm_g2p(zsmpm_scene *scene, void *stream);
+/* The scene's transfer pair (zsmpm_transfer; ZSMPM_TRANSFER_APIC by default).
+ * ZSMPM_TRANSFER_CELL replaces P2G / G2P in zsmpm_p2g, zsmpm_g2p, zsmpm_substep and zsmpm_run
+ * with the cell-centric pair; it needs a single fixed-corotated scene without a learned closure.
+ * The stored C attribute keeps its numbers: set the scheme before the upload whose C holds the
+ * scheme's matrix.  With particles present, the pair's affine term of the stored state is
+ * formed on `stream`. */
+ZSMPM_API zsmpm_status zsmpm_scene_set_transfer(zsmpm_scene *scene, int32_t transfer, void *stream);
+/* P2C2GTransfer / P2C2GTransferMomentum / P2C2GTransferForce (zsmpm_p2c2g_part) over every
+ * cell of the active blocks (simulation/transfer/P2C2G.hpp:27-420), adding into the grid that
+ * the binning zeroed; ZSMPM_TRANSFER_CELL scenes only.  zsmpm_p2g runs the ALL part. */
+ZSMPM_API zsmpm_status zsmpm_p2c2g(zsmpm_scene *scene, int32_t part, void *stream);
+/* PreG2C2PTransfer + G2C2PTransfer + PostG2C2PTransfer (simulation/transfer/G2C2P.hpp:36-278):
+ * v and B from the updated grid, F <- (I + dt B Dinv) F, x += v dt; ZSMPM_TRANSFER_CELL scenes
+ * only (the same call as zsmpm_g2p there). */
+ZSMPM_API zsmpm_status zsmpm_g2c2p(zsmpm_scene *scene, void *stream);
 /* One full substep (activate, bin, P2G, grid update + walls, G2P). */
 ZSMPM_API zsmpm_status zsmpm_substep(zsmpm_scene *scene, void *stream);
 /* nsteps substeps, replayed from a CUDA graph of two substeps (captured on first use per

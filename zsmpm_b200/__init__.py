@@ -109,7 +109,7 @@ class Scene:
     """One MPM system on one GPU (wraps a zsmpm_scene handle)."""
 
     def __init__(self, spec: SceneSpec, particles: Particles | None = None, device: int = 0,
-                 table_expected: int = 0, max_particles: int = 0):
+                 table_expected: int = 0, max_particles: int = 0, transfer: str = "apic"):
         self.spec = spec
         self.device = device
         self._lib = _abi.lib()
@@ -118,6 +118,8 @@ class Scene:
                           table_expected=table_expected)
         _abi.check(self._lib.zsmpm_scene_create(C.byref(desc), C.byref(self._h)), "scene_create")
         self.n = 0
+        if transfer != "apic":
+            self.set_transfer(transfer)
         if particles is not None:
             self.upload(particles)
 
@@ -208,6 +210,21 @@ class Scene:
 
     def g2p(self, stream: int = 0):
         _abi.check(self._lib.zsmpm_g2p(self._h, C.c_void_p(stream)), "g2p")
+
+    TRANSFERS = {"apic": 0, "cell": 1}
+    P2C2G_PARTS = {"all": 0, "momentum": 1, "force": 2}
+
+    def set_transfer(self, transfer: str, stream: int = 0):
+        """"apic" (P2GTransfer / G2PTransfer) or "cell" (P2C2GTransfer / G2C2PTransfer, fixed
+        corotated; the C attribute then holds the pair's B matrix), see zsmpm_scene_set_transfer."""
+        _abi.check(self._lib.zsmpm_scene_set_transfer(self._h, self.TRANSFERS[transfer], C.c_void_p(stream)),
+                   "scene_set_transfer")
+
+    def p2c2g(self, part: str = "all", stream: int = 0):
+        _abi.check(self._lib.zsmpm_p2c2g(self._h, self.P2C2G_PARTS[part], C.c_void_p(stream)), "p2c2g")
+
+    def g2c2p(self, stream: int = 0):
+        _abi.check(self._lib.zsmpm_g2c2p(self._h, C.c_void_p(stream)), "g2c2p")
 
     def substep(self, stream: int = 0):
         _abi.check(self._lib.zsmpm_substep(self._h, C.c_void_p(stream)), "substep")

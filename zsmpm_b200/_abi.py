@@ -127,6 +127,9 @@ SIGNATURES = {
     "zsmpm_p2g": (_S, [_P, _P]),
     "zsmpm_grid_update": (_S, [_P, _P]),
     "zsmpm_g2p": (_S, [_P, _P]),
+    "zsmpm_scene_set_transfer": (_S, [_P, C.c_int32, _P]),
+    "zsmpm_p2c2g": (_S, [_P, C.c_int32, _P]),
+    "zsmpm_g2c2p": (_S, [_P, _P]),
     "zsmpm_substep": (_S, [_P, _P]),
     "zsmpm_run": (_S, [_P, C.c_int32, _P]),
     "zsmpm_get_table_view": (_S, [_P, C.POINTER(TableView)]),

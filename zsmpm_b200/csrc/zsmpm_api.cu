@@ -737,6 +737,54 @@ ZSMPM_API zsmpm_status zsmpm_g2p(zsmpm_scene *s, void *stream) {
   return ZSMPM_OK;
 }
 
+ZSMPM_API zsmpm_status zsmpm_scene_set_transfer(zsmpm_scene *s, int32_t transfer, void *stream) {
+  zsmpm_status st = check_scene(s, false);
+  if (st != ZSMPM_OK) return st;
+  if (transfer != ZSMPM_TRANSFER_APIC && transfer != ZSMPM_TRANSFER_CELL)
+    return fail(ZSMPM_ERR_INVALID_ARG, "unknown transfer scheme");
+  if (transfer == ZSMPM_TRANSFER_CELL) {
+    if (s->nscenes > 0) return fail(ZSMPM_ERR_INVALID_ARG, "the cell-centric transfers run on single scenes");
+    if (s->desc.material.model != ZSMPM_FIXED_COROTATED)
+      return fail(ZSMPM_ERR_INVALID_ARG,
+                  "the cell-centric transfers are built for fixed corotated (P2C2G's plasticity branch "
+                  "writes the plastic state once per visiting cell)");
+    if (s->dev.aux.learned) return fail(ZSMPM_ERR_INVALID_ARG, "detach the learned closure first");
+  }
+  if (s->dev.prm.transfer == transfer) return ZSMPM_OK;
+  invalidate_graphs(s);
+  s->dev.prm.transfer = transfer;
+  if (s->uploaded) {
+    // the affine term the next transfer reads, from the stored state
+    cudaStream_t cs = as_stream(stream);
+    bind_buffers(s);
+    ZS_TRY(launch_prime(s->dev, cs), "transfer affine term");
+    s->binned = false;
+    s->last_stream = cs;
+  }
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_p2c2g(zsmpm_scene *s, int32_t part, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (s->dev.prm.transfer != kTransferCell)
+    return fail(ZSMPM_ERR_INVALID_ARG, "zsmpm_p2c2g needs zsmpm_scene_set_transfer(ZSMPM_TRANSFER_CELL)");
+  if (part < ZSMPM_P2C2G_ALL || part > ZSMPM_P2C2G_FORCE) return fail(ZSMPM_ERR_INVALID_ARG, "unknown P2C2G part");
+  if (!s->binned) return fail(ZSMPM_ERR_NOT_READY, "p2c2g needs zsmpm_activate_blocks and zsmpm_bin_particles first");
+  bind_buffers(s);
+  ZS_TRY(launch_p2c2g(s->dev, part, as_stream(stream)), "p2c2g");
+  s->last_stream = as_stream(stream);
+  return ZSMPM_OK;
+}
+
+ZSMPM_API zsmpm_status zsmpm_g2c2p(zsmpm_scene *s, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (s->dev.prm.transfer != kTransferCell)
+    return fail(ZSMPM_ERR_INVALID_ARG, "zsmpm_g2c2p needs zsmpm_scene_set_transfer(ZSMPM_TRANSFER_CELL)");
+  return zsmpm_g2p(s, stream);
+}
+
 ZSMPM_API zsmpm_status zsmpm_substep(zsmpm_scene *s, void *stream) {
   zsmpm_status st = check_scene(s, true);
   if (st != ZSMPM_OK) return st;
@@ -917,6 +965,8 @@ ZSMPM_API zsmpm_status zsmpm_scene_set_closure(zsmpm_scene *s, zsmpm_closure *c,
     s->dev.aux.learned = 0;
     return ZSMPM_OK;
   }
+  if (s->dev.prm.transfer != kTransferApic)
+    return fail(ZSMPM_ERR_INVALID_ARG, "the learned closure replaces G2P's return map (APIC transfers only)");
   closure_dev cd{};
   if (!closure_device_view(c, &cd)) return fail(ZSMPM_ERR_NOT_READY, "closure has no dataset or state yet");
   // a batch runs the closure on the scenes of its model and the plain return map on the others

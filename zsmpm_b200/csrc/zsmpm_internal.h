@@ -93,7 +93,10 @@ struct scene_params {
   // incremental binning
   int mover_cap;                    // entries of the mover list
   int bin_full;                     // 1: this binning launch recounts every particle
+  int transfer;                     // kTransferApic (P2G / G2P) or kTransferCell (P2C2G / G2C2P)
 };
+
+constexpr int kTransferApic = 0, kTransferCell = 1;
 
 // floats of a queue entry: U 9, V 9, S 3, plastic state, m, C 9
 constexpr int kQueueFloats = 32;
@@ -169,6 +172,8 @@ cudaError_t prepare_kernels();
 cudaError_t launch_activate(scene_device &s, cudaStream_t st);
 cudaError_t launch_bin(scene_device &s, cudaStream_t st);
 cudaError_t launch_p2g(scene_device &s, cudaStream_t st);
+// P2C2G of the cell-centric pair: part 0 all, 1 the momentum part, 2 the force part
+cudaError_t launch_p2c2g(scene_device &s, int part, cudaStream_t st);
 cudaError_t launch_grid_update(scene_device &s, cudaStream_t st);
 cudaError_t launch_g2p(scene_device &s, cudaStream_t st);
 int kernels_per_substep();

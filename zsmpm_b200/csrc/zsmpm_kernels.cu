@@ -1173,6 +1173,157 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s
   }
 }
 
+// ----------------------------------------------------------------- the cell-centric pair
+// P2C2GTransfer (simulation/transfer/P2C2G.hpp:27-189) and G2C2PTransfer with its Pre and Post
+// passes (G2C2P.hpp:36-278), the fixed-corotated branch.  Both go through the grid cells: the
+// particles within dx of a cell's center x_c (per axis) carry the tent weight
+// W = prod (1 - |x_c - x_p| / dx), and a cell passes its sums to its 8 corner nodes (and takes
+// its velocity from them) with weight 1/8.  A particle's cells are those of the index buckets
+// floor(x / dx + 0.5) in {c, c + 1}^3 around it, i.e. the binning's cells c - 2 + {0,1}^3 (the
+// binning keys a particle by floor(x / dx + 0.5) - 2).
+//
+// Per particle the pair carries x, m, v, F and B (the reference's C attribute) and, written at
+// the end of G2C2P for the next P2C2G, the affine term
+//   A = (m B - dt V0 P(F) F^T) Dinv,   Dinv_k = 2 / (dx^2 - 2 r_k^2),  r = x - dx round(x / dx),
+// columns k scaled (P2C2G.hpp:86-146); it is the same array the APIC path keeps its affine
+// momentum in.
+
+// Dinv of one position component, as P2C2G.hpp:87-91 and PostG2C2PTransfer compute it
+__device__ __forceinline__ float cell_dinv(const scene_params &p, float x) {
+  const float r = x - floorf(x * p.inv_dx + 0.5f) * p.dx;
+  return 2.f / (p.dx * p.dx - 2.f * r * r);
+}
+
+// The pair's per-particle affine term A of the stored state, in the particle order of cur:
+// part 0 the whole term (P2C2GTransfer; the cell-scheme counterpart of k_prime), 1 the momentum
+// part m B Dinv (P2C2GTransferMomentum), 2 the force part -dt V0 P F^T Dinv (P2C2GTransferForce).
+__global__ void __launch_bounds__(kThreads) k_cell_affine(scene_device s, int part, float *out) {
+  if (part == 0 && blockIdx.x == 0 && threadIdx.x == 0) s.ctr[kCtrMaskFrom] = 0;
+  const scene_params &p = s.prm;
+  const size_t cap = (size_t)p.cap;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += grid_threads()) {
+    const float4 xm = s.cur.xm[i];
+    const float dinv[3] = {cell_dinv(p, xm.x), cell_dinv(p, xm.y), cell_dinv(p, xm.z)};
+    float F[9], tau[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) F[k] = s.cur.F[k * cap + i];
+    float pl = 0.f;
+    if (part != 1) constitutive(p.mat, F, pl, tau);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float mB = part == 2 ? 0.f : xm.w * s.cur.C[k * cap + i];
+      const float f = part == 1 ? 0.f : p.dt * tau[k];
+      out[k * cap + i] = (mB - f) * dinv[k / 3];
+    }
+  }
+}
+
+// P2C2G: one CTA of 512 threads per block (persistent), one thread per cell.  Stage 1: the
+// thread walks its cell's 8 buckets (particles within them in the binned order, which is upload
+// order within a cell) and sums W m, W m v, W A and W A (x_p - x_c).  Stage 2: the 8 corner nodes
+// receive 1/8 of (m, m v + A (x_i - x_c) - sum W A (x_p - x_c)), i.e. sum_p W/8 (m v + A (x_i -
+// x_p)), through a shared-memory halo of the block's 9^3 nodes, which is then added to the grid
+// (the nodes 8b + 8 belong to the neighbour blocks).  The cell-relative positions are the
+// reference's absolute-position sums rearranged; they keep the affine term from cancelling
+// against x ~ 0.5 in FP32.  with_mass = 0 (the force part alone) leaves the mass channel and
+// the m v term out, as P2C2GTransferForce does.
+constexpr int kCellThreads = 512;
+constexpr int kCellHalo = 9;
+constexpr int kCellHaloNodes = kCellHalo * kCellHalo * kCellHalo;
+
+__global__ void __launch_bounds__(kCellThreads, 2) k_p2c2g(scene_device s, const float *affine, int with_mass) {
+  __shared__ float sh[kGridChannels * kCellHaloNodes];
+  __shared__ int s_nb[8];  // the blocks at offsets {-1, 0}^3: index (ox + 1) * 4 + (oy + 1) * 2 + (oz + 1)
+  __shared__ int s_b;
+  const scene_params &p = s.prm;
+  const int nb = s.ctr[kCtrBlocks];
+  const size_t cap = (size_t)p.cap;
+  const int t = threadIdx.x;
+  const int lx = t >> 6, ly = (t >> 3) & 7, lz = t & 7;
+  for (int q = t; q < kGridChannels * kCellHaloNodes; q += blockDim.x) sh[q] = 0.f;
+  for (;;) {
+    const int w = grab_block(&s.ctr[kCtrWork + kWorkP2G], &s_b);  // also orders the halo's zeroing
+    if (w >= nb) break;
+    const int b = s.work_order[w];
+    const int3 key = unpack_key(s.blk_pk[b]);
+    if (t < 8) {
+      const int3 k = make_int3(key.x - 1 + (t >> 2), key.y - 1 + ((t >> 1) & 1), key.z - 1 + (t & 1));
+      s_nb[t] = t == 7 ? b : table_query(s, pack_key(k.x, k.y, k.z), k);
+    }
+    __syncthreads();
+    const int cx = key.x * 8 + lx, cy = key.y * 8 + ly, cz = key.z * 8 + lz;
+    const float pcx = ((float)cx + 0.5f) * p.dx, pcy = ((float)cy + 0.5f) * p.dx, pcz = ((float)cz + 0.5f) * p.dx;
+    float mc = 0.f, mv[3] = {0.f, 0.f, 0.f}, QD[9], QX[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < 9; ++k) QD[k] = 0.f;
+#pragma unroll 1
+    for (int o = 0; o < 8; ++o) {
+      // bucket c + (ox, oy, oz) = binned cell c - 2 + (ox, oy, oz)
+      const int gx = lx - 2 + (o >> 2), gy = ly - 2 + ((o >> 1) & 1), gz = lz - 2 + (o & 1);
+      const int nbk = s_nb[(gx >= 0 ? 4 : 0) + (gy >= 0 ? 2 : 0) + (gz >= 0 ? 1 : 0)];
+      if (nbk < 0) continue;
+      const int cell = ((gx & 7) << 6) | ((gy & 7) << 3) | (gz & 7);
+      const int j0 = s.cell_start[nbk * 512 + cell];
+      const int j1 = cell < 511 ? s.cell_start[nbk * 512 + cell + 1] : s.block_start[nbk + 1];
+      for (int j = j0; j < j1; ++j) {
+        const int i = s.src[j];
+        const float4 xm = s.cur.xm[i];
+        const float rx = xm.x - pcx, ry = xm.y - pcy, rz = xm.z - pcz;  // x_p - x_c
+        if (fabsf(rx) > p.dx || fabsf(ry) > p.dx || fabsf(rz) > p.dx) continue;
+        const float W = (1.f - fabsf(rx * p.inv_dx)) * (1.f - fabsf(ry * p.inv_dx)) * (1.f - fabsf(rz * p.inv_dx));
+        float A[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) A[k] = affine[k * cap + i];
+        if (with_mass) {
+          const float4 v = s.cur.v[i];
+          const float wm = W * xm.w;
+          mc += wm;
+          mv[0] = fmaf(wm, v.x, mv[0]);
+          mv[1] = fmaf(wm, v.y, mv[1]);
+          mv[2] = fmaf(wm, v.z, mv[2]);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          QD[d] = fmaf(W, A[d], QD[d]);
+          QD[3 + d] = fmaf(W, A[3 + d], QD[3 + d]);
+          QD[6 + d] = fmaf(W, A[6 + d], QD[6 + d]);
+          QX[d] = fmaf(W, A[d] * rx + A[3 + d] * ry + A[6 + d] * rz, QX[d]);
+        }
+      }
+    }
+    // stage 2: corner (a, b, c) of the cell at x_c + (a - 1/2, b - 1/2, c - 1/2) dx
+    const float h = 0.5f * p.dx;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+      const float ex = (o >> 2) ? h : -h, ey = ((o >> 1) & 1) ? h : -h, ez = (o & 1) ? h : -h;
+      const int node = ((lx + (o >> 2)) * kCellHalo + ly + ((o >> 1) & 1)) * kCellHalo + lz + (o & 1);
+      if (with_mass) atomicAdd(&sh[node], 0.125f * mc);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float val = mv[d] + (QD[d] * ex + QD[3 + d] * ey + QD[6 + d] * ez) - QX[d];
+        atomicAdd(&sh[(1 + d) * kCellHaloNodes + node], 0.125f * val);
+      }
+    }
+    __syncthreads();
+    // flush: node (nx, ny, nz) of the halo is cell (n & 7) of block b + (n >= 8); each value is
+    // sent and the halo zeroed for the next block
+    for (int q = t; q < kGridChannels * kCellHaloNodes; q += blockDim.x) {
+      const int c = q / kCellHaloNodes, node = q - c * kCellHaloNodes;
+      const float val = sh[q];
+      if (val == 0.f) continue;
+      sh[q] = 0.f;
+      const int nx = node / (kCellHalo * kCellHalo), ny = (node / kCellHalo) % kCellHalo, nz = node % kCellHalo;
+      const int tb = s.nbr[b * 8 + ((nx >> 3) << 2) + ((ny >> 3) << 1) + (nz >> 3)];
+      if (tb < 0) {
+        set_status(s.ctr, kStatusMissingBlock);
+        continue;
+      }
+      const int cell = ((nx & 7) << 6) | ((ny & 7) << 3) | (nz & 7);
+      atomicAdd(&s.grid[((size_t)tb * kGridChannels + c) * 512 + cell], val);
+    }
+  }
+}
+
 // ----------------------------------------------------------------- grid update
 // ComputeGridBlockVelocity with the rhs term (v = (mv + rhs)/m + g dt; GridOp.hpp:93-99
 // restated) and ApplyBoundaryConditionOnGridBlocks with six planes wall_cells*dx inside
@@ -1528,9 +1679,16 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // threads) resident CTAs per SM: the kernel is issue- and latency-bound, and the extra warps
 // hide more latency than the cap costs (2.41 -> 2.09 ms on the 30 M-particle sand scene, no
 // spills).
-template <bool kLearned, bool kBatch, int NT>
+// kCell: G2C2PTransfer with PreG2C2PTransfer and PostG2C2PTransfer (the cell-centric pair,
+// fixed corotated), gathered per particle: a particle takes sum_c W_c/8 v_i over the 8 corners i
+// of its cells c, i.e. the node weights (3/4 - f/2, 1/2, f/2 - 1/4) per axis over the same three
+// nodes as the quadratic stencil (f = x/dx - base, base = floor(x/dx + 1/2) - 1), and
+// B = sum W v_i (x_i - x_p)^T; then F <- (I + dt B Dinv) F, x += v dt, and the affine term A of
+// the next P2C2G from the new state.
+template <bool kLearned, bool kBatch, int NT, bool kCell = false>
 __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
   static_assert(!kLearned || NT == kThreads, "learned G2P runs at 256 threads");
+  static_assert(!kCell || (!kLearned && !kBatch), "the cell-centric pair runs on single fixed-corotated scenes");
   extern __shared__ __align__(16) float g2p_smem[];
   float4 *svf = reinterpret_cast<float4 *>(g2p_smem);
   __shared__ int s_b;
@@ -1622,19 +1780,34 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
       buf ^= 1;
       i = inext;
       inext = inext2;
-      const float X[3] = {over_dx(p, xm.x), over_dx(p, xm.y), over_dx(p, xm.z)};
       int hb[3];
       float w[3][3], f[3];
+      if (kCell) {
+        // the index bucket floor(x / dx + 1/2) as the binning computes it; its cells are
+        // bucket - 1 and bucket, their corners the nodes bucket - 1 .. bucket + 1
+        const float X[3] = {xm.x * p.inv_dx, xm.y * p.inv_dx, xm.z * p.inv_dx};
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const float bs = floorf(X[d] - 0.5f);
-        f[d] = X[d] - bs;
-        hb[d] = (int)bs - org[d];
-        w[d][0] = 0.5f * (1.5f - f[d]) * (1.5f - f[d]);
-        const float f1 = f[d] - 1.f;
-        w[d][1] = 0.75f - f1 * f1;
-        const float f2 = 0.5f + f1;
-        w[d][2] = 0.5f * f2 * f2;
+        for (int d = 0; d < 3; ++d) {
+          const float bs = floorf(X[d] + 0.5f) - 1.f;
+          f[d] = X[d] - bs;
+          hb[d] = (int)bs - org[d];
+          w[d][0] = 0.75f - 0.5f * f[d];
+          w[d][1] = 0.5f;
+          w[d][2] = 0.5f * f[d] - 0.25f;
+        }
+      } else {
+        const float X[3] = {over_dx(p, xm.x), over_dx(p, xm.y), over_dx(p, xm.z)};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const float bs = floorf(X[d] - 0.5f);
+          f[d] = X[d] - bs;
+          hb[d] = (int)bs - org[d];
+          w[d][0] = 0.5f * (1.5f - f[d]) * (1.5f - f[d]);
+          const float f1 = f[d] - 1.f;
+          w[d][1] = 0.75f - f1 * f1;
+          const float f2 = 0.5f + f1;
+          w[d][2] = 0.5f * f2 * f2;
+        }
       }
       const bool inside = hb[0] >= 0 && hb[0] <= kHalo - 3 && hb[1] >= 0 && hb[1] <= kHalo - 3 &&
                           hb[2] >= 0 && hb[2] <= kHalo - 3;
@@ -1680,9 +1853,20 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
           }
         }
       }
-      float C[9];
+      float C[9];  // APIC: C = (4/dx^2) sum W v (x_i - x_p)^T; the cell pair: B = sum W v (x_i - x_p)^T
 #pragma unroll
-      for (int k = 0; k < 9; ++k) C[k] = B[k] * p.four_over_dx;
+      for (int k = 0; k < 9; ++k) C[k] = B[k] * (kCell ? p.dx : p.four_over_dx);
+      // the cell pair updates F with B Dinv at the position before the move
+      // (PostG2C2PTransfer); APIC with C
+      float Cs[9];
+      if (kCell) {
+        const float dold[3] = {cell_dinv(p, xm.x), cell_dinv(p, xm.y), cell_dinv(p, xm.z)};
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Cs[k] = C[k] * dold[k / 3];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Cs[k] = C[k];
+      }
       xm.x += vel[0] * p.dt;
       xm.y += vel[1] * p.dt;
       xm.z += vel[2] * p.dt;
@@ -1730,7 +1914,7 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int r = 0; r < 3; ++r)
-          Fn[3 * c + r] = F[3 * c + r] + p.dt * (C[r] * F[3 * c] + C[3 + r] * F[3 * c + 1] + C[6 + r] * F[3 * c + 2]);
+          Fn[3 * c + r] = F[3 * c + r] + p.dt * (Cs[r] * F[3 * c] + Cs[3 + r] * F[3 * c + 1] + Cs[6 + r] * F[3 * c + 2]);
       // trial-state log for the closure's training set
       if (!kBatch && s.aux.log_period > 0 && active && p.mat.model != 0 &&
           ((unsigned)id + (unsigned)substep) % (unsigned)s.aux.log_period == 0u) {
@@ -1758,7 +1942,16 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
       s.nxt.v[slot] = make_float4(vel[0], vel[1], vel[2], 0.f);
 #pragma unroll
       for (int k = 0; k < 9; ++k) s.nxt.C[k * cap + slot] = C[k];
-      if (!queued) {
+      if (kCell) {
+        // the affine term of the next P2C2G, from the new position and F (P2C2G.hpp:86-146)
+        const float dnew[3] = {cell_dinv(p, xm.x), cell_dinv(p, xm.y), cell_dinv(p, xm.z)};
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          s.nxt.A[k * cap + slot] = (xm.w * C[k] - p.dt * tau[k]) * dnew[k / 3];
+          s.nxt.F[k * cap + slot] = Fn[k];
+        }
+        if (s.nxt.plastic) s.nxt.plastic[slot] = pl;
+      } else if (!queued) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
           s.nxt.A[k * cap + slot] = xm.w * C[k] - p.kappa * tau[k];
@@ -2561,13 +2754,32 @@ cudaError_t prepare_kernels() {
   e = cudaFuncSetAttribute(k_g2p<false, true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)g2p_smem_bytes(128));
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_g2p<false, false, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)g2p_smem_bytes(128));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_g2p<false, false, kThreads, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)g2p_smem_bytes(kThreads));
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_g2p<false, false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)g2p_smem_bytes(128));
 }
 
 cudaError_t launch_p2g(scene_device &s, cudaStream_t st) {
+  if (s.prm.transfer == kTransferCell) return launch_p2c2g(s, 0, st);
   const int per_sm = s.prm.p2g_ctas_per_sm > 0 ? s.prm.p2g_ctas_per_sm : kP2GMinCtas;
   k_p2g<<<num_sms() * per_sm, kP2GThreads, kP2GSmemBytes, st>>>(s);
+  return cudaGetLastError();
+}
+
+// part 0: P2C2GTransfer from the stored affine term; 1 (momentum) and 2 (force): the part's
+// affine term is formed first, into the next buffer's A (G2C2P rewrites it)
+cudaError_t launch_p2c2g(scene_device &s, int part, cudaStream_t st) {
+  const float *affine = s.cur.A;
+  if (part != 0) {
+    k_cell_affine<<<num_sms() * 4, kThreads, 0, st>>>(s, part, s.nxt.A);
+    affine = s.nxt.A;
+  }
+  k_p2c2g<<<num_sms() * 2, kCellThreads, 0, st>>>(s, affine, part == 2 ? 0 : 1);
   return cudaGetLastError();
 }
 
@@ -2581,6 +2793,11 @@ cudaError_t launch_g2p(scene_device &s, cudaStream_t st) {
   const int per_sm = s.prm.g2p_ctas_per_sm > 0 ? s.prm.g2p_ctas_per_sm : 3;
   const int grid = num_sms() * per_sm;
   const bool small = s.prm.g2p_threads == 128;
+  if (s.prm.transfer == kTransferCell) {
+    small ? k_g2p<false, false, 128, true><<<grid, 128, g2p_smem_bytes(128), st>>>(s)
+          : k_g2p<false, false, kThreads, true><<<grid, kThreads, g2p_smem_bytes(kThreads), st>>>(s);
+    return cudaGetLastError();
+  }
   if (s.aux.learned) {
     // G2P queues the projections, the network runs over the queue on the tensor cores, and
     // k_closure_finish completes the queued particles
@@ -2689,7 +2906,10 @@ cudaError_t launch_import_tilevector(scene_device &s, const float *base, int nch
 }
 
 cudaError_t launch_prime(scene_device &s, cudaStream_t st) {
-  k_prime<<<num_sms() * 4, kThreads, 0, st>>>(s);
+  if (s.prm.transfer == kTransferCell)
+    k_cell_affine<<<num_sms() * 4, kThreads, 0, st>>>(s, 0, s.cur.A);
+  else
+    k_prime<<<num_sms() * 4, kThreads, 0, st>>>(s);
   return cudaGetLastError();
 }
 
