@@ -712,6 +712,58 @@ def extra_leg(args, name, ws, local, stream, learned: bool):
     return out
 
 
+def cell_leg(args, ws, local, stream, cpu: bool) -> dict:
+    """The cell-centric transfer pair (P2C2GTransfer / G2C2PTransfer) against the APIC pair on
+    the benchmark's two-box geometry in fixed corotated (the pair has no plasticity branch):
+    30,089,900 particles, each pair measured like the main leg, and the reference's own cell
+    path under zs::omp_exec on a bounded slab."""
+    import dataclasses
+
+    import zsmpm_b200 as zs
+    from zsmpm_b200 import scenes
+    spec = dataclasses.replace(scenes.config2(), name="fc_two_boxes_dx256",
+                               material=scenes.MaterialSpec(model=zs.FIXED_COROTATED, E=3.5e5, nu=0.3, rho=2200.0))
+    p = scenes.generate(spec)
+    w = Workload(zs, spec, p, None, local, stream)
+    try:
+        apic = plain_leg(args, w, ws, local, with_e2e=False)
+        w.sc.set_transfer("cell")
+        cell = plain_leg(args, w, ws, local, with_e2e=False)
+    finally:
+        w.close()
+    peak, peak_kind = hbm_peak()
+    n, nb = cell["particles"], cell["active_blocks"]
+    # P2C2G's algorithmic bytes: x|m 16, v 12 and the affine term 36 per particle read once, and
+    # the block's 512 nodes x 4 channels written
+    p2c2g_bytes = n * 64 + nb * 512 * 16
+    p2c2g_ms = cell["stage_ms"]["p2g"]
+    out = {"workload": "fc_two_boxes_dx256_8ppc", "particles": n, "material": "fixed_corotated",
+           "apic": {k: apic[k] for k in ("value", "ms_per_step", "stage_ms", "launch_shapes", "clocks")},
+           "cell": {k: cell[k] for k in ("value", "ms_per_step", "stage_ms", "launch_shapes", "clocks",
+                                         "gpu_launches")},
+           "cell_vs_apic": cell["value"] / apic["value"],
+           "p2c2g_roofline": {"kernel": "k_p2g (cell variant: P2C2G)", "bound": "hbm",
+                              "algorithmic_bytes_per_launch": p2c2g_bytes,
+                              "achieved": p2c2g_bytes / (p2c2g_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                              "frac": p2c2g_bytes / (p2c2g_ms * 1e-3) / 1e9 / peak,
+                              "peak_kind": f"{peak_kind} copy bandwidth", "launch_ms": p2c2g_ms},
+           "g2c2p_roofline": {**cell["g2p_roofline"], "kernel": "k_g2p (cell variant: G2C2P)"}}
+    if cpu:
+        try:
+            from oracle import reference
+            if reference.available():
+                threads = os.cpu_count() or 1
+                q, desc = cpu_baseline_sample(spec, p, min(args.ref_particles, 500_000))
+                r = reference.run(spec, q, args.ref_steps, policy=reference.POLICY_OMP, threads=threads,
+                                  cap_blocks=0, cell=True, timeout=900)
+                out["cpu_baseline"] = {"value": q.n * args.ref_steps / r.seconds, "unit": UNIT, "cores": threads,
+                                       "kind": "reference",
+                                       "sample": f"{desc}, {args.ref_steps} substeps of the cell pair, zs::omp_exec"}
+        except Exception as exc:
+            out["cpu_baseline"] = {"value": None, "sample": f"failed: {exc}"}
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -727,7 +779,7 @@ def main(argv=None):
     ap.add_argument("--no-implicit", action="store_true", help="skip the implicit-system leg")
     ap.add_argument("--no-extra", action="store_true",
                     help="measure only --scene (by default the sand scene run also measures the 16 M snow "
-                         "scene, plain and learned, and the 256-scene batch)")
+                         "scene, plain and learned, the 256-scene batch and the cell-centric transfer pair)")
     # 20 M training states in all, as the learned-closure configuration states: random trial
     # states plus states logged from the plain path
     ap.add_argument("--train-random", type=int, default=16_000_000)
@@ -783,6 +835,8 @@ def main(argv=None):
     if args.scene == "dp" and not args.no_extra:
         legs["snow16m"] = extra_leg(args, "snow16m", ws, local, stream, learned=not args.no_learned)
         legs["batch256"] = extra_leg(args, "batch256", ws, local, stream, learned=False)
+        legs["cell_transfer"] = cell_leg(args, ws, local, stream,
+                                         cpu=rank == 0 and ws == 1 and not args.no_cpu_baseline)
 
     # ---------------------------------------------------------------- CPU baseline (rank 0, N=1)
     cpu = None

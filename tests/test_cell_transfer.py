@@ -76,11 +76,11 @@ def test_cell_graph_run_matches_stages(zs, gpu):
         b.status()
         ra, rb = a.download(), b.download()
     # the float atomics of P2C2G sum in another order in each run: v agrees to rounding, and B,
-    # a small difference of nearly equal node velocities (the box moves rigidly), to 1e-4
+    # a small difference of nearly equal node velocities (the box moves rigidly), to 3e-4
     assert rel_l2(ra.x, rb.x) < 1e-7
     assert rel_l2(ra.v, rb.v) < 1e-6
-    assert rel_l2(ra.C, rb.C) < 1e-4
-    assert rel_l2(ra.F - p.F, rb.F - p.F) < 1e-4
+    assert rel_l2(ra.C, rb.C) < 3e-4
+    assert rel_l2(ra.F - p.F, rb.F - p.F) < 3e-4
 
 
 @pytest.mark.gpu

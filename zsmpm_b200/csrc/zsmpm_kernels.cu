@@ -858,33 +858,55 @@ __device__ __forceinline__ void bspline_weights(float f, float *w) {
   w[2] = 0.5f * f2 * f2;
 }
 
+// The node weights of the cell-centric pair (P2C2GTransfer): a particle's tent weights to the
+// centers of its two cells per axis, 1/2 - fx and 1/2 + fx with fx = x/dx - floor(x/dx + 1/2),
+// each passed half to either corner, over the nodes base .. base + 2 (base = floor(x/dx + 1/2)
+// - 1, f = x/dx - base = fx + 1).
+__device__ __forceinline__ void cell_weights(float f, float *w) {
+  w[0] = 0.75f - 0.5f * f;
+  w[1] = 0.5f;
+  w[2] = 0.5f * f - 0.25f;
+}
+
 struct p2g_raw {
   float4 xm, v;
   float A[9];
 };
 
-__device__ __forceinline__ void p2g_load(const scene_device &s, int i, p2g_raw &r) {
+__device__ __forceinline__ void p2g_load(const scene_device &s, const float *affine, int i, p2g_raw &r) {
   r.xm = s.cur.xm[i];
   r.v = s.cur.v[i];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) r.A[k] = s.cur.A[(size_t)k * s.prm.cap + i];
+  for (int k = 0; k < 9; ++k) r.A[k] = affine[(size_t)k * s.prm.cap + i];
 }
 
+// kCell: the cell-centric pair's weights and stencil origin; with_mass = false leaves the mass
+// and the m v term out (P2C2GTransferForce)
+template <bool kCell>
 __device__ __forceinline__ void p2g_prepare(const scene_params &p, const p2g_raw &r, int ox, int oy, int oz,
-                                            p2g_particle &pp) {
-  // x / dx as P2G.hpp:62 divides; a multiplication when dx is a power of two (the same number)
-  const float X[3] = {over_dx(p, r.xm.x), over_dx(p, r.xm.y), over_dx(p, r.xm.z)};
+                                            p2g_particle &pp, bool with_mass) {
+  // APIC: x / dx as P2G.hpp:62 divides (a multiplication when dx is a power of two, the same
+  // number).  The cell pair: the index bucket floor(x * (1/dx) + 1/2) as the binning keys it.
+  float X[3];
+  if (kCell) {
+    X[0] = r.xm.x * p.inv_dx, X[1] = r.xm.y * p.inv_dx, X[2] = r.xm.z * p.inv_dx;
+  } else {
+    X[0] = over_dx(p, r.xm.x), X[1] = over_dx(p, r.xm.y), X[2] = over_dx(p, r.xm.z);
+  }
   float lp[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const float base = floorf(X[d] - 0.5f);
+    const float base = kCell ? floorf(X[d] + 0.5f) - 1.f : floorf(X[d] - 0.5f);
     const float f = X[d] - base;
     pp.hb[d] = (int)base - (d == 0 ? ox : d == 1 ? oy : oz);
     pp.f[d] = f;
-    bspline_weights(f, pp.w[d]);
+    if (kCell)
+      cell_weights(f, pp.w[d]);
+    else
+      bspline_weights(f, pp.w[d]);
     lp[d] = f * p.dx;
   }
-  pp.m = r.xm.w;
+  pp.m = with_mass ? r.xm.w : 0.f;
   const float vel[3] = {r.v.x, r.v.y, r.v.z};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -948,13 +970,20 @@ constexpr size_t kP2GSmemBytes = sizeof(float) * kGridChannels * kP2GHaloNodes +
                                  sizeof(unsigned char) * 2 * kP2GMap;
 
 // the weights and the mass of staged rank r of cell cl
+template <bool kCell>
 __device__ __forceinline__ void staged_weights(const float4 (*stg)[kP2GRanks][kP2GRow], int r, int cl, float (&w)[3][3],
                                                float &m) {
   if (kP2GStageF) {
     const float4 fm = stg[0][r][cl];
-    bspline_weights(fm.x, w[0]);
-    bspline_weights(fm.y, w[1]);
-    bspline_weights(fm.z, w[2]);
+    if (kCell) {
+      cell_weights(fm.x, w[0]);
+      cell_weights(fm.y, w[1]);
+      cell_weights(fm.z, w[2]);
+    } else {
+      bspline_weights(fm.x, w[0]);
+      bspline_weights(fm.y, w[1]);
+      bspline_weights(fm.z, w[2]);
+    }
     m = fm.w;
   } else {
     const float4 wa = stg[0][r][cl], wb = stg[1][r][cl], wc = stg[2][r][cl];
@@ -965,7 +994,11 @@ __device__ __forceinline__ void staged_weights(const float4 (*stg)[kP2GRanks][kP
   }
 }
 
-__global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s) {
+// kCell: P2C2GTransfer of the cell-centric pair (below) with the pair's node weights and
+// affine term; `affine` is the affine term (A = m C - (4 dt/dx^2) tau for APIC), with_mass = 0
+// leaves the mass channel and the m v term out.
+template <bool kCell>
+__global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s, const float *affine, int with_mass) {
   extern __shared__ __align__(16) float p2g_smem[];
   float *sh = p2g_smem;
   auto stg = reinterpret_cast<float4(*)[kP2GRanks][kP2GRow]>(p2g_smem + kGridChannels * kP2GHaloNodes);
@@ -1069,15 +1102,15 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s
           const bool in2 = r2 >= 0 && r2 < kP2GRanks;
           if (!in1 && !in2) continue;
           p2g_raw ra, rb;
-          p2g_load(s, s.src[in1 ? slot : slot2], ra);
-          p2g_load(s, s.src[in2 ? slot2 : slot], rb);
+          p2g_load(s, affine, s.src[in1 ? slot : slot2], ra);
+          p2g_load(s, affine, s.src[in2 ? slot2 : slot], rb);
           p2g_particle pp;
           if (in1) {
-            p2g_prepare(s.prm, ra, ox, oy, oz, pp);
+            p2g_prepare<kCell>(s.prm, ra, ox, oy, oz, pp, with_mass != 0);
             stage_one(cl1, r1, pp);
           }
           if (in2) {
-            p2g_prepare(s.prm, rb, ox, oy, oz, pp);
+            p2g_prepare<kCell>(s.prm, rb, ox, oy, oz, pp, with_mass != 0);
             stage_one(cl2, r2, pp);
           }
         }
@@ -1094,7 +1127,7 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s
             // mass: W m (the warp is channel-uniform)
             for (int r = 0; r < cnt; ++r) {
               float w[3][3], m;
-              staged_weights(stg, r, my_cell, w, m);
+              staged_weights<kCell>(stg, r, my_cell, w, m);
 #pragma unroll
               for (int ii = 0; ii < 3; ++ii) {
                 const float wm = w[0][ii] * m;
@@ -1113,7 +1146,7 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s
             // momentum: W (q + ii ax + jj ay + kk az), in cell units of the node offset
             for (int r = 0; r < cnt; ++r) {
               float w[3][3], m_unused;
-              staged_weights(stg, r, my_cell, w, m_unused);
+              staged_weights<kCell>(stg, r, my_cell, w, m_unused);
               const float4 qa = stg[kP2GQ + d][r][my_cell];
               const float q = qa.x, ax = qa.y, ay = qa.z, az = qa.w;
               // wz (qij + kk az) = wz qij + cz[kk], cz = (0, wz1 az, 2 wz2 az): two operations
@@ -1179,8 +1212,13 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s
 // particles within dx of a cell's center x_c (per axis) carry the tent weight
 // W = prod (1 - |x_c - x_p| / dx), and a cell passes its sums to its 8 corner nodes (and takes
 // its velocity from them) with weight 1/8.  A particle's cells are those of the index buckets
-// floor(x / dx + 0.5) in {c, c + 1}^3 around it, i.e. the binning's cells c - 2 + {0,1}^3 (the
-// binning keys a particle by floor(x / dx + 0.5) - 2).
+// floor(x / dx + 0.5) in {c, c + 1}^3 around it.  The cells are linear stages between the
+// particles and the nodes, so each node receives sum_p w_p (m v + A (x_i - x_p)) with the
+// composed node weights of cell_weights, and each particle takes sum_i w_i v_i: P2C2G runs as
+// the staged P2G kernel with those weights (k_p2g<true>) and G2C2P as a variant of the G2P
+// kernel (k_g2p<..., true>), both without per-particle atomics.  (A literal cell-gather P2C2G,
+// one thread per cell walking its 8 buckets, measured 5.1 ms against 1.5 ms for P2G on 30 M
+// particles: its loads are dependent and scattered.)
 //
 // Per particle the pair carries x, m, v, F and B (the reference's C attribute) and, written at
 // the end of G2C2P for the next P2C2G, the affine term
@@ -1214,112 +1252,6 @@ __global__ void __launch_bounds__(kThreads) k_cell_affine(scene_device s, int pa
       const float mB = part == 2 ? 0.f : xm.w * s.cur.C[k * cap + i];
       const float f = part == 1 ? 0.f : p.dt * tau[k];
       out[k * cap + i] = (mB - f) * dinv[k / 3];
-    }
-  }
-}
-
-// P2C2G: one CTA of 512 threads per block (persistent), one thread per cell.  Stage 1: the
-// thread walks its cell's 8 buckets (particles within them in the binned order, which is upload
-// order within a cell) and sums W m, W m v, W A and W A (x_p - x_c).  Stage 2: the 8 corner nodes
-// receive 1/8 of (m, m v + A (x_i - x_c) - sum W A (x_p - x_c)), i.e. sum_p W/8 (m v + A (x_i -
-// x_p)), through a shared-memory halo of the block's 9^3 nodes, which is then added to the grid
-// (the nodes 8b + 8 belong to the neighbour blocks).  The cell-relative positions are the
-// reference's absolute-position sums rearranged; they keep the affine term from cancelling
-// against x ~ 0.5 in FP32.  with_mass = 0 (the force part alone) leaves the mass channel and
-// the m v term out, as P2C2GTransferForce does.
-constexpr int kCellThreads = 512;
-constexpr int kCellHalo = 9;
-constexpr int kCellHaloNodes = kCellHalo * kCellHalo * kCellHalo;
-
-__global__ void __launch_bounds__(kCellThreads, 2) k_p2c2g(scene_device s, const float *affine, int with_mass) {
-  __shared__ float sh[kGridChannels * kCellHaloNodes];
-  __shared__ int s_nb[8];  // the blocks at offsets {-1, 0}^3: index (ox + 1) * 4 + (oy + 1) * 2 + (oz + 1)
-  __shared__ int s_b;
-  const scene_params &p = s.prm;
-  const int nb = s.ctr[kCtrBlocks];
-  const size_t cap = (size_t)p.cap;
-  const int t = threadIdx.x;
-  const int lx = t >> 6, ly = (t >> 3) & 7, lz = t & 7;
-  for (int q = t; q < kGridChannels * kCellHaloNodes; q += blockDim.x) sh[q] = 0.f;
-  for (;;) {
-    const int w = grab_block(&s.ctr[kCtrWork + kWorkP2G], &s_b);  // also orders the halo's zeroing
-    if (w >= nb) break;
-    const int b = s.work_order[w];
-    const int3 key = unpack_key(s.blk_pk[b]);
-    if (t < 8) {
-      const int3 k = make_int3(key.x - 1 + (t >> 2), key.y - 1 + ((t >> 1) & 1), key.z - 1 + (t & 1));
-      s_nb[t] = t == 7 ? b : table_query(s, pack_key(k.x, k.y, k.z), k);
-    }
-    __syncthreads();
-    const int cx = key.x * 8 + lx, cy = key.y * 8 + ly, cz = key.z * 8 + lz;
-    const float pcx = ((float)cx + 0.5f) * p.dx, pcy = ((float)cy + 0.5f) * p.dx, pcz = ((float)cz + 0.5f) * p.dx;
-    float mc = 0.f, mv[3] = {0.f, 0.f, 0.f}, QD[9], QX[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-    for (int k = 0; k < 9; ++k) QD[k] = 0.f;
-#pragma unroll 1
-    for (int o = 0; o < 8; ++o) {
-      // bucket c + (ox, oy, oz) = binned cell c - 2 + (ox, oy, oz)
-      const int gx = lx - 2 + (o >> 2), gy = ly - 2 + ((o >> 1) & 1), gz = lz - 2 + (o & 1);
-      const int nbk = s_nb[(gx >= 0 ? 4 : 0) + (gy >= 0 ? 2 : 0) + (gz >= 0 ? 1 : 0)];
-      if (nbk < 0) continue;
-      const int cell = ((gx & 7) << 6) | ((gy & 7) << 3) | (gz & 7);
-      const int j0 = s.cell_start[nbk * 512 + cell];
-      const int j1 = cell < 511 ? s.cell_start[nbk * 512 + cell + 1] : s.block_start[nbk + 1];
-      for (int j = j0; j < j1; ++j) {
-        const int i = s.src[j];
-        const float4 xm = s.cur.xm[i];
-        const float rx = xm.x - pcx, ry = xm.y - pcy, rz = xm.z - pcz;  // x_p - x_c
-        if (fabsf(rx) > p.dx || fabsf(ry) > p.dx || fabsf(rz) > p.dx) continue;
-        const float W = (1.f - fabsf(rx * p.inv_dx)) * (1.f - fabsf(ry * p.inv_dx)) * (1.f - fabsf(rz * p.inv_dx));
-        float A[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) A[k] = affine[k * cap + i];
-        if (with_mass) {
-          const float4 v = s.cur.v[i];
-          const float wm = W * xm.w;
-          mc += wm;
-          mv[0] = fmaf(wm, v.x, mv[0]);
-          mv[1] = fmaf(wm, v.y, mv[1]);
-          mv[2] = fmaf(wm, v.z, mv[2]);
-        }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          QD[d] = fmaf(W, A[d], QD[d]);
-          QD[3 + d] = fmaf(W, A[3 + d], QD[3 + d]);
-          QD[6 + d] = fmaf(W, A[6 + d], QD[6 + d]);
-          QX[d] = fmaf(W, A[d] * rx + A[3 + d] * ry + A[6 + d] * rz, QX[d]);
-        }
-      }
-    }
-    // stage 2: corner (a, b, c) of the cell at x_c + (a - 1/2, b - 1/2, c - 1/2) dx
-    const float h = 0.5f * p.dx;
-#pragma unroll
-    for (int o = 0; o < 8; ++o) {
-      const float ex = (o >> 2) ? h : -h, ey = ((o >> 1) & 1) ? h : -h, ez = (o & 1) ? h : -h;
-      const int node = ((lx + (o >> 2)) * kCellHalo + ly + ((o >> 1) & 1)) * kCellHalo + lz + (o & 1);
-      if (with_mass) atomicAdd(&sh[node], 0.125f * mc);
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const float val = mv[d] + (QD[d] * ex + QD[3 + d] * ey + QD[6 + d] * ez) - QX[d];
-        atomicAdd(&sh[(1 + d) * kCellHaloNodes + node], 0.125f * val);
-      }
-    }
-    __syncthreads();
-    // flush: node (nx, ny, nz) of the halo is cell (n & 7) of block b + (n >= 8); each value is
-    // sent and the halo zeroed for the next block
-    for (int q = t; q < kGridChannels * kCellHaloNodes; q += blockDim.x) {
-      const int c = q / kCellHaloNodes, node = q - c * kCellHaloNodes;
-      const float val = sh[q];
-      if (val == 0.f) continue;
-      sh[q] = 0.f;
-      const int nx = node / (kCellHalo * kCellHalo), ny = (node / kCellHalo) % kCellHalo, nz = node % kCellHalo;
-      const int tb = s.nbr[b * 8 + ((nx >> 3) << 2) + ((ny >> 3) << 1) + (nz >> 3)];
-      if (tb < 0) {
-        set_status(s.ctr, kStatusMissingBlock);
-        continue;
-      }
-      const int cell = ((nx & 7) << 6) | ((ny & 7) << 3) | (nz & 7);
-      atomicAdd(&s.grid[((size_t)tb * kGridChannels + c) * 512 + cell], val);
     }
   }
 }
@@ -2733,9 +2665,13 @@ cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
 // per-device kernel attributes; called once per scene with its device current, before any
 // capture of its launches
 cudaError_t prepare_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
+  cudaError_t e = cudaFuncSetAttribute(k_p2g<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_p2g, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  e = cudaFuncSetAttribute(k_p2g<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_p2g<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_p2g<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_g2p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kG2P2GSmem);
   if (e != cudaSuccess) return e;
@@ -2767,7 +2703,7 @@ cudaError_t prepare_kernels() {
 cudaError_t launch_p2g(scene_device &s, cudaStream_t st) {
   if (s.prm.transfer == kTransferCell) return launch_p2c2g(s, 0, st);
   const int per_sm = s.prm.p2g_ctas_per_sm > 0 ? s.prm.p2g_ctas_per_sm : kP2GMinCtas;
-  k_p2g<<<num_sms() * per_sm, kP2GThreads, kP2GSmemBytes, st>>>(s);
+  k_p2g<false><<<num_sms() * per_sm, kP2GThreads, kP2GSmemBytes, st>>>(s, s.cur.A, 1);
   return cudaGetLastError();
 }
 
@@ -2779,7 +2715,8 @@ cudaError_t launch_p2c2g(scene_device &s, int part, cudaStream_t st) {
     k_cell_affine<<<num_sms() * 4, kThreads, 0, st>>>(s, part, s.nxt.A);
     affine = s.nxt.A;
   }
-  k_p2c2g<<<num_sms() * 2, kCellThreads, 0, st>>>(s, affine, part == 2 ? 0 : 1);
+  const int per_sm = s.prm.p2g_ctas_per_sm > 0 ? s.prm.p2g_ctas_per_sm : kP2GMinCtas;
+  k_p2g<true><<<num_sms() * per_sm, kP2GThreads, kP2GSmemBytes, st>>>(s, affine, part == 2 ? 0 : 1);
   return cudaGetLastError();
 }
 
