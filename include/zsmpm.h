@@ -458,13 +458,18 @@ ZSMPM_API zsmpm_status zsmpm_batch_num_scenes(const zsmpm_scene *s, int32_t *out
 typedef struct {
   int32_t g2p_threads;      /* G2P CTA size: 128 or 256 (0 = default 256) */
   int32_t g2p_ctas_per_sm;  /* persistent G2P CTAs per SM, 1-6 (0 = default: 3, learned 2) */
-  int32_t p2g_ctas_per_sm;  /* persistent P2G CTAs per SM, 1-4 (0 = default 3) */
+  int32_t p2g_ctas_per_sm;  /* persistent P2G CTAs per SM, 1-4 (0 = the staging depth's
+                               default: 4 for 8 ranks, 3 for 12, 2 for 16) */
   float g2p_ms, p2g_ms;     /* stage times of the chosen shapes (autotune output) */
+  int32_t p2g_ranks;        /* P2G staging depth: particles per cell staged per round, 8, 12 or
+                               16 (0 = 12); deeper staging means fewer rounds on dense cells and
+                               more shared memory per CTA */
 } zsmpm_tuning;
 
-/* Times G2P over CTA size x CTAs per SM and P2G over CTAs per SM on the uploaded particles
- * (one untimed and `trials` timed substeps per candidate; this advances the simulation by
- * those substeps), keeps the fastest of each and returns them in *out (optional). */
+/* Times G2P over CTA size x CTAs per SM, and P2G over staging depth x CTAs per SM, on the
+ * uploaded particles (one untimed and `trials` timed substeps per candidate; this advances the
+ * simulation by those substeps), keeps the fastest of each and returns them in *out
+ * (optional). */
 ZSMPM_API zsmpm_status zsmpm_autotune(zsmpm_scene *s, int32_t trials, zsmpm_tuning *out, void *stream);
 ZSMPM_API zsmpm_status zsmpm_set_tuning(zsmpm_scene *s, const zsmpm_tuning *t);
 

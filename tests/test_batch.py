@@ -90,7 +90,8 @@ def test_autotune_picks_a_valid_shape_and_keeps_results(zs, gpu):
     a = batch.Batch(specs, parts)
     choice = a.autotune(trials=1)
     assert choice["g2p_threads"] in (128, 256)
-    assert 1 <= choice["g2p_ctas_per_sm"] <= 6 and 1 <= choice["p2g_ctas_per_sm"] <= 2
+    assert 1 <= choice["g2p_ctas_per_sm"] <= 6 and 1 <= choice["p2g_ctas_per_sm"] <= 4
+    assert choice["p2g_ranks"] in (8, 12, 16)
     assert choice["g2p_ms"] > 0 and choice["p2g_ms"] > 0
     a.upload(parts)
     a.run(20)
@@ -168,3 +169,39 @@ def test_learned_closure_on_a_batch(zs, gpu):
             assert np.max(np.abs(g.x - r.x)) <= 1e-6  # the plain path, up to the P2G summation order
         else:
             assert err < 0.05, (sp.material.friction_deg, err)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("transfer", ["apic", "cell"])
+def test_p2g_staging_depths_agree(zs, gpu, transfer):
+    """P2G (and P2C2G) with 8, 12 and 16 staged particles per cell and round, at the CTA counts
+    the tuner tries, give the default's grid up to the order of the float sums.  The box is
+    compressed so that cells hold more than 8 particles and the shallow staging runs several
+    rounds."""
+    from zsmpm_b200 import scenes
+    spec = scenes.small_scene(model=0, n_side=0.1, velocity=(0.0, 0.0, 0.0))
+    p = scenes.generate(spec)
+    c = p.x.mean(0)
+    p.x = (c + (p.x - c) * np.float32(0.6)).astype(np.float32)  # 8 ppc -> ~37 ppc
+    rng = np.random.default_rng(2)
+    p.v = rng.normal(size=p.v.shape).astype(np.float32)
+    p.C = (rng.normal(size=p.C.shape) * 0.1).astype(np.float32)
+    grids = {}
+    for ranks, ctas in [(12, 0), (8, 4), (8, 3), (12, 2), (16, 2), (16, 1)]:
+        with zs.Scene(spec, p, transfer=transfer) as sc:
+            sc.set_tuning(p2g_ctas_per_sm=ctas, p2g_ranks=ranks)
+            sc.activate_blocks()
+            sc.bin_particles()
+            sc.p2g()
+            sc.status()
+            grids[(ranks, ctas)] = sc.download_grid()
+    k0, g0 = grids[(12, 0)]
+    for key, (k, g) in grids.items():
+        assert np.array_equal(k, k0), key
+        assert np.max(np.abs(g[:, 0] - g0[:, 0])) <= 1e-6 * np.abs(g0[:, 0]).max(), key
+        assert np.max(np.abs(g[:, 1:] - g0[:, 1:])) <= 1e-5 * np.abs(g0[:, 1:]).max(), key
+    with zs.Scene(spec, p) as sc:
+        with pytest.raises(zs.ZsmpmError):
+            sc.set_tuning(p2g_ranks=10)
+        with pytest.raises(zs.ZsmpmError):
+            sc.set_tuning(p2g_ctas_per_sm=3, p2g_ranks=16)  # 88 KB of staging: at most 2 resident

@@ -299,8 +299,11 @@ class Scene:
         t = _abi.Tuning()
         _abi.check(self._lib.zsmpm_autotune(self._h, trials, C.byref(t), C.c_void_p(stream)), "autotune")
         return {"g2p_threads": t.g2p_threads, "g2p_ctas_per_sm": t.g2p_ctas_per_sm,
-                "p2g_ctas_per_sm": t.p2g_ctas_per_sm, "g2p_ms": t.g2p_ms, "p2g_ms": t.p2g_ms}
+                "p2g_ctas_per_sm": t.p2g_ctas_per_sm, "p2g_ranks": t.p2g_ranks, "g2p_ms": t.g2p_ms,
+                "p2g_ms": t.p2g_ms}
 
-    def set_tuning(self, g2p_threads: int = 0, g2p_ctas_per_sm: int = 0, p2g_ctas_per_sm: int = 0) -> None:
-        t = _abi.Tuning(g2p_threads=g2p_threads, g2p_ctas_per_sm=g2p_ctas_per_sm, p2g_ctas_per_sm=p2g_ctas_per_sm)
+    def set_tuning(self, g2p_threads: int = 0, g2p_ctas_per_sm: int = 0, p2g_ctas_per_sm: int = 0,
+                   p2g_ranks: int = 0) -> None:
+        t = _abi.Tuning(g2p_threads=g2p_threads, g2p_ctas_per_sm=g2p_ctas_per_sm, p2g_ctas_per_sm=p2g_ctas_per_sm,
+                        p2g_ranks=p2g_ranks)
         _abi.check(self._lib.zsmpm_set_tuning(self._h, C.byref(t)), "set_tuning")

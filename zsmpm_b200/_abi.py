@@ -67,7 +67,7 @@ class BhtView(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("g2p_threads", C.c_int32), ("g2p_ctas_per_sm", C.c_int32), ("p2g_ctas_per_sm", C.c_int32),
-                ("g2p_ms", C.c_float), ("p2g_ms", C.c_float)]
+                ("g2p_ms", C.c_float), ("p2g_ms", C.c_float), ("p2g_ranks", C.c_int32)]
 
 
 MLP_PARAMS = 9158  # 6 -> 64 -> 64 -> 64 -> 6

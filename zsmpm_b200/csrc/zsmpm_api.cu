@@ -1219,16 +1219,21 @@ ZSMPM_API zsmpm_status zsmpm_autotune(zsmpm_scene *s, int32_t trials, zsmpm_tuni
         best.g2p_ctas_per_sm = b;
       }
     }
+  // P2G: staging depth x CTAs per SM, up to what the depth's shared memory lets stay resident
+  // (8 ranks: 55 KB, 4 CTAs; 12: 72 KB, 3; 16: 88 KB, 2)
   float best_p2g = 3.4e38f;
+  const int p2g_shapes[6][2] = {{12, 3}, {12, 2}, {8, 4}, {8, 3}, {16, 2}, {16, 1}};
   if (st == ZSMPM_OK)
-    for (int b : {2, 3, 4}) {
-      p.p2g_ctas_per_sm = b;
+    for (const auto &shape : p2g_shapes) {
+      p.p2g_ranks = shape[0];
+      p.p2g_ctas_per_sm = shape[1];
       float ms = 0.f;
       st = time_stage(2, &ms);
       if (st != ZSMPM_OK) break;
       if (ms < best_p2g) {
         best_p2g = ms;
-        best.p2g_ctas_per_sm = b;
+        best.p2g_ranks = shape[0];
+        best.p2g_ctas_per_sm = shape[1];
       }
     }
   s->timing = was_timing;
@@ -1236,6 +1241,7 @@ ZSMPM_API zsmpm_status zsmpm_autotune(zsmpm_scene *s, int32_t trials, zsmpm_tuni
   p.g2p_threads = best.g2p_threads;
   p.g2p_ctas_per_sm = best.g2p_ctas_per_sm;
   p.p2g_ctas_per_sm = best.p2g_ctas_per_sm;
+  p.p2g_ranks = best.p2g_ranks;
   best.g2p_ms = best_g2p;
   best.p2g_ms = best_p2g;
   invalidate_graphs(s);
@@ -1249,13 +1255,20 @@ ZSMPM_API zsmpm_status zsmpm_set_tuning(zsmpm_scene *s, const zsmpm_tuning *t) {
   if (st != ZSMPM_OK) return st;
   if (!t) return fail(ZSMPM_ERR_INVALID_ARG, "null tuning");
   if ((t->g2p_threads != 0 && t->g2p_threads != 128 && t->g2p_threads != 256) || t->g2p_ctas_per_sm < 0 ||
-      t->g2p_ctas_per_sm > 6 || t->p2g_ctas_per_sm < 0 || t->p2g_ctas_per_sm > 4)
+      t->g2p_ctas_per_sm > 6 || t->p2g_ctas_per_sm < 0 || t->p2g_ctas_per_sm > 4 ||
+      (t->p2g_ranks != 0 && t->p2g_ranks != 8 && t->p2g_ranks != 12 && t->p2g_ranks != 16))
     return fail(ZSMPM_ERR_INVALID_ARG, "tuning out of range");
+  // more CTAs than the staging depth's shared memory lets stay resident would queue, not run
+  const int ranks = t->p2g_ranks ? t->p2g_ranks : 12;
+  const int max_p2g = ranks == 8 ? 4 : ranks == 12 ? 3 : 2;
+  if (t->p2g_ctas_per_sm > max_p2g)
+    return fail(ZSMPM_ERR_INVALID_ARG, "p2g_ctas_per_sm beyond what the staging depth's shared memory allows");
   if (s->dev.aux.learned && t->g2p_threads == 128)
     return fail(ZSMPM_ERR_INVALID_ARG, "the learned G2P runs 256-thread CTAs");
   s->dev.prm.g2p_threads = t->g2p_threads;
   s->dev.prm.g2p_ctas_per_sm = t->g2p_ctas_per_sm;
   s->dev.prm.p2g_ctas_per_sm = t->p2g_ctas_per_sm;
+  s->dev.prm.p2g_ranks = t->p2g_ranks;
   invalidate_graphs(s);
   return ZSMPM_OK;
 }

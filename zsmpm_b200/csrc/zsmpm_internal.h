@@ -90,6 +90,7 @@ struct scene_params {
   // launch shapes (set by the autotuner; 0 = default)
   int g2p_threads;                  // 128 or 256
   int g2p_ctas_per_sm, p2g_ctas_per_sm;
+  int p2g_ranks;                    // P2G staging depth per round: 8, 12 or 16 (0 = 12)
   // incremental binning
   int mover_cap;                    // entries of the mover list
   int bin_full;                     // 1: this binning launch recounts every particle

@@ -811,31 +811,26 @@ __global__ void __launch_bounds__(kThreads) k_inc_finalize(scene_device s) {
 //  2. one thread per (cell, channel) sums the cell's particles into 27 registers -- all
 //     particles of a cell share the same 27 stencil nodes -- and adds them to a halo of the
 //     grid in shared memory.
-// Ranks are staged kP2GRanks at a time: a chunk with a cell of more particles runs phases 1-2
-// again for the next ranks (a round), so that no particle needs the slow per-node path for
-// lack of staging room and the staging stays small enough for three CTAs per SM.
+// Ranks are staged R at a time: a chunk with a cell of more particles runs phases 1-2 again for
+// the next ranks (a round), so that no particle needs the slow per-node path for lack of
+// staging room and the staging stays small enough for several CTAs per SM.
 // The halo holds the nodes the block's particles reach: a particle binned in cell c of the
 // block has its stencil origin at c + 1 (SparsityOp.hpp:72-77 against P2G.hpp:62-66), so its
 // nodes lie in [8b + 1, 8b + 11) per axis; the halo spans exactly that in x and y and
 // [8b, 8b + 12) in z, so that the flush moves whole 16-byte quads of the neighbour blocks.
 // Grid channels: m and p = sum W (m v + A (x_i - x_p)), the reference's mv + rhs
 // (P2G.hpp:108-125) with A = m C - (4 dt/dx^2) tau precomputed by G2P.
-// Staging variants (compile-time): ZSMPM_P2G_RANKS particles per cell per round,
-// ZSMPM_P2G_STAGE_F = 1 stages the particle's fractional position in the cell instead of its
-// nine weights (phase 2 recomputes them: more arithmetic, a third less shared memory), and
-// ZSMPM_P2G_MIN_CTAS resident CTAs per SM that the register budget is cut for.
-#ifndef ZSMPM_P2G_RANKS
-#define ZSMPM_P2G_RANKS 12
-#endif
+// The staging depth is a tile choice of the autotuner: R particles per cell are staged per
+// round, with the register budget cut for the CTAs per SM that R's shared memory allows --
+// 8 ranks (55 KB) for 4 CTAs per SM, 12 (72 KB, the default) for 3, 16 (88 KB) for 2.
+// ZSMPM_P2G_STAGE_F = 1 (compile-time) stages the particle's fractional position in the cell
+// instead of its nine weights (phase 2 recomputes them: more arithmetic, a third less shared
+// memory).
 #ifndef ZSMPM_P2G_STAGE_F
 #define ZSMPM_P2G_STAGE_F 1
 #endif
-#ifndef ZSMPM_P2G_MIN_CTAS
-#define ZSMPM_P2G_MIN_CTAS 3
-#endif
 constexpr int kP2GChunk = 64;     // cells per chunk
-constexpr int kP2GRanks = ZSMPM_P2G_RANKS;  // particles per cell staged per round
-constexpr int kP2GMinCtas = ZSMPM_P2G_MIN_CTAS;
+constexpr int kP2GRanksDefault = 12;  // particles per cell staged per round, unless tuned
 constexpr bool kP2GStageF = ZSMPM_P2G_STAGE_F != 0;
 constexpr int kP2GRow = kP2GChunk + 1;  // padded row of float4: rank r of cell c at bank 4 (r + c) % 32
 constexpr int kP2GThreads = 256;  // 4 channels x 64 cells
@@ -964,14 +959,14 @@ __device__ __forceinline__ void p2g_direct(const scene_device &s, float *sh, con
 // fractional position: fx fy fz m | (q ax ay az) x 3
 constexpr int kP2GVec = kP2GStageF ? 4 : 6;
 constexpr int kP2GQ = kP2GVec - 3;  // first momentum field
-constexpr size_t kP2GSmemBytes = sizeof(float) * kGridChannels * kP2GHaloNodes +
-                                 sizeof(float4) * kP2GVec * kP2GRanks * kP2GRow +
-                                 sizeof(int) * 2 * (kP2GChunk + 1) + sizeof(int) * 4 +
-                                 sizeof(unsigned char) * 2 * kP2GMap;
+constexpr size_t p2g_smem_bytes(int ranks) {
+  return sizeof(float) * kGridChannels * kP2GHaloNodes + sizeof(float4) * kP2GVec * ranks * kP2GRow +
+         sizeof(int) * 2 * (kP2GChunk + 1) + sizeof(int) * 4 + sizeof(unsigned char) * 2 * kP2GMap;
+}
 
 // the weights and the mass of staged rank r of cell cl
-template <bool kCell>
-__device__ __forceinline__ void staged_weights(const float4 (*stg)[kP2GRanks][kP2GRow], int r, int cl, float (&w)[3][3],
+template <bool kCell, int R>
+__device__ __forceinline__ void staged_weights(const float4 (*stg)[R][kP2GRow], int r, int cl, float (&w)[3][3],
                                                float &m) {
   if (kP2GStageF) {
     const float4 fm = stg[0][r][cl];
@@ -996,14 +991,15 @@ __device__ __forceinline__ void staged_weights(const float4 (*stg)[kP2GRanks][kP
 
 // kCell: P2C2GTransfer of the cell-centric pair (below) with the pair's node weights and
 // affine term; `affine` is the affine term (A = m C - (4 dt/dx^2) tau for APIC), with_mass = 0
-// leaves the mass channel and the m v term out.
-template <bool kCell>
-__global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s, const float *affine, int with_mass) {
+// leaves the mass channel and the m v term out.  R staged ranks per round, registers cut for
+// MinCtas CTAs per SM.
+template <bool kCell, int R, int MinCtas>
+__global__ void __launch_bounds__(kP2GThreads, MinCtas) k_p2g(scene_device s, const float *affine, int with_mass) {
   extern __shared__ __align__(16) float p2g_smem[];
   float *sh = p2g_smem;
-  auto stg = reinterpret_cast<float4(*)[kP2GRanks][kP2GRow]>(p2g_smem + kGridChannels * kP2GHaloNodes);
+  auto stg = reinterpret_cast<float4(*)[R][kP2GRow]>(p2g_smem + kGridChannels * kP2GHaloNodes);
   int *s_cs = reinterpret_cast<int *>(p2g_smem + kGridChannels * kP2GHaloNodes +
-                                      4 * kP2GVec * kP2GRanks * kP2GRow);
+                                      4 * kP2GVec * R * kP2GRow);
   int *const s_wmax = s_cs + 2 * (kP2GChunk + 1);  // per chunk parity: the largest cell count of each half
   unsigned char *const s_map0 = reinterpret_cast<unsigned char *>(s_wmax + 4);
   __shared__ int s_b;
@@ -1050,8 +1046,8 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s
       for (int round = 0;; ++round) {
         __syncthreads();  // previous staging consumed, this chunk's starts loaded, halo zeroed
         const int maxc = max(s_wmax[2 * par], s_wmax[2 * par + 1]);
-        const int rlo = round * kP2GRanks;
-        const bool last = rlo + kP2GRanks >= maxc;
+        const int rlo = round * R;
+        const bool last = rlo + R >= maxc;
         // ---- phase 1: consecutive threads take consecutive slots (coalesced gathers); the
         // slots whose rank falls in this round's window are staged
         const int c0 = s_cs[0], c1 = s_cs[kP2GChunk];
@@ -1093,13 +1089,13 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s
         for (int slot = c0 + t; slot < c1; slot += 2 * blockDim.x) {
           const int slot2 = slot + blockDim.x;
           const int cl1 = cell_of_slot(slot), r1 = slot - s_cs[cl1] - rlo;
-          const bool in1 = r1 >= 0 && r1 < kP2GRanks;
+          const bool in1 = r1 >= 0 && r1 < R;
           int cl2 = 0, r2 = -1;
           if (slot2 < c1) {
             cl2 = cell_of_slot(slot2);
             r2 = slot2 - s_cs[cl2] - rlo;
           }
-          const bool in2 = r2 >= 0 && r2 < kP2GRanks;
+          const bool in2 = r2 >= 0 && r2 < R;
           if (!in1 && !in2) continue;
           p2g_raw ra, rb;
           p2g_load(s, affine, s.src[in1 ? slot : slot2], ra);
@@ -1117,7 +1113,7 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s
         __syncthreads();
         if (last && chunk + 1 < 512 / kP2GChunk) fill(chunk + 1);
         // ---- phase 2: thread (cell, channel) sums the staged particles of its cell
-        const int cnt = min(s_cs[my_cell + 1] - s_cs[my_cell] - rlo, kP2GRanks);
+        const int cnt = min(s_cs[my_cell + 1] - s_cs[my_cell] - rlo, R);
         if (cnt > 0) {
           float acc[27];
 #pragma unroll
@@ -1127,7 +1123,7 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s
             // mass: W m (the warp is channel-uniform)
             for (int r = 0; r < cnt; ++r) {
               float w[3][3], m;
-              staged_weights<kCell>(stg, r, my_cell, w, m);
+              staged_weights<kCell, R>(stg, r, my_cell, w, m);
 #pragma unroll
               for (int ii = 0; ii < 3; ++ii) {
                 const float wm = w[0][ii] * m;
@@ -1146,7 +1142,7 @@ __global__ void __launch_bounds__(kP2GThreads, kP2GMinCtas) k_p2g(scene_device s
             // momentum: W (q + ii ax + jj ay + kk az), in cell units of the node offset
             for (int r = 0; r < cnt; ++r) {
               float w[3][3], m_unused;
-              staged_weights<kCell>(stg, r, my_cell, w, m_unused);
+              staged_weights<kCell, R>(stg, r, my_cell, w, m_unused);
               const float4 qa = stg[kP2GQ + d][r][my_cell];
               const float q = qa.x, ax = qa.y, ay = qa.z, az = qa.w;
               // wz (qij + kk az) = wz qij + cz[kk], cz = (0, wz1 az, 2 wz2 az): two operations
@@ -2665,13 +2661,18 @@ cudaError_t launch_bin(scene_device &s, cudaStream_t st) {
 // per-device kernel attributes; called once per scene with its device current, before any
 // capture of its launches
 cudaError_t prepare_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(k_p2g<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_p2g<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_p2g<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kP2GSmemBytes);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_p2g<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  cudaError_t e = cudaSuccess;
+  auto p2g_attrs = [&](const void *fn, int ranks) {
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem_bytes(ranks));
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  };
+  p2g_attrs((const void *)k_p2g<false, 8, 4>, 8);
+  p2g_attrs((const void *)k_p2g<false, 12, 3>, 12);
+  p2g_attrs((const void *)k_p2g<false, 16, 2>, 16);
+  p2g_attrs((const void *)k_p2g<true, 8, 4>, 8);
+  p2g_attrs((const void *)k_p2g<true, 12, 3>, 12);
+  p2g_attrs((const void *)k_p2g<true, 16, 2>, 16);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_g2p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kG2P2GSmem);
   if (e != cudaSuccess) return e;
@@ -2700,10 +2701,23 @@ cudaError_t prepare_kernels() {
                               (int)g2p_smem_bytes(128));
 }
 
+// the staged P2G kernel of the scene's staging depth (p2g_ranks: 8, 12 or 16; 0 = 12)
+template <bool kCell>
+static void launch_staged_p2g(scene_device &s, const float *affine, int with_mass, cudaStream_t st) {
+  const int ranks = s.prm.p2g_ranks > 0 ? s.prm.p2g_ranks : kP2GRanksDefault;
+  const int dflt = ranks == 8 ? 4 : ranks == 16 ? 2 : 3;
+  const int grid = num_sms() * (s.prm.p2g_ctas_per_sm > 0 ? s.prm.p2g_ctas_per_sm : dflt);
+  if (ranks == 8)
+    k_p2g<kCell, 8, 4><<<grid, kP2GThreads, p2g_smem_bytes(8), st>>>(s, affine, with_mass);
+  else if (ranks == 16)
+    k_p2g<kCell, 16, 2><<<grid, kP2GThreads, p2g_smem_bytes(16), st>>>(s, affine, with_mass);
+  else
+    k_p2g<kCell, 12, 3><<<grid, kP2GThreads, p2g_smem_bytes(12), st>>>(s, affine, with_mass);
+}
+
 cudaError_t launch_p2g(scene_device &s, cudaStream_t st) {
   if (s.prm.transfer == kTransferCell) return launch_p2c2g(s, 0, st);
-  const int per_sm = s.prm.p2g_ctas_per_sm > 0 ? s.prm.p2g_ctas_per_sm : kP2GMinCtas;
-  k_p2g<false><<<num_sms() * per_sm, kP2GThreads, kP2GSmemBytes, st>>>(s, s.cur.A, 1);
+  launch_staged_p2g<false>(s, s.cur.A, 1, st);
   return cudaGetLastError();
 }
 
@@ -2715,8 +2729,7 @@ cudaError_t launch_p2c2g(scene_device &s, int part, cudaStream_t st) {
     k_cell_affine<<<num_sms() * 4, kThreads, 0, st>>>(s, part, s.nxt.A);
     affine = s.nxt.A;
   }
-  const int per_sm = s.prm.p2g_ctas_per_sm > 0 ? s.prm.p2g_ctas_per_sm : kP2GMinCtas;
-  k_p2g<true><<<num_sms() * per_sm, kP2GThreads, kP2GSmemBytes, st>>>(s, affine, part == 2 ? 0 : 1);
+  launch_staged_p2g<true>(s, affine, part == 2 ? 0 : 1, st);
   return cudaGetLastError();
 }
 
