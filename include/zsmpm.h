@@ -285,6 +285,16 @@ ZSMPM_API zsmpm_status zsmpm_bht_build_device(const int32_t *keys, int32_t nkeys
                                               int32_t *table_keys, int32_t *indices, int32_t *status,
                                               int32_t cap_slots, int32_t *table_size, uint32_t *hashers,
                                               void *stream);
+/* Copies the block table of the last activation into a zs::HashTable<int, 3, int>'s storage
+ * (container/HashTable.hpp:45-60, 195-199) held by the caller, in host or device memory:
+ * keys [table_size][3], indices and status [table_size], the active keys [count][3] and the
+ * count.  table_size must equal the scene's (a HashTable sized for the same expected entry
+ * count, next_2pow(n) * 16 slots); cap_active is the active-key array's capacity.  Synchronises
+ * `stream`.  The slots are those the reference's insert would give the same keys in the
+ * canonical order, so zpc's own HashTableView::query finds every block at its index. */
+ZSMPM_API zsmpm_status zsmpm_download_table(zsmpm_scene *scene, int32_t *keys, int32_t *indices,
+                                            int32_t *status, int32_t *active_keys, int32_t cap_active,
+                                            int32_t *count, int32_t table_size, void *stream);
 /* Number of active blocks of the last activation (synchronises). */
 ZSMPM_API zsmpm_status zsmpm_num_blocks(zsmpm_scene *scene, int32_t *out);
 /* Copies the active keys [nb][3] and the grid [nb][4][512] to host memory. */

@@ -2,7 +2,9 @@
 # Test infrastructure: builds the reference's own OpenMP/sequential MPM path
 # (littlemine/zpc, its include/ tree at $ZSMPM_REFERENCE_ROOT, by default the directory
 # "reference" beside this repository) into the executable oracle/_ref/zsref_cli,
-# driven by oracle/ref_driver.cpp and oracle/ref_cli.cpp.  The output is the checker and the CPU baseline, never the product.
+# driven by oracle/ref_driver.cpp and oracle/ref_cli.cpp, and the check of include/zsmpm_zpc.hpp
+# against zpc's containers (oracle/zpc_adapter_check, linked with libzsmpm.so).  The output is
+# the checker and the CPU baseline, never the product.
 #
 # zpc's CMake build needs the zpc_tpls submodule, which is not checked out, so the needed
 # translation units are compiled directly with g++.  Several reference headers do not parse
@@ -93,3 +95,11 @@ for p in "${pids[@]}"; do wait "$p"; done
 g++ -fopenmp -o "$OUT/zsref_cli" "$OUT/obj/ref_cli.o" "$OUT/obj/ref_driver.o" \
   "$OUT/obj/cpp_timer.o" "${OBJS[@]}" -lpthread -ldl
 echo "build_ref: wrote $OUT/zsref_cli"
+# the check of include/zsmpm_zpc.hpp against zpc's own containers, linked with libzsmpm.so
+LIBDIR="$HERE/../zsmpm_b200/lib"
+if [ -f "$LIBDIR/libzsmpm.so" ]; then
+  g++ "${CXXFLAGS[@]}" -I"$HERE/../include" -c "$HERE/zpc_adapter_check.cpp" -o "$OUT/obj/zpc_adapter_check.o"
+  g++ -fopenmp -o "$OUT/zpc_adapter_check" "$OUT/obj/zpc_adapter_check.o" "$OUT/obj/cpp_timer.o" "${OBJS[@]}" \
+    -L"$LIBDIR" -lzsmpm -Wl,-rpath,'$ORIGIN/../../zsmpm_b200/lib' -lpthread -ldl
+  echo "build_ref: wrote $OUT/zpc_adapter_check"
+fi

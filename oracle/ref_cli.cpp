@@ -40,6 +40,8 @@
 #include <cstdlib>
 #include <vector>
 
+#include "zeroed_new.hpp"  // the reference registry's mutex starts unlocked
+
 extern "C" {
 struct zsref_params {
   int model, policy, threads, order, wall_type, wall_cells, table_expected, volume_correction;

@@ -1,9 +1,12 @@
 """Test infrastructure: runs the reference's own MPM path (oracle/_ref/zsref_cli, compiled from
 the zpc sources by oracle/build_ref.sh) in a subprocess, exchanging raw little-endian files.
 
-The reference's host runtime is run in its own process because, loaded into a Python process,
-it intermittently blocked on a futex before its first operator launch; the same calls from a
-plain C++ process never did.  Every call has a timeout and is retried once.
+The reference's host runtime is run in its own process.  Loaded into a Python process, it
+intermittently blocked on a futex before its first operator launch.  The cause is in the
+reference: zs::MemoryBackendRegistry is allocated with `new` and its zs::Mutex member has no
+initializer, so the first lock waits forever when the heap word under it is nonzero
+(oracle/ref_shims/zeroed_new.hpp, which the CLI now links, gives it zeroed memory).  Every call
+has a timeout and is retried once.
 """
 from __future__ import annotations
 

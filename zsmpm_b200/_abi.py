@@ -130,6 +130,7 @@ SIGNATURES = {
     "zsmpm_scene_set_transfer": (_S, [_P, C.c_int32, _P]),
     "zsmpm_p2c2g": (_S, [_P, C.c_int32, _P]),
     "zsmpm_g2c2p": (_S, [_P, _P]),
+    "zsmpm_download_table": (_S, [_P, _P, _P, _P, _P, C.c_int32, _P, C.c_int32, _P]),
     "zsmpm_substep": (_S, [_P, _P]),
     "zsmpm_run": (_S, [_P, C.c_int32, _P]),
     "zsmpm_get_table_view": (_S, [_P, C.POINTER(TableView)]),

@@ -869,6 +869,36 @@ ZSMPM_API zsmpm_status zsmpm_get_table_view(zsmpm_scene *s, zsmpm_table_view *ou
   return ZSMPM_OK;
 }
 
+ZSMPM_API zsmpm_status zsmpm_download_table(zsmpm_scene *s, int32_t *keys, int32_t *indices, int32_t *status,
+                                            int32_t *active_keys, int32_t cap_active, int32_t *count,
+                                            int32_t table_size, void *stream) {
+  zsmpm_status st = check_scene(s, true);
+  if (st != ZSMPM_OK) return st;
+  if (!keys || !indices || !status || !active_keys || !count)
+    return fail(ZSMPM_ERR_INVALID_ARG, "null table array");
+  if (table_size != s->dev.prm.table_size)
+    return fail(ZSMPM_ERR_INVALID_ARG, ("the destination table has " + std::to_string(table_size) +
+                                        " slots, the scene's " + std::to_string(s->dev.prm.table_size) +
+                                        " (size it for the same expected entry count)")
+                                           .c_str());
+  cudaStream_t cs = as_stream(stream);
+  int nb = 0;
+  ZS_TRY(cudaMemcpyAsync(&nb, s->dev.view_cnt, sizeof(int), cudaMemcpyDeviceToHost, cs), "table count");
+  ZS_TRY(cudaStreamSynchronize(cs), "table count");
+  if (nb > cap_active) return fail(ZSMPM_ERR_CAPACITY, "active-key array too small");
+  const size_t T = (size_t)table_size;
+  // cudaMemcpyDefault: the destination may be host or device memory (unified addressing)
+  ZS_TRY(cudaMemcpyAsync(keys, s->dev.tkeys, T * 3 * sizeof(int), cudaMemcpyDefault, cs), "table keys");
+  ZS_TRY(cudaMemcpyAsync(indices, s->dev.tidx, T * sizeof(int), cudaMemcpyDefault, cs), "table indices");
+  ZS_TRY(cudaMemcpyAsync(status, s->dev.tstatus, T * sizeof(int), cudaMemcpyDefault, cs), "table status");
+  ZS_TRY(cudaMemcpyAsync(active_keys, s->dev.active_keys, (size_t)nb * 3 * sizeof(int), cudaMemcpyDefault, cs),
+         "active keys");
+  ZS_TRY(cudaMemcpyAsync(count, s->dev.view_cnt, sizeof(int), cudaMemcpyDefault, cs), "table count");
+  ZS_TRY(cudaStreamSynchronize(cs), "table copy");
+  s->last_stream = cs;
+  return ZSMPM_OK;
+}
+
 ZSMPM_API zsmpm_status zsmpm_num_blocks(zsmpm_scene *s, int32_t *out) {
   zsmpm_status st = check_scene(s, true);
   if (st != ZSMPM_OK) return st;
