@@ -55,6 +55,15 @@ def scene_for(name: str):
         return scenes.config2(dx=1 / 128), "dp_two_boxes_dx128_8ppc"
     if name == "fc":
         return scenes.config1(), "fc_cube_dx128_8ppc"
+    if name in ("fc_boxes", "fc_boxes128"):
+        # the two-box geometry in fixed corotated (the cell-centric transfers have no plasticity)
+        import dataclasses
+        from zsmpm_b200 import _abi
+        dx = 1 / 256 if name == "fc_boxes" else 1 / 128
+        spec = dataclasses.replace(scenes.config2(dx=dx), name=f"fc_two_boxes_dx{round(1 / dx)}",
+                                   material=scenes.MaterialSpec(model=_abi.FIXED_COROTATED, E=3.5e5, nu=0.3,
+                                                                rho=2200.0))
+        return spec, f"fc_two_boxes_dx{round(1 / dx)}_8ppc"
     if name == "snow16m":
         return scenes.config5_16m(), "snow_sphere_slab_dx295_4ppc"
     if name == "batch256":
@@ -487,7 +496,7 @@ def cpu_baseline_sample(spec, p, max_particles: int):
     return p.subset(idx), f"slab z < {cut:.4f} of the workload ({len(idx)} particles)"
 
 
-def reference_cpu_rate(spec, p, parts, steps, warmup, max_particles, threads, timeout):
+def reference_cpu_rate(spec, p, parts, steps, warmup, max_particles, threads, timeout, cell=False):
     """Particle-substeps/s of the reference's omp_exec path (oracle/_ref) on a bounded sample:
     a z-slab of a single scene, or the first scenes of a batch (each its own system, as the
     reference advances them one after another) up to max_particles."""
@@ -505,10 +514,12 @@ def reference_cpu_rate(spec, p, parts, steps, warmup, max_particles, threads, ti
         desc = f"the first {len(jobs)} of {len(spec)} scenes ({total} particles), run one after another"
     if warmup:
         sp0, q0 = jobs[0]
-        reference.run(sp0, q0, warmup, policy=reference.POLICY_OMP, threads=threads, cap_blocks=0, timeout=timeout)
+        reference.run(sp0, q0, warmup, policy=reference.POLICY_OMP, threads=threads, cap_blocks=0, timeout=timeout,
+                      cell=cell)
     seconds, work = 0.0, 0
     for sp, q in jobs:
-        r = reference.run(sp, q, steps, policy=reference.POLICY_OMP, threads=threads, cap_blocks=0, timeout=timeout)
+        r = reference.run(sp, q, steps, policy=reference.POLICY_OMP, threads=threads, cap_blocks=0, timeout=timeout,
+                          cell=cell)
         seconds += r.seconds
         work += q.n * steps
     return work / seconds, desc, sum(q.n for _, q in jobs)
@@ -529,7 +540,7 @@ def run_reference_arm(args, spec, workload, n_full):
     # (about 1.5e8 particle-substeps at ~3e6 particle-substeps/s on 16 cores)
     sample_particles = max(100_000, min(args.ref_particles, int(1.5e8 // max(args.steps, 1))))
     value, desc, sampled = reference_cpu_rate(spec, p, parts, args.steps, max(args.warmup, 1),
-                                              sample_particles, threads, 3600)
+                                              sample_particles, threads, 3600, cell=args.transfer == "cell")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * n_full / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -550,7 +561,7 @@ class Workload:
     """One scene (or batch) resident on the GPU, with pinned host copies of its inputs for the
     end-to-end leg."""
 
-    def __init__(self, zs, spec, p, parts, local, stream):
+    def __init__(self, zs, spec, p, parts, local, stream, transfer: str = "apic"):
         import torch
         self.zs, self.spec, self.p, self.parts = zs, spec, p, parts
         self.n = p.n
@@ -564,7 +575,7 @@ class Workload:
         self.d2h_bytes = (self.out_x.numel() + self.out_v.numel()) * 4 + 4
         self.lib = zs._abi.lib()
         if parts is None:
-            self.sc = zs.Scene(spec, device=local)
+            self.sc = zs.Scene(spec, device=local, transfer=transfer)
         else:
             from zsmpm_b200 import batch
             self.sc = batch.Batch(spec, device=local)
@@ -679,11 +690,13 @@ def cpu_baselines(args, spec, p, parts):
                 "sample": "unavailable: oracle/_ref/zsref_cli not built"}
     try:
         threads = os.cpu_count() or 1
-        rate, desc, sampled = reference_cpu_rate(spec, p, parts, args.ref_steps, 0, args.ref_particles, threads, 900)
+        cell = args.transfer == "cell"
+        rate, desc, sampled = reference_cpu_rate(spec, p, parts, args.ref_steps, 0, args.ref_particles, threads, 900,
+                                                 cell=cell)
         out = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                "sample": f"{desc}, {args.ref_steps} substeps, zs::omp_exec", "extrapolated_from": sampled}
         # zpc's own default: omp_exec() with hardware_concurrency - 1 threads (threads <= 0 in the driver)
-        rate_d, _, _ = reference_cpu_rate(spec, p, parts, args.ref_steps, 0, args.ref_particles, 0, 900)
+        rate_d, _, _ = reference_cpu_rate(spec, p, parts, args.ref_steps, 0, args.ref_particles, 0, 900, cell=cell)
         out["zpc_default_threads"] = {"value": rate_d, "unit": UNIT, "cores": max(threads - 1, 1),
                                       "what": "zs::omp_exec() default, hardware_concurrency - 1 threads"}
         return out
@@ -717,12 +730,9 @@ def cell_leg(args, ws, local, stream, cpu: bool) -> dict:
     the benchmark's two-box geometry in fixed corotated (the pair has no plasticity branch):
     30,089,900 particles, each pair measured like the main leg, and the reference's own cell
     path under zs::omp_exec on a bounded slab."""
-    import dataclasses
-
     import zsmpm_b200 as zs
     from zsmpm_b200 import scenes
-    spec = dataclasses.replace(scenes.config2(), name="fc_two_boxes_dx256",
-                               material=scenes.MaterialSpec(model=zs.FIXED_COROTATED, E=3.5e5, nu=0.3, rho=2200.0))
+    spec, _ = scene_for("fc_boxes")
     p = scenes.generate(spec)
     w = Workload(zs, spec, p, None, local, stream)
     try:
@@ -770,7 +780,11 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scene", default="dp", choices=["dp", "dp128", "fc", "snow16m", "batch256"])
+    ap.add_argument("--scene", default="dp", choices=["dp", "dp128", "fc", "fc_boxes", "fc_boxes128", "snow16m",
+                                                      "batch256"])
+    ap.add_argument("--transfer", default="apic", choices=["apic", "cell"],
+                    help="the transfer pair of the main leg: P2G / G2P, or the cell-centric P2C2G / G2C2P "
+                         "(fixed-corotated scenes)")
     ap.add_argument("--ref-particles", type=int, default=1_500_000)
     ap.add_argument("--ref-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -801,7 +815,7 @@ def main(argv=None):
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
     p, parts = generate_workload(spec)
-    w = Workload(zs, spec, p, parts, local, stream)
+    w = Workload(zs, spec, p, parts, local, stream, transfer=args.transfer)
     n = w.n
     specs = w.specs
     main_leg = plain_leg(args, w, ws, local, with_e2e=True)
@@ -809,7 +823,9 @@ def main(argv=None):
 
     # ---------------------------------------------------------------- learned-closure leg
     learned = None
-    if w.plastic and parts is None and not args.no_learned:
+    if args.transfer != "apic":
+        pass  # the learned closure and the implicit system work with the APIC pair
+    elif w.plastic and parts is None and not args.no_learned:
         learned = learned_leg(args, zs, w.sc, spec, n, w.upload_pinned, stream, w.sptr, ws, ms / args.steps)
     elif w.plastic and not args.no_learned:
         learned = batch_learned_leg(args, zs, w.sc, specs, parts, w.upload_pinned, stream, w.sptr, ws,
@@ -817,7 +833,7 @@ def main(argv=None):
 
     # ---------------------------------------------------------------- implicit-system leg
     implicit = None
-    if parts is None and not args.no_implicit:
+    if parts is None and not args.no_implicit and args.transfer == "apic":
         sample = None
         if rank == 0 and ws == 1 and not args.no_cpu_baseline:
             try:
@@ -854,7 +870,7 @@ def main(argv=None):
                        "material": "mixed fixed_corotated / drucker_prager" if len(specs) > 1 else
                        ("drucker_prager" if specs[0].material.model == zs.DRUCKER_PRAGER else
                         ("snow" if specs[0].material.model == zs.SNOW else "fixed_corotated")),
-                       "closure": "plain", "parallelism": f"replicas{ws}",
+                       "closure": "plain", "transfer": args.transfer, "parallelism": f"replicas{ws}",
                        "launch_shapes": main_leg["launch_shapes"],
                        "l2": "inputs larger than L2 (particle state 2+ GB per workload)",
                        "substep_graph": "CUDA graph of 2 substeps"},
