@@ -38,6 +38,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "MPM particle-substeps/sec on 1 B200, learned vs plain closure at stated error"
 UNIT = "particle-substeps/s"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
+# the closure's training: (epochs, batch, learning rate) stages of Adam over the projected states
+TRAIN_SCHEDULE = ((20, 4096, 2e-3), (20, 4096, 5e-4), (16, 8192, 1e-4), (12, 16384, 3e-5), (8, 32768, 1e-5))
 
 
 def hbm_peak():
@@ -258,7 +260,7 @@ def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms
     c = cl.Closure(spec.material, spec.volume, device=torch.cuda.current_device())
     t0 = time.perf_counter()
     c.build_dataset(args.train_random, seed=7, logged=buf[:n_log].contiguous())
-    schedule = ((6, 4096, 2e-3), (6, 4096, 5e-4), (4, 8192, 1e-4))
+    schedule = TRAIN_SCHEDULE
     losses = c.fit(schedule)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
@@ -302,8 +304,9 @@ def learned_leg(args, zs, sc, spec, n, upload_pinned, stream, sptr, ws, plain_ms
                          "epochs": sum(e for e, _, _ in schedule), "seconds": train_s,
                          "first_loss": float(losses[0]), "final_loss": float(losses[-1])},
             "inference": ("exact branch test in G2P; projections inside the training hull queued and run "
-                          "through the network by tcgen05.mma (BF16 operands, FP32 accumulators in tensor "
-                          "memory, 128-row tiles), completed by a finish kernel"),
+                          "through the network by tcgen05.mma (split-BF16 operands: hi + lo pairs, three MMAs "
+                          "per step; FP32 accumulators in tensor memory, 128-row tiles), completed by a finish "
+                          "kernel"),
             "mlp_inference": mlp}
 
 
@@ -326,7 +329,7 @@ def batch_learned_leg(args, zs, sc, specs, parts, upload_pinned, stream, sptr, w
     c = cl.Closure(specs[k].material, specs[k].volume, device=torch.cuda.current_device())
     t0 = time.perf_counter()
     c.build_dataset(args.train_random, seed=7, logged=buf[:n_log].contiguous())
-    schedule = ((6, 4096, 2e-3), (6, 4096, 5e-4), (4, 8192, 1e-4))
+    schedule = TRAIN_SCHEDULE
     losses = c.fit(schedule)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
@@ -360,9 +363,10 @@ def batch_learned_leg(args, zs, sc, specs, parts, upload_pinned, stream, sptr, w
 
 
 def mlp_inference_leg(c, n_rows: int, reps: int = 5) -> dict:
-    """The closure's network alone over n_rows feature rows, on both tensor-core paths: the
-    mma.sync forward that G2P fuses and the tcgen05 forward (tensor-memory accumulators).
-    17,920 FLOP per row (6-64-64-64-6); peak = measured dense BF16 (burst)."""
+    """The closure's network alone over n_rows feature rows, on the tensor-core paths: the
+    mma.sync forward, the tcgen05 forward (tensor-memory accumulators) with BF16 operands, and
+    the tcgen05 forward with split-BF16 operands that the substep runs (three MMAs per step).
+    17,920 useful FLOP per row (6-64-64-64-6); peak = measured dense BF16 (burst)."""
     import torch
     try:
         peak = float(json.loads(PEAKS.read_text())["bf16_tflops"])
@@ -375,7 +379,7 @@ def mlp_inference_leg(c, n_rows: int, reps: int = 5) -> dict:
     x[:, :3] = torch.sort(x[:, :3], dim=1, descending=True).values
     x[:, 3] = 30.0
     out = {"rows": n_rows, "flop_per_row": 17920, "peak_tflops": peak, "peak_kind": peak_kind}
-    for path in ("mma_sync", "tcgen05"):
+    for path in ("mma_sync", "tcgen05", "tcgen05_split"):
         c.infer(x, path=path)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

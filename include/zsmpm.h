@@ -542,7 +542,10 @@ ZSMPM_API zsmpm_status zsmpm_closure_loss_grad(zsmpm_closure *c, const float *x,
  * path: 0 an FP32 forward of the master weights; 1 the BF16 mma.sync forward that G2P runs
  * (one warp per 32 rows, activations in registers); 2 a BF16 tcgen05 forward (5th-generation
  * tensor cores: 128-row tiles per CTA, operands in shared memory, FP32 accumulators in tensor
- * memory).  Asynchronous; zsmpm_closure_status reports a tcgen05 wait that gave up. */
+ * memory); 3 the tcgen05 forward with split-BF16 operands (weights and activations as hi + lo
+ * BF16 pairs, A_hi W_hi + A_hi W_lo + A_lo W_hi per layer into the FP32 accumulator; SiLU in
+ * FP32), the path the substep's projections take.  Asynchronous; zsmpm_closure_status reports a
+ * tcgen05 wait that gave up. */
 ZSMPM_API zsmpm_status zsmpm_closure_infer(zsmpm_closure *c, const float *x, float *y, int64_t n, int32_t bf16,
                                            void *stream);
 /* Synchronises the device and reports (then clears) a bounded tensor-core wait that gave up

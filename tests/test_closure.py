@@ -194,6 +194,8 @@ def test_tcgen05_inference_matches_mma_sync_and_oracle(zs, gpu, model):
         x = torch.from_numpy(rows).to(gpu)
         ytc = c.infer(x, path="tcgen05").cpu().numpy().astype(np.float64)
         c.status()
+        ysplit = c.infer(x, path="tcgen05_split").cpu().numpy().astype(np.float64)
+        c.status()
         ymma = c.infer(x, path="mma_sync").cpu().numpy().astype(np.float64)
         xin = mlp.inputs(model, rows, k, xi)[0]
         ref = mlp.from_net(model, rows, mlp.forward(st["params"], (xin - st["in_mean"]) * st["in_inv_std"])
@@ -206,6 +208,9 @@ def test_tcgen05_inference_matches_mma_sync_and_oracle(zs, gpu, model):
                 assert np.linalg.norm(ytc[:, col] - ref[:, col]) <= 3e-2 * scale
                 # the two tensor-core paths round the same values; they differ by accumulation order
                 assert np.linalg.norm(ytc[:, col] - ymma[:, col]) <= 5e-3 * scale
+                # split-BF16 operands (hi + lo pairs, three MMAs per step) and FP32 SiLU: products
+                # to about 16 significant bits
+                assert np.linalg.norm(ysplit[:, col] - ref[:, col]) <= 3e-4 * scale
     c.close()
 
 

@@ -103,10 +103,11 @@ class Closure:
         return loss, grad
 
     def infer(self, x, bf16: bool = True, stream=None, path: str | None = None):
-        """Network outputs (D, tau) of raw rows x.  path: "fp32", "mma_sync" (the G2P forward)
-        or "tcgen05"; by default "mma_sync" when bf16 else "fp32"."""
+        """Network outputs (D, tau) of raw rows x.  path: "fp32", "mma_sync", "tcgen05" (BF16
+        operands) or "tcgen05_split" (split-BF16 operands, the substep's path); by default
+        "mma_sync" when bf16 else "fp32"."""
         import torch
-        mode = {"fp32": 0, "mma_sync": 1, "tcgen05": 2}[path or ("mma_sync" if bf16 else "fp32")]
+        mode = {"fp32": 0, "mma_sync": 1, "tcgen05": 2, "tcgen05_split": 3}[path or ("mma_sync" if bf16 else "fp32")]
         y = torch.empty_like(x)
         _abi.check(self._lib.zsmpm_closure_infer(self._h, _rows(x, "x"), _rows(y, "y"), int(x.shape[0]),
                                                  mode, _stream(stream)), "closure_infer")

@@ -1004,6 +1004,7 @@ ZSMPM_API zsmpm_status zsmpm_scene_set_closure(zsmpm_scene *s, zsmpm_closure *c,
     return fail(ZSMPM_ERR_INVALID_ARG, "closure was built for another material model");
   if (s->desc.material.plasticity_mode != ZSMPM_PLASTICITY_COMMITTED && s->desc.material.model != ZSMPM_SNOW)
     return fail(ZSMPM_ERR_INVALID_ARG, "the learned closure runs in the committed plasticity ordering");
+  ZS_TRY(prepare_closure_kernels(), "closure kernel attributes");
   if (!s->audit) {
     double *a = nullptr;
     ZS_TRY(cudaMalloc(&a, sizeof(double) * 8), "alloc audit");

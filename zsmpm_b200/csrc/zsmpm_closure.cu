@@ -480,6 +480,11 @@ constexpr int kTcW4 = kTcW3 + 64 * 64 * 2;       // 16 x 64 (6 rows used)
 constexpr int kTcA = kTcW4 + 16 * 64 * 2;        // 128 x 64 activations
 constexpr int kTcSmem = kTcA + kTcRows * 64 * 2;
 constexpr int kTcWBytes = kTcA;                  // the packed weights
+// the split-BF16 variant: weights and activations as hi + lo BF16 pairs (hi = bf16(v),
+// lo = bf16(v - hi)), each layer A_hi W_hi + A_hi W_lo + A_lo W_hi into one FP32 accumulator:
+// products to about 16 significant bits, against 8 for plain BF16 operands
+constexpr int kTcSplitA = 2 * kTcWBytes;                       // A_hi, then A_lo
+constexpr int kTcSplitSmem = kTcSplitA + 2 * kTcRows * 64 * 2;  // 72 KB: 3 CTAs per SM
 constexpr int kTcTmemCols = 64;
 constexpr long long kTcWaitLimit = 1ll << 22;    // try_wait rounds before giving up
 
@@ -487,7 +492,8 @@ __host__ __device__ constexpr int umma_offset(int R, int r, int k) {
   return (k >> 3) * (16 * R) + (r >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
 }
 
-// weights -> bf16 in the K-major layout (W[out][in]; zero padding to K = 16 and N = 16)
+// weights -> bf16 in the K-major layout (W[out][in]; zero padding to K = 16 and N = 16): the
+// rounded weights at w, and their rounding residuals bf16(v - bf16(v)) kTcWBytes further on
 __global__ void k_pack_umma(const float *p, __nv_bfloat16 *w) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // element index over all four matrices
   int base, R, K, layer, local;
@@ -502,7 +508,9 @@ __global__ void k_pack_umma(const float *p, __nv_bfloat16 *w) {
   else if (layer == 1) v = p[kOffW2 + r * 64 + k];
   else if (layer == 2) v = p[kOffW3 + r * 64 + k];
   else v = r < 6 ? p[kOffW4 + r * 64 + k] : 0.f;
-  w[(base + umma_offset(R, r, k)) / 2] = __float2bfloat16_rn(v);
+  const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+  w[(base + umma_offset(R, r, k)) / 2] = hi;
+  w[(kTcWBytes + base + umma_offset(R, r, k)) / 2] = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo) {
@@ -581,6 +589,36 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
   for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
 
+// v as a hi + lo pair of bf16 (two bf16x2 words for two values)
+__device__ __forceinline__ void split_bf16x2(float a, float b, uint32_t &hi, uint32_t &lo) {
+  const __nv_bfloat16 ha = __float2bfloat16_rn(a), hb = __float2bfloat16_rn(b);
+  hi = (uint32_t)__bfloat16_as_ushort(ha) | ((uint32_t)__bfloat16_as_ushort(hb) << 16);
+  lo = pack_bf16x2(a - __bfloat162float(ha), b - __bfloat162float(hb));
+}
+
+// the split variant's epilogue: bias + SiLU in FP32, written as hi and lo rows
+__device__ __forceinline__ void tc_hidden_epilogue_split(uint32_t tmem_row, const float *bias, unsigned char *a_hi,
+                                                         unsigned char *a_lo, int row) {
+  float v[64];
+  tmem_ld64(tmem_row, v);
+#pragma unroll
+  for (int kc = 0; kc < 8; ++kc) {
+    float a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const float z = v[8 * kc + j] + bias[8 * kc + j];
+      a[j] = __fdividef(z, 1.f + __expf(-z));
+    }
+    uint4 h, l;
+    split_bf16x2(a[0], a[1], h.x, l.x);
+    split_bf16x2(a[2], a[3], h.y, l.y);
+    split_bf16x2(a[4], a[5], h.z, l.z);
+    split_bf16x2(a[6], a[7], h.w, l.w);
+    *reinterpret_cast<uint4 *>(a_hi + umma_offset(kTcRows, row, 8 * kc)) = h;
+    *reinterpret_cast<uint4 *>(a_lo + umma_offset(kTcRows, row, 8 * kc)) = l;
+  }
+}
+
 // one hidden layer's epilogue: bias + SiLU (bf16x2) of this thread's 64 accumulators into its
 // row of the A tile
 __device__ __forceinline__ void tc_hidden_epilogue(uint32_t tmem_row, const float *bias, unsigned char *a_tile,
@@ -598,7 +636,9 @@ __device__ __forceinline__ void tc_hidden_epilogue(uint32_t tmem_row, const floa
   }
 }
 
-// n_dev (optional): the row count in device memory, at most n (the G2P queue of a substep)
+// n_dev (optional): the row count in device memory, at most n (the G2P queue of a substep).
+// kSplit: the split-BF16 variant (weights and activations as hi + lo BF16, three MMAs per K step).
+template <bool kSplit>
 __global__ void __launch_bounds__(kTcRows) k_closure_infer_tc(closure_dev cd, const uint4 *wpack, const float *x,
                                                               float *y, int64_t n, const int *n_dev, int *status) {
   if (n_dev) n = min(n, (int64_t)*n_dev);
@@ -608,7 +648,7 @@ __global__ void __launch_bounds__(kTcRows) k_closure_infer_tc(closure_dev cd, co
   __shared__ uint32_t taddr_s;
   __shared__ float sbias[kBiasTotal];
   const int t = threadIdx.x, warp = t >> 5;
-  for (int i = t; i < kTcA / 16; i += kTcRows) reinterpret_cast<uint4 *>(tsm)[i] = wpack[i];
+  for (int i = t; i < (kSplit ? 2 : 1) * kTcWBytes / 16; i += kTcRows) reinterpret_cast<uint4 *>(tsm)[i] = wpack[i];
   for (int i = t; i < kBiasTotal; i += kTcRows) sbias[i] = cd.bias[i];
   const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&mbar);
   if (warp == 0) {
@@ -624,8 +664,10 @@ __global__ void __launch_bounds__(kTcRows) k_closure_infer_tc(closure_dev cd, co
   const uint32_t tmem = taddr_s;
   const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 lanes
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(tsm);
-  unsigned char *a_tile = tsm + kTcA;
-  const uint32_t a_addr = sbase + kTcA;
+  constexpr int a_off = kSplit ? kTcSplitA : kTcA;
+  unsigned char *a_tile = tsm + a_off;  // A_hi (the only A tile without the split)
+  unsigned char *a_lo = tsm + a_off + kTcRows * 64 * 2;
+  const uint32_t a_addr = sbase + a_off, alo_addr = a_addr + kTcRows * 64 * 2;
   const uint32_t id64 = umma_idesc(64), id16 = umma_idesc(16);
   uint32_t parity = 0;
   bool ok = true;
@@ -640,10 +682,20 @@ __global__ void __launch_bounds__(kTcRows) k_closure_infer_tc(closure_dev cd, co
 #pragma unroll
     for (int k = 0; k < kMlpIn; ++k) in[k] = (in[k] - cd.in_mean[k]) * cd.in_inv_std[k];
     uint4 q0;
-    q0.x = pack_bf16x2(in[0], in[1]);
-    q0.y = pack_bf16x2(in[2], in[3]);
-    q0.z = pack_bf16x2(in[4], in[5]);
-    q0.w = 0u;
+    if (kSplit) {
+      uint4 l0;
+      split_bf16x2(in[0], in[1], q0.x, l0.x);
+      split_bf16x2(in[2], in[3], q0.y, l0.y);
+      split_bf16x2(in[4], in[5], q0.z, l0.z);
+      q0.w = l0.w = 0u;
+      *reinterpret_cast<uint4 *>(a_lo + umma_offset(kTcRows, t, 0)) = l0;
+      *reinterpret_cast<uint4 *>(a_lo + umma_offset(kTcRows, t, 8)) = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+      q0.x = pack_bf16x2(in[0], in[1]);
+      q0.y = pack_bf16x2(in[2], in[3]);
+      q0.z = pack_bf16x2(in[4], in[5]);
+      q0.w = 0u;
+    }
     *reinterpret_cast<uint4 *>(a_tile + umma_offset(kTcRows, t, 0)) = q0;
     *reinterpret_cast<uint4 *>(a_tile + umma_offset(kTcRows, t, 8)) = make_uint4(0u, 0u, 0u, 0u);
     // four layers: MMA by one thread, completion through the mbarrier, epilogue by all
@@ -657,10 +709,17 @@ __global__ void __launch_bounds__(kTcRows) k_closure_infer_tc(closure_dev cd, co
         const int ksteps = layer == 0 ? 1 : 4;
         const uint32_t w_off = layer == 0 ? kTcW1 : layer == 1 ? kTcW2 : layer == 2 ? kTcW3 : kTcW4;
         const uint32_t w_rows = layer == 3 ? 16 : 64;
-        for (int ks = 0; ks < ksteps; ++ks)
-          umma_bf16(tmem, umma_desc(a_addr + 2 * ks * (16 * kTcRows), 16 * kTcRows),
-                    umma_desc(sbase + w_off + 2 * ks * (16 * w_rows), 16 * w_rows), layer == 3 ? id16 : id64,
-                    ks > 0 ? 1u : 0u);
+        const uint32_t idesc = layer == 3 ? id16 : id64;
+        for (int ks = 0; ks < ksteps; ++ks) {
+          const uint64_t a_hi = umma_desc(a_addr + 2 * ks * (16 * kTcRows), 16 * kTcRows);
+          const uint64_t w_hi = umma_desc(sbase + w_off + 2 * ks * (16 * w_rows), 16 * w_rows);
+          umma_bf16(tmem, a_hi, w_hi, idesc, ks > 0 ? 1u : 0u);
+          if (kSplit) {
+            umma_bf16(tmem, a_hi, umma_desc(sbase + kTcWBytes + w_off + 2 * ks * (16 * w_rows), 16 * w_rows),
+                      idesc, 1u);
+            umma_bf16(tmem, umma_desc(alo_addr + 2 * ks * (16 * kTcRows), 16 * kTcRows), w_hi, idesc, 1u);
+          }
+        }
         umma_commit(bar);
       }
       const bool done = mbar_wait(bar, parity);
@@ -669,7 +728,10 @@ __global__ void __launch_bounds__(kTcRows) k_closure_infer_tc(closure_dev cd, co
       if (!ok) break;
       tc_fence_after();
       if (layer < 3) {
-        tc_hidden_epilogue(tmem_row, sbias + 64 * layer, a_tile, t);
+        if (kSplit)
+          tc_hidden_epilogue_split(tmem_row, sbias + 64 * layer, a_tile, a_lo, t);
+        else
+          tc_hidden_epilogue(tmem_row, sbias + 64 * layer, a_tile, t);
       } else {
         float o[16];
         tmem_ld16(tmem_row, o);
@@ -775,10 +837,17 @@ bool closure_device_view(const zsmpm_closure *c, closure_dev *out) {
   return true;
 }
 
+// the G2P queue's network pass: the split-BF16 tcgen05 forward (three CTAs of 72 KB per SM)
 cudaError_t launch_closure_rows(const closure_dev &cd, const float *x, float *y, const int *n_dev, long long cap,
                                 cudaStream_t st) {
-  k_closure_infer_tc<<<sms() * 6, kTcRows, kTcSmem, st>>>(cd, cd.umma_w, x, y, cap, n_dev, cd.tc_status);
+  k_closure_infer_tc<true><<<sms() * 3, kTcRows, kTcSplitSmem, st>>>(cd, cd.umma_w, x, y, cap, n_dev, cd.tc_status);
   return cudaGetLastError();
+}
+
+// the split variant's shared memory exceeds the 48 KB default: set once per device, before any
+// capture of its launches
+cudaError_t prepare_closure_kernels() {
+  return cudaFuncSetAttribute(k_closure_infer_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSplitSmem);
 }
 }  // namespace zsmpm
 
@@ -818,7 +887,7 @@ ZSMPM_API zsmpm_status zsmpm_closure_create(const zsmpm_material *mat, int32_t d
   if (e == cudaSuccess) e = cudaMalloc(&c->adam_m, sizeof(float) * kMlpParams);
   if (e == cudaSuccess) e = cudaMalloc(&c->adam_v, sizeof(float) * kMlpParams);
   if (e == cudaSuccess) e = cudaMalloc(&c->frag, sizeof(uint2) * kFragTotal);
-  if (e == cudaSuccess) e = cudaMalloc(&c->umma_w, kTcWBytes);
+  if (e == cudaSuccess) e = cudaMalloc(&c->umma_w, 2 * kTcWBytes);  // rounded weights and residuals
   if (e == cudaSuccess) e = cudaMalloc(&c->tc_status, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->tc_status, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&c->bias, sizeof(float) * kBiasTotal);
@@ -1029,14 +1098,21 @@ ZSMPM_API zsmpm_status zsmpm_closure_infer(zsmpm_closure *c, const float *x, flo
   if (!c || !x || !y || n < 1) return cerr(ZSMPM_ERR_INVALID_ARG, "bad arguments");
   CZ_TRY(cudaSetDevice(c->device), "cudaSetDevice");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (bf16 == 2) {
+  if (bf16 == 2 || bf16 == 3) {
     const zsmpm_status ps = pack(c, st);
     if (ps != ZSMPM_OK) return ps;
     const int64_t tiles = (n + kTcRows - 1) / kTcRows;
-    // six resident CTAs per SM (37.7 KB of shared memory and 64 tensor-memory columns each), so
-    // that six tiles' layer chains overlap on the SM's tensor core
-    const int grid = (int)std::min<int64_t>(tiles, (int64_t)sms() * 6);
-    k_closure_infer_tc<<<grid, kTcRows, kTcSmem, st>>>(c->cd, c->umma_w, x, y, n, nullptr, c->tc_status);
+    if (bf16 == 2) {
+      // six resident CTAs per SM (37.7 KB of shared memory and 64 tensor-memory columns each), so
+      // that six tiles' layer chains overlap on the SM's tensor core
+      const int grid = (int)std::min<int64_t>(tiles, (int64_t)sms() * 6);
+      k_closure_infer_tc<false><<<grid, kTcRows, kTcSmem, st>>>(c->cd, c->umma_w, x, y, n, nullptr, c->tc_status);
+    } else {
+      CZ_TRY(prepare_closure_kernels(), "closure kernel attributes");
+      const int grid = (int)std::min<int64_t>(tiles, (int64_t)sms() * 3);
+      k_closure_infer_tc<true><<<grid, kTcRows, kTcSplitSmem, st>>>(c->cd, c->umma_w, x, y, n, nullptr,
+                                                                    c->tc_status);
+    }
   } else if (bf16) {
     const zsmpm_status ps = pack(c, st);
     if (ps != ZSMPM_OK) return ps;

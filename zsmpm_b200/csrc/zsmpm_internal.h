@@ -225,6 +225,8 @@ cudaError_t launch_activate_static(scene_device &s, const float *x, int *keys_ou
 bool closure_device_view(const zsmpm_closure *c, closure_dev *out);
 // the network (tcgen05) over rows x[0, min(*n_dev, cap)) of raw features into y; fixed launch
 // shape, so that it can be captured in a CUDA graph
+// the closure kernels' attributes (the split-BF16 forward's 72 KB of shared memory), per device
+cudaError_t prepare_closure_kernels();
 cudaError_t launch_closure_rows(const closure_dev &cd, const float *x, float *y, const int *n_dev, long long cap,
                                 cudaStream_t st);
 // records the calling thread's error message (read back by zsmpm_last_error_string)
