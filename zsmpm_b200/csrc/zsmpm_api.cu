@@ -188,9 +188,9 @@ zsmpm_status allocate_particles(zsmpm_scene *s, int64_t cap) {
     particle_buffers &b = s->bufs[k];
     ZS_ALLOC(b.xm, cap, "alloc xm");
     ZS_ALLOC(b.v, cap, "alloc v");
-    ZS_ALLOC(b.C, 9 * cap, "alloc C");
-    ZS_ALLOC(b.A, 9 * cap, "alloc A");
-    ZS_ALLOC(b.F, 9 * cap, "alloc F");
+    ZS_ALLOC(b.C, 9 * mat_capacity(cap), "alloc C");
+    ZS_ALLOC(b.A, 9 * mat_capacity(cap), "alloc A");
+    ZS_ALLOC(b.F, 9 * mat_capacity(cap), "alloc F");
     if (plastic) ZS_ALLOC(b.plastic, cap, "alloc plastic");
     ZS_ALLOC(b.id, cap, "alloc id");
     if (s->nscenes > 0) ZS_ALLOC(b.sid, cap, "alloc scene ids");

@@ -11,9 +11,18 @@ struct zsmpm_closure;
 
 namespace zsmpm {
 
-// One particle buffer set.  Vectors are float4 (x,y,z,m) / (vx,vy,vz,0); 3x3 matrices are
-// stored component-major (component k of particle i at M[k*cap + i]) so that a warp's
-// loads of one component are contiguous.
+// One particle buffer set.  Vectors are float4 (x,y,z,m) / (vx,vy,vz,0).  3x3 matrices (C, A,
+// F) are stored in tiles of 32 particles: component k (column-major) of particle i at
+// mat_at(k, i) = ((i / 32) * 9 + k) * 32 + i % 32, the layout of one 3x3 property of a
+// TileVector<float, 32>.  A warp's load of one component is 128 contiguous bytes, as with one
+// array per component, and its nine components of 32 particles are 1152 contiguous bytes: one
+// DRAM stream per matrix rather than nine (the G2P writes three matrices per particle).
+// A matrix array holds 9 * mat_capacity(cap) floats.
+__host__ __device__ __forceinline__ size_t mat_at(int k, size_t i) {
+  return ((i >> 5) * 9 + (size_t)k) * 32 + (i & 31);
+}
+__host__ __device__ __forceinline__ int64_t mat_capacity(int64_t cap) { return (cap + 31) & ~int64_t(31); }
+
 struct particle_buffers {
   float4 *xm = nullptr;
   float4 *v = nullptr;

@@ -872,7 +872,7 @@ __device__ __forceinline__ void p2g_load(const scene_device &s, const float *aff
   r.xm = s.cur.xm[i];
   r.v = s.cur.v[i];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) r.A[k] = affine[(size_t)k * s.prm.cap + i];
+  for (int k = 0; k < 9; ++k) r.A[k] = affine[mat_at(k, i)];
 }
 
 // kCell: the cell-centric pair's weights and stencil origin; with_mass = false leaves the mass
@@ -1234,20 +1234,19 @@ __device__ __forceinline__ float cell_dinv(const scene_params &p, float x) {
 __global__ void __launch_bounds__(kThreads) k_cell_affine(scene_device s, int part, float *out) {
   if (part == 0 && blockIdx.x == 0 && threadIdx.x == 0) s.ctr[kCtrMaskFrom] = 0;
   const scene_params &p = s.prm;
-  const size_t cap = (size_t)p.cap;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += grid_threads()) {
     const float4 xm = s.cur.xm[i];
     const float dinv[3] = {cell_dinv(p, xm.x), cell_dinv(p, xm.y), cell_dinv(p, xm.z)};
     float F[9], tau[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) F[k] = s.cur.F[k * cap + i];
+    for (int k = 0; k < 9; ++k) F[k] = s.cur.F[mat_at(k, i)];
     float pl = 0.f;
     if (part != 1) constitutive(p.mat, F, pl, tau);
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      const float mB = part == 2 ? 0.f : xm.w * s.cur.C[k * cap + i];
+      const float mB = part == 2 ? 0.f : xm.w * s.cur.C[mat_at(k, i)];
       const float f = part == 1 ? 0.f : p.dt * tau[k];
-      out[k * cap + i] = (mB - f) * dinv[k / 3];
+      out[mat_at(k, i)] = (mB - f) * dinv[k / 3];
     }
   }
 }
@@ -1507,7 +1506,6 @@ __global__ void __launch_bounds__(kThreads) k_closure_finish(scene_device s) {
     if (cd.tc_status && *cd.tc_status) set_status(s.ctr, kStatusTimeout);
   }
   const int substep = s.ctr[kCtrSubstep];
-  const size_t cap = (size_t)s.prm.cap;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nq; k += grid_threads()) {
     const int2 sl = s.aux.q_slot[k];
     const int slot = sl.x;
@@ -1574,8 +1572,8 @@ __global__ void __launch_bounds__(kThreads) k_closure_finish(scene_device s) {
     const float m = u[22];
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
-      s.nxt.F[c * cap + slot] = Fn[c];
-      s.nxt.A[c * cap + slot] = m * u[23 + c] - s.prm.kappa * tau[c];
+      s.nxt.F[mat_at(c, slot)] = Fn[c];
+      s.nxt.A[mat_at(c, slot)] = m * u[23 + c] - s.prm.kappa * tau[c];
     }
     if (s.nxt.plastic) s.nxt.plastic[slot] = pl_new;
   }
@@ -1628,7 +1626,6 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
   if (blockIdx.x == 0 && threadIdx.x == 0) s.ctr[kCtrMaskFrom] = nb;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float *const pf = g2p_smem + 4 * kHaloCells + warp * 2 * kG2PPrefetch;
-  const size_t cap = (size_t)p.cap;
   unsigned all_updates = 0;  // learned closure: particle updates of this warp
   // the lane's particle of a batch into prefetch buffer `buf` (lanes past the block's end copy
   // the block's first particle)
@@ -1636,7 +1633,7 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
     float *b = pf + buf * kG2PPrefetch;
     cp_async16(b + 4 * lane, &s.cur.xm[i]);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) cp_async4(b + 128 + 32 * k + lane, &s.cur.F[k * cap + i]);
+    for (int k = 0; k < 9; ++k) cp_async4(b + 128 + 32 * k + lane, &s.cur.F[mat_at(k, i)]);
     if (s.cur.plastic) cp_async4(b + 416 + lane, &s.cur.plastic[i]);
     cp_async4(b + 448 + lane, &s.cur.id[i]);
     cp_async_commit();
@@ -1668,10 +1665,10 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
         vz = *reinterpret_cast<const float4 *>(g + 1024);
       }
       float4 *dst = svf + (hx * kHalo + hy) * kHalo + quad * 4;
-      dst[0] = make_float4(vx.x, vy.x, vz.x, 0.f);
-      dst[1] = make_float4(vx.y, vy.y, vz.y, 0.f);
-      dst[2] = make_float4(vx.z, vy.z, vz.z, 0.f);
-      dst[3] = make_float4(vx.w, vy.w, vz.w, 0.f);
+      dst[0] = make_float4(vx.x, vy.x, vz.x, vz.x);
+      dst[1] = make_float4(vx.y, vy.y, vz.y, vz.y);
+      dst[2] = make_float4(vx.z, vy.z, vz.z, vz.z);
+      dst[3] = make_float4(vx.w, vy.w, vz.w, vz.w);
     }
     __syncthreads();
     const int3 bk = kBatch ? local_block(p, gk) : gk;
@@ -1698,11 +1695,6 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
       cp_async_wait_all();  // this batch's copies (the only group in flight)
       const float *pb = pf + buf * kG2PPrefetch;
       float4 xm = reinterpret_cast<const float4 *>(pb)[lane];
-      float F[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) F[k] = pb[128 + 32 * k + lane];
-      float pl = s.cur.plastic ? pb[416 + lane] : 0.f;
-      const int id = __float_as_int(pb[448 + lane]);
       const int icur = i;
       if (more) prefetch(buf ^ 1, inext);
       buf ^= 1;
@@ -1747,6 +1739,19 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
       float vel[3] = {0.f, 0.f, 0.f};
       float B[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // sum W v (node - f)^T
       if (inside) {
+        // paired FP32 arithmetic (fma.rn.f32x2): the x and y components of a node go as one
+        // pair, and z as the pair (z, z) that the halo stores in the fourth slot, taking the
+        // weights (wz, wz (k - fz)); every lane of a pair is the same correctly rounded
+        // operation as the scalar form
+        float2 wzp[3], wdp[3], wzz[3];  // (wz, wz), (wzd, wzd), (wz, wzd) of node k
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) {
+          const float wz = w[2][kk], wzd = wz * ((float)kk - f[2]);
+          wzp[kk] = make_float2(wz, wz);
+          wdp[kk] = make_float2(wzd, wzd);
+          wzz[kk] = make_float2(wz, wzd);
+        }
+        float2 vxy = make_float2(0.f, 0.f), bxy0 = vxy, bxy3 = vxy, bxy6 = vxy;
 #pragma unroll
         for (int ii = 0; ii < 3; ++ii) {
           const float dxi = (float)ii - f[0];
@@ -1755,31 +1760,32 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
             const float dyj = (float)jj - f[1];
             const float wij = w[0][ii] * w[1][jj];
             const int hrow = ((hb[0] + ii) * kHalo + (hb[1] + jj)) * kHalo + hb[2];
-            // separable accumulation over k: s0 = sum_k wz v, s1 = sum_k wz (k - fz) v
-            float s0[3] = {0.f, 0.f, 0.f}, s1[3] = {0.f, 0.f, 0.f};
+            // separable accumulation over k: s0 = sum_k wz v, s1 = sum_k wz (k - fz) v, the
+            // xy parts as pairs and the z parts as the pair (s0z, s1z)
+            float2 s0 = make_float2(0.f, 0.f), s1 = s0, sz = s0;
 #pragma unroll
             for (int kk = 0; kk < 3; ++kk) {
-              const float wz = w[2][kk], wzd = wz * ((float)kk - f[2]);
-              const int h = hrow + kk;
-              const float4 node = svf[h];
-              const float vx = node.x, vy = node.y, vz = node.z;
-              s0[0] += wz * vx;
-              s0[1] += wz * vy;
-              s0[2] += wz * vz;
-              s1[0] += wzd * vx;
-              s1[1] += wzd * vy;
-              s1[2] += wzd * vz;
+              const float4 node = svf[hrow + kk];
+              const float2 nxy = make_float2(node.x, node.y), nzz = make_float2(node.z, node.w);
+              s0 = __ffma2_rn(wzp[kk], nxy, s0);
+              s1 = __ffma2_rn(wdp[kk], nxy, s1);
+              sz = __ffma2_rn(wzz[kk], nzz, sz);
             }
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const float a = wij * s0[d];
-              vel[d] += a;
-              B[d] += a * dxi;
-              B[3 + d] += a * dyj;
-              B[6 + d] += wij * s1[d];
-            }
+            const float2 wij2 = make_float2(wij, wij);
+            const float2 axy = __fmul2_rn(wij2, s0);
+            vxy = __fadd2_rn(vxy, axy);
+            bxy0 = __ffma2_rn(axy, make_float2(dxi, dxi), bxy0);
+            bxy3 = __ffma2_rn(axy, make_float2(dyj, dyj), bxy3);
+            bxy6 = __ffma2_rn(wij2, s1, bxy6);
+            const float az = wij * sz.x;
+            vel[2] += az;
+            B[2] = fmaf(az, dxi, B[2]);
+            B[5] = fmaf(az, dyj, B[5]);
+            B[8] = fmaf(wij, sz.y, B[8]);
           }
         }
+        vel[0] = vxy.x, vel[1] = vxy.y;
+        B[0] = bxy0.x, B[1] = bxy0.y, B[3] = bxy3.x, B[4] = bxy3.y, B[6] = bxy6.x, B[7] = bxy6.y;
       }
       float C[9];  // APIC: C = (4/dx^2) sum W v (x_i - x_p)^T; the cell pair: B = sum W v (x_i - x_p)^T
 #pragma unroll
@@ -1836,6 +1842,14 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
         }
         if (__any_sync(kFull, bad) && lane == 0) s.ctr[kCtrMaskBad] = 1;
       }
+      // F, the plastic state and the id from the prefetch buffer, read after the gather so
+      // that they take no registers during it (the buffer is next written by the prefetch of
+      // the following batch)
+      float F[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) F[k] = pb[128 + 32 * k + lane];
+      float pl = s.cur.plastic ? pb[416 + lane] : 0.f;
+      const int id = __float_as_int(pb[448 + lane]);
       // F <- (I + dt C) F
       float Fn[9];
 #pragma unroll
@@ -1869,21 +1883,21 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
       s.nxt.xm[slot] = xm;
       s.nxt.v[slot] = make_float4(vel[0], vel[1], vel[2], 0.f);
 #pragma unroll
-      for (int k = 0; k < 9; ++k) s.nxt.C[k * cap + slot] = C[k];
+      for (int k = 0; k < 9; ++k) s.nxt.C[mat_at(k, slot)] = C[k];
       if (kCell) {
         // the affine term of the next P2C2G, from the new position and F (P2C2G.hpp:86-146)
         const float dnew[3] = {cell_dinv(p, xm.x), cell_dinv(p, xm.y), cell_dinv(p, xm.z)};
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
-          s.nxt.A[k * cap + slot] = (xm.w * C[k] - p.dt * tau[k]) * dnew[k / 3];
-          s.nxt.F[k * cap + slot] = Fn[k];
+          s.nxt.A[mat_at(k, slot)] = (xm.w * C[k] - p.dt * tau[k]) * dnew[k / 3];
+          s.nxt.F[mat_at(k, slot)] = Fn[k];
         }
         if (s.nxt.plastic) s.nxt.plastic[slot] = pl;
       } else if (!queued) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
-          s.nxt.A[k * cap + slot] = xm.w * C[k] - p.kappa * tau[k];
-          s.nxt.F[k * cap + slot] = Fn[k];
+          s.nxt.A[mat_at(k, slot)] = xm.w * C[k] - p.kappa * tau[k];
+          s.nxt.F[mat_at(k, slot)] = Fn[k];
         }
         if (s.nxt.plastic) s.nxt.plastic[slot] = pl;
       }
@@ -2003,7 +2017,7 @@ __global__ void __launch_bounds__(kG2P2GThreads, 2)
         const float4 xm = s.cur.xm[i];
         float F[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) F[k] = s.cur.F[(size_t)k * p.cap + i];
+        for (int k = 0; k < 9; ++k) F[k] = s.cur.F[mat_at(k, i)];
         float pl = s.cur.plastic ? s.cur.plastic[i] : 0.f;
         const float X[3] = {over_dx(p, xm.x), over_dx(p, xm.y), over_dx(p, xm.z)};
         int hb[3];
@@ -2374,7 +2388,6 @@ __device__ __forceinline__ int scene_of_index(const scene_params &p, int i) {
 
 __global__ void k_import(scene_device s, const float *m, const float *x, const float *v,
                          const float *C, const float *F, const float *pl, int n) {
-  const size_t cap = (size_t)s.prm.cap;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += grid_threads()) {
     int model = s.prm.mat.model;
     if (s.prm.batch) {
@@ -2387,8 +2400,8 @@ __global__ void k_import(scene_device s, const float *m, const float *x, const f
     s.cur.v[i] = v ? make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      s.cur.C[k * cap + i] = C ? C[9 * (size_t)i + k] : 0.f;
-      s.cur.F[k * cap + i] = F ? F[9 * (size_t)i + k] : ((k & 3) == 0 ? 1.f : 0.f);
+      s.cur.C[mat_at(k, i)] = C ? C[9 * (size_t)i + k] : 0.f;
+      s.cur.F[mat_at(k, i)] = F ? F[9 * (size_t)i + k] : ((k & 3) == 0 ? 1.f : 0.f);
     }
     if (s.cur.plastic) s.cur.plastic[i] = pl ? pl[i] : plastic_default;
     s.cur.id[i] = i;
@@ -2397,7 +2410,6 @@ __global__ void k_import(scene_device s, const float *m, const float *x, const f
 
 __global__ void k_import_tv(scene_device s, const float *base, int nchn, int om, int ox, int ov,
                             int oC, int oF, int opl, int n) {
-  const size_t cap = (size_t)s.prm.cap;
   const float plastic_default = s.prm.mat.model == 2 ? 1.f : 0.f;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += grid_threads()) {
     const size_t tile = (size_t)(i / 32) * nchn * 32 + (i % 32);
@@ -2406,8 +2418,8 @@ __global__ void k_import_tv(scene_device s, const float *base, int nchn, int om,
     s.cur.v[i] = ov >= 0 ? make_float4(at(ov), at(ov + 1), at(ov + 2), 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      s.cur.C[k * cap + i] = oC >= 0 ? at(oC + k) : 0.f;
-      s.cur.F[k * cap + i] = oF >= 0 ? at(oF + k) : ((k & 3) == 0 ? 1.f : 0.f);
+      s.cur.C[mat_at(k, i)] = oC >= 0 ? at(oC + k) : 0.f;
+      s.cur.F[mat_at(k, i)] = oF >= 0 ? at(oF + k) : ((k & 3) == 0 ? 1.f : 0.f);
     }
     if (s.cur.plastic) s.cur.plastic[i] = opl >= 0 ? at(opl) : plastic_default;
     s.cur.id[i] = i;
@@ -2417,11 +2429,10 @@ __global__ void k_import_tv(scene_device s, const float *base, int nchn, int om,
 // stress of the stored state; A = m C - kappa tau (what the previous G2P would have written)
 __global__ void k_prime(scene_device s) {
   if (blockIdx.x == 0 && threadIdx.x == 0) s.ctr[kCtrMaskFrom] = 0;  // new particles: no move masks
-  const size_t cap = (size_t)s.prm.cap;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s.prm.n; i += grid_threads()) {
     float F[9], tau[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) F[k] = s.cur.F[k * cap + i];
+    for (int k = 0; k < 9; ++k) F[k] = s.cur.F[mat_at(k, i)];
     float pl = s.cur.plastic ? s.cur.plastic[i] : 0.f;
     if (s.prm.batch)
       constitutive(s.prm.mats[s.cur.sid[i]], F, pl, tau);
@@ -2430,15 +2441,14 @@ __global__ void k_prime(scene_device s) {
     const float m = s.cur.xm[i].w;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      s.cur.F[k * cap + i] = F[k];
-      s.cur.A[k * cap + i] = m * s.cur.C[k * cap + i] - s.prm.kappa * tau[k];
+      s.cur.F[mat_at(k, i)] = F[k];
+      s.cur.A[mat_at(k, i)] = m * s.cur.C[mat_at(k, i)] - s.prm.kappa * tau[k];
     }
     if (s.cur.plastic) s.cur.plastic[i] = pl;
   }
 }
 
 __global__ void k_export(scene_device s, float *m, float *x, float *v, float *C, float *F, float *pl) {
-  const size_t cap = (size_t)s.prm.cap;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s.prm.n; i += grid_threads()) {
     const int o = s.cur.id[i];
     const float4 xm = s.cur.xm[i], vv = s.cur.v[i];
@@ -2455,8 +2465,8 @@ __global__ void k_export(scene_device s, float *m, float *x, float *v, float *C,
     }
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      if (C) C[9 * (size_t)o + k] = s.cur.C[k * cap + i];
-      if (F) F[9 * (size_t)o + k] = s.cur.F[k * cap + i];
+      if (C) C[9 * (size_t)o + k] = s.cur.C[mat_at(k, i)];
+      if (F) F[9 * (size_t)o + k] = s.cur.F[mat_at(k, i)];
     }
     if (pl) pl[o] = s.cur.plastic ? s.cur.plastic[i] : 0.f;
   }
@@ -2464,7 +2474,6 @@ __global__ void k_export(scene_device s, float *m, float *x, float *v, float *C,
 
 __global__ void k_export_tv(scene_device s, float *base, int nchn, int om, int ox, int ov, int oC,
                             int oF, int opl) {
-  const size_t cap = (size_t)s.prm.cap;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s.prm.n; i += grid_threads()) {
     const int o = s.cur.id[i];
     const size_t tile = (size_t)(o / 32) * nchn * 32 + (o % 32);
@@ -2482,8 +2491,8 @@ __global__ void k_export_tv(scene_device s, float *base, int nchn, int om, int o
       at(ov + 2) = vv.z;
     }
     for (int k = 0; k < 9; ++k) {
-      if (oC >= 0) at(oC + k) = s.cur.C[k * cap + i];
-      if (oF >= 0) at(oF + k) = s.cur.F[k * cap + i];
+      if (oC >= 0) at(oC + k) = s.cur.C[mat_at(k, i)];
+      if (oF >= 0) at(oF + k) = s.cur.F[mat_at(k, i)];
     }
     if (opl >= 0) at(opl) = s.cur.plastic ? s.cur.plastic[i] : 0.f;
   }
