@@ -211,10 +211,10 @@ def barrier(ws: int):
 # kernel (dram__bytes_read.sum + dram__bytes_write.sum over the particles of the launch):
 #   two-box sand scene: captured at dx = 1/128 (3.7 M particles; the 30 M workload is scaled by
 #   the particle count, traffic grows in proportion): 756.4 MB / 3,703,824
-#   256-scene batch: captured at full size: 3.495 GB / 15,386,080
+#   256-scene batch: captured at full size: 3.569 GB / 15,386,080
 G2P_TRAFFIC_PER_PARTICLE = {"dp_two_boxes_dx256_8ppc": 756.44e6 / 3703824,
                             "dp_two_boxes_dx128_8ppc": 756.44e6 / 3703824,
-                            "batch_256_scenes_dx128_8ppc": 3.4949e9 / 15386080}
+                            "batch_256_scenes_dx128_8ppc": 3.5687e9 / 15386080}
 
 
 def g2p_algorithmic_bytes(n: int, nb: int, plastic: bool) -> int:
