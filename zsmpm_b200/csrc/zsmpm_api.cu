@@ -33,9 +33,14 @@ struct zsmpm_scene {
   int *cell_start_buf[2] = {nullptr, nullptr};
   int *block_start_buf[2] = {nullptr, nullptr};
   cudaStream_t last_stream = nullptr;
-  // graphs of two consecutive substeps, one per starting buffer parity
+  // graphs of kGraphSubsteps consecutive substeps, one per starting buffer parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   cudaStream_t graph_stream = nullptr;
+  // the learned closure's pass (network and finish) deferred to a second stream beside the next
+  // substep's activation and binning, joined before that substep's P2G
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  bool join_pending = false;
   // stage timing
   bool timing = false;
   cudaEvent_t ev[6] = {};
@@ -270,6 +275,12 @@ void release(zsmpm_scene *s) {
     if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
   for (auto &e : s->ev)
     if (e) cudaEventDestroy(e);
+  if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+  if (s->join_ev) cudaEventDestroy(s->join_ev);
+  if (s->side_stream) cudaStreamDestroy(s->side_stream);
+  if (s->graph_stream) cudaStreamDestroy(s->graph_stream);
+  s->fork_ev = s->join_ev = nullptr;
+  s->side_stream = s->graph_stream = nullptr;
   for (void *p : s->allocations) cudaFree(p);
   s->allocations.clear();
   for (void *p : s->levelset_buffers) cudaFree(p);
@@ -294,7 +305,14 @@ zsmpm_status read_status(zsmpm_scene *s) {
   return status_from_word(w);
 }
 
-zsmpm_status substep_enqueue(zsmpm_scene *s, cudaStream_t st) {
+// Substeps kept in one CUDA graph: the closure pass of every substep but the last runs beside
+// the next substep's activation and binning.
+constexpr int kGraphSubsteps = 4;
+
+// defer_closure: with a learned closure attached, leave the closure pass (network and finish)
+// to the side stream and have the next substep_enqueue join it before its P2G (zsmpm_run's
+// graphs only; the side stream and its events must exist)
+zsmpm_status substep_enqueue(zsmpm_scene *s, cudaStream_t st, bool defer_closure = false) {
   bind_buffers(s);
   if (s->timing) cudaEventRecord(s->ev[0], st);
   ZS_TRY(launch_activate(s->dev, st), "activate");
@@ -302,11 +320,25 @@ zsmpm_status substep_enqueue(zsmpm_scene *s, cudaStream_t st) {
   s->dev.prm.bin_full = 0;
   ZS_TRY(launch_bin(s->dev, st), "bin");
   if (s->timing) cudaEventRecord(s->ev[2], st);
+  if (s->join_pending) {
+    // the last substep's closure pass writes F, the affine momentum and the plastic state that
+    // this P2G and G2P read
+    ZS_TRY(cudaStreamWaitEvent(st, s->join_ev, 0), "join the closure pass");
+    s->join_pending = false;
+  }
   ZS_TRY(launch_p2g(s->dev, st), "p2g");
   if (s->timing) cudaEventRecord(s->ev[3], st);
   ZS_TRY(launch_grid_update(s->dev, st), "grid update");
   if (s->timing) cudaEventRecord(s->ev[4], st);
-  ZS_TRY(launch_g2p(s->dev, st), "g2p");
+  const bool deferred = defer_closure && s->dev.aux.learned && s->side_stream;
+  ZS_TRY(launch_g2p(s->dev, st, !deferred), "g2p");
+  if (deferred) {
+    ZS_TRY(cudaEventRecord(s->fork_ev, st), "fork the closure pass");
+    ZS_TRY(cudaStreamWaitEvent(s->side_stream, s->fork_ev, 0), "fork the closure pass");
+    ZS_TRY(launch_closure_pass(s->dev, s->side_stream), "closure pass");
+    ZS_TRY(cudaEventRecord(s->join_ev, s->side_stream), "closure pass done");
+    s->join_pending = true;
+  }
   if (s->timing) cudaEventRecord(s->ev[5], st);
   s->cur ^= 1;
   bind_buffers(s);
@@ -806,22 +838,29 @@ ZSMPM_API zsmpm_status zsmpm_run(zsmpm_scene *s, int32_t nsteps, void *stream) {
   cudaStream_t cs = as_stream(stream);
   const bool timing = s->timing;
   s->timing = false;
-  // capture the pair of substeps starting from the current parity once, on a private
-  // stream (capture is not allowed on the legacy default stream)
+  // capture kGraphSubsteps substeps starting from the current parity once, on a private
+  // stream (capture is not allowed on the legacy default stream); with a learned closure the
+  // closure pass of each substep but the last forks to the side stream and joins the next
+  // substep before its P2G, so the graph's own end joins every stream it forked
   const int parity = s->cur;
-  if (nsteps >= 2 && !s->graph[parity]) {
+  if (nsteps >= kGraphSubsteps && !s->graph[parity]) {
     if (!s->graph_stream) ZS_TRY(cudaStreamCreateWithFlags(&s->graph_stream, cudaStreamNonBlocking), "graph stream");
+    if (!s->side_stream) ZS_TRY(cudaStreamCreateWithFlags(&s->side_stream, cudaStreamNonBlocking), "side stream");
+    if (!s->fork_ev) ZS_TRY(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming), "fork event");
+    if (!s->join_ev) ZS_TRY(cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming), "join event");
     ZS_TRY(cudaStreamBeginCapture(s->graph_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-    zsmpm_status a = substep_enqueue(s, s->graph_stream);
-    zsmpm_status b = a == ZSMPM_OK ? substep_enqueue(s, s->graph_stream) : a;
+    zsmpm_status a = ZSMPM_OK;
+    for (int k = 0; k < kGraphSubsteps && a == ZSMPM_OK; ++k)
+      a = substep_enqueue(s, s->graph_stream, k + 1 < kGraphSubsteps);
+    s->join_pending = false;  // the last substep joined the pass before it (or capture failed)
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s->graph_stream, &g);
     s->cur = parity;  // capture enqueued nothing; restore the parity it advanced
     bind_buffers(s);
-    if (a != ZSMPM_OK || b != ZSMPM_OK) {
+    if (a != ZSMPM_OK) {
       if (g) cudaGraphDestroy(g);
       s->timing = timing;
-      return a != ZSMPM_OK ? a : b;
+      return a;
     }
     if (e != cudaSuccess) {
       s->timing = timing;
@@ -835,15 +874,15 @@ ZSMPM_API zsmpm_status zsmpm_run(zsmpm_scene *s, int32_t nsteps, void *stream) {
     }
   }
   int done = 0;
-  for (; done + 2 <= nsteps; done += 2) {
+  for (; done + kGraphSubsteps <= nsteps; done += kGraphSubsteps) {
     cudaError_t e = cudaGraphLaunch(s->graph[parity], cs);
     if (e != cudaSuccess) {
       s->timing = timing;
       return cuda_fail(e, "graph launch");
     }
   }
-  // the pair leaves the parity unchanged
-  if (done < nsteps) {
+  // an even number of substeps leaves the parity unchanged
+  for (; done < nsteps; ++done) {
     st = substep_enqueue(s, cs);
     if (st != ZSMPM_OK) {
       s->timing = timing;

@@ -41,8 +41,8 @@ constexpr int kBatchSlot = 32;
 constexpr int kBatchMargin = 4;
 constexpr int kBatchMaxScenes = 1 << 16;
 
-// Device counters (int32), zeroed at the start of every substep except the status word and
-// the substep counter.
+// Device counters (int32), zeroed at the start of every substep except the status word, the
+// substep counter and the learned G2P's queue counters.
 enum counter_slot : int {
   kCtrParticleBlocks = 0,  // blocks inserted from particles (insertion indices [0, npb))
   kCtrEnlarged = 1,        // blocks inserted by the enlargement
@@ -62,7 +62,8 @@ enum counter_slot : int {
   kCtrIncBin = 27,         // 1: this substep's binning merges the movers into the last binning's order
   kCtrBinInfo = 28,        // the last binning: -1 full, else the number of movers it merged
   kCtrDirty = 29,          // cells the incremental binning's movers arrived in (to be sorted by id)
-  kCtrQueue = 30,          // projections the last G2P queued for the closure's network
+  kCtrQueue = 30,          // projections the last learned G2P queued for the closure's network
+  kCtrQueueSubstep = 31,   // the substep number of that G2P (the closure pass samples its audit by it)
   kCtrCount = 32
 };
 enum work_slot : int {
@@ -185,7 +186,8 @@ cudaError_t launch_p2g(scene_device &s, cudaStream_t st);
 // P2C2G of the cell-centric pair: part 0 all, 1 the momentum part, 2 the force part
 cudaError_t launch_p2c2g(scene_device &s, int part, cudaStream_t st);
 cudaError_t launch_grid_update(scene_device &s, cudaStream_t st);
-cudaError_t launch_g2p(scene_device &s, cudaStream_t st);
+cudaError_t launch_g2p(scene_device &s, cudaStream_t st, bool closure_pass = true);
+cudaError_t launch_closure_pass(scene_device &s, cudaStream_t st);
 int kernels_per_substep();
 // the implicit system (ImplicitMPM.hpp) over node-major dof vectors [nb * 512 * 3]; a kernel
 // returns at once when `skip` (device, may be null) holds a nonzero value

@@ -237,7 +237,11 @@ __global__ void __launch_bounds__(kThreads) k_begin(scene_device s) {
   if (blockIdx.x == 0 && threadIdx.x < kCtrCount) {
     const int t = threadIdx.x;
     // k_bitmap_prepare resets the two mask counters; the binning clears the mover count
-    if (t == kCtrStatus || t == kCtrMaskFrom || t == kCtrMaskBad || t == kCtrMovers) return;
+    // the learned G2P's queue counters stay for a closure pass that runs beside this substep's
+    // activation and binning (the learned G2P clears the queue before it fills it)
+    if (t == kCtrStatus || t == kCtrMaskFrom || t == kCtrMaskBad || t == kCtrMovers || t == kCtrQueue ||
+        t == kCtrQueueSubstep)
+      return;
     if (t == kCtrUseMasks) {
       s.ctr[t] = s.ctr[kCtrMaskBad] == 0 ? s.ctr[kCtrMaskFrom] : 0;
       return;
@@ -465,7 +469,6 @@ __global__ void __launch_bounds__(kThreads) k_bin_count(scene_device s) {
     s.ctr[kCtrWork + kWorkP2G] = 0;
     s.ctr[kCtrWork + kWorkG2P] = 0;
     s.ctr[kCtrDirty] = 0;
-    s.ctr[kCtrQueue] = 0;  // the next G2P queues its projections afresh
   }
   if (incremental_binning(s)) return;  // k_inc_stayers and k_inc_movers count this substep
   const int lane = threadIdx.x & 31;
@@ -1505,7 +1508,7 @@ __global__ void __launch_bounds__(kThreads) k_closure_finish(scene_device s) {
     // a bounded tensor-core wait of the network pass that gave up is the scene's error too
     if (cd.tc_status && *cd.tc_status) set_status(s.ctr, kStatusTimeout);
   }
-  const int substep = s.ctr[kCtrSubstep];
+  const int substep = s.ctr[kCtrQueueSubstep];  // of the G2P that queued the rows
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nq; k += grid_threads()) {
     const int2 sl = s.aux.q_slot[k];
     const int slot = sl.x;
@@ -1623,7 +1626,10 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 5) k_g2p(scene_device s) {
   const scene_params &p = s.prm;
   const int nb = s.ctr[kCtrBlocks];
   const int substep = s.ctr[kCtrSubstep];
-  if (blockIdx.x == 0 && threadIdx.x == 0) s.ctr[kCtrMaskFrom] = nb;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s.ctr[kCtrMaskFrom] = nb;
+    if (kLearned) s.ctr[kCtrQueueSubstep] = substep;  // for the closure pass's audit sampling
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float *const pf = g2p_smem + 4 * kHaloCells + warp * 2 * kG2PPrefetch;
   unsigned all_updates = 0;  // learned closure: particle updates of this warp
@@ -2748,7 +2754,19 @@ cudaError_t launch_grid_update(scene_device &s, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_g2p(scene_device &s, cudaStream_t st) {
+// The learned closure's pass over the projections the last learned G2P queued: the network on
+// the tensor cores, then k_closure_finish.  It writes F, the affine momentum and the plastic
+// state of the queued particles only, and reads the queue counter and the substep number the
+// G2P recorded, which the next substep's activation and binning leave alone: so it may run
+// beside them (a deferred pass), joining before the next P2G.
+cudaError_t launch_closure_pass(scene_device &s, cudaStream_t st) {
+  cudaError_t e = launch_closure_rows(s.aux.cd, s.aux.q_feat, s.aux.q_out, &s.ctr[kCtrQueue], s.aux.qcap, st);
+  if (e != cudaSuccess) return e;
+  k_closure_finish<<<num_sms() * 4, kThreads, 0, st>>>(s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_g2p(scene_device &s, cudaStream_t st, bool closure_pass) {
   const int per_sm = s.prm.g2p_ctas_per_sm > 0 ? s.prm.g2p_ctas_per_sm : 3;
   const int grid = num_sms() * per_sm;
   const bool small = s.prm.g2p_threads == 128;
@@ -2758,16 +2776,17 @@ cudaError_t launch_g2p(scene_device &s, cudaStream_t st) {
     return cudaGetLastError();
   }
   if (s.aux.learned) {
-    // G2P queues the projections, the network runs over the queue on the tensor cores, and
-    // k_closure_finish completes the queued particles
+    // G2P queues the projections (from an empty queue), the network runs over the queue on the
+    // tensor cores, and k_closure_finish completes the queued particles; closure_pass = false
+    // leaves the last two to a deferred launch_closure_pass
+    cudaError_t e = cudaMemsetAsync(&s.ctr[kCtrQueue], 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
     if (s.prm.batch)
       k_g2p<true, true, kThreads><<<grid, kThreads, g2p_smem_bytes(kThreads), st>>>(s);
     else
       k_g2p<true, false, kThreads><<<grid, kThreads, g2p_smem_bytes(kThreads), st>>>(s);
-    cudaError_t e = launch_closure_rows(s.aux.cd, s.aux.q_feat, s.aux.q_out, &s.ctr[kCtrQueue], s.aux.qcap, st);
-    if (e != cudaSuccess) return e;
-    k_closure_finish<<<num_sms() * 4, kThreads, 0, st>>>(s);
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return closure_pass ? launch_closure_pass(s, st) : cudaSuccess;
   }
   if (s.prm.batch)
     small ? k_g2p<false, true, 128><<<grid, 128, g2p_smem_bytes(128), st>>>(s)
