@@ -877,7 +877,7 @@ def main(argv=None):
                        "closure": "plain", "transfer": args.transfer, "parallelism": f"replicas{ws}",
                        "launch_shapes": main_leg["launch_shapes"],
                        "l2": "inputs larger than L2 (particle state 2+ GB per workload)",
-                       "substep_graph": "CUDA graph of 2 substeps"},
+                       "substep_graph": "CUDA graph of 4 substeps"},
             "roofline": {**g2p,
                          "traffic": (G2P_TRAFFIC_PER_PARTICLE[workload] * n if workload in G2P_TRAFFIC_PER_PARTICLE
                                      else None),

@@ -255,9 +255,12 @@ ZSMPM_API zsmpm_status zsmpm_p2c2g(zsmpm_scene *scene, int32_t part, void *strea
 ZSMPM_API zsmpm_status zsmpm_g2c2p(zsmpm_scene *scene, void *stream);
 /* One full substep (activate, bin, P2G, grid update + walls, G2P). */
 ZSMPM_API zsmpm_status zsmpm_substep(zsmpm_scene *scene, void *stream);
-/* nsteps substeps, replayed from a CUDA graph of two substeps (captured on first use per
- * buffer parity; an odd last substep is launched directly).  Asynchronous: capacity and
- * domain errors collect in the device status word, which zsmpm_scene_status reads. */
+/* nsteps substeps, replayed from a CUDA graph of four substeps (captured on first use per
+ * buffer parity; the substeps beyond a multiple of four are launched directly).  With a learned
+ * closure attached, the closure's network pass of each graph substep but the last runs on a
+ * second stream of the scene beside the next substep's activation and binning; the state is
+ * complete when the work enqueued on `stream` is.  Asynchronous: capacity and domain errors
+ * collect in the device status word, which zsmpm_scene_status reads. */
 ZSMPM_API zsmpm_status zsmpm_run(zsmpm_scene *scene, int32_t nsteps, void *stream);
 
 /* ---- views and diagnostics ------------------------------------------------------- */

@@ -3,7 +3,7 @@
 // A scene owns every device buffer of one MPM system (particles double-buffered in binned
 // order, the HashTable<i32,3,int>-layout block table, the sparse grid of 8^3 blocks and
 // the binning scratch).  Stages enqueue kernels on the caller's stream; zsmpm_run replays
-// a CUDA graph of two substeps (the particle buffers alternate between them).
+// a CUDA graph of four substeps (the particle buffers alternate between them).
 #include <algorithm>
 #include <cstdint>
 #include <initializer_list>
