@@ -143,7 +143,7 @@ def test_learned_closure_on_a_batch(zs, gpu):
     sc.close()
     c = cl.Closure(specs[dp].material, specs[dp].volume)
     c.build_dataset(300000, seed=8, logged=buf[:min(n_log, 200000)].contiguous())
-    c.fit()
+    c.fit(cl.SCHEDULE_LONG)
     plain = batch.Batch(specs, parts)
     plain.run(steps)
     plain.status()
@@ -161,7 +161,8 @@ def test_learned_closure_on_a_batch(zs, gpu):
     print(f"\nbatched learned closure: audit {a}")
     # per-particle stress error and the aggregate over the audit (the network was trained on
     # random states and on the states of one sand scene only; the others differ in friction)
-    assert a["audited"] > 0 and a["mean_rel_error"] < 1e-3 and a["agg_rel_error"] < 0.1
+    # (measured: mean 6.6e-5, aggregate 2.1e-2)
+    assert a["audited"] > 0 and a["mean_rel_error"] < 3e-4 and a["agg_rel_error"] < 0.05
     for sp, p0, g, r in zip(specs, parts, got, ref):
         disp = np.linalg.norm(r.x.astype(np.float64) - p0.x)
         err = np.linalg.norm(g.x.astype(np.float64) - r.x) / max(disp, 1e-12)

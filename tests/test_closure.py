@@ -302,7 +302,7 @@ def test_learned_scene_follows_plain_and_audits(zs, gpu):
     sc.close()
     c = cl.Closure(spec.material, spec.volume)
     c.build_dataset(200000, seed=4, logged=logged)
-    c.fit()
+    c.fit(cl.SCHEDULE_LONG)
     learned, a = _run_scene(zs, spec, steps, closure=c, audit_period=100)
     # the method without the return map: the same box in fixed corotated
     el_spec = dataclasses.replace(spec, material=dataclasses.replace(spec.material, model=0))
@@ -318,7 +318,8 @@ def test_learned_scene_follows_plain_and_audits(zs, gpu):
     expect = a["network_updates"] / 100
     assert 0.7 * expect < a["audited"] < 1.3 * expect + 5
     assert np.isfinite(a["mean_rel_error"]) and a["max_rel_error"] >= a["mean_rel_error"]
-    assert a["mean_rel_error"] < 1e-2 and a["agg_rel_error"] < 2e-2
+    # the long schedule gives mean 1.9e-3 and aggregate 1.5e-3 on this scene
+    assert a["mean_rel_error"] < 5e-3 and a["agg_rel_error"] < 5e-3
     assert err_learned < 0.2 * err_elastic
     c.close()
 

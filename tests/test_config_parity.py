@@ -192,7 +192,7 @@ def test_snow_with_active_plasticity_plain_and_learned_vs_fp64(zs, gpu):
         cl.set_state_log(sc, None, 0)
         c = cl.Closure(spec.material, spec.volume)
         c.build_dataset(1_000_000, seed=5, logged=buf[:min(n_log, 400_000)].contiguous())
-        c.fit()
+        c.fit(cl.SCHEDULE_LONG)
         sc.upload(q)
         cl.attach(sc, c, audit_period=20)
         sc.run(steps)
@@ -224,3 +224,7 @@ def test_snow_with_active_plasticity_plain_and_learned_vs_fp64(zs, gpu):
     # the plain path
     assert a["network_updates"] > 0 and a["audited"] > 0
     assert err["learned_v"] < 1e-2
+    # the snow stress is steep in the projected strain (a log-strain error d moves it by about
+    # d / theta_c, and the hardening exp(xi (1 - Jp)) multiplies the Jp error by xi = 10):
+    # measured aggregate 2.9e-2 with the long schedule
+    assert a["agg_rel_error"] < 0.1

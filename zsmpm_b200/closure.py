@@ -33,6 +33,11 @@ def _rows(t, name):
     return C.c_void_p(t.data_ptr())
 
 
+# A longer schedule than fit()'s default: five stages of falling learning rate, 76 epochs in
+# all (the bench trains its closures with the same stages).
+SCHEDULE_LONG = ((20, 4096, 2e-3), (20, 4096, 5e-4), (16, 8192, 1e-4), (12, 16384, 3e-5), (8, 32768, 1e-5))
+
+
 class Closure:
     """Owns one zsmpm_closure handle (weights, Adam state, training set) on one GPU."""
 
