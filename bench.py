@@ -212,9 +212,11 @@ def barrier(ws: int):
 #   two-box sand scene: captured at dx = 1/128 (3.7 M particles; the 30 M workload is scaled by
 #   the particle count, traffic grows in proportion): 756.4 MB / 3,703,824
 #   256-scene batch: captured at full size: 3.569 GB / 15,386,080
+#   16 M snow scene: captured at full size: 3.522 GB / 15,988,466
 G2P_TRAFFIC_PER_PARTICLE = {"dp_two_boxes_dx256_8ppc": 756.44e6 / 3703824,
                             "dp_two_boxes_dx128_8ppc": 756.44e6 / 3703824,
-                            "batch_256_scenes_dx128_8ppc": 3.5687e9 / 15386080}
+                            "batch_256_scenes_dx128_8ppc": 3.5687e9 / 15386080,
+                            "snow_sphere_slab_dx295_4ppc": 3.5218e9 / 15988466}
 
 
 def g2p_algorithmic_bytes(n: int, nb: int, plastic: bool) -> int:
@@ -717,6 +719,8 @@ def extra_leg(args, name, ws, local, stream, learned: bool):
     w = Workload(zs, spec, p, parts, local, stream)
     try:
         out = {"workload": workload, **plain_leg(args, w, ws, local, with_e2e=False)}
+        if workload in G2P_TRAFFIC_PER_PARTICLE and "g2p_roofline" in out:
+            out["g2p_roofline"]["traffic"] = G2P_TRAFFIC_PER_PARTICLE[workload] * w.n
         if learned:
             if parts is None:
                 out["learned"] = learned_leg(args, zs, w.sc, spec, w.n, w.upload_pinned, stream, w.sptr, ws,
