@@ -259,8 +259,9 @@ ZSMPM_API zsmpm_status zsmpm_substep(zsmpm_scene *scene, void *stream);
  * buffer parity; the substeps beyond a multiple of four are launched directly).  With a learned
  * closure attached, the closure's network pass of each graph substep but the last runs on a
  * second stream of the scene beside the next substep's activation and binning; the state is
- * complete when the work enqueued on `stream` is.  Asynchronous: capacity and domain errors
- * collect in the device status word, which zsmpm_scene_status reads. */
+ * complete when the work enqueued on `stream` is.  nsteps = 0 captures the graph for the
+ * current buffer parity, if it is not captured yet, and runs nothing.  Asynchronous: capacity
+ * and domain errors collect in the device status word, which zsmpm_scene_status reads. */
 ZSMPM_API zsmpm_status zsmpm_run(zsmpm_scene *scene, int32_t nsteps, void *stream);
 
 /* ---- views and diagnostics ------------------------------------------------------- */

@@ -213,3 +213,28 @@ def test_position_that_becomes_nan_is_reported_after_moved_blocks(zs, gpu):
         with pytest.raises(zs.ZsmpmError) as e:
             sc.status()
         assert e.value.status == zs._abi.ERR_OUT_OF_DOMAIN
+
+
+def test_run_zero_captures_without_stepping(zs, gpu):
+    """zsmpm_run with nsteps = 0 captures the substep graph and leaves the state as it was; the
+    graph of four substeps plus a direct one (run(5)) then gives the state of five single
+    substeps, up to the order of P2G's float sums."""
+    from zsmpm_b200 import scenes
+    spec = scenes.small_scene(model=1)
+    p = zs.generate(spec)
+    with zs.Scene(spec, p) as a, zs.Scene(spec, p) as b:
+        before = a.download()
+        a.run(0)
+        a.status()
+        same = a.download()
+        for k in ("x", "v", "C", "F", "plastic"):
+            assert np.array_equal(getattr(before, k), getattr(same, k)), k
+        a.run(5)
+        a.status()
+        for _ in range(5):
+            b.substep()
+        b.status()
+        ga, gb = a.download(), b.download()
+    assert rel_l2(ga.x - p.x, gb.x - p.x) < 1e-5
+    assert rel_l2(ga.v, gb.v) < 1e-5
+    assert rel_l2(ga.F, gb.F) < 1e-5

@@ -230,6 +230,8 @@ class Scene:
         _abi.check(self._lib.zsmpm_substep(self._h, C.c_void_p(stream)), "substep")
 
     def run(self, nsteps: int, stream: int = 0):
+        """nsteps substeps from the scene's CUDA graph of four; run(0) only captures that graph
+        for the current buffer parity (to keep the capture out of a timed region)."""
         _abi.check(self._lib.zsmpm_run(self._h, nsteps, C.c_void_p(stream)), "run")
 
     def status(self) -> None:

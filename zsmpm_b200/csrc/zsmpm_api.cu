@@ -843,7 +843,8 @@ ZSMPM_API zsmpm_status zsmpm_run(zsmpm_scene *s, int32_t nsteps, void *stream) {
   // closure pass of each substep but the last forks to the side stream and joins the next
   // substep before its P2G, so the graph's own end joins every stream it forked
   const int parity = s->cur;
-  if (nsteps >= kGraphSubsteps && !s->graph[parity]) {
+  // (nsteps == 0 only captures: a caller prepares the graph outside a timed region)
+  if ((nsteps >= kGraphSubsteps || nsteps == 0) && !s->graph[parity]) {
     if (!s->graph_stream) ZS_TRY(cudaStreamCreateWithFlags(&s->graph_stream, cudaStreamNonBlocking), "graph stream");
     if (!s->side_stream) ZS_TRY(cudaStreamCreateWithFlags(&s->side_stream, cudaStreamNonBlocking), "side stream");
     if (!s->fork_ev) ZS_TRY(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming), "fork event");
