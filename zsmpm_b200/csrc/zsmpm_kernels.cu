@@ -1583,8 +1583,9 @@ __global__ void __launch_bounds__(kThreads) k_closure_finish(scene_device s) {
 }
 
 // Shared memory of k_g2p: the velocity halo, one float4 (vx, vy, vz, vz) per node so that a
-// node is one 16-byte load (z twice: the gather's pairs are (x, y) and (z, z)); then per warp two prefetch buffers of 32 particles, each laid out
-// as x|m float4[32], F[9][32], plastic[32], id[32] (kG2PPrefetch floats).
+// node is one 16-byte load (z twice: the gather's pairs are (x, y) and (z, z)); then per warp
+// two prefetch buffers of 32 particles, each laid out as x|m float4[32], F[9][32],
+// plastic[32], id[32] (kG2PPrefetch floats).
 constexpr int kG2PPrefetch = 4 * 32 + 9 * 32 + 32 + 32;
 constexpr size_t g2p_smem_bytes(int nt) {
   return sizeof(float4) * kHaloCells + sizeof(float) * 2 * kG2PPrefetch * (size_t)(nt / 32);
